@@ -1,0 +1,123 @@
+"""Checks the oracle's parts that no reference test pins (sample_latent_blas, CondNormalWishart,
+MvNormal draws, block-CG at K RHS) against closed forms computed with numpy/scipy on small
+cases."""
+import numpy as np
+import scipy.linalg as sla
+import scipy.sparse as sp
+
+from oracle import oracle as orc
+
+
+def rand_csr(rng, nrow, ncol, density, vals=True):
+    m = sp.random(nrow, ncol, density=density, random_state=rng, format="csr")
+    if vals:
+        m.data = rng.normal(3.0, 1.0, m.nnz)
+    return m
+
+
+def test_normal_and_gamma_draws_moments():
+    z = np.array([orc.normal(7, 3, "row_noise", 1, i, j) for i in range(4000) for j in range(8)])
+    assert abs(z.mean()) < 0.02 and abs(z.var() - 1) < 0.03
+    g = np.array([orc.gamma(7, s, "wishart_diag", 0, 0, 2.5) for s in range(20000)])
+    assert abs(g.mean() - 2.5) < 0.05 and abs(g.var() - 2.5) < 0.15
+    g = np.array([orc.gamma(7, s, "wishart_diag", 0, 0, 0.4) for s in range(20000)])
+    assert abs(g.mean() - 0.4) < 0.02
+
+
+def test_sample_latents_matches_numpy_closed_form():
+    rng = np.random.default_rng(0)
+    K, nrow, ncol = 6, 40, 30
+    Y = rand_csr(rng, nrow, ncol, 0.2)
+    R = orc.Csr.from_scipy(Y)
+    V = rng.normal(size=(ncol, K))
+    A = rng.normal(size=(K, K))
+    Lam = A @ A.T + K * np.eye(K)
+    mu = rng.normal(size=K)
+    Uhat = rng.normal(size=(nrow, K))
+    z = rng.normal(size=(nrow, K))
+    alpha, mean = 2.0, 3.1
+    U, st = orc.sample_latents(K, R, V, mean, alpha, mu, Lam, Uhat=Uhat, z=z)
+    assert st == 0
+    for n in range(nrow):
+        cols = Y.indices[Y.indptr[n]:Y.indptr[n + 1]]
+        ys = Y.data[Y.indptr[n]:Y.indptr[n + 1]]
+        Vn = V[cols]
+        MM = Lam + alpha * Vn.T @ Vn
+        rr = alpha * Vn.T @ (ys - mean) + Lam @ (mu + Uhat[n])
+        L = np.linalg.cholesky(MM)
+        x = sla.solve_triangular(L.T, sla.solve_triangular(L, rr, lower=True) + z[n],
+                                 lower=False)
+        np.testing.assert_allclose(U[n], x, rtol=1e-11, atol=1e-12)
+
+
+def test_sample_latents_reports_cholesky_failure():
+    K = 3
+    R = orc.Csr(np.array([0, 0]), np.zeros(0, np.int32), np.zeros(0), 1, 1)
+    U, st = orc.sample_latents(K, R, np.zeros((1, K)), 0.0, 1.0, np.zeros(K), -np.eye(K))
+    assert st == -1
+
+
+def test_cond_normal_wishart_moments():
+    # Lambda ~ W(T_c, nu_c) has mean nu_c * T_c; mu | Lambda ~ N(mu_c, (kappa_c Lambda)^-1).
+    rng = np.random.default_rng(1)
+    K, N = 3, 25
+    U = rng.normal(size=(N, K)) + np.array([0.5, -1.0, 2.0])
+    mu0 = np.zeros(K)
+    kappa, nu, T = 2.0, K, np.eye(K)
+    NU = U.sum(0)
+    mu_c = (kappa * mu0 + NU) / (kappa + N)
+    X = T + U.T @ U + kappa * np.outer(mu0, mu0) - (kappa + N) * np.outer(mu_c, mu_c)
+    Tc = np.linalg.inv(X)
+    lams, mus = [], []
+    for s in range(3000):
+        mu, Lam, st = orc.cond_normal_wishart(U, mu0, kappa, T, nu, seed=11, sweep=s)
+        assert st == 0
+        lams.append(Lam)
+        mus.append(mu)
+    lams = np.array(lams)
+    mus = np.array(mus)
+    want = (nu + N) * Tc
+    np.testing.assert_allclose(lams.mean(0), want, atol=0.06 * np.abs(want).max())
+    np.testing.assert_allclose(mus.mean(0), mu_c, atol=0.05)
+    assert np.allclose(lams, np.transpose(lams, (0, 2, 1)), atol=1e-12)
+
+
+def test_blockcg_solves_regularised_normal_equations():
+    rng = np.random.default_rng(2)
+    nrow, nfeat, nrhs = 200, 120, 7
+    F = sp.random(nrow, nfeat, density=0.05, random_state=rng, format="csr")
+    F.data[:] = 1.0
+    B = rng.normal(size=(nfeat, nrhs))
+    reg = 1.5
+    Fc, Ftc = orc.Csr.from_scipy(F, True), orc.Csr.from_scipy(F.T, True)
+    X, it = orc.blockcg(Fc, Ftc, reg, B, 1e-8)
+    A = (F.T @ F).toarray() + reg * np.eye(nfeat)
+    np.testing.assert_allclose(X, np.linalg.solve(A, B), rtol=1e-5, atol=1e-6)
+    assert 0 < it < 200
+    # blocked wrapper with 32+8 blocking on 45 RHS (two blocks)
+    B2 = rng.normal(size=(nfeat, 45))
+    X2, _ = orc.blockcg(Fc, Ftc, reg, B2, 1e-8, blocksize=32, excess=8)
+    np.testing.assert_allclose(X2, np.linalg.solve(A, B2), rtol=1e-5, atol=1e-6)
+
+
+def test_model_runs_and_learns_small_bpmf():
+    rng = np.random.default_rng(3)
+    nrow, ncol, K = 120, 80, 4
+    Ut = rng.normal(size=(nrow, 3))
+    Vt = rng.normal(size=(ncol, 3))
+    Yfull = Ut @ Vt.T + rng.normal(scale=0.3, size=(nrow, ncol))
+    mask = rng.random((nrow, ncol)) < 0.3
+    r, c = np.nonzero(mask)
+    test = rng.random(len(r)) < 0.1
+    Ytr = sp.coo_matrix((Yfull[r[~test], c[~test]], (r[~test], c[~test])), shape=(nrow, ncol))
+    Yte = sp.csc_matrix((Yfull[r[test], c[test]], (r[test], c[test])), shape=(nrow, ncol))
+    Yte.sort_indices()
+    te = Yte.tocoo()
+    m = orc.Model(K, 1.0 / 0.09, 5)
+    Rr, Rc = orc.Csr.from_scipy(Ytr), orc.Csr.from_scipy(Ytr.T)
+    m.set_train(Rr, Rc, Ytr.tocsc().sum() / Ytr.nnz)
+    m.set_test(te.row, te.col, te.data)
+    for it in range(60):
+        assert m.sweep(it, 30) == 0
+    rmse, rmse1 = m.rmse()
+    assert rmse < 0.6, rmse

@@ -1,0 +1,160 @@
+/* macau_b200.h -- C ABI of the sm_100a Gibbs-sweep library for BPMF / Macau.
+ *
+ * The library replaces the hot path of jaak-s/macau 0.5.3 (one Gibbs sweep of MacauX::run,
+ * lib/macau-cpp/macau.cpp:110-147): the per-row latent sampler (sample_latent_blas,
+ * latentprior.cpp:361-385), the Normal-Wishart hyperprior update (CondNormalWishart,
+ * mvnormal.cpp:314-336) and, for side information, the block-CG solve of the link matrix
+ * (solve_blockcg, linop.h:207-343).  The reference has no C ABI; each entry below names the
+ * C++ member or Cython function it stands in for.
+ *
+ * Conventions
+ *   - Matrices are column-major like the reference's Eigen storage: a latent matrix is K x N
+ *     (column n = the K-vector of entity n), Lambda is K x K, beta is K x nfeat.
+ *   - Every entry point returns 0 on success or a negative MG_ERR_* code; mg_last_error()
+ *     gives the message.  Entry points never throw and are not thread-safe per context.
+ *   - All device work of one context runs on one CUDA stream owned by the context; calls are
+ *     synchronous from the caller's point of view unless stated otherwise.
+ *   - Random draws are keyed (seed, sweep, mode, purpose, index) through Philox-4x32-10, so a
+ *     run is reproducible for a given seed.
+ */
+#ifndef MACAU_B200_H
+#define MACAU_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes (negative) */
+#define MG_OK 0
+#define MG_ERR_ARG (-1)        /* invalid argument (reference: ValueError / runtime_error) */
+#define MG_ERR_CHOL (-2)       /* "Cholesky Decomposition failed!" (latentprior.cpp:374-376) */
+#define MG_ERR_CG (-3)         /* block-CG breakdown or iteration cap (linop.h:279) */
+#define MG_ERR_CUDA (-4)       /* CUDA runtime error */
+#define MG_ERR_STATE (-5)      /* call out of order (e.g. sweep before data) */
+#define MG_ERR_TIMEOUT (-6)    /* a bounded device-side wait gave up */
+#define MG_ERR_NOGPU (-7)      /* no sm_100 device */
+
+/* Arithmetic of the sampler. */
+#define MG_COMPUTE_FP64 0      /* everything in FP64 (parity with the FP64 oracle <= 1e-9) */
+#define MG_COMPUTE_MIXED 1     /* BF16 Gram / FP32 accumulate, FP32 Cholesky + FP64 retry,
+                                  FP32 block-CG with FP64 residual replacement; FP64 hyperprior */
+
+typedef struct mg_ctx mg_ctx;
+
+typedef struct mg_config {
+  int num_latent;     /* K: Macau::num_latent (macau.h:13) */
+  double precision;   /* alpha of FixedGaussianNoise (noisemodels.h:32-39) */
+  uint64_t seed;      /* key of every random draw */
+  int compute;        /* MG_COMPUTE_FP64 or MG_COMPUTE_MIXED */
+  int verbose;        /* print one status line per iteration like MacauX::printStatus */
+  int device;         /* CUDA device ordinal */
+} mg_config;
+
+typedef struct mg_stats {
+  double sweeps;            /* sweeps run since mg_init */
+  double seconds_sample;    /* device time in the latent samplers (CUDA events) */
+  double seconds_prior;     /* device time in the hyperprior / beta updates */
+  double seconds_eval;      /* device time in test evaluation */
+  int64_t retries[2];       /* mixed mode: rows re-factorised in FP64, per mode (cumulative) */
+  int64_t rows_sampled[2];  /* rows sampled, per mode (cumulative) */
+  int cg_iters[2];          /* block-CG iterations of the last beta update, per mode */
+  int graph_captured;       /* 1 when sweeps replay a captured CUDA graph */
+} mg_stats;
+
+/* Context lifetime.  Replaces `make_macau_fixed(2, K, precision)` (macau.cpp:214-220) plus
+ * MacauX construction; only fixed Gaussian noise on a 2-mode matrix is supported. */
+int mg_create(mg_ctx** out, const mg_config* cfg);
+void mg_destroy(mg_ctx* ctx);
+const char* mg_last_error(const mg_ctx* ctx);
+
+/* Macau::setRelationData(int* idx, int nmodes, double* values, int nnz, int* dims)
+ * (macau.h:39; MatrixData::setTrain, sparsetensor.cpp:92-106).  idx is nnz x nmodes
+ * column-major (row indices, then column indices); nmodes must be 2.  Duplicate (i, j) entries
+ * are summed like Eigen's setFromTriplets.  The arrays are copied; host buffers may be freed
+ * afterwards. */
+int mg_set_relation_data(mg_ctx* ctx, const int32_t* idx, int nmodes, const double* values,
+                         int64_t nnz, const int32_t* dims);
+
+/* Macau::setRelationDataTest(...) (macau.h:40; MatrixData::setTest, sparsetensor.cpp:108-117). */
+int mg_set_relation_data_test(mg_ctx* ctx, const int32_t* idx, int nmodes,
+                              const double* values, int64_t nnz, const int32_t* dims);
+
+/* Side information for `mode` (MacauPrior<SparseDoubleFeat>, latentprior.h:82-125, built by
+ * make_prior, macau.pyx:154-192): F is nrows x nfeat given as COO; vals == NULL means a binary
+ * matrix (all ones).  lambda_beta / tol are MacauPrior::setLambdaBeta / setTol.  Without this
+ * call the mode uses the BPMF prior (BPMFPrior, latentprior.h:53-79). */
+int mg_set_side(mg_ctx* ctx, int mode, const int32_t* rows, const int32_t* cols,
+                const double* vals, int64_t nnz, int nrows, int nfeat, double lambda_beta,
+                double tol);
+
+/* Macau::setSamples (macau.h:36). */
+int mg_set_samples(mg_ctx* ctx, int burnin, int nsamples);
+
+/* MacauX::init (macau.cpp:72-86): latents to zero, priors to their initial hyperparameters
+ * (BPMFPrior::init / MacauPrior::init, latentprior.cpp:84-99, 181-216). */
+int mg_init(mg_ctx* ctx);
+
+/* One iteration `iter` of MacauX::run (macau.cpp:110-147): sample mode 0, sample mode 1,
+ * update prior 0, update prior 1, evaluate the test set with n = iter < burnin ? 0 : iter-burnin
+ * (when eval != 0).  Replays a captured CUDA graph when the sweep has no host-side decision. */
+int mg_sweep(mg_ctx* ctx, int iter, int eval);
+
+/* `count` consecutive sweeps starting at `first_iter` without returning to the caller in
+ * between (no per-sweep host synchronisation). */
+int mg_sweeps(mg_ctx* ctx, int first_iter, int count, int eval);
+
+/* MacauX::run (macau.cpp:94-148): mg_init, then burnin + nsamples sweeps with evaluation. */
+int mg_run(mg_ctx* ctx);
+
+/* Phase-level entry points (used by parity tests and by hosts that drive the loop):
+ * ILatentPrior::sample_latents for one mode (latentprior.cpp:30-37, 69-77, 219-227) and
+ * ILatentPrior::update_prior (latentprior.cpp:79-81, 255-264), with the draws of sweep `iter`.
+ * `z` optionally injects the K x N standard normals of the row sampler (NULL = keyed draws). */
+int mg_sample_latents(mg_ctx* ctx, int mode, int iter, const double* z);
+int mg_update_prior(mg_ctx* ctx, int mode, int iter);
+
+/* FixedGaussianNoise::evalModel -> eval_rmse (noisemodels.cpp:161-166, bpmfutils.h:86-114). */
+int mg_eval(mg_ctx* ctx, int n);
+
+/* State access (K x N column-major latents; K x K Lambda; K mu; K x nfeat beta; K x N Uhat). */
+int mg_get_latents(mg_ctx* ctx, int mode, double* out);
+int mg_set_latents(mg_ctx* ctx, int mode, const double* in);
+int mg_get_hyper(mg_ctx* ctx, int mode, double* mu, double* Lambda, double* lambda_beta);
+int mg_set_hyper(mg_ctx* ctx, int mode, const double* mu, const double* Lambda,
+                 const double* lambda_beta);
+int mg_get_beta(mg_ctx* ctx, int mode, double* beta);
+int mg_get_uhat(mg_ctx* ctx, int mode, double* uhat);
+int mg_get_dims(mg_ctx* ctx, int64_t* nrow, int64_t* ncol, int64_t* ntrain, int64_t* ntest,
+                double* mean_value);
+
+/* Results: Macau::getRmseTest / getPredictions / getStds / getTestData (macau.h:45-51,
+ * macau.cpp:174-188).  rmse[0] = posterior-mean RMSE, rmse[1] = last single-sample RMSE.
+ * Test data rows are (row, col, value) in the CSC order of the test matrix, ntest x 3
+ * column-major like MatrixData::getTestData (sparsetensor.cpp:63-76). */
+int mg_get_rmse(mg_ctx* ctx, double* rmse);
+int mg_get_predictions(mg_ctx* ctx, double* out);
+int mg_get_stds(mg_ctx* ctx, double* out);
+int mg_get_test_data(mg_ctx* ctx, double* out);
+int mg_get_stats(mg_ctx* ctx, mg_stats* out);
+
+/* Switches of the implementation (no reference counterpart; defaults 1):
+ *   "graph"            replay captured CUDA graphs for sweeps without host-side decisions
+ *   "tensor_core_gram" mixed mode: run the K = 32 row Grams on the tcgen05 tensor cores */
+int mg_set_option(mg_ctx* ctx, const char* name, int value);
+
+/* macau.blockcg(X, B, reg, tol) (macau.pyx:67-91 -> solve_blockcg, linop.h:229-343) on the GPU:
+ * solves (F'F + reg I) X' = B' for nrhs right-hand sides with the reference's 32+8 RHS blocking
+ * (linop.h:207-226).  F is nrows x nfeat COO (vals NULL = binary); B and X are nrhs x nfeat
+ * column-major.  Unlike the reference wrapper (which drops its solution), X is returned.
+ * compute selects FP64 or FP32-with-FP64-residual-replacement.  *niter receives the summed
+ * iteration count of the blocks and *seconds the device time. */
+int mg_blockcg(const int32_t* rows, const int32_t* cols, const double* vals, int64_t nnz,
+               int nrows, int nfeat, const double* B, int nrhs, double reg, double tol,
+               int compute, double* X, int* niter, double* seconds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MACAU_B200_H */

@@ -1,0 +1,677 @@
+// Side-information kernels: CSR SpMM (compute_uhat, A_mul_B(tmp, F), A_mul_Bx<N>), the
+// right-hand side of MacauPrior::sample_beta and the block-CG solver solve_blockcg
+// (linop.h:207-343) for (F^T F + reg I) X = B with up to 64 right-hand sides per block.
+//
+// Layout: a K x nfeat matrix of the reference is stored feature-major with a padded row of
+// NRP (32 or 64) values, so one warp owns one feature / CSR row and lane l owns components
+// l and l + 32.  SpMMs are warp-per-row gathers of whole 128/256-byte rows (binary F: adds only).
+// The K x K reductions (P KP^T, R R^T) are per-block register-tile partials reduced in block
+// order by one CTA (deterministic), which also does the small Cholesky solves.
+//
+// Precision: FP64, or FP32 vectors (P, R, KP, F P) with FP64 X, FP64 K x K algebra and an FP64
+// residual replacement R = B - (F^T F + reg I) X every kReplaceEvery iterations.
+#include <cmath>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "rng.cuh"
+
+namespace mg {
+namespace {
+
+constexpr int kReplaceEvery = 20;
+constexpr int kOuterThreads = 256;
+constexpr int kOuterRows = 32;
+
+template <typename V>
+__device__ __forceinline__ V ldv(const V* p) { return *p; }
+
+// ---------------- SpMM: out[r] = sum val * src[idx] (+ reg * add[r]) ----------------
+template <typename V, int NRP>
+__global__ void __launch_bounds__(256)
+    k_spmm(const long long* __restrict__ ptr, const int* __restrict__ idx,
+           const double* __restrict__ val, const float* __restrict__ valf, long long nrow,
+           const V* __restrict__ src, int sstride, V* __restrict__ dst, int dstride, int ncomp,
+           const V* __restrict__ add, int astride, double reg, const double* __restrict__ reg_dev) {
+  constexpr int C = NRP / 32;
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  const V r = (V)(reg_dev ? *reg_dev : reg);
+  for (long long row = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       row < nrow; row += nw) {
+    V acc[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) acc[c] = (V)0;
+    const long long b = ptr[row], e = ptr[row + 1];
+    for (long long q = b; q < e; q++) {
+      const V* s = src + (size_t)idx[q] * sstride;
+      V w = (V)1;
+      if constexpr (sizeof(V) == 8) {
+        if (val) w = (V)val[q];
+      } else {
+        if (valf) w = (V)valf[q];
+      }
+#pragma unroll
+      for (int c = 0; c < C; c++) {
+        const int k = lane + 32 * c;
+        if (k < ncomp) acc[c] += (val || valf) ? s[k] * w : s[k];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+      const int k = lane + 32 * c;
+      if (k < ncomp) {
+        V o = acc[c];
+        if (add) o += r * add[(size_t)row * astride + k];
+        dst[(size_t)row * dstride + k] = o;
+      }
+    }
+  }
+}
+
+// ---------------- per-block partial of sum_f a_f b_f^T (NRP x NRP, full) ----------------
+template <typename V, int NRP>
+__global__ void __launch_bounds__(kOuterThreads)
+    k_outer(const V* __restrict__ A, const V* __restrict__ B, int stride, long long nrow,
+            long long rows_per_block, double* __restrict__ partials) {
+  constexpr int PER = NRP * NRP / kOuterThreads;  // 4 or 16
+  __shared__ double as[kOuterRows * NRP], bs[kOuterRows * NRP];
+  const long long r0 = (long long)blockIdx.x * rows_per_block;
+  const long long r1 = min(nrow, r0 + rows_per_block);
+  double acc[PER];
+#pragma unroll
+  for (int q = 0; q < PER; q++) acc[q] = 0.0;
+  for (long long b = r0; b < r1; b += kOuterRows) {
+    const int cnt = (int)min((long long)kOuterRows, r1 - b);
+    __syncthreads();
+    for (int e = threadIdx.x; e < cnt * NRP; e += kOuterThreads) {
+      const int rr = e / NRP, k = e % NRP;
+      as[e] = (double)A[(b + rr) * stride + k];
+      bs[e] = (double)B[(b + rr) * stride + k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      const int ent = threadIdx.x + q * kOuterThreads;
+      const int i = ent % NRP, j = ent / NRP;  // entry (i, j) = sum a_i b_j
+      double s = acc[q];
+      for (int rr = 0; rr < cnt; rr++) s += as[rr * NRP + i] * bs[rr * NRP + j];
+      acc[q] = s;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < PER; q++)
+    partials[(size_t)blockIdx.x * NRP * NRP + threadIdx.x + q * kOuterThreads] = acc[q];
+}
+
+// Sum of the block partials of entry (i, j), i,j < n.
+__device__ __forceinline__ double sum_part(const double* partials, int nparts, int NRP, int i,
+                                           int j) {
+  double s = 0.0;
+  for (int b = 0; b < nparts; b++) s += partials[(size_t)b * NRP * NRP + i + j * NRP];
+  return s;
+}
+
+// Left-looking lower Cholesky of the n x n matrix A (leading dimension ld) by one CTA, column by
+// column; thread i computes L(i, j).  On a non-positive pivot it stops and leaves column j and
+// the columns after it as they were, like the unchecked Eigen llt() the reference uses
+// (linop.h:287, 313): the caller's solves then read that partial factor.  Returns false then.
+__device__ bool cta_chol_n(double* A, int n, int ld) {
+  __syncthreads();
+  for (int j = 0; j < n; j++) {
+    double d = A[j + j * ld];
+    for (int p = 0; p < j; p++) d -= A[j + p * ld] * A[j + p * ld];
+    if (!(d > 0.0)) {
+      __syncthreads();
+      return false;
+    }
+    const double ljj = sqrt(d);
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+      double s = A[i + j * ld];
+      for (int p = 0; p < j; p++) s -= A[i + p * ld] * A[j + p * ld];
+      A[i + j * ld] = s / ljj;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) A[j + j * ld] = ljj;
+    __syncthreads();
+  }
+  return true;
+}
+
+// small layout (doubles): RtR[64*64] | RtR2[64*64] | M[64*64] | A[64*64] | Psi[64*64] | norms[64]
+//                         | inorms[64] | flags[4]
+constexpr int kSq = 64 * 64;
+struct SmallView {
+  double *RtR, *RtR2, *M, *A, *Psi, *norms, *inorms, *flags;
+  __host__ __device__ explicit SmallView(double* s)
+      : RtR(s), RtR2(s + kSq), M(s + 2 * kSq), A(s + 3 * kSq), Psi(s + 4 * kSq),
+        norms(s + 5 * kSq), inorms(s + 5 * kSq + 64), flags(s + 5 * kSq + 128) {}
+};
+
+// RtR = sum partials (full matrix from the lower triangle, A_mul_At_combo + makeSymmetric)
+__global__ void k_cg_rtr(const double* partials, int nparts, int NRP, int n, double* small) {
+  SmallView v(small);
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e % n, j = e / n;
+    const int lo = i > j ? i : j, hi = i > j ? j : i;
+    v.RtR[i + j * 64] = sum_part(partials, nparts, NRP, lo, hi);
+  }
+}
+
+// norms of the RHS rows (B.row(rhs) over all features) from the outer partials of (B, B)
+__global__ void k_cg_norms(const double* partials, int nparts, int NRP, int n, double* small) {
+  SmallView v(small);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double s = sum_part(partials, nparts, NRP, i, i);
+    v.norms[i] = sqrt(s);
+    v.inorms[i] = 1.0 / v.norms[i];
+  }
+}
+
+// R = P = B * inorms (V), X = 0, Bn = B * inorms (FP64, for residual replacement)
+template <typename V>
+__global__ void k_cg_init(const double* __restrict__ B, int bstride, long long nfeat, int n,
+                          int NRP, const double* small, V* R, V* P, double* X, double* Bn) {
+  SmallView v(const_cast<double*>(small));
+  const long long total = nfeat * NRP;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long f = e / NRP;
+    const int k = (int)(e % NRP);
+    double r = 0.0;
+    if (k < n) r = B[f * bstride + k] * v.inorms[k];
+    R[e] = (V)r;
+    P[e] = (V)r;
+    X[e] = 0.0;
+    if (Bn) Bn[e] = r;
+  }
+}
+
+// A = (chol(PtKP) \ RtR)^T  (linop.h:286-289); PtKP from the lower triangle of sum P KP^T.
+__global__ void k_cg_solve_a(const double* partials, int nparts, int NRP, int n, double* small,
+                             Ctl* ctl) {
+  SmallView v(small);
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e % n, j = e / n;
+    if (i >= j) v.M[i + j * 64] = sum_part(partials, nparts, NRP, i, j);  // P(i) . KP(j)
+  }
+  cta_chol_n(v.M, n, 64);  // a failed pivot is not an error in the reference either
+  __syncthreads();
+  // columns c of RtR solved: Y = L^{-T} L^{-1} RtR ; A(c, i) = Y(i, c)
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    double y[64];
+    for (int i = 0; i < n; i++) y[i] = v.RtR[i + c * 64];
+    for (int i = 0; i < n; i++) {
+      double s = y[i];
+      for (int p = 0; p < i; p++) s -= v.M[i + p * 64] * y[p];
+      y[i] = s / v.M[i + i * 64];
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double s = y[i];
+      for (int p = i + 1; p < n; p++) s -= v.M[p + i * 64] * y[p];
+      y[i] = s / v.M[i + i * 64];
+    }
+    for (int i = 0; i < n; i++) v.A[c + i * 64] = y[i];
+  }
+}
+
+// RtR2 = sum R R^T; converged = all diag < tol^2; Psi = (chol(RtR) \ RtR2)^T; RtR <- RtR2.
+__global__ void k_cg_solve_psi(const double* partials, int nparts, int NRP, int n, double tolsq,
+                               double* small, Ctl* ctl, int* flag_out) {
+  SmallView v(small);
+  __shared__ int conv;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e % n, j = e / n;
+    const int lo = i > j ? i : j, hi = i > j ? j : i;
+    v.RtR2[i + j * 64] = sum_part(partials, nparts, NRP, lo, hi);
+  }
+  if (threadIdx.x == 0) conv = 1;
+  __syncthreads();
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  if (threadIdx.x < n) {
+    const double d = v.RtR2[threadIdx.x + threadIdx.x * 64];
+    if (!(d < tolsq)) atomicAnd(&conv, 0);
+    if (!isfinite(d)) atomicOr(&bad, 1);
+  }
+  __syncthreads();
+  if (bad) {  // non-finite residual: stop the iteration and report a breakdown
+    if (threadIdx.x == 0) {
+      conv = 1;
+      atomicOr(&ctl->status, kStatCgFail);
+    }
+  }
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e % n, j = e / n;
+    v.M[i + j * 64] = v.RtR[i + j * 64];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    v.flags[0] = conv;
+    ctl->cg_done = (uint32_t)conv;
+    if (flag_out) *flag_out = conv;
+  }
+  if (conv) return;
+  cta_chol_n(v.M, n, 64);
+  __syncthreads();
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    double y[64];
+    for (int i = 0; i < n; i++) y[i] = v.RtR2[i + c * 64];
+    for (int i = 0; i < n; i++) {
+      double s = y[i];
+      for (int p = 0; p < i; p++) s -= v.M[i + p * 64] * y[p];
+      y[i] = s / v.M[i + i * 64];
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double s = y[i];
+      for (int p = i + 1; p < n; p++) s -= v.M[p + i * 64] * y[p];
+      y[i] = s / v.M[i + i * 64];
+    }
+    for (int i = 0; i < n; i++) v.Psi[c + i * 64] = y[i];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e % n, j = e / n;
+    v.RtR[i + j * 64] = v.RtR2[i + j * 64];
+  }
+}
+
+// Broadcast of component k of a feature row held as lane-distributed registers.
+template <typename V, int C>
+__device__ __forceinline__ V bcast_comp(const V (&x)[C], int k) {
+  V out = (V)0;
+#pragma unroll
+  for (int c = 0; c < C; c++)
+    if ((k >> 5) == c) out = __shfl_sync(0xffffffffu, x[c], k & 31);
+  return out;
+}
+
+// X += A P ; R -= A KP  (linop.h:292-300), warp per feature; A (n x n) in shared memory.
+template <typename V, int NRP>
+__global__ void __launch_bounds__(256)
+    k_cg_update(long long nfeat, int n, const double* small, const V* __restrict__ P,
+                const V* __restrict__ KPm, V* __restrict__ R, double* __restrict__ X) {
+  constexpr int C = NRP / 32;
+  __shared__ double As[64 * 64];
+  SmallView v(const_cast<double*>(small));
+  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) As[e] = v.A[e];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long f = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); f < nfeat;
+       f += nw) {
+    V p[C], kp[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+      p[c] = P[f * NRP + lane + 32 * c];
+      kp[c] = KPm[f * NRP + lane + 32 * c];
+    }
+    double sx[C], sr[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) sx[c] = sr[c] = 0.0;
+    for (int k = 0; k < n; k++) {
+      const double pk = (double)bcast_comp<V, C>(p, k);
+      const double kk = (double)bcast_comp<V, C>(kp, k);
+#pragma unroll
+      for (int c = 0; c < C; c++) {
+        const int i = lane + 32 * c;
+        const double a = (i < n) ? As[i + k * 64] : 0.0;
+        sx[c] += a * pk;
+        sr[c] += a * kk;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+      const int i = lane + 32 * c;
+      if (i < n) {
+        X[f * NRP + i] += sx[c];
+        R[f * NRP + i] = (V)((double)R[f * NRP + i] - sr[c]);
+      }
+    }
+  }
+}
+
+// P = R + Psi P  (linop.h:319-326)
+template <typename V, int NRP>
+__global__ void __launch_bounds__(256)
+    k_cg_pupdate(long long nfeat, int n, const double* small, const V* __restrict__ R,
+                 V* __restrict__ P) {
+  constexpr int C = NRP / 32;
+  __shared__ double Ps[64 * 64];
+  SmallView v(const_cast<double*>(small));
+  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) Ps[e] = v.Psi[e];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long f = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); f < nfeat;
+       f += nw) {
+    V p[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) p[c] = P[f * NRP + lane + 32 * c];
+    double s[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) s[c] = 0.0;
+    for (int k = 0; k < n; k++) {
+      const double pk = (double)bcast_comp<V, C>(p, k);
+#pragma unroll
+      for (int c = 0; c < C; c++) {
+        const int i = lane + 32 * c;
+        s[c] += (i < n ? Ps[i + k * 64] : 0.0) * pk;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+      const int i = lane + 32 * c;
+      if (i < n) P[f * NRP + i] = (V)((double)R[f * NRP + i] + s[c]);
+    }
+  }
+}
+
+// R = Bn - KX (FP64 residual replacement, rounded to V)
+template <typename V>
+__global__ void k_cg_resid(long long total, int NRP, int n, const double* __restrict__ Bn,
+                           const double* __restrict__ KX, V* __restrict__ R) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(e % NRP);
+    R[e] = (V)(k < n ? Bn[e] - KX[e] : 0.0);
+  }
+}
+
+// X_out[f, k] = X[f, k] * norms[k]
+__global__ void k_cg_finish(long long nfeat, int NRP, int n, const double* small,
+                            const double* __restrict__ X, double* __restrict__ out,
+                            int ostride) {
+  SmallView v(const_cast<double*>(small));
+  const long long total = nfeat * n;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long f = e / n;
+    const int k = (int)(e % n);
+    out[f * ostride + k] = X[f * NRP + k] * v.norms[k];
+  }
+}
+
+// ---------------- sample_beta right-hand side ----------------
+// MvNormal_prec_omp(Lambda, n) column c (mvnormal.cpp:186-201): x = L^{-T} z with z keyed
+// (purpose, c); one thread per column, back substitution in the reference's order.
+__device__ __forceinline__ void mvn_col(const double* Ls, int K, unsigned long long seed,
+                                        uint32_t sweep, uint32_t stream, uint32_t col,
+                                        double* z) {
+  for (int i = 0; i < K; i += 2) {
+    double z0, z1;
+    normal_pair(seed, sweep, stream, col, (uint32_t)(i >> 1), &z0, &z1);
+    z[i] = z0;
+    if (i + 1 < K) z[i + 1] = z1;
+  }
+  for (int i = K - 1; i >= 0; i--) {
+    double s = z[i];
+    for (int p = i + 1; p < K; p++) s -= Ls[p + i * K] * z[p];
+    z[i] = s / Ls[i + i * K];
+  }
+}
+
+// tmp[n] = (U[n] + MvNormal_prec(Lambda)[n]) - mu   (latentprior.cpp:277)
+template <typename T>
+__global__ void __launch_bounds__(128)
+    k_beta_tmp(const T* __restrict__ U, int ustride, long long N, int K,
+               const double* __restrict__ L, const double* __restrict__ mu, const Ctl* ctl,
+               unsigned long long seed, int mode, double* __restrict__ tmp, int tstride) {
+  __shared__ double Ls[64 * 64];
+  for (int e = threadIdx.x; e < K * K; e += blockDim.x) Ls[e] = L[e];
+  __syncthreads();
+  const uint32_t sweep = ctl->sweep;
+  const uint32_t st = stream_id(kMvnN, (uint32_t)mode);
+  double z[64];
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < N;
+       n += (long long)gridDim.x * blockDim.x) {
+    mvn_col(Ls, K, seed, sweep, st, (uint32_t)n, z);
+    for (int k = 0; k < K; k++) tmp[n * tstride + k] = ((double)U[n * ustride + k] + z[k]) - mu[k];
+  }
+}
+
+// B[f] += sqrt(lambda_beta) * MvNormal_prec(Lambda)[f]   (latentprior.cpp:278)
+__global__ void __launch_bounds__(128)
+    k_beta_noise(long long nfeat, int K, const double* __restrict__ L,
+                 const double* __restrict__ lb, const Ctl* ctl, unsigned long long seed,
+                 int mode, double* __restrict__ B, int bstride) {
+  __shared__ double Ls[64 * 64];
+  for (int e = threadIdx.x; e < K * K; e += blockDim.x) Ls[e] = L[e];
+  __syncthreads();
+  const uint32_t sweep = ctl->sweep;
+  const uint32_t st = stream_id(kMvnF, (uint32_t)mode);
+  const double slb = sqrt(*lb);
+  double z[64];
+  for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < nfeat;
+       f += (long long)gridDim.x * blockDim.x) {
+    mvn_col(Ls, K, seed, sweep, st, (uint32_t)f, z);
+    for (int k = 0; k < K; k++) B[f * bstride + k] += slb * z[k];
+  }
+}
+
+__global__ void k_small_chol(const double* A, int K, double* L, Ctl* ctl) {
+  __shared__ double M[64 * 64];
+  for (int e = threadIdx.x; e < K * K; e += blockDim.x) M[e] = A[e];
+  cta_chol_n(M, K, K);  // LLT of MvNormal_prec_omp (mvnormal.cpp:190) is not checked either
+  __syncthreads();
+  for (int e = threadIdx.x; e < K * K; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    L[e] = (i >= j) ? M[e] : 0.0;
+  }
+}
+
+int grid_for(long long rows, int rows_per_block) {
+  long long b = (rows + rows_per_block - 1) / rows_per_block;
+  if (b > 148 * 16) b = 148 * 16;
+  return (int)(b < 1 ? 1 : b);
+}
+
+int outer_blocks(long long nrow) {
+  long long b = (nrow + 255) / 256;
+  if (b > 296) b = 296;
+  return (int)(b < 1 ? 1 : b);
+}
+
+template <typename V, int NRP>
+void outer(const V* A, const V* B, long long nrow, double* partials, int nb, cudaStream_t s) {
+  const long long rpb = (nrow + nb - 1) / nb;
+  k_outer<V, NRP><<<nb, kOuterThreads, 0, s>>>(A, B, NRP, nrow, rpb, partials);
+  MG_CUDA(cudaGetLastError());
+}
+
+template <typename V, int NRP>
+void spmm_t(const DevCsr& A, const V* src, int sstride, V* dst, int dstride, int ncomp,
+            const V* add, int astride, double reg, const double* reg_dev, cudaStream_t s) {
+  k_spmm<V, NRP><<<grid_for(A.nrow, 8), 256, 0, s>>>(A.ptr, A.idx, A.val, A.valf, A.nrow, src,
+                                                      sstride, dst, dstride, ncomp, add,
+                                                      astride, reg, reg_dev);
+  MG_CUDA(cudaGetLastError());
+}
+
+template <typename V, int NRP>
+int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev,
+            const double* B, int bstride, int n, double tol, double* Xout, int xstride,
+            Ctl* ctl, cudaStream_t s, V* R, V* P, V* KPm, V* inner, double* Xd, double* Bn,
+            double* KX, double* innerd, double* small, double* partials, int* flag_dev,
+            volatile int* flag_host) {
+  const long long nfeat = Ft.nrow;
+  const int nb = outer_blocks(nfeat);
+  const int eg = grid_for(nfeat * NRP, 256);
+  // Bn <- B padded to NRP columns, then the RHS norms from diag(B B^T)
+  MG_CUDA(cudaMemcpy2DAsync(Bn, NRP * sizeof(double), B, bstride * sizeof(double),
+                            n * sizeof(double), nfeat, cudaMemcpyDeviceToDevice, s));
+  if (n < NRP)
+    MG_CUDA(cudaMemset2DAsync(Bn + n, NRP * sizeof(double), 0, (NRP - n) * sizeof(double),
+                              nfeat, s));
+  outer<double, NRP>(Bn, Bn, nfeat, partials, nb, s);
+  k_cg_norms<<<1, 64, 0, s>>>(partials, nb, NRP, n, small);
+  MG_CUDA(cudaGetLastError());
+  k_cg_init<V><<<eg, 256, 0, s>>>(Bn, NRP, nfeat, n, NRP, small, R, P, Xd,
+                                  sizeof(V) == 4 ? Bn : nullptr);
+  MG_CUDA(cudaGetLastError());
+  outer<V, NRP>(R, R, nfeat, partials, nb, s);
+  k_cg_rtr<<<1, 256, 0, s>>>(partials, nb, NRP, n, small);
+  MG_CUDA(cudaGetLastError());
+  const double tolsq = tol * tol;
+  int iter = 0;
+  const int fg = grid_for(nfeat, 8);
+  for (iter = 0; iter < 100000; iter++) {
+    spmm_t<V, NRP>(F, P, NRP, inner, NRP, n, nullptr, 0, 0.0, nullptr, s);
+    spmm_t<V, NRP>(Ft, inner, NRP, KPm, NRP, n, P, NRP, reg, reg_dev, s);
+    outer<V, NRP>(P, KPm, nfeat, partials, nb, s);
+    k_cg_solve_a<<<1, 64, 0, s>>>(partials, nb, NRP, n, small, ctl);
+    MG_CUDA(cudaGetLastError());
+    k_cg_update<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, P, KPm, R, Xd);
+    MG_CUDA(cudaGetLastError());
+    if (sizeof(V) == 4 && (iter + 1) % kReplaceEvery == 0) {
+      spmm_t<double, NRP>(F, Xd, NRP, innerd, NRP, n, nullptr, 0, 0.0, nullptr, s);
+      spmm_t<double, NRP>(Ft, innerd, NRP, KX, NRP, n, Xd, NRP, reg, reg_dev, s);
+      k_cg_resid<V><<<eg, 256, 0, s>>>(nfeat * NRP, NRP, n, Bn, KX, R);
+      MG_CUDA(cudaGetLastError());
+    }
+    outer<V, NRP>(R, R, nfeat, partials, nb, s);
+    k_cg_solve_psi<<<1, 64, 0, s>>>(partials, nb, NRP, n, tolsq, small, ctl, flag_dev);
+    MG_CUDA(cudaGetLastError());
+    MG_CUDA(cudaStreamSynchronize(s));
+    if (*flag_host) break;
+    k_cg_pupdate<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, R, P);
+    MG_CUDA(cudaGetLastError());
+  }
+  k_cg_finish<<<grid_for(nfeat * n, 256), 256, 0, s>>>(nfeat, NRP, n, small, Xd, Xout, xstride);
+  MG_CUDA(cudaGetLastError());
+  return iter;
+}
+
+}  // namespace
+
+void launch_spmm(const DevCsr& A, const void* src, int src_stride, void* dst, int dst_stride,
+                 int ncomp, bool f32, cudaStream_t s) {
+  if (ncomp > 64) throw MgError(MG_ERR_ARG, "spmm: more than 64 components");
+  if (f32) {
+    if (ncomp <= 32)
+      spmm_t<float, 32>(A, (const float*)src, src_stride, (float*)dst, dst_stride, ncomp,
+                        nullptr, 0, 0.0, nullptr, s);
+    else
+      spmm_t<float, 64>(A, (const float*)src, src_stride, (float*)dst, dst_stride, ncomp,
+                        nullptr, 0, 0.0, nullptr, s);
+  } else {
+    if (ncomp <= 32)
+      spmm_t<double, 32>(A, (const double*)src, src_stride, (double*)dst, dst_stride, ncomp,
+                         nullptr, 0, 0.0, nullptr, s);
+    else
+      spmm_t<double, 64>(A, (const double*)src, src_stride, (double*)dst, dst_stride, ncomp,
+                         nullptr, 0, 0.0, nullptr, s);
+  }
+}
+
+void launch_beta_rhs_tmp(const void* U, bool f32, int ustride, long long N, int K,
+                         const double* Lchol, const double* mu, const Ctl* ctl,
+                         unsigned long long seed, int mode, double* tmp, int tstride,
+                         cudaStream_t s) {
+  const int g = grid_for(N, 128);
+  if (f32)
+    k_beta_tmp<float><<<g, 128, 0, s>>>((const float*)U, ustride, N, K, Lchol, mu, ctl, seed,
+                                        mode, tmp, tstride);
+  else
+    k_beta_tmp<double><<<g, 128, 0, s>>>((const double*)U, ustride, N, K, Lchol, mu, ctl, seed,
+                                         mode, tmp, tstride);
+  MG_CUDA(cudaGetLastError());
+}
+
+void launch_beta_rhs_b(const DevCsr& Ft, const double* tmp, int tstride, int K,
+                       const double* Lchol, const double* lambda_beta, const Ctl* ctl,
+                       unsigned long long seed, int mode, double* B, int bstride,
+                       cudaStream_t s) {
+  // Ft_y = tmp * F (A_mul_B(tmp, F) -> csr_A_mul_Bn over the rows of F^T) ...
+  launch_spmm(Ft, tmp, tstride, B, bstride, K, false, s);
+  // ... + sqrt(lambda_beta) * MvNormal_prec_omp(Lambda, nfeat)
+  k_beta_noise<<<grid_for(Ft.nrow, 128), 128, 0, s>>>(Ft.nrow, K, Lchol, lambda_beta, ctl, seed,
+                                                      mode, B, bstride);
+  MG_CUDA(cudaGetLastError());
+}
+
+void launch_small_chol(const double* A, int K, double* L, Ctl* ctl, cudaStream_t s) {
+  k_small_chol<<<1, 64, 0, s>>>(A, K, L, ctl);
+  MG_CUDA(cudaGetLastError());
+}
+
+void BlockCg::reserve(long long nrow, long long nfeat, int max_rhs, bool f32) {
+  if (nrow <= nrow_ && nfeat <= nfeat_ && max_rhs <= maxr_ && f32 == f32_ && R_) return;
+  release();
+  nrow_ = nrow;
+  nfeat_ = nfeat;
+  maxr_ = max_rhs;
+  f32_ = f32;
+  const size_t es = f32 ? 4 : 8;
+  const size_t NRP = 64;
+  MG_CUDA(cudaMalloc(&R_, es * nfeat * NRP));
+  MG_CUDA(cudaMalloc(&P_, es * nfeat * NRP));
+  MG_CUDA(cudaMalloc(&KP_, es * nfeat * NRP));
+  MG_CUDA(cudaMalloc(&inner_, es * nrow * NRP));
+  MG_CUDA(cudaMalloc(&Xd_, 8 * nfeat * NRP));
+  MG_CUDA(cudaMalloc(&Bn_, 8 * nfeat * NRP));
+  if (f32) {
+    MG_CUDA(cudaMalloc(&KX_, 8 * nfeat * NRP));
+    MG_CUDA(cudaMalloc(&innerd_, 8 * nrow * NRP));
+  }
+  MG_CUDA(cudaMalloc(&small_, sizeof(double) * (5 * kSq + 256)));
+  MG_CUDA(cudaMalloc(&partials_, sizeof(double) * 296 * 64 * 64));
+  MG_CUDA(cudaHostAlloc(&flag_host_, sizeof(int), cudaHostAllocMapped));
+}
+
+void BlockCg::release() {
+  for (void* p : {R_, P_, KP_, inner_, (void*)Xd_, (void*)Bn_, (void*)KX_, (void*)innerd_,
+                  (void*)small_, (void*)partials_})
+    if (p) cudaFree(p);
+  if (flag_host_) cudaFreeHost(flag_host_);
+  R_ = P_ = KP_ = inner_ = nullptr;
+  Xd_ = Bn_ = KX_ = innerd_ = small_ = partials_ = nullptr;
+  flag_host_ = nullptr;
+  nrow_ = nfeat_ = 0;
+  maxr_ = 0;
+}
+
+int BlockCg::core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev,
+                  const double* B, int bstride, int n, double tol, double* X, int xstride,
+                  Ctl* ctl, cudaStream_t s, bool f32) {
+  int* flag_dev = nullptr;
+  MG_CUDA(cudaHostGetDevicePointer((void**)&flag_dev, flag_host_, 0));
+  *flag_host_ = 0;
+  if (f32) {
+    if (n <= 32)
+      return cg_core<float, 32>(F, Ft, reg, reg_dev, B, bstride, n, tol, X, xstride, ctl, s,
+                                (float*)R_, (float*)P_, (float*)KP_, (float*)inner_, Xd_, Bn_,
+                                KX_, innerd_, small_, partials_, flag_dev, flag_host_);
+    return cg_core<float, 64>(F, Ft, reg, reg_dev, B, bstride, n, tol, X, xstride, ctl, s,
+                              (float*)R_, (float*)P_, (float*)KP_, (float*)inner_, Xd_, Bn_,
+                              KX_, innerd_, small_, partials_, flag_dev, flag_host_);
+  }
+  if (n <= 32)
+    return cg_core<double, 32>(F, Ft, reg, reg_dev, B, bstride, n, tol, X, xstride, ctl, s,
+                               (double*)R_, (double*)P_, (double*)KP_, (double*)inner_, Xd_,
+                               Bn_, KX_, innerd_, small_, partials_, flag_dev, flag_host_);
+  return cg_core<double, 64>(F, Ft, reg, reg_dev, B, bstride, n, tol, X, xstride, ctl, s,
+                             (double*)R_, (double*)P_, (double*)KP_, (double*)inner_, Xd_, Bn_,
+                             KX_, innerd_, small_, partials_, flag_dev, flag_host_);
+}
+
+int BlockCg::solve(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev,
+                   const double* B, int bstride, int nrhs, double tol, double* X, int xstride,
+                   Ctl* ctl, cudaStream_t s, bool f32) {
+  // solve_blockcg(X, K, reg, B, tol, 32, 8) (linop.h:207-226), including the reference's
+  // overlapping extra block when a remainder block is followed by one more start index.
+  const int blocksize = 32, excess = 8;
+  reserve(F.nrow, Ft.nrow, 64, f32);
+  if (nrhs <= excess + blocksize)
+    return core(F, Ft, reg, reg_dev, B, bstride, nrhs, tol, X, xstride, ctl, s, f32);
+  int total = 0;
+  for (int i = 0; i < nrhs; i += blocksize) {
+    int nr = blocksize;
+    if (i + blocksize + excess >= nrhs) nr = nrhs - i;
+    total += core(F, Ft, reg, reg_dev, B + i, bstride, nr, tol, X + i, xstride, ctl, s, f32);
+  }
+  return total;
+}
+
+}  // namespace mg

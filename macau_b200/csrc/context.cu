@@ -1,0 +1,1055 @@
+// Host side of the library: the C ABI of include/macau_b200.h over a C++ context that owns the
+// device data of one Gibbs sampler (the B200 counterpart of MacauX<MatrixData,
+// FixedGaussianNoise> with BPMFPrior / MacauPrior<SparseDoubleFeat>, macau.h:56-81,
+// latentprior.h:53-125).
+//
+// Device data layout
+//   * Ratings: one CSR per mode (mode 0 = rows of Y, mode 1 = columns), int64 row pointers,
+//     int32 indices sorted ascending, duplicates summed (Eigen setFromTriplets semantics).
+//     Mixed mode adds a packed (index, (y - mean) * alpha as FP32) pair per entry.
+//   * Latents: N x KP, row n = the K-vector of entity n, zero padded to KP in {8,..,128}.
+//     FP64 mode keeps FP64; mixed mode keeps an FP32 master plus a BF16 copy that the other
+//     mode's sampler gathers.
+//   * Hyperparameters (mu, Lambda, lambda_beta) and the Macau link matrix stay on the device;
+//     a sweep needs no host round trip except the block-CG convergence check.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mg {
+namespace {
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    reset();
+    if (count == 0) count = 1;
+    MG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void alloc_zero(size_t count, cudaStream_t s) {
+    alloc(count);
+    MG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) MG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+};
+
+struct HostCsr {
+  std::vector<long long> ptr;
+  std::vector<int> idx;
+  std::vector<double> val;
+};
+
+// COO -> CSR over `nrow` rows with indices sorted ascending and duplicates summed.
+HostCsr coo_to_csr(const int* r, const int* c, const double* v, long long nnz, long long nrow,
+                   long long ncol) {
+  // counting sort by column, then stable counting sort by row => (row, col) order
+  std::vector<long long> cnt(std::max(nrow, ncol) + 1, 0);
+  std::vector<long long> ord(nnz), ord2(nnz);
+  for (long long e = 0; e < nnz; e++) cnt[c[e] + 1]++;
+  for (long long i = 0; i < ncol; i++) cnt[i + 1] += cnt[i];
+  for (long long e = 0; e < nnz; e++) ord[cnt[c[e]]++] = e;
+  std::fill(cnt.begin(), cnt.end(), 0);
+  for (long long e = 0; e < nnz; e++) cnt[r[e] + 1]++;
+  for (long long i = 0; i < nrow; i++) cnt[i + 1] += cnt[i];
+  for (long long q = 0; q < nnz; q++) {
+    const long long e = ord[q];
+    ord2[cnt[r[e]]++] = e;
+  }
+  HostCsr out;
+  out.ptr.assign(nrow + 1, 0);
+  out.idx.reserve(nnz);
+  out.val.reserve(nnz);
+  long long prev_r = -1, prev_c = -1;
+  for (long long q = 0; q < nnz; q++) {
+    const long long e = ord2[q];
+    if (r[e] == prev_r && c[e] == prev_c) {
+      out.val.back() += v ? v[e] : 1.0;
+      continue;
+    }
+    out.idx.push_back(c[e]);
+    out.val.push_back(v ? v[e] : 1.0);
+    out.ptr[r[e] + 1]++;
+    prev_r = r[e];
+    prev_c = c[e];
+  }
+  for (long long i = 0; i < nrow; i++) out.ptr[i + 1] += out.ptr[i];
+  return out;
+}
+
+// Transpose of a CSR (rows sorted within each output row because input rows are scanned in
+// order).
+HostCsr transpose(const HostCsr& a, long long nrow, long long ncol) {
+  HostCsr t;
+  const long long nnz = (long long)a.idx.size();
+  t.ptr.assign(ncol + 1, 0);
+  t.idx.resize(nnz);
+  t.val.resize(nnz);
+  for (long long e = 0; e < nnz; e++) t.ptr[a.idx[e] + 1]++;
+  for (long long i = 0; i < ncol; i++) t.ptr[i + 1] += t.ptr[i];
+  std::vector<long long> pos(t.ptr.begin(), t.ptr.end() - 1);
+  for (long long r = 0; r < nrow; r++)
+    for (long long e = a.ptr[r]; e < a.ptr[r + 1]; e++) {
+      const long long q = pos[a.idx[e]]++;
+      t.idx[q] = (int)r;
+      t.val[q] = a.val[e];
+    }
+  return t;
+}
+
+struct ModeData {
+  long long N = 0, nnz = 0;
+  DBuf<long long> ptr;
+  DBuf<int> idx;
+  DBuf<double> val;
+  DBuf<uint2> packed;
+  DBuf<RowTask> tasks;
+  DBuf<unsigned> split_cnt;
+  int ntasks = 0, nsplit = 0, nslots = 0;
+  long long max_len = 0;
+};
+
+struct Prior {
+  bool macau = false;
+  DBuf<double> mu, Lambda, WI, mu0;
+  double b0 = 2.0;
+  int df = 0;
+  // side information (MacauPrior<SparseDoubleFeat>)
+  long long nfeat = 0;
+  DBuf<long long> fptr, tptr;
+  DBuf<int> fidx, tidx;
+  DBuf<double> fval, tval;
+  DBuf<float> fvalf, tvalf;
+  DevCsr F, Ft;
+  DBuf<double> beta, uhat, tmp, B, Lchol, lambda_beta, bb_partials;
+  double lambda_beta0 = 5.0, tol = 1e-6;
+  double lb_mu0 = 1.0, lb_nu0 = 1e-3;
+  BlockCg cg;
+  int cg_iters = 0;
+};
+
+}  // namespace
+
+class Context {
+ public:
+  explicit Context(const mg_config& c) : cfg_(c) {
+    if (c.num_latent < 1 || c.num_latent > 128)
+      throw MgError(MG_ERR_ARG, "num_latent must be in [1, 128]");
+    K_ = c.num_latent;
+    KP_ = kpad(K_);
+    CP_ = K_ <= 32 ? 32 : 64;
+    mixed_ = c.compute == MG_COMPUTE_MIXED;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+      throw MgError(MG_ERR_NOGPU, "no CUDA device");
+    dev_ = c.device;
+    MG_CUDA(cudaSetDevice(dev_));
+    cudaDeviceProp prop;
+    MG_CUDA(cudaGetDeviceProperties(&prop, dev_));
+    if (prop.major < 10)
+      throw MgError(MG_ERR_NOGPU, std::string("sm_100a device required, found ") + prop.name);
+    num_sms_ = prop.multiProcessorCount;
+    MG_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    ctl_.alloc_zero(1, s_);
+    for (int m = 0; m < 2; m++) prior_[m].df = K_;
+    MG_CUDA(cudaEventCreate(&ev0_));
+    MG_CUDA(cudaEventCreate(&ev1_));
+  }
+
+  ~Context() {
+    drop_graphs();
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (s_) cudaStreamDestroy(s_);
+  }
+
+  void set_train(const int32_t* idx, int nmodes, const double* vals, long long nnz,
+                 const int32_t* dims) {
+    if (nmodes != 2) throw MgError(MG_ERR_ARG, "MatrixData: tensor training input not supported.");
+    if (nnz < 1) throw MgError(MG_ERR_ARG, "training data is empty");
+    dims_[0] = dims[0];
+    dims_[1] = dims[1];
+    const int* r = idx;
+    const int* c = idx + nnz;
+    for (long long e = 0; e < nnz; e++)
+      if (r[e] < 0 || r[e] >= dims_[0] || c[e] < 0 || c[e] >= dims_[1])
+        throw MgError(MG_ERR_ARG, "training index out of range");
+    HostCsr rows = coo_to_csr(r, c, vals, nnz, dims_[0], dims_[1]);
+    HostCsr cols = transpose(rows, dims_[0], dims_[1]);
+    // mean_value = Y.sum() / Y.nonZeros() over the column-major storage (sparsetensor.cpp:82)
+    double sum = 0.0;
+    for (double v : cols.val) sum += v;
+    ntrain_ = (long long)cols.val.size();
+    mean_ = sum / (double)ntrain_;
+    upload_mode(0, rows);
+    upload_mode(1, cols);
+    drop_graphs();
+    have_data_ = true;
+    initialised_ = false;
+  }
+
+  void set_test(const int32_t* idx, int nmodes, const double* vals, long long nnz,
+                const int32_t* dims) {
+    if (nmodes != 2) throw MgError(MG_ERR_ARG, "MatrixData: tensor test input not supported.");
+    const int* r = idx;
+    const int* c = idx + nnz;
+    for (long long e = 0; e < nnz; e++)
+      if (r[e] < 0 || r[e] >= dims[0] || c[e] < 0 || c[e] >= dims[1])
+        throw MgError(MG_ERR_ARG, "test index out of range");
+    // Ytest in CSC order (sparseFromIJV -> column-major storage): CSR of the transpose.
+    HostCsr cs = coo_to_csr(c, r, vals, nnz, dims[1], dims[0]);
+    ntest_ = (long long)cs.idx.size();
+    test_row_.resize(ntest_);
+    test_col_.resize(ntest_);
+    test_val_ = cs.val;
+    for (long long col = 0; col < dims[1]; col++)
+      for (long long e = cs.ptr[col]; e < cs.ptr[col + 1]; e++) {
+        test_row_[e] = cs.idx[e];
+        test_col_[e] = (int)col;
+      }
+    trow_.upload(test_row_.data(), ntest_, s_);
+    tcol_.upload(test_col_.data(), ntest_, s_);
+    tval_.upload(test_val_.data(), ntest_, s_);
+    pred_.alloc_zero(ntest_, s_);
+    pvar_.alloc_zero(ntest_, s_);
+    eval_partials_.alloc(2 * (size_t)eval_blocks(ntest_));
+    rmse_.alloc(2);
+    const double nan2[2] = {NAN, NAN};
+    MG_CUDA(cudaMemcpyAsync(rmse_.p, nan2, sizeof(nan2), cudaMemcpyHostToDevice, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    drop_graphs();
+  }
+
+  void set_side(int mode, const int32_t* rows, const int32_t* cols, const double* vals,
+                long long nnz, int nrows, int nfeat, double lambda_beta, double tol) {
+    if (mode < 0 || mode > 1) throw MgError(MG_ERR_ARG, "mode must be 0 or 1");
+    if (!have_data_) throw MgError(MG_ERR_STATE, "set the training data before side info");
+    if (nrows != dims_[mode])
+      throw MgError(MG_ERR_ARG, "side information rows must equal the mode's dimension");
+    if (K_ > 64) throw MgError(MG_ERR_ARG, "side information supports num_latent <= 64");
+    for (long long e = 0; e < nnz; e++)
+      if (rows[e] < 0 || rows[e] >= nrows || cols[e] < 0 || cols[e] >= nfeat)
+        throw MgError(MG_ERR_ARG, "side information index out of range");
+    Prior& p = prior_[mode];
+    HostCsr f = coo_to_csr(rows, cols, vals, nnz, nrows, nfeat);
+    HostCsr t = transpose(f, nrows, nfeat);
+    bool binary = true;
+    for (double v : f.val) binary = binary && (v == 1.0);
+    p.macau = true;
+    p.nfeat = nfeat;
+    p.fptr.upload(f.ptr.data(), f.ptr.size(), s_);
+    p.fidx.upload(f.idx.data(), f.idx.size(), s_);
+    p.tptr.upload(t.ptr.data(), t.ptr.size(), s_);
+    p.tidx.upload(t.idx.data(), t.idx.size(), s_);
+    p.F = DevCsr{};
+    p.Ft = DevCsr{};
+    if (!binary) {
+      p.fval.upload(f.val.data(), f.val.size(), s_);
+      p.tval.upload(t.val.data(), t.val.size(), s_);
+      std::vector<float> ff(f.val.begin(), f.val.end()), tf(t.val.begin(), t.val.end());
+      p.fvalf.upload(ff.data(), ff.size(), s_);
+      p.tvalf.upload(tf.data(), tf.size(), s_);
+      p.F.val = p.fval.p;
+      p.F.valf = p.fvalf.p;
+      p.Ft.val = p.tval.p;
+      p.Ft.valf = p.tvalf.p;
+    }
+    p.F.ptr = p.fptr.p;
+    p.F.idx = p.fidx.p;
+    p.F.nrow = nrows;
+    p.F.ncol = nfeat;
+    p.F.nnz = (long long)f.idx.size();
+    p.Ft.ptr = p.tptr.p;
+    p.Ft.idx = p.tidx.p;
+    p.Ft.nrow = nfeat;
+    p.Ft.ncol = nrows;
+    p.Ft.nnz = p.F.nnz;
+    p.lambda_beta0 = lambda_beta;
+    p.tol = tol;
+    MG_CUDA(cudaStreamSynchronize(s_));
+    drop_graphs();
+    initialised_ = false;
+  }
+
+  void set_samples(int burnin, int nsamples) {
+    burnin_ = burnin;
+    nsamples_ = nsamples;
+  }
+
+  // MacauX::init (macau.cpp:72-86) + prior init (latentprior.cpp:84-99, 181-216)
+  void init() {
+    if (!have_data_) throw MgError(MG_ERR_STATE, "no training data");
+    for (int m = 0; m < 2; m++) {
+      const size_t n = (size_t)dims_[m] * KP_;
+      if (mixed_) {
+        lat32_[m].alloc_zero(n, s_);
+        lat16_[m].alloc_zero(n, s_);
+        lat64_[m].reset();
+      } else {
+        lat64_[m].alloc_zero(n, s_);
+        lat32_[m].reset();
+        lat16_[m].reset();
+      }
+      Prior& p = prior_[m];
+      std::vector<double> eye((size_t)K_ * K_, 0.0), lam((size_t)K_ * K_, 0.0), z(K_, 0.0);
+      for (int i = 0; i < K_; i++) {
+        eye[i + (size_t)i * K_] = 1.0;
+        lam[i + (size_t)i * K_] = 10.0;
+      }
+      p.mu.upload(z.data(), K_, s_);
+      p.mu0.upload(z.data(), K_, s_);
+      p.Lambda.upload(lam.data(), lam.size(), s_);
+      p.WI.upload(eye.data(), eye.size(), s_);
+      p.b0 = 2.0;
+      p.df = K_;
+      if (p.macau) {
+        p.beta.alloc_zero((size_t)p.nfeat * CP_, s_);
+        p.uhat.alloc_zero((size_t)dims_[m] * KP_, s_);
+        p.tmp.alloc_zero((size_t)dims_[m] * CP_, s_);
+        p.B.alloc_zero((size_t)p.nfeat * CP_, s_);
+        p.Lchol.alloc_zero((size_t)K_ * K_, s_);
+        p.lambda_beta.upload(&p.lambda_beta0, 1, s_);
+        p.bb_partials.alloc((size_t)stats_blocks(p.nfeat) * (K_ + K_ * K_));
+        p.cg.reserve(p.F.nrow, p.nfeat, 64, mixed_);
+      }
+    }
+    const long long maxN = std::max(dims_[0], dims_[1]);
+    stat_partials_.alloc((size_t)stats_blocks(maxN) * (K_ + K_ * K_));
+    nwbuf_.alloc(3 * (size_t)K_ + 4 * (size_t)K_ * K_);
+    nw_.vec = nwbuf_.p;
+    nw_.m0 = nwbuf_.p + 3 * K_;
+    nw_.m1 = nw_.m0 + K_ * K_;
+    nw_.m2 = nw_.m1 + K_ * K_;
+    nw_.m3 = nw_.m2 + K_ * K_;
+    if (ntest_ > 0) {
+      MG_CUDA(cudaMemsetAsync(pred_.p, 0, ntest_ * sizeof(double), s_));
+      MG_CUDA(cudaMemsetAsync(pvar_.p, 0, ntest_ * sizeof(double), s_));
+    }
+    Ctl zero{};
+    zero.bad_row = -1;
+    MG_CUDA(cudaMemcpyAsync(ctl_.p, &zero, sizeof(Ctl), cudaMemcpyHostToDevice, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    retries_[0] = retries_[1] = 0;
+    rows_[0] = rows_[1] = 0;
+    sweeps_done_ = 0;
+    t_sample_ = t_prior_ = t_eval_ = 0.0;
+    drop_graphs();
+    initialised_ = true;
+  }
+
+  // ---- phases ----
+  void sample(int mode, const double* znoise_dev) {
+    ModeData& md = md_[mode];
+    Prior& p = prior_[mode];
+    const int other = 1 - mode;
+    MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[mode], 0, sizeof(uint32_t), s_));
+    SampleParams sp{};
+    sp.tasks = md.tasks.p;
+    sp.ntasks = md.ntasks;
+    sp.nrows = (int)md.N;
+    sp.K = K_;
+    sp.rowptr = md.ptr.p;
+    sp.colidx = md.idx.p;
+    sp.vals = md.val.p;
+    sp.packed = md.packed.p;
+    sp.mean = mean_;
+    sp.alpha = cfg_.precision;
+    sp.other = mixed_ ? (const void*)lat16_[other].p : (const void*)lat64_[other].p;
+    sp.Lambda = p.Lambda.p;
+    sp.mu = p.mu.p;
+    sp.uhat = p.macau ? p.uhat.p : nullptr;
+    sp.out_f64 = lat64_[mode].p;
+    sp.out_f32 = lat32_[mode].p;
+    sp.out_bf16 = lat16_[mode].p;
+    sp.scratch = scratch_.p;
+    sp.split_cnt = md.split_cnt.p;
+    sp.ctl = ctl_.p;
+    sp.qslot = mode;
+    sp.mode = mode;
+    sp.seed = cfg_.seed;
+    sp.znoise = znoise_dev;
+    if (!(mixed_ && use_tc_ && launch_sample_tc(sp, KP_, s_, num_sms_)))
+      launch_sample(sp, KP_, mixed_, s_, num_sms_);
+  }
+
+  const void* latents(int mode) const {
+    return mixed_ ? (const void*)lat32_[mode].p : (const void*)lat64_[mode].p;
+  }
+
+  void update_prior(int mode) {
+    Prior& p = prior_[mode];
+    const long long N = dims_[mode];
+    const int nb = stats_blocks(N);
+    launch_stats(latents(mode), mixed_, p.macau ? p.uhat.p : nullptr, N, K_, KP_, KP_,
+                 stat_partials_.p, nb, s_);
+    if (!p.macau) {  // BPMFPrior::update_prior (latentprior.cpp:79-81)
+      launch_normal_wishart(stat_partials_.p, nb, N, K_, p.mu0.p, p.b0, p.WI.p, p.df, nullptr,
+                            0, nullptr, nw_, ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
+      return;
+    }
+    // MacauPrior::update_prior (latentprior.cpp:255-264)
+    const int nbb = stats_blocks(p.nfeat);
+    launch_stats(p.beta.p, false, nullptr, p.nfeat, K_, CP_, 0, p.bb_partials.p, nbb, s_);
+    launch_normal_wishart(stat_partials_.p, nb, N, K_, p.mu0.p, p.b0, p.WI.p,
+                          p.df + (int)p.nfeat, p.bb_partials.p, nbb, p.lambda_beta.p, nw_,
+                          ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
+    // sample_beta (latentprior.cpp:273-293)
+    launch_small_chol(p.Lambda.p, K_, p.Lchol.p, ctl_.p, s_);
+    launch_beta_rhs_tmp(latents(mode), mixed_, KP_, N, K_, p.Lchol.p, p.mu.p, ctl_.p, cfg_.seed,
+                        mode, p.tmp.p, CP_, s_);
+    launch_beta_rhs_b(p.Ft, p.tmp.p, CP_, K_, p.Lchol.p, p.lambda_beta.p, ctl_.p, cfg_.seed,
+                      mode, p.B.p, CP_, s_);
+    p.cg_iters = p.cg.solve(p.F, p.Ft, 0.0, p.lambda_beta.p, p.B.p, CP_, K_, p.tol, p.beta.p,
+                            CP_, ctl_.p, s_, mixed_);
+    // compute_uhat (linop.h:196-198): Uhat = beta F^T, one K-vector per row of F
+    launch_spmm(p.F, p.beta.p, CP_, p.uhat.p, KP_, K_, false, s_);
+    // sample_lambda_beta with the new beta and Lambda (latentprior.cpp:263)
+    launch_stats(p.beta.p, false, nullptr, p.nfeat, K_, CP_, 0, p.bb_partials.p, nbb, s_);
+    launch_lambda_beta(p.bb_partials.p, nbb, K_, p.nfeat, p.Lambda.p, p.lb_nu0, p.lb_mu0,
+                       ctl_.p, cfg_.seed, mode, p.lambda_beta.p, s_);
+  }
+
+  void eval(int n_fixed) {
+    if (ntest_ == 0) return;
+    launch_eval(trow_.p, tcol_.p, tval_.p, ntest_, latents(0), latents(1), mixed_, K_, KP_,
+                mean_, n_fixed, ctl_.p, pred_.p, pvar_.p, eval_partials_.p,
+                eval_blocks(ntest_), rmse_.p, s_);
+  }
+
+  bool graphable() const { return !prior_[0].macau && !prior_[1].macau; }
+
+  void sweep_body(bool do_eval) {
+    sample(0, nullptr);
+    sample(1, nullptr);
+    update_prior(0);
+    update_prior(1);
+    if (do_eval) eval(-1);
+    launch_advance(ctl_.p, s_);
+  }
+
+  void check_status() {
+    Ctl h;
+    MG_CUDA(cudaMemcpyAsync(&h, ctl_.p, sizeof(Ctl), cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    retries_[0] = h.retries[0];
+    retries_[1] = h.retries[1];
+    if (h.status & kStatCholFail)
+      throw MgError(MG_ERR_CHOL, "Cholesky Decomposition failed!");
+    if (h.status & kStatHyperFail)
+      throw MgError(MG_ERR_CHOL, "Cholesky Decomposition failed! (hyperprior)");
+    if (h.status & kStatCgFail) throw MgError(MG_ERR_CG, "block-CG breakdown");
+    if (h.status & kStatTimeout) throw MgError(MG_ERR_TIMEOUT, "device wait timed out");
+  }
+
+  void sweeps(int first_iter, int count, bool do_eval, bool sync = true) {
+    if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_init first");
+    launch_set_sweep(ctl_.p, (uint32_t)first_iter, burnin_, s_);
+    rows_[0] += md_[0].N * count;
+    rows_[1] += md_[1].N * count;
+    sweeps_done_ += count;
+    if (graphable() && use_graph_) {
+      cudaGraphExec_t& ge = graph_[do_eval ? 1 : 0];
+      if (!ge && count > 0) {
+        // first sweep runs eagerly (one-time kernel attribute set-up happens outside capture)
+        sweep_body(do_eval);
+        count--;
+        cudaGraph_t g = nullptr;
+        MG_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        try {
+          sweep_body(do_eval);
+        } catch (...) {
+          cudaStreamEndCapture(s_, &g);
+          if (g) cudaGraphDestroy(g);
+          throw;
+        }
+        MG_CUDA(cudaStreamEndCapture(s_, &g));
+        MG_CUDA(cudaGraphInstantiate(&ge, g, 0));
+        cudaGraphDestroy(g);
+      }
+      for (int i = 0; i < count; i++) MG_CUDA(cudaGraphLaunch(ge, s_));
+    } else {
+      for (int i = 0; i < count; i++) sweep_body(do_eval);
+    }
+    if (sync) check_status();
+  }
+
+  void run() {
+    init();
+    if (cfg_.verbose) {
+      printf("Noise precision: %f (fixed)\nSampling\n", cfg_.precision);
+      fflush(stdout);
+    }
+    const int total = burnin_ + nsamples_;
+    for (int i = 0; i < total; i++) {
+      const auto t0 = std::chrono::steady_clock::now();
+      if (cfg_.verbose && i == burnin_)
+        printf(" ====== Burn-in complete, averaging samples ====== \n");
+      sweeps(i, 1, true, true);
+      if (cfg_.verbose) {
+        double r[2];
+        get_rmse(r);
+        const double took =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        printf("Iter %3d: RMSE: %.5f (1samp: %.5f)  U:[%1.2e, %1.2e]\tSide:[%s, %s] [took %0.1fs]\n",
+               i, r[0], r[1], latent_norm(0), latent_norm(1), link_norm_str(0).c_str(),
+               link_norm_str(1).c_str(), took);
+        fflush(stdout);
+      }
+    }
+  }
+
+  double latent_norm(int mode) {
+    std::vector<double> u((size_t)dims_[mode] * K_);
+    get_latents(mode, u.data());
+    double s = 0.0;
+    for (double x : u) s += x * x;
+    return std::sqrt(s);
+  }
+  std::string link_norm_str(int mode) {
+    if (!prior_[mode].macau) return "nan";
+    std::vector<double> b((size_t)prior_[mode].nfeat * K_);
+    get_beta(mode, b.data());
+    double s = 0.0;
+    for (double x : b) s += x * x;
+    char buf[32];
+    snprintf(buf, sizeof buf, "%1.2e", std::sqrt(s));
+    return buf;
+  }
+
+  // ---- state access ----
+  void get_latents(int mode, double* out) {
+    const long long N = dims_[mode];
+    if (mixed_) {
+      std::vector<float> h((size_t)N * KP_);
+      MG_CUDA(cudaMemcpyAsync(h.data(), lat32_[mode].p, h.size() * 4, cudaMemcpyDeviceToHost, s_));
+      MG_CUDA(cudaStreamSynchronize(s_));
+      for (long long n = 0; n < N; n++)
+        for (int k = 0; k < K_; k++) out[n * K_ + k] = h[n * KP_ + k];
+    } else {
+      MG_CUDA(cudaMemcpy2DAsync(out, K_ * 8, lat64_[mode].p, KP_ * 8, K_ * 8, N,
+                                cudaMemcpyDeviceToHost, s_));
+      MG_CUDA(cudaStreamSynchronize(s_));
+    }
+  }
+  void set_latents(int mode, const double* in) {
+    const long long N = dims_[mode];
+    if (mixed_) {
+      std::vector<float> h((size_t)N * KP_, 0.f);
+      std::vector<uint16_t> hb((size_t)N * KP_, 0);
+      for (long long n = 0; n < N; n++)
+        for (int k = 0; k < K_; k++) {
+          const float f = (float)in[n * K_ + k];
+          h[n * KP_ + k] = f;
+          uint32_t bits;
+          std::memcpy(&bits, &f, 4);
+          const uint32_t lsb = (bits >> 16) & 1u;  // round to nearest even
+          hb[n * KP_ + k] = (uint16_t)((bits + 0x7FFFu + lsb) >> 16);
+        }
+      MG_CUDA(cudaMemcpyAsync(lat32_[mode].p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, s_));
+      MG_CUDA(cudaMemcpyAsync(lat16_[mode].p, hb.data(), hb.size() * 2, cudaMemcpyHostToDevice, s_));
+    } else {
+      MG_CUDA(cudaMemcpy2DAsync(lat64_[mode].p, KP_ * 8, in, K_ * 8, K_ * 8, N,
+                                cudaMemcpyHostToDevice, s_));
+    }
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+  void get_hyper(int mode, double* mu, double* Lambda, double* lb) {
+    Prior& p = prior_[mode];
+    if (mu) MG_CUDA(cudaMemcpyAsync(mu, p.mu.p, K_ * 8, cudaMemcpyDeviceToHost, s_));
+    if (Lambda)
+      MG_CUDA(cudaMemcpyAsync(Lambda, p.Lambda.p, (size_t)K_ * K_ * 8, cudaMemcpyDeviceToHost, s_));
+    if (lb) {
+      if (p.macau) MG_CUDA(cudaMemcpyAsync(lb, p.lambda_beta.p, 8, cudaMemcpyDeviceToHost, s_));
+      else *lb = NAN;
+    }
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+  void set_hyper(int mode, const double* mu, const double* Lambda, const double* lb) {
+    Prior& p = prior_[mode];
+    if (mu) MG_CUDA(cudaMemcpyAsync(p.mu.p, mu, K_ * 8, cudaMemcpyHostToDevice, s_));
+    if (Lambda)
+      MG_CUDA(cudaMemcpyAsync(p.Lambda.p, Lambda, (size_t)K_ * K_ * 8, cudaMemcpyHostToDevice, s_));
+    if (lb && p.macau) MG_CUDA(cudaMemcpyAsync(p.lambda_beta.p, lb, 8, cudaMemcpyHostToDevice, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+  void get_beta(int mode, double* out) {
+    Prior& p = prior_[mode];
+    if (!p.macau) throw MgError(MG_ERR_STATE, "mode has no side information");
+    MG_CUDA(cudaMemcpy2DAsync(out, K_ * 8, p.beta.p, CP_ * 8, K_ * 8, p.nfeat,
+                              cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+  void get_uhat(int mode, double* out) {
+    Prior& p = prior_[mode];
+    if (!p.macau) throw MgError(MG_ERR_STATE, "mode has no side information");
+    MG_CUDA(cudaMemcpy2DAsync(out, K_ * 8, p.uhat.p, KP_ * 8, K_ * 8, dims_[mode],
+                              cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+  void get_rmse(double* r) {
+    if (ntest_ == 0) {
+      r[0] = r[1] = NAN;
+      return;
+    }
+    MG_CUDA(cudaMemcpyAsync(r, rmse_.p, 16, cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+  void get_predictions(double* out) {
+    if (ntest_ == 0) return;
+    MG_CUDA(cudaMemcpyAsync(out, pred_.p, ntest_ * 8, cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+  // MacauX::getStds (macau.cpp:175-188)
+  void get_stds(double* out) {
+    if (ntest_ == 0) return;
+    if (nsamples_ <= 1) {
+      for (long long i = 0; i < ntest_; i++) out[i] = NAN;
+      return;
+    }
+    MG_CUDA(cudaMemcpyAsync(out, pvar_.p, ntest_ * 8, cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    const double inorm = 1.0 / (nsamples_ - 1);
+    for (long long i = 0; i < ntest_; i++) out[i] = std::sqrt(out[i] * inorm);
+  }
+  void get_test_data(double* out) {
+    for (long long i = 0; i < ntest_; i++) {
+      out[i] = test_row_[i];
+      out[i + ntest_] = test_col_[i];
+      out[i + 2 * ntest_] = test_val_[i];
+    }
+  }
+  void get_stats(mg_stats* st) {
+    Ctl h;
+    MG_CUDA(cudaMemcpyAsync(&h, ctl_.p, sizeof(Ctl), cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    std::memset(st, 0, sizeof(*st));
+    st->sweeps = (double)sweeps_done_;
+    st->seconds_sample = t_sample_;
+    st->seconds_prior = t_prior_;
+    st->seconds_eval = t_eval_;
+    st->retries[0] = h.retries[0];
+    st->retries[1] = h.retries[1];
+    st->rows_sampled[0] = rows_[0];
+    st->rows_sampled[1] = rows_[1];
+    st->cg_iters[0] = prior_[0].cg_iters;
+    st->cg_iters[1] = prior_[1].cg_iters;
+    st->graph_captured = (graph_[0] || graph_[1]) ? 1 : 0;
+  }
+  void dims(int64_t* nrow, int64_t* ncol, int64_t* ntrain, int64_t* ntest, double* mean) {
+    if (nrow) *nrow = dims_[0];
+    if (ncol) *ncol = dims_[1];
+    if (ntrain) *ntrain = ntrain_;
+    if (ntest) *ntest = ntest_;
+    if (mean) *mean = mean_;
+  }
+
+  void count_rows(int mode) { rows_[mode] += md_[mode].N; }
+  cudaStream_t stream() const { return s_; }
+  Ctl* ctl() const { return ctl_.p; }
+  int K() const { return K_; }
+  int KP() const { return KP_; }
+  long long dim(int m) const { return dims_[m]; }
+  bool initialised() const { return initialised_; }
+  void set_use_graph(bool b) { use_graph_ = b; drop_graphs(); }
+  void set_use_tc(bool b) { use_tc_ = b; drop_graphs(); }
+
+  std::string err;
+
+ private:
+  void drop_graphs() {
+    for (auto& g : graph_)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
+
+  void upload_mode(int m, const HostCsr& h) {
+    ModeData& md = md_[m];
+    md.N = dims_[m];
+    md.nnz = (long long)h.idx.size();
+    md.ptr.upload(h.ptr.data(), h.ptr.size(), s_);
+    md.idx.upload(h.idx.data(), h.idx.size(), s_);
+    md.val.upload(h.val.data(), h.val.size(), s_);
+    if (mixed_) {
+      std::vector<uint2> pk(md.nnz);
+      for (long long e = 0; e < md.nnz; e++) {
+        const float w = (float)((h.val[e] - mean_) * cfg_.precision);
+        uint32_t bits;
+        std::memcpy(&bits, &w, 4);
+        pk[e] = make_uint2((unsigned)h.idx[e], bits);
+      }
+      md.packed.upload(pk.data(), pk.size(), s_);
+    }
+    // Task list: rows sorted by descending length; rows above the split threshold are cut into
+    // near-equal parts so that no task is much longer than the average work per row group.
+    const long long groups = (long long)num_sms_ * 16;
+    long long thr = md.nnz / (2 * groups);
+    thr = std::max(256LL, std::min(16384LL, thr));
+    std::vector<long long> order(md.N);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](long long a, long long b) {
+      return (h.ptr[a + 1] - h.ptr[a]) > (h.ptr[b + 1] - h.ptr[b]);
+    });
+    std::vector<RowTask> tasks;
+    tasks.reserve(md.N + 16);
+    int nsplit = 0, nslots = 0;
+    md.max_len = 0;
+    for (long long r : order) {
+      const long long len = h.ptr[r + 1] - h.ptr[r];
+      md.max_len = std::max(md.max_len, len);
+      if (len <= thr) {
+        tasks.push_back(RowTask{h.ptr[r], (int)r, (int)len, 0, 1, 0, 0});
+        continue;
+      }
+      const int parts = (int)((len + thr - 1) / thr);
+      for (int q = 0; q < parts; q++) {
+        const long long b = h.ptr[r] + len * q / parts;
+        const long long e = h.ptr[r] + len * (q + 1) / parts;
+        tasks.push_back(RowTask{b, (int)r, (int)(e - b), q, parts, nslots, nsplit});
+      }
+      nslots += parts;
+      nsplit++;
+    }
+    // longest tasks first
+    std::stable_sort(tasks.begin(), tasks.end(),
+                     [](const RowTask& a, const RowTask& b) { return a.len > b.len; });
+    md.ntasks = (int)tasks.size();
+    md.nsplit = nsplit;
+    md.nslots = nslots;
+    md.tasks.upload(tasks.data(), tasks.size(), s_);
+    md.split_cnt.alloc_zero(std::max(1, nsplit), s_);
+    const size_t need = (size_t)std::max(md_[0].nslots, md_[1].nslots) * (KP_ * KP_ + KP_);
+    if (need > scratch_.n) scratch_.alloc(need);
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+
+  mg_config cfg_;
+  int K_ = 0, KP_ = 0, CP_ = 32;
+  bool mixed_ = false;
+  int dev_ = 0, num_sms_ = 148;
+  cudaStream_t s_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  long long dims_[2] = {0, 0};
+  long long ntrain_ = 0, ntest_ = 0;
+  double mean_ = 0.0;
+  bool have_data_ = false, initialised_ = false;
+  bool use_graph_ = true, use_tc_ = true;
+  int burnin_ = 50, nsamples_ = 400;
+  ModeData md_[2];
+  Prior prior_[2];
+  DBuf<double> lat64_[2];
+  DBuf<float> lat32_[2];
+  DBuf<__nv_bfloat16> lat16_[2];
+  DBuf<double> scratch_, stat_partials_, nwbuf_;
+  NwWork nw_{};
+  DBuf<Ctl> ctl_;
+  DBuf<int> trow_, tcol_;
+  DBuf<double> tval_, pred_, pvar_, eval_partials_, rmse_;
+  std::vector<int> test_row_, test_col_;
+  std::vector<double> test_val_;
+  cudaGraphExec_t graph_[2] = {nullptr, nullptr};
+  long long retries_[2] = {0, 0}, rows_[2] = {0, 0};
+  long long sweeps_done_ = 0;
+  double t_sample_ = 0, t_prior_ = 0, t_eval_ = 0;
+};
+
+}  // namespace mg
+
+// ============================== C ABI ==============================
+struct mg_ctx {
+  std::unique_ptr<mg::Context> c;
+  std::string err;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <typename F>
+int guarded(mg_ctx* ctx, F&& f) {
+  if (!ctx || !ctx->c) return MG_ERR_ARG;
+  try {
+    f(*ctx->c);
+    ctx->err.clear();
+    return MG_OK;
+  } catch (const mg::MgError& e) {
+    ctx->err = e.what();
+    return e.code;
+  } catch (const mg::CudaError& e) {
+    ctx->err = e.what();
+    return MG_ERR_CUDA;
+  } catch (const std::exception& e) {
+    ctx->err = e.what();
+    return MG_ERR_ARG;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int mg_create(mg_ctx** out, const mg_config* cfg) {
+  if (!out || !cfg) return MG_ERR_ARG;
+  *out = nullptr;
+  try {
+    auto* h = new mg_ctx();
+    h->c.reset(new mg::Context(*cfg));
+    *out = h;
+    return MG_OK;
+  } catch (const mg::MgError& e) {
+    g_create_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    return MG_ERR_CUDA;
+  }
+}
+
+void mg_destroy(mg_ctx* ctx) { delete ctx; }
+
+const char* mg_last_error(const mg_ctx* ctx) {
+  if (!ctx) return g_create_error.c_str();
+  return ctx->err.c_str();
+}
+
+int mg_set_relation_data(mg_ctx* ctx, const int32_t* idx, int nmodes, const double* values,
+                         int64_t nnz, const int32_t* dims) {
+  if (!idx || !values || !dims) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.set_train(idx, nmodes, values, nnz, dims); });
+}
+
+int mg_set_relation_data_test(mg_ctx* ctx, const int32_t* idx, int nmodes,
+                              const double* values, int64_t nnz, const int32_t* dims) {
+  if ((nnz > 0 && (!idx || !values)) || !dims) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.set_test(idx, nmodes, values, nnz, dims); });
+}
+
+int mg_set_side(mg_ctx* ctx, int mode, const int32_t* rows, const int32_t* cols,
+                const double* vals, int64_t nnz, int nrows, int nfeat, double lambda_beta,
+                double tol) {
+  if ((nnz > 0 && (!rows || !cols)) || nfeat < 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) {
+    c.set_side(mode, rows, cols, vals, nnz, nrows, nfeat, lambda_beta, tol);
+  });
+}
+
+int mg_set_samples(mg_ctx* ctx, int burnin, int nsamples) {
+  if (burnin < 0 || nsamples < 0) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.set_samples(burnin, nsamples); });
+}
+
+int mg_init(mg_ctx* ctx) {
+  return guarded(ctx, [&](mg::Context& c) { c.init(); });
+}
+
+int mg_sweep(mg_ctx* ctx, int iter, int eval) {
+  return guarded(ctx, [&](mg::Context& c) { c.sweeps(iter, 1, eval != 0, true); });
+}
+
+int mg_sweeps(mg_ctx* ctx, int first_iter, int count, int eval) {
+  if (count < 0) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.sweeps(first_iter, count, eval != 0, true); });
+}
+
+int mg_run(mg_ctx* ctx) {
+  return guarded(ctx, [&](mg::Context& c) { c.run(); });
+}
+
+int mg_sample_latents(mg_ctx* ctx, int mode, int iter, const double* z) {
+  if (mode < 0 || mode > 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) {
+    if (!c.initialised()) throw mg::MgError(MG_ERR_STATE, "call mg_init first");
+    mg::launch_set_sweep(c.ctl(), (uint32_t)iter, 0, c.stream());
+    double* zd = nullptr;
+    const size_t bytes = (size_t)c.dim(mode) * c.K() * sizeof(double);
+    if (z) {
+      MG_CUDA(cudaMalloc(&zd, bytes));
+      MG_CUDA(cudaMemcpyAsync(zd, z, bytes, cudaMemcpyHostToDevice, c.stream()));
+    }
+    try {
+      c.sample(mode, zd);
+      c.count_rows(mode);
+      c.check_status();
+    } catch (...) {
+      if (zd) cudaFree(zd);
+      throw;
+    }
+    if (zd) {
+      MG_CUDA(cudaStreamSynchronize(c.stream()));
+      cudaFree(zd);
+    }
+  });
+}
+
+int mg_update_prior(mg_ctx* ctx, int mode, int iter) {
+  if (mode < 0 || mode > 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) {
+    if (!c.initialised()) throw mg::MgError(MG_ERR_STATE, "call mg_init first");
+    mg::launch_set_sweep(c.ctl(), (uint32_t)iter, 0, c.stream());
+    c.update_prior(mode);
+    c.check_status();
+  });
+}
+
+int mg_eval(mg_ctx* ctx, int n) {
+  if (n < 0) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) {
+    c.eval(n);
+    c.check_status();
+  });
+}
+
+int mg_get_latents(mg_ctx* ctx, int mode, double* out) {
+  if (mode < 0 || mode > 1 || !out) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.get_latents(mode, out); });
+}
+int mg_set_latents(mg_ctx* ctx, int mode, const double* in) {
+  if (mode < 0 || mode > 1 || !in) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) {
+    if (!c.initialised()) throw mg::MgError(MG_ERR_STATE, "call mg_init first");
+    c.set_latents(mode, in);
+  });
+}
+int mg_get_hyper(mg_ctx* ctx, int mode, double* mu, double* Lambda, double* lambda_beta) {
+  if (mode < 0 || mode > 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.get_hyper(mode, mu, Lambda, lambda_beta); });
+}
+int mg_set_hyper(mg_ctx* ctx, int mode, const double* mu, const double* Lambda,
+                 const double* lambda_beta) {
+  if (mode < 0 || mode > 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.set_hyper(mode, mu, Lambda, lambda_beta); });
+}
+int mg_get_beta(mg_ctx* ctx, int mode, double* beta) {
+  if (mode < 0 || mode > 1 || !beta) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.get_beta(mode, beta); });
+}
+int mg_get_uhat(mg_ctx* ctx, int mode, double* uhat) {
+  if (mode < 0 || mode > 1 || !uhat) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.get_uhat(mode, uhat); });
+}
+int mg_get_dims(mg_ctx* ctx, int64_t* nrow, int64_t* ncol, int64_t* ntrain, int64_t* ntest,
+                double* mean_value) {
+  return guarded(ctx, [&](mg::Context& c) { c.dims(nrow, ncol, ntrain, ntest, mean_value); });
+}
+int mg_get_rmse(mg_ctx* ctx, double* rmse) {
+  if (!rmse) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.get_rmse(rmse); });
+}
+int mg_get_predictions(mg_ctx* ctx, double* out) {
+  return guarded(ctx, [&](mg::Context& c) { c.get_predictions(out); });
+}
+int mg_get_stds(mg_ctx* ctx, double* out) {
+  return guarded(ctx, [&](mg::Context& c) { c.get_stds(out); });
+}
+int mg_get_test_data(mg_ctx* ctx, double* out) {
+  return guarded(ctx, [&](mg::Context& c) { c.get_test_data(out); });
+}
+int mg_get_stats(mg_ctx* ctx, mg_stats* out) {
+  if (!out) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.get_stats(out); });
+}
+
+int mg_set_option(mg_ctx* ctx, const char* name, int value) {
+  if (!name) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) {
+    const std::string n(name);
+    if (n == "graph") c.set_use_graph(value != 0);
+    else if (n == "tensor_core_gram") c.set_use_tc(value != 0);
+    else throw mg::MgError(MG_ERR_ARG, "unknown option " + n);
+  });
+}
+
+int mg_blockcg(const int32_t* rows, const int32_t* cols, const double* vals, int64_t nnz,
+               int nrows, int nfeat, const double* B, int nrhs, double reg, double tol,
+               int compute, double* X, int* niter, double* seconds) {
+  if (!rows || !cols || !B || !X || nrhs < 1 || nfeat < 1 || nrows < 1) return MG_ERR_ARG;
+  try {
+    for (int64_t e = 0; e < nnz; e++)
+      if (rows[e] < 0 || rows[e] >= nrows || cols[e] < 0 || cols[e] >= nfeat) return MG_ERR_ARG;
+    int dev = 0;
+    MG_CUDA(cudaGetDevice(&dev));
+    cudaStream_t s;
+    MG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    mg::HostCsr f = mg::coo_to_csr(rows, cols, vals, nnz, nrows, nfeat);
+    mg::HostCsr t = mg::transpose(f, nrows, nfeat);
+    mg::DBuf<long long> fp, tp;
+    mg::DBuf<int> fi, ti;
+    mg::DBuf<double> fv, tv, Bd, Xd;
+    mg::DBuf<float> fvf, tvf;
+    mg::DBuf<mg::Ctl> ctl;
+    fp.upload(f.ptr.data(), f.ptr.size(), s);
+    fi.upload(f.idx.data(), f.idx.size(), s);
+    tp.upload(t.ptr.data(), t.ptr.size(), s);
+    ti.upload(t.idx.data(), t.idx.size(), s);
+    mg::DevCsr F, Ft;
+    F.ptr = fp.p; F.idx = fi.p; F.nrow = nrows; F.ncol = nfeat; F.nnz = (long long)f.idx.size();
+    Ft.ptr = tp.p; Ft.idx = ti.p; Ft.nrow = nfeat; Ft.ncol = nrows; Ft.nnz = F.nnz;
+    if (vals) {
+      fv.upload(f.val.data(), f.val.size(), s);
+      tv.upload(t.val.data(), t.val.size(), s);
+      std::vector<float> a(f.val.begin(), f.val.end()), b(t.val.begin(), t.val.end());
+      fvf.upload(a.data(), a.size(), s);
+      tvf.upload(b.data(), b.size(), s);
+      F.val = fv.p; F.valf = fvf.p; Ft.val = tv.p; Ft.valf = tvf.p;
+    }
+    // B is nrhs x nfeat column-major == nfeat rows of nrhs values
+    Bd.upload(B, (size_t)nrhs * nfeat, s);
+    Xd.alloc_zero((size_t)nrhs * nfeat, s);
+    ctl.alloc_zero(1, s);
+    mg::BlockCg cg;
+    cudaEvent_t e0, e1;
+    MG_CUDA(cudaEventCreate(&e0));
+    MG_CUDA(cudaEventCreate(&e1));
+    MG_CUDA(cudaEventRecord(e0, s));
+    const int it = cg.solve(F, Ft, reg, nullptr, Bd.p, nrhs, nrhs, tol, Xd.p, nrhs, ctl.p, s,
+                            compute == MG_COMPUTE_MIXED);
+    MG_CUDA(cudaEventRecord(e1, s));
+    MG_CUDA(cudaMemcpyAsync(X, Xd.p, sizeof(double) * nrhs * nfeat, cudaMemcpyDeviceToHost, s));
+    mg::Ctl h;
+    MG_CUDA(cudaMemcpyAsync(&h, ctl.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    if (niter) *niter = it;
+    if (seconds) *seconds = ms * 1e-3;
+    if (h.status & mg::kStatCgFail) {
+      g_create_error = "block-CG breakdown";
+      return MG_ERR_CG;
+    }
+    return MG_OK;
+  } catch (const mg::MgError& e) {
+    g_create_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    return MG_ERR_CUDA;
+  }
+}
+
+}  // extern "C"

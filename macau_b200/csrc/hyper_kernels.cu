@@ -1,0 +1,412 @@
+// Normal-Wishart hyperprior update and test-set evaluation.
+//
+//   k_stats           per-block partial sums of x and x x^T over the rows of a latent matrix
+//                     (optionally x = U - Uhat, the Macau residual of latentprior.cpp:257);
+//                     FP64 accumulation from FP64 or FP32 latents.
+//   k_normal_wishart  one CTA: reduces the partials in block order (deterministic), then
+//                     CondNormalWishart -> NormalWishart -> Wishart/WishartUnit -> MvNormal_prec
+//                     (mvnormal.cpp:169-184, 217-287, 314-336) in FP64 with keyed draws.
+//   k_lambda_beta     one CTA: posterior_lambda_beta + rgamma (latentprior.cpp:317-331).
+//   k_eval / k_eval_finish  eval_rmse (bpmfutils.h:86-114): online posterior mean / variance of
+//                     the test predictions and the two RMSEs.
+#include "common.cuh"
+#include "kernels.h"
+#include "rng.cuh"
+
+namespace mg {
+namespace {
+
+constexpr int kStatThreads = 256;
+constexpr int kStatRows = 32;  // rows staged per step
+
+template <typename T, int PER>
+__global__ void __launch_bounds__(kStatThreads)
+    k_stats(const T* __restrict__ U, const double* __restrict__ Uhat, long long N, int K,
+            int stride, int uhat_stride, long long rows_per_block, double* __restrict__ partials) {
+  __shared__ double xs[kStatRows * 128];
+  const int KK = K * K;
+  const long long r0 = (long long)blockIdx.x * rows_per_block;
+  const long long r1 = min(N, r0 + rows_per_block);
+  double acc[PER];
+  int ii[PER], jj[PER];
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    acc[q] = 0.0;
+    const int e = threadIdx.x + q * kStatThreads;
+    ii[q] = e < KK ? e % K : 0;
+    jj[q] = e < KK ? e / K : 0;
+  }
+  double su = 0.0;
+  for (long long b = r0; b < r1; b += kStatRows) {
+    const int cnt = (int)min((long long)kStatRows, r1 - b);
+    __syncthreads();
+    for (int e = threadIdx.x; e < cnt * K; e += kStatThreads) {
+      const int r = e / K, k = e % K;
+      double x = (double)U[(b + r) * stride + k];
+      if (Uhat) x -= Uhat[(b + r) * uhat_stride + k];
+      xs[r * K + k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < K)
+      for (int r = 0; r < cnt; r++) su += xs[r * K + threadIdx.x];
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      double s = acc[q];
+      for (int r = 0; r < cnt; r++) s += xs[r * K + ii[q]] * xs[r * K + jj[q]];
+      acc[q] = s;
+    }
+  }
+  double* out = partials + (size_t)blockIdx.x * (K + KK);
+  if (threadIdx.x < K) out[threadIdx.x] = su;
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int e = threadIdx.x + q * kStatThreads;
+    if (e < KK) out[K + e] = acc[q];
+  }
+}
+
+// In-place left-looking lower Cholesky of the K x K column-major matrix A by one CTA (thread i
+// computes L(i, j)); the strict upper triangle is zeroed.  Returns false on a non-positive pivot
+// (same value in every thread).
+__device__ bool cta_chol(double* A, int K, bool* flag) {
+  (void)flag;
+  __syncthreads();
+  for (int j = 0; j < K; j++) {
+    double d = A[j + j * K];
+    for (int p = 0; p < j; p++) d -= A[j + p * K] * A[j + p * K];
+    if (!(d > 0.0)) {
+      __syncthreads();
+      return false;
+    }
+    const double ljj = sqrt(d);
+    for (int i = j + 1 + threadIdx.x; i < K; i += blockDim.x) {
+      double s = A[i + j * K];
+      for (int p = 0; p < j; p++) s -= A[i + p * K] * A[j + p * K];
+      A[i + j * K] = s / ljj;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) A[j + j * K] = ljj;
+    __syncthreads();
+  }
+  for (int q = threadIdx.x; q < K * K; q += blockDim.x) {
+    const int i = q % K, k = q / K;
+    if (i < k) A[i + k * K] = 0.0;
+  }
+  __syncthreads();
+  return true;
+}
+
+// x <- L^{-1} x then L^{-T} x for one column, sequential in the calling thread.
+__device__ void col_solve_llt(const double* L, double* x, int K, int xs) {
+  for (int i = 0; i < K; i++) {
+    double s = x[i * xs];
+    for (int p = 0; p < i; p++) s -= L[i + p * K] * x[p * xs];
+    x[i * xs] = s / L[i + i * K];
+  }
+  for (int i = K - 1; i >= 0; i--) {
+    double s = x[i * xs];
+    for (int p = i + 1; p < K; p++) s -= L[p + i * K] * x[p * xs];
+    x[i * xs] = s / L[i + i * K];
+  }
+}
+
+__global__ void __launch_bounds__(256)
+    k_normal_wishart(const double* __restrict__ partials, int nparts, long long N, int K,
+                     const double* __restrict__ mu0, double kappa, const double* __restrict__ T0,
+                     int nu, const double* __restrict__ bb_partials, int bb_nparts,
+                     const double* __restrict__ lambda_beta, NwWork w, Ctl* ctl,
+                     unsigned long long seed, int mode, double* __restrict__ mu_out,
+                     double* __restrict__ Lambda_out) {
+  const int KK = K * K;
+  const uint32_t sweep = ctl->sweep;
+  double* NU = w.vec;          // K
+  double* muc = w.vec + K;     // K
+  double* z = w.vec + 2 * K;   // K
+  double* X = w.m0;            // K x K
+  double* Tc = w.m1;
+  double* cB = w.m2;           // Bartlett factor (upper)
+  double* W = w.m3;
+  // 1. reduce partials in block order
+  for (int e = threadIdx.x; e < K + KK; e += blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < nparts; b++) s += partials[(size_t)b * (K + KK) + e];
+    if (e < K) NU[e] = s;
+    else X[e - K] = s;
+  }
+  if (bb_partials) {  // T = WI + lambda_beta * beta beta^T  (latentprior.cpp:258-260)
+    const double lb = *lambda_beta;
+    for (int e = threadIdx.x; e < KK; e += blockDim.x) {
+      double s = 0.0;
+      for (int b = 0; b < bb_nparts; b++) s += bb_partials[(size_t)b * (K + KK) + K + e];
+      W[e] = T0[e] + lb * s;
+    }
+  } else {
+    for (int e = threadIdx.x; e < KK; e += blockDim.x) W[e] = T0[e];
+  }
+  __syncthreads();
+  const double kappa_c = kappa + (double)N;
+  const int nu_c = nu + (int)N;
+  for (int i = threadIdx.x; i < K; i += blockDim.x) muc[i] = (kappa * mu0[i] + NU[i]) / kappa_c;
+  __syncthreads();
+  // 2. X = T + NS + kappa mu0 mu0^T - kappa_c mu_c mu_c^T
+  for (int e = threadIdx.x; e < KK; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    X[e] = W[e] + X[e] + kappa * mu0[i] * mu0[j] - kappa_c * muc[i] * muc[j];
+  }
+  // 3. T_c = X^{-1} through the Cholesky factor of X
+  bool ok = cta_chol(X, K, nullptr);
+  if (!ok) {
+    if (threadIdx.x == 0) atomicOr(&ctl->status, kStatHyperFail);
+    return;
+  }
+  for (int c = threadIdx.x; c < K; c += blockDim.x) {
+    for (int i = 0; i < K; i++) Tc[i + c * K] = (i == c) ? 1.0 : 0.0;
+    col_solve_llt(X, Tc + c * K, K, 1);
+  }
+  // 4. L = chol(T_c)
+  ok = cta_chol(Tc, K, nullptr);
+  if (!ok) {
+    if (threadIdx.x == 0) atomicOr(&ctl->status, kStatHyperFail);
+    return;
+  }
+  // 5. Bartlett factor c: c_ii = sqrt(2 Gamma((nu_c - i)/2)), c_ij ~ N(0,1) for j > i
+  for (int e = threadIdx.x; e < KK; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    double v = 0.0;
+    if (i == j)
+      v = sqrt(2.0 * gamma_draw(seed, sweep, stream_id(kWishartDiag, mode), (uint32_t)i,
+                                0.5 * (double)(nu_c - i)));
+    else if (j > i)
+      v = normal_draw(seed, sweep, stream_id(kWishartOff, mode), (uint32_t)i,
+                      (uint32_t)(j - i - 1));
+    cB[e] = v;
+  }
+  __syncthreads();
+  // 6. W = c^T c ; M = L W (into X) ; Lambda = M L^T
+  for (int e = threadIdx.x; e < KK; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    double s = 0.0;
+    for (int p = 0; p < K; p++) s += cB[p + i * K] * cB[p + j * K];
+    W[e] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < KK; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    double s = 0.0;
+    for (int p = 0; p < K; p++) s += Tc[i + p * K] * W[p + j * K];
+    X[e] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < KK; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    double s = 0.0;
+    for (int p = 0; p < K; p++) s += X[i + p * K] * Tc[j + p * K];
+    Lambda_out[e] = s;
+    cB[e] = s * kappa_c;
+  }
+  // 7. mu = mu_c + chol(kappa_c Lambda)^{-T} z
+  ok = cta_chol(cB, K, nullptr);
+  if (!ok) {
+    if (threadIdx.x == 0) atomicOr(&ctl->status, kStatHyperFail);
+    return;
+  }
+  for (int i = threadIdx.x; i < K; i += blockDim.x)
+    z[i] = normal_draw(seed, sweep, stream_id(kMuDraw, mode), 0u, (uint32_t)i);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = K - 1; i >= 0; i--) {
+      double s = z[i];
+      for (int p = i + 1; p < K; p++) s -= cB[p + i * K] * z[p];
+      z[i] = s / cB[i + i * K];
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < K; i += blockDim.x) mu_out[i] = z[i] + muc[i];
+}
+
+// lambda_beta ~ Gamma(nux/2, 2 mux/nux), nux = nu + K nfeat,
+// mux = mu nux / (nu + mu tr(B B^T Lambda))   (latentprior.cpp:317-331)
+__global__ void k_lambda_beta(const double* __restrict__ bb_partials, int nparts, int K,
+                              long long nfeat, const double* __restrict__ Lambda, double nu,
+                              double mu, const Ctl* ctl, unsigned long long seed, int mode,
+                              double* lambda_beta) {
+  __shared__ double red[256];
+  const int KK = K * K;
+  double tr = 0.0;
+  for (int e = threadIdx.x; e < KK; e += blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < nparts; b++) s += bb_partials[(size_t)b * (K + KK) + K + e];
+    const int i = e % K, j = e / K;
+    tr += s * Lambda[j + i * K];
+  }
+  red[threadIdx.x] = tr;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < (int)blockDim.x; q++) t += red[q];
+    const double nux = nu + (double)K * (double)nfeat;
+    const double mux = mu * nux / (nu + mu * t);
+    const double b = nux / 2, c = 2 * mux / nux;
+    *lambda_beta = c * gamma_draw(seed, ctl->sweep, stream_id(kLambdaBeta, mode), 0u, b);
+  }
+}
+
+constexpr int kEvalThreads = 256;
+
+// One warp per test entry: lanes split the K-dot product (coalesced row reads), lane 0 does
+// the online mean / variance update of that entry.
+template <typename T>
+__global__ void __launch_bounds__(kEvalThreads)
+    k_eval(const int* __restrict__ trow, const int* __restrict__ tcol,
+           const double* __restrict__ tval, long long ntest, const T* __restrict__ U,
+           const T* __restrict__ V, int K, int stride, double mean, int n_fixed, const Ctl* ctl,
+           double* __restrict__ pred, double* __restrict__ pvar, double* __restrict__ partials) {
+  __shared__ double r1[kEvalThreads / 32], r2[kEvalThreads / 32];
+  int n = n_fixed;
+  if (n < 0) n = ((int)ctl->sweep < ctl->burnin) ? 0 : (int)ctl->sweep - ctl->burnin;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double se = 0.0, sea = 0.0;
+  const long long nw = (long long)gridDim.x * (kEvalThreads / 32);
+  for (long long t = (long long)blockIdx.x * (kEvalThreads / 32) + wid; t < ntest; t += nw) {
+    const T* v = V + (size_t)tcol[t] * stride;
+    const T* u = U + (size_t)trow[t] * stride;
+    double dot = 0.0;
+    for (int k = lane; k < K; k += 32) dot += (double)v[k] * (double)u[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+    if (lane == 0) {
+      const double p = dot + mean;
+      const double y = tval[t];
+      se += (y - p) * (y - p);
+      double pavg;
+      if (n == 0) {
+        pavg = p;
+      } else {
+        const double delta = p - pred[t];
+        pavg = pred[t] + delta / (n + 1);
+        pvar[t] += delta * (p - pavg);
+      }
+      sea += (y - pavg) * (y - pavg);
+      pred[t] = pavg;
+    }
+  }
+  if (lane == 0) {
+    r1[wid] = se;
+    r2[wid] = sea;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < kEvalThreads / 32; q++) {
+      a += r1[q];
+      b += r2[q];
+    }
+    partials[2 * blockIdx.x] = a;
+    partials[2 * blockIdx.x + 1] = b;
+  }
+}
+
+__global__ void k_eval_finish(const double* partials, int nparts, long long ntest,
+                              double* rmse) {
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < nparts; q++) {
+      a += partials[2 * q];
+      b += partials[2 * q + 1];
+    }
+    rmse[0] = sqrt(b / (double)ntest);  // posterior-mean RMSE (rmse_test)
+    rmse[1] = sqrt(a / (double)ntest);  // single-sample RMSE (rmse_test_onesample)
+  }
+}
+
+__global__ void k_set_sweep(Ctl* ctl, uint32_t sweep, int burnin) {
+  ctl->sweep = sweep;
+  ctl->burnin = burnin;
+}
+
+__global__ void k_advance(Ctl* ctl) { ctl->sweep += 1u; }
+
+}  // namespace
+
+int stats_blocks(long long N) {
+  long long b = (N + 511) / 512;
+  if (b > 1184) b = 1184;
+  return (int)(b < 1 ? 1 : b);
+}
+
+void launch_stats(const void* U, bool f32, const double* Uhat, long long N, int K, int stride,
+                  int uhat_stride, double* partials, int nblocks, cudaStream_t s) {
+  if (K > 128) throw MgError(MG_ERR_ARG, "K > 128 is not supported");
+  const long long rpb = (N + nblocks - 1) / nblocks;
+  const int per = (K * K + kStatThreads - 1) / kStatThreads;
+#define MG_STATS(P)                                                                         \
+  if (per <= P) {                                                                           \
+    if (f32)                                                                                \
+      k_stats<float, P><<<nblocks, kStatThreads, 0, s>>>((const float*)U, Uhat, N, K, stride, \
+                                                         uhat_stride, rpb, partials);       \
+    else                                                                                    \
+      k_stats<double, P><<<nblocks, kStatThreads, 0, s>>>((const double*)U, Uhat, N, K,     \
+                                                          stride, uhat_stride, rpb, partials); \
+    MG_CUDA(cudaGetLastError());                                                            \
+    return;                                                                                 \
+  }
+  MG_STATS(1)
+  MG_STATS(4)
+  MG_STATS(16)
+  MG_STATS(64)
+#undef MG_STATS
+}
+
+void launch_normal_wishart(const double* partials, int nparts, long long N, int K,
+                           const double* mu0, double kappa, const double* T0, int nu,
+                           const double* bb_partials, int bb_nparts, const double* lambda_beta,
+                           const NwWork& w, Ctl* ctl, unsigned long long seed, int mode,
+                           double* mu_out, double* Lambda_out, cudaStream_t s) {
+  k_normal_wishart<<<1, 256, 0, s>>>(partials, nparts, N, K, mu0, kappa, T0, nu, bb_partials,
+                                     bb_nparts, lambda_beta, w, ctl, seed, mode, mu_out,
+                                     Lambda_out);
+  MG_CUDA(cudaGetLastError());
+}
+
+void launch_lambda_beta(const double* bb_partials, int nparts, int K, long long nfeat,
+                        const double* Lambda, double nu, double mu, const Ctl* ctl,
+                        unsigned long long seed, int mode, double* lambda_beta, cudaStream_t s) {
+  k_lambda_beta<<<1, 256, 0, s>>>(bb_partials, nparts, K, nfeat, Lambda, nu, mu, ctl, seed,
+                                  mode, lambda_beta);
+  MG_CUDA(cudaGetLastError());
+}
+
+int eval_blocks(long long ntest) {
+  long long b = (ntest + kEvalThreads / 32 - 1) / (kEvalThreads / 32);
+  if (b > 592) b = 592;
+  return (int)(b < 1 ? 1 : b);
+}
+
+void launch_eval(const int* trow, const int* tcol, const double* tval, long long ntest,
+                 const void* U, const void* V, bool f32, int K, int stride, double mean,
+                 int n_fixed, const Ctl* ctl, double* pred, double* pvar, double* partials,
+                 int nblocks, double* rmse, cudaStream_t s) {
+  if (f32)
+    k_eval<float><<<nblocks, kEvalThreads, 0, s>>>(trow, tcol, tval, ntest, (const float*)U,
+                                                   (const float*)V, K, stride, mean, n_fixed,
+                                                   ctl, pred, pvar, partials);
+  else
+    k_eval<double><<<nblocks, kEvalThreads, 0, s>>>(trow, tcol, tval, ntest, (const double*)U,
+                                                    (const double*)V, K, stride, mean, n_fixed,
+                                                    ctl, pred, pvar, partials);
+  MG_CUDA(cudaGetLastError());
+  k_eval_finish<<<1, 32, 0, s>>>(partials, nblocks, ntest, rmse);
+  MG_CUDA(cudaGetLastError());
+}
+
+void launch_set_sweep(Ctl* ctl, uint32_t sweep, int burnin, cudaStream_t s) {
+  k_set_sweep<<<1, 1, 0, s>>>(ctl, sweep, burnin);
+  MG_CUDA(cudaGetLastError());
+}
+
+void launch_advance(Ctl* ctl, cudaStream_t s) {
+  k_advance<<<1, 1, 0, s>>>(ctl);
+  MG_CUDA(cudaGetLastError());
+}
+
+}  // namespace mg

@@ -1,0 +1,97 @@
+// Host-side launch functions of the sm_100a kernels (one translation unit per kernel family).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace mg {
+
+// ---- latent sampler (sample_kernels.cu, gram_tc.cu) ----
+void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, int num_sms);
+// Mixed-precision sampler whose Gram runs on the tcgen05 tensor cores (K = 32 only).  Returns
+// false when the configuration is not covered (caller falls back to the CUDA-core kernel).
+bool launch_sample_tc(const SampleParams& p, int KP, cudaStream_t s, int num_sms);
+
+// ---- hyperprior / eval (hyper_kernels.cu) ----
+struct NwWork {
+  double* vec;  // 3*K
+  double* m0;   // K*K each
+  double* m1;
+  double* m2;
+  double* m3;
+};
+int stats_blocks(long long N);
+void launch_stats(const void* U, bool f32, const double* Uhat, long long N, int K, int stride,
+                  int uhat_stride, double* partials, int nblocks, cudaStream_t s);
+void launch_normal_wishart(const double* partials, int nparts, long long N, int K,
+                           const double* mu0, double kappa, const double* T0, int nu,
+                           const double* bb_partials, int bb_nparts, const double* lambda_beta,
+                           const NwWork& w, Ctl* ctl, unsigned long long seed, int mode,
+                           double* mu_out, double* Lambda_out, cudaStream_t s);
+void launch_lambda_beta(const double* bb_partials, int nparts, int K, long long nfeat,
+                        const double* Lambda, double nu, double mu, const Ctl* ctl,
+                        unsigned long long seed, int mode, double* lambda_beta, cudaStream_t s);
+int eval_blocks(long long ntest);
+void launch_eval(const int* trow, const int* tcol, const double* tval, long long ntest,
+                 const void* U, const void* V, bool f32, int K, int stride, double mean,
+                 int n_fixed, const Ctl* ctl, double* pred, double* pvar, double* partials,
+                 int nblocks, double* rmse, cudaStream_t s);
+void launch_set_sweep(Ctl* ctl, uint32_t sweep, int burnin, cudaStream_t s);
+void launch_advance(Ctl* ctl, cudaStream_t s);
+
+// ---- side information / block-CG (cg_kernels.cu) ----
+struct DevCsr {
+  const long long* ptr = nullptr;
+  const int* idx = nullptr;
+  const double* val = nullptr;  // null = binary
+  const float* valf = nullptr;  // FP32 copy of val (mixed CG), null = binary
+  long long nrow = 0;
+  long long ncol = 0;
+  long long nnz = 0;
+};
+
+// out[r, :ncomp] = sum_{e in row r} val_e * src[idx_e, :]   (csr_A_mul_Bn / A_mul_Bx<N>)
+void launch_spmm(const DevCsr& A, const void* src, int src_stride, void* dst, int dst_stride,
+                 int ncomp, bool f32, cudaStream_t s);
+
+// sample_beta pieces (latentprior.cpp:273-293)
+//   tmp[n] = U[n] + chol(Lambda)^{-T} z_n - mu      (n < N; z keyed (kMvnN, n))
+void launch_beta_rhs_tmp(const void* U, bool f32, int ustride, long long N, int K,
+                         const double* Lchol, const double* mu, const Ctl* ctl,
+                         unsigned long long seed, int mode, double* tmp, int tstride,
+                         cudaStream_t s);
+//   B[f] = sum_{n in Ft row f} tmp[n] + sqrt(lambda_beta) chol(Lambda)^{-T} z_f
+void launch_beta_rhs_b(const DevCsr& Ft, const double* tmp, int tstride, int K,
+                       const double* Lchol, const double* lambda_beta, const Ctl* ctl,
+                       unsigned long long seed, int mode, double* B, int bstride,
+                       cudaStream_t s);
+// one-CTA Cholesky of a K x K matrix into L (lower, zero upper); status on failure
+void launch_small_chol(const double* A, int K, double* L, Ctl* ctl, cudaStream_t s);
+
+class BlockCg {
+ public:
+  // Workspace for nfeat features, F with `nrow` rows, up to 64 right-hand sides.
+  void reserve(long long nrow, long long nfeat, int max_rhs, bool f32);
+  void release();
+  // Solves (F^T F + reg I) X = B for the nrhs columns of B (nfeat x stride, row f = the nrhs
+  // values of feature f) with the blocked wrapper (blocks of 32, +8 excess).  reg is a host
+  // value or, when reg_dev != null, read on the device.  Returns the summed iteration count.
+  int solve(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev,
+            const double* B, int bstride, int nrhs, double tol, double* X, int xstride,
+            Ctl* ctl, cudaStream_t s, bool f32);
+  ~BlockCg() { release(); }
+
+ private:
+  int core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev,
+           const double* B, int bstride, int nrhs, double tol, double* X, int xstride, Ctl* ctl,
+           cudaStream_t s, bool f32);
+  long long nrow_ = 0, nfeat_ = 0;
+  int maxr_ = 0;
+  bool f32_ = false;
+  void *R_ = nullptr, *P_ = nullptr, *KP_ = nullptr, *inner_ = nullptr;
+  double *Xd_ = nullptr, *Bn_ = nullptr, *KX_ = nullptr, *innerd_ = nullptr;
+  double *small_ = nullptr, *partials_ = nullptr, *norms_ = nullptr;
+  int *flag_host_ = nullptr;
+};
+
+}  // namespace mg

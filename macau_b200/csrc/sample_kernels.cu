@@ -1,0 +1,379 @@
+// Per-row latent sampler (sample_latent_blas, latentprior.cpp:361-385, driven by the OpenMP row
+// loops of latentprior.cpp:69-77 / 219-227), as one persistent sm_100a launch per mode.
+//
+// Work decomposition
+//   * A "row group" of T = 32*WPR threads samples one row at a time; a CTA holds G groups.
+//   * Rows come from a task list sorted by descending length and are taken from a device work
+//     queue (atomic head in the control block), so power-law rows balance dynamically.
+//   * Rows longer than the split threshold are cut into parts; each part writes its partial
+//     Gram + right-hand side into a scratch slot, and the part that arrives last (per-row
+//     atomic counter) sums the parts in part order (deterministic) and finishes the row.
+//
+// Per row: the gathered other-factor rows are staged in shared memory 32 at a time with 16-byte
+// vector loads; each thread accumulates a TR x TC tile of the KP x KP Gram in registers and the
+// first KP threads accumulate the right-hand side.  Finishing builds MM = Lambda + alpha*G and
+// rr = sum v (y - mean) alpha + Lambda mu in shared memory, factorises MM = L L^T, solves
+// L y = rr, adds N(0,1) draws and solves L^T x = y.
+//
+// FP64 path: FP64 everything (parity with the FP64 oracle).  Mixed path: BF16 gathered rows,
+// FP32 Gram/factor/solves; a row whose FP32 pivot is not positive or falls below 2^-20 of its
+// original diagonal is re-factorised in FP64 in the same launch (counted in ctl->retries).
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "rng.cuh"
+
+namespace mg {
+namespace {
+
+constexpr int kChunk = 32;  // gathered rows staged per step
+
+__device__ __forceinline__ float mfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double mfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float msqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ double msqrt(double a) { return sqrt(a); }
+
+template <int T>
+__device__ __forceinline__ void gsync(int g) {
+  if constexpr (T == 32) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "n"(T) : "memory");
+  }
+}
+
+template <int KP, int WPR, bool MIXED>
+struct Cfg {
+  using Acc = typename std::conditional<MIXED, float, double>::type;
+  using Elem = typename std::conditional<MIXED, __nv_bfloat16, double>::type;
+  static constexpr int T = 32 * WPR;
+  static constexpr int S = WPR == 1 ? 1 : (WPR == 4 ? 2 : 4);
+  static constexpr int GR = 8 * S, GC = 4 * S;
+  static constexpr int TR = KP / GR, TC = KP / GC;
+  static constexpr int LD = KP + 1;  // leading dimension of MM in shared memory
+  static constexpr int EV = 16 / sizeof(Elem);  // elements per 16-byte vector load
+  static constexpr int VPR = KP / EV;           // vectors per gathered row
+  static constexpr size_t kGath = sizeof(Acc) * kChunk * KP;
+  static constexpr size_t kMM = sizeof(double) * KP * LD;
+  static constexpr size_t kWork = (kGath > kMM ? kGath : kMM);
+  // work | cidx[kChunk] | cw[kChunk] (double) | rr[KP] (double) | mun[KP] | diag[KP] | bcast[4]
+  static constexpr size_t kGroupBytes =
+      kWork + sizeof(int) * kChunk + sizeof(double) * (kChunk + 3 * KP) + 16;
+  static_assert(TR >= 1 && TC >= 1 && GR * TR == KP && GC * TC == KP, "tile");
+  static_assert(VPR >= 1, "vector width");
+};
+
+// Cholesky + solves + noise for one row, in factor precision F.  MM (lower triangle, K x K),
+// rr (right-hand side) and diag (original diagonal) are in shared memory.  Returns false if a
+// pivot fails (nothing is written then).  All threads of the group return the same value.
+template <typename F, int T, int GR, int GC>
+__device__ bool factor_solve(F* M, int ld, F* rr, const double* diag, int K, int t, int g,
+                             double rel_floor) {
+  const int rt = t / GC, ct = t % GC;
+  for (int j = 0; j < K; j++) {
+    const F d = M[j * ld + j];
+    const bool bad = !(d > (F)0) || !((double)d > rel_floor * diag[j]);
+    gsync<T>(g);
+    if (bad) return false;
+    const F ljj = msqrt(d);
+    for (int i = j + t; i < K; i += T) M[i * ld + j] = (i == j) ? ljj : M[i * ld + j] / ljj;
+    gsync<T>(g);
+    for (int i = j + 1 + rt; i < K; i += GR) {
+      const F lij = M[i * ld + j];
+      for (int k = j + 1 + ct; k <= i; k += GC) M[i * ld + k] -= lij * M[k * ld + j];
+    }
+    gsync<T>(g);
+  }
+  // L y = rr
+  for (int j = 0; j < K; j++) {
+    if (t == 0) rr[j] = rr[j] / M[j * ld + j];
+    gsync<T>(g);
+    const F yj = rr[j];
+    for (int i = j + 1 + t; i < K; i += T) rr[i] -= M[i * ld + j] * yj;
+    gsync<T>(g);
+  }
+  return true;
+}
+
+template <typename F, int T>
+__device__ void back_solve(const F* M, int ld, F* rr, int K, int t, int g) {
+  for (int j = K - 1; j >= 0; j--) {
+    if (t == 0) rr[j] = rr[j] / M[j * ld + j];
+    gsync<T>(g);
+    const F xj = rr[j];
+    for (int i = t; i < j; i += T) rr[i] -= M[j * ld + i] * xj;
+    gsync<T>(g);
+  }
+}
+
+template <typename F, int T>
+__device__ void add_noise(const SampleParams& p, F* rr, int row, int K, int t, int g,
+                          uint32_t sweep) {
+  if (p.znoise) {
+    for (int k = t; k < K; k += T) rr[k] += (F)p.znoise[(size_t)row * K + k];
+  } else {
+    const uint32_t st = stream_id(kRowNoise, (uint32_t)p.mode);
+    for (int q = t; q < (K + 1) / 2; q += T) {
+      double z0, z1;
+      normal_pair(p.seed, sweep, st, (uint32_t)row, (uint32_t)q, &z0, &z1);
+      rr[2 * q] += (F)z0;
+      if (2 * q + 1 < K) rr[2 * q + 1] += (F)z1;
+    }
+  }
+  gsync<T>(g);
+}
+
+template <int KP, int WPR, int G, bool MIXED>
+__global__ void __launch_bounds__(32 * WPR * G) k_sample(const SampleParams p) {
+  using C = Cfg<KP, WPR, MIXED>;
+  using Acc = typename C::Acc;
+  using Elem = typename C::Elem;
+  constexpr int T = C::T, GR = C::GR, GC = C::GC, TR = C::TR, TC = C::TC, LD = C::LD;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  unsigned char* base = smem_raw + (size_t)g * C::kGroupBytes;
+  Acc* gath = reinterpret_cast<Acc*>(base);
+  int* cidx = reinterpret_cast<int*>(base + C::kWork);
+  double* cw = reinterpret_cast<double*>(cidx + kChunk);
+  double* rrd = cw + kChunk;
+  double* mun = rrd + KP;
+  double* diag = mun + KP;
+  int* bcast = reinterpret_cast<int*>(diag + KP);
+  const int rt = t / GC, ct = t % GC;
+  const int K = p.K;
+  const uint32_t sweep = p.ctl->sweep;
+  const Elem* other = reinterpret_cast<const Elem*>(p.other);
+
+  for (;;) {
+    if (t == 0) bcast[0] = (int)atomicAdd(&p.ctl->queue[p.qslot], 1u);
+    gsync<T>(g);
+    const int ti = bcast[0];
+    if (ti >= p.ntasks) break;
+    const RowTask tk = p.tasks[ti];
+    Acc acc[TR][TC];
+#pragma unroll
+    for (int i = 0; i < TR; i++)
+#pragma unroll
+      for (int j = 0; j < TC; j++) acc[i][j] = (Acc)0;
+    Acc racc = (Acc)0;
+
+    const long long end = tk.begin + tk.len;
+    for (long long b = tk.begin; b < end; b += kChunk) {
+      const int cnt = (int)min((long long)kChunk, end - b);
+      for (int e = t; e < kChunk; e += T) {
+        int c = 0;
+        double w = 0.0;
+        if (e < cnt) {
+          if constexpr (MIXED) {
+            const uint2 pk = p.packed[b + e];
+            c = (int)pk.x;
+            w = (double)__uint_as_float(pk.y);
+          } else {
+            c = p.colidx[b + e];
+            w = (p.vals[b + e] - p.mean) * p.alpha;
+          }
+        }
+        cidx[e] = c;
+        cw[e] = w;
+      }
+      gsync<T>(g);
+      // gather: 16-byte vectors of the other factor's rows
+#pragma unroll 4
+      for (int e = t; e < kChunk * C::VPR; e += T) {
+        const int r = e / C::VPR, v = e % C::VPR;
+        if (r < cnt) {
+          const uint4 raw = __ldg(reinterpret_cast<const uint4*>(other + (size_t)cidx[r] * KP) + v);
+          Acc* dst = gath + r * KP + v * C::EV;
+          if constexpr (MIXED) {
+            const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&raw);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+              const float2 f = __bfloat1622float2(h[q]);
+              dst[2 * q] = f.x;
+              dst[2 * q + 1] = f.y;
+            }
+          } else {
+            const double2 d = *reinterpret_cast<const double2*>(&raw);
+            dst[0] = d.x;
+            dst[1] = d.y;
+          }
+        }
+      }
+      gsync<T>(g);
+      if (t < KP) {
+        for (int r = 0; r < cnt; r++) racc += gath[r * KP + t] * (Acc)cw[r];
+      }
+      for (int r = 0; r < cnt; r++) {
+        Acc a[TR], bb[TC];
+#pragma unroll
+        for (int i = 0; i < TR; i++) a[i] = gath[r * KP + rt * TR + i];
+#pragma unroll
+        for (int j = 0; j < TC; j++) bb[j] = gath[r * KP + ct * TC + j];
+#pragma unroll
+        for (int i = 0; i < TR; i++)
+#pragma unroll
+          for (int j = 0; j < TC; j++) acc[i][j] = mfma(a[i], bb[j], acc[i][j]);
+      }
+      gsync<T>(g);
+    }
+
+    if (tk.nparts > 1) {
+      double* sp = p.scratch + (size_t)(tk.slot + tk.part) * (KP * KP + KP);
+#pragma unroll
+      for (int i = 0; i < TR; i++)
+#pragma unroll
+        for (int j = 0; j < TC; j++) sp[(rt * TR + i) * KP + ct * TC + j] = (double)acc[i][j];
+      if (t < KP) sp[KP * KP + t] = (double)racc;
+      __threadfence();
+      gsync<T>(g);
+      if (t == 0)
+        bcast[1] = (atomicAdd(&p.split_cnt[tk.split], 1u) == (unsigned)(tk.nparts - 1)) ? 1 : 0;
+      gsync<T>(g);
+      if (!bcast[1]) continue;
+      __threadfence();
+      double dacc[TR][TC];
+      double dr = 0.0;
+#pragma unroll
+      for (int i = 0; i < TR; i++)
+#pragma unroll
+        for (int j = 0; j < TC; j++) dacc[i][j] = 0.0;
+      for (int q = 0; q < tk.nparts; q++) {
+        const double* s = p.scratch + (size_t)(tk.slot + q) * (KP * KP + KP);
+#pragma unroll
+        for (int i = 0; i < TR; i++)
+#pragma unroll
+          for (int j = 0; j < TC; j++) dacc[i][j] += __ldcg(s + (rt * TR + i) * KP + ct * TC + j);
+        if (t < KP) dr += __ldcg(s + KP * KP + t);
+      }
+#pragma unroll
+      for (int i = 0; i < TR; i++)
+#pragma unroll
+        for (int j = 0; j < TC; j++) acc[i][j] = (Acc)dacc[i][j];
+      racc = (Acc)dr;
+      if (t == 0) p.split_cnt[tk.split] = 0u;
+    }
+
+    // ---- finish the row ----
+    const int row = tk.row;
+    if (t < K) mun[t] = p.mu[t] + (p.uhat ? p.uhat[(size_t)row * KP + t] : 0.0);
+    gsync<T>(g);
+    double lmu = 0.0;
+    if (t < K) {
+      for (int j = 0; j < K; j++) lmu += p.Lambda[t + j * K] * mun[j];
+    }
+    gsync<T>(g);
+    bool done = false;
+    if constexpr (MIXED) {
+      float* M = reinterpret_cast<float*>(base);
+      float* rr = reinterpret_cast<float*>(rrd);
+      const float af = (float)p.alpha;
+#pragma unroll
+      for (int i = 0; i < TR; i++)
+#pragma unroll
+        for (int j = 0; j < TC; j++) {
+          const int gi = rt * TR + i, gj = ct * TC + j;
+          if (gi < K && gj <= gi) {
+            const float v = (float)p.Lambda[gi + gj * K] + af * acc[i][j];
+            M[gi * LD + gj] = v;
+            if (gi == gj) diag[gi] = (double)v;
+          }
+        }
+      if (t < K) rr[t] = (float)((double)racc + lmu);
+      gsync<T>(g);
+      done = factor_solve<float, T, GR, GC>(M, LD, rr, diag, K, t, g, 0x1p-20);
+      if (done) {
+        add_noise<float, T>(p, rr, row, K, t, g, sweep);
+        back_solve<float, T>(M, LD, rr, K, t, g);
+        if (t < K) {
+          p.out_f32[(size_t)row * KP + t] = rr[t];
+          p.out_bf16[(size_t)row * KP + t] = __float2bfloat16_rn(rr[t]);
+        }
+      } else if (t == 0) {
+        atomicAdd(&p.ctl->retries[p.mode], 1u);
+      }
+      gsync<T>(g);
+    }
+    if (!done) {
+      double* M = reinterpret_cast<double*>(base);
+      double* rr = rrd;
+#pragma unroll
+      for (int i = 0; i < TR; i++)
+#pragma unroll
+        for (int j = 0; j < TC; j++) {
+          const int gi = rt * TR + i, gj = ct * TC + j;
+          if (gi < K && gj <= gi) {
+            const double v = p.Lambda[gi + gj * K] + p.alpha * (double)acc[i][j];
+            M[gi * LD + gj] = v;
+            if (gi == gj) diag[gi] = v;
+          }
+        }
+      if (t < K) rr[t] = (double)racc + lmu;
+      gsync<T>(g);
+      const bool ok = factor_solve<double, T, GR, GC>(M, LD, rr, diag, K, t, g, 0.0);
+      if (ok) {
+        add_noise<double, T>(p, rr, row, K, t, g, sweep);
+        back_solve<double, T>(M, LD, rr, K, t, g);
+        if (t < K) {
+          if constexpr (MIXED) {
+            p.out_f32[(size_t)row * KP + t] = (float)rr[t];
+            p.out_bf16[(size_t)row * KP + t] = __float2bfloat16_rn((float)rr[t]);
+          } else {
+            p.out_f64[(size_t)row * KP + t] = rr[t];
+          }
+        }
+      } else if (t == 0) {
+        atomicOr(&p.ctl->status, kStatCholFail);
+        atomicCAS(&p.ctl->bad_row, -1, row);
+      }
+      gsync<T>(g);
+    }
+  }
+}
+
+template <int KP, int WPR, int G, bool MIXED>
+void launch_t(const SampleParams& p, cudaStream_t s, int num_sms) {
+  using C = Cfg<KP, WPR, MIXED>;
+  auto kern = k_sample<KP, WPR, G, MIXED>;
+  const size_t smem = C::kGroupBytes * G;
+  static int per_sm_cache[64] = {0};  // per template instance and device
+  int dev = 0;
+  MG_CUDA(cudaGetDevice(&dev));
+  int& per_sm = per_sm_cache[dev & 63];
+  if (per_sm == 0) {
+    MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int n = 0;
+    MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, 32 * WPR * G, smem));
+    per_sm = n < 1 ? 1 : n;
+  }
+  const int need = (p.ntasks + G - 1) / G;
+  int blocks = num_sms * per_sm;
+  if (need < blocks) blocks = need > 0 ? need : 1;
+  kern<<<blocks, 32 * WPR * G, smem, s>>>(p);
+  MG_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, int num_sms) {
+  if (mixed) {
+    switch (KP) {
+      case 8: return launch_t<8, 1, 4, true>(p, s, num_sms);
+      case 16: return launch_t<16, 1, 4, true>(p, s, num_sms);
+      case 32: return launch_t<32, 1, 4, true>(p, s, num_sms);
+      case 64: return launch_t<64, 4, 2, true>(p, s, num_sms);
+      case 128: return launch_t<128, 16, 1, true>(p, s, num_sms);
+    }
+  } else {
+    switch (KP) {
+      case 8: return launch_t<8, 1, 4, false>(p, s, num_sms);
+      case 16: return launch_t<16, 1, 4, false>(p, s, num_sms);
+      case 32: return launch_t<32, 1, 4, false>(p, s, num_sms);
+      case 64: return launch_t<64, 4, 2, false>(p, s, num_sms);
+      case 128: return launch_t<128, 16, 1, false>(p, s, num_sms);
+    }
+  }
+  throw MgError(MG_ERR_ARG, "unsupported latent dimension");
+}
+
+}  // namespace mg

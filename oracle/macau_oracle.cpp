@@ -123,15 +123,29 @@ void ata_mul_bx(const Csr& F, const Csr& Ft, double reg, const double* B, int N,
   }
 }
 
+// Number of partial sums of the K x K reductions.  The reference accumulates one partial per
+// OpenMP thread over contiguous column ranges and adds the partials in thread order
+// (A_mul_At_omp / A_mul_Bt_omp_sym, linop.cpp:280-317, 332-371), so its summation order depends
+// on the thread count; the oracle takes the count as a parameter (1 = one sequential sum).
+static int g_reduce_parts = 1;
+
 // Lower triangle of A * B^T for n x k column-major A, B (A_mul_Bt_omp_sym, linop.cpp:320-372;
-// A_mul_At_omp, linop.cpp:271-318), then mirrored to the upper triangle when `sym`.
+// A_mul_At_omp, linop.cpp:271-318), then mirrored to the upper triangle when `sym`.  Partial
+// sums over g_reduce_parts contiguous chunks of ceil(k / parts) columns, added in chunk order.
 void a_mul_bt_lower(const double* A, const double* B, int n, int k, double* out, bool sym) {
-  std::vector<double> acc((size_t)n * n, 0.0);
-  for (int64_t c = 0; c < k; c++) {
-    const double* a = A + c * n;
-    const double* b = B + c * n;
-    for (int i = 0; i < n; i++)
-      for (int j = i; j < n; j++) acc[j + (size_t)i * n] += a[j] * b[i];
+  std::vector<double> acc((size_t)n * n, 0.0), part((size_t)n * n);
+  const int parts = std::max(1, g_reduce_parts);
+  const int64_t chunk = ((int64_t)k + parts - 1) / parts;
+  for (int q = 0; q < parts; q++) {
+    std::fill(part.begin(), part.end(), 0.0);
+    const int64_t c1 = std::min<int64_t>(k, (q + 1) * chunk);
+    for (int64_t c = q * chunk; c < c1; c++) {
+      const double* a = A + c * n;
+      const double* b = B + c * n;
+      for (int i = 0; i < n; i++)
+        for (int j = i; j < n; j++) part[j + (size_t)i * n] += a[j] * b[i];
+    }
+    for (size_t t = 0; t < acc.size(); t++) acc[t] += part[t];
   }
   for (int i = 0; i < n; i++)
     for (int j = 0; j < n; j++) {
@@ -169,6 +183,12 @@ double orc_normal(uint64_t seed, uint32_t sweep, uint32_t stream, uint32_t index
 
 double orc_gamma(uint64_t seed, uint32_t sweep, uint32_t stream, uint32_t index, double shape) {
   return gamma_draw(seed, sweep, stream, index, shape);
+}
+
+// Sets the number of partial sums of the K x K reductions (see g_reduce_parts); returns it.
+int orc_set_reduce_parts(int parts) {
+  if (parts > 0) g_reduce_parts = parts;
+  return g_reduce_parts;
 }
 
 int orc_set_threads(int n) {
@@ -322,11 +342,13 @@ int orc_blockcg_core(int nrhs, int nrow, int nfeat, const int64_t* fptr, const i
   const double tolsq = tol * tol;
   const size_t sz = (size_t)nrhs * nfeat;
   std::vector<double> norms(nrhs), inorms(nrhs);
-  for (int r = 0; r < nrhs; r++) {
-    double s = 0.0;
-    for (int f = 0; f < nfeat; f++) s += B[r + (size_t)f * nrhs] * B[r + (size_t)f * nrhs];
-    norms[r] = std::sqrt(s);
-    inorms[r] = 1.0 / norms[r];
+  {
+    std::vector<double> BBt((size_t)nrhs * nrhs);
+    a_mul_bt_lower(B, B, nrhs, nfeat, BBt.data(), false);
+    for (int r = 0; r < nrhs; r++) {
+      norms[r] = std::sqrt(BBt[r + (size_t)r * nrhs]);
+      inorms[r] = 1.0 / norms[r];
+    }
   }
   std::vector<double> R(sz), P(sz), KP(sz), inner((size_t)nrow * nrhs);
   std::fill(X, X + sz, 0.0);

@@ -38,6 +38,7 @@ def _load():
         "orc_normal": (_d, [_u64, _u32, _u32, _u32, _u32]),
         "orc_gamma": (_d, [_u64, _u32, _u32, _u32, _d]),
         "orc_set_threads": (_i, [_i]),
+        "orc_set_reduce_parts": (_i, [_i]),
         "orc_sample_latents": (_i, [_i, _i, _i, _p, _p, _p, _d, _p, _d, _p, _p, _p, _u64, _u32,
                                     _u32, _p, _p]),
         "orc_cond_normal_wishart": (_i, [_i, _i, _p, _p, _d, _p, _i, _u64, _u32, _u32, _p, _p]),
@@ -86,6 +87,12 @@ def f64(a):
 
 def set_threads(n=0):
     return lib().orc_set_threads(int(n))
+
+
+def set_reduce_parts(n):
+    """Partial-sum count of the oracle's K x K reductions (the reference uses one per OpenMP
+    thread; linop.cpp:280-317).  Returns the value in force."""
+    return lib().orc_set_reduce_parts(int(n))
 
 
 def philox(ctr, key):

@@ -1,0 +1,300 @@
+"""GPU parity of the CUDA library against the CPU oracle, through the C ABI.
+
+Bar (FP64 mode): per-row samples, hyperparameters and beta within 1e-9 (norm-wise relative) of
+the FP64 oracle fed the same keyed or injected N(0,1) draws.  Mixed mode: stated tolerances
+against the same FP64 oracle."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from macau_b200 import _lib, workloads
+from oracle import oracle as orc
+from tests.gpu_helpers import gpu_sampler, oracle_model, random_spd, relerr, train_matrix
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-9
+MIXED_SAMPLE_TOL = 2e-2   # BF16 Gram + FP32 factor vs FP64, norm-wise relative per sweep
+
+
+def small_uniform(seed=0, nrow=300, ncol=200, nobs=6000):
+    return workloads.bpmf_uniform(nrow=nrow, ncol=ncol, nobs=nobs, seed=seed)
+
+
+@pytest.mark.parametrize("K", [4, 10, 16, 32, 50, 64, 128])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_row_sampler_fp64_injected_draws(K, mode):
+    rng = np.random.default_rng(K + 100 * mode)
+    w = small_uniform(seed=K)
+    s = gpu_sampler(w, K, 4.0, seed=7)
+    Y = train_matrix(w)
+    other = 1 - mode
+    Vo = rng.normal(scale=0.5, size=(w["shape"][other], K))
+    s.set_latents(other, Vo)
+    mu = rng.normal(size=K)
+    Lam = random_spd(rng, K, 5.0)
+    s.set_hyper(mode, mu, Lam)
+    N = w["shape"][mode]
+    z = rng.normal(size=(N, K))
+    s.sample_latents(mode, 3, z)
+    got = s.latents(mode)
+    R = orc.Csr.from_scipy(Y if mode == 0 else Y.T)
+    want, st = orc.sample_latents(K, R, Vo, s.mean_value(), 4.0, mu, Lam, z=z)
+    assert st == 0
+    assert relerr(got, want) < FP64_TOL
+
+
+@pytest.mark.parametrize("K", [10, 32])
+def test_row_sampler_fp64_keyed_draws(K):
+    rng = np.random.default_rng(5)
+    w = small_uniform(seed=1)
+    s = gpu_sampler(w, K, 2.0, seed=12345)
+    Y = train_matrix(w)
+    V = rng.normal(scale=0.5, size=(w["shape"][1], K))
+    s.set_latents(1, V)
+    mu0, Lam0, _ = s.hyper(0)
+    s.sample_latents(0, 17)
+    want, _ = orc.sample_latents(K, orc.Csr.from_scipy(Y), V, s.mean_value(), 2.0, mu0, Lam0,
+                                 seed=12345, sweep=17, mode=0)
+    assert relerr(s.latents(0), want) < FP64_TOL
+
+
+def test_row_sampler_split_heavy_rows():
+    # rows with thousands of entries are split into parts and reduced by the last part
+    rng = np.random.default_rng(9)
+    nrow, ncol, K = 64, 4000, 32
+    r, c = [], []
+    for i in range(nrow):
+        n = 3900 if i % 7 == 0 else rng.integers(1, 60)
+        cols = rng.choice(ncol, size=n, replace=False)
+        r += [i] * n
+        c += list(cols)
+    r = np.array(r, np.int32)
+    c = np.array(c, np.int32)
+    v = rng.normal(3.0, 1.0, size=len(r))
+    w = dict(rows=r, cols=c, vals=v, shape=(nrow, ncol))
+    s = gpu_sampler(w, K, 1.5, seed=3)
+    V = rng.normal(scale=0.3, size=(ncol, K))
+    s.set_latents(1, V)
+    z = rng.normal(size=(nrow, K))
+    mu, Lam, _ = s.hyper(0)
+    s.sample_latents(0, 0, z)
+    Y = train_matrix(w)
+    want, _ = orc.sample_latents(K, orc.Csr.from_scipy(Y), V, s.mean_value(), 1.5, mu, Lam, z=z)
+    assert relerr(s.latents(0), want) < FP64_TOL
+
+
+@pytest.mark.parametrize("K", [3, 10, 32, 64])
+def test_hyperprior_fp64(K):
+    rng = np.random.default_rng(K)
+    w = small_uniform(seed=2)
+    s = gpu_sampler(w, K, 1.0, seed=99)
+    U = rng.normal(0.3, 1.0, size=(w["shape"][0], K))
+    s.set_latents(0, U)
+    s.update_prior(0, 11)
+    mu, Lam, _ = s.hyper(0)
+    mu_o, Lam_o, st = orc.cond_normal_wishart(U, np.zeros(K), 2.0, np.eye(K), K, seed=99,
+                                              sweep=11, mode=0)
+    assert st == 0
+    assert relerr(Lam, Lam_o) < FP64_TOL
+    assert relerr(mu, mu_o) < FP64_TOL
+
+
+def test_full_sweeps_fp64_match_oracle():
+    w = workloads.bpmf_uniform(nrow=400, ncol=300, nobs=12000, seed=4)
+    K, alpha, seed, burnin = 10, 4.0, 2024, 4
+    s = gpu_sampler(w, K, alpha, seed, burnin=burnin, nsamples=6)
+    m = oracle_model(w, K, alpha, seed)
+    for it in range(10):
+        s.sweep(it, eval=True)
+        assert m.sweep(it, burnin) == 0
+        for mode in (0, 1):
+            assert relerr(s.latents(mode), m.latents(mode)) < 1e-8, (it, mode)
+            mu, Lam, _ = s.hyper(mode)
+            assert relerr(Lam, m.Lambda(mode)) < 1e-8
+        r, r1 = s.rmse()
+        ro, r1o = m.rmse()
+        assert abs(r - ro) < 1e-9 and abs(r1 - r1o) < 1e-9
+    np.testing.assert_allclose(s.predictions(), m.predictions(), rtol=1e-9, atol=1e-12)
+
+
+def gpu_cg_parts(nfeat):
+    """Number of contiguous partial sums the CUDA block-CG uses for its K x K reductions; the
+    oracle is given the same count so both add in the same order (the reference's own order
+    depends on its OpenMP thread count, linop.cpp:280-317)."""
+    return min(296, max(1, -(-nfeat // 256)))
+
+
+@pytest.fixture
+def oracle_parts():
+    yield orc.set_reduce_parts
+    orc.set_reduce_parts(1)
+
+
+def test_macau_update_prior_fp64_tight_tolerance(oracle_parts):
+    # With the CG solved to 1e-12 the link matrix is determined to far below 1e-9, so the whole
+    # MacauPrior::update_prior chain (Wishart, sample_beta RHS, CG, Uhat, lambda_beta) is
+    # compared at the FP64 bar.
+    w = workloads.macau_side(scale=0.02, seed=5)
+    K, alpha, seed = 8, 1.0, 77
+    s = gpu_sampler(w, K, alpha, seed, lambda_beta=5.0, tol=1e-12)
+    m = oracle_model(w, K, alpha, seed, lambda_beta=5.0, tol=1e-12)
+    oracle_parts(gpu_cg_parts(w["side"][3][1]))
+    for it in range(2):
+        for mode in (0, 1):
+            s.sample_latents(mode, it)
+            m.sample_mode(mode, it)
+            m.set("latents", mode, s.latents(mode))  # identical inputs for the next phase
+        s.update_prior(0, it)
+        m.update_prior(0, it)
+        mu, Lam, lb = s.hyper(0)
+        assert relerr(Lam, m.Lambda(0)) < FP64_TOL
+        assert relerr(mu, m.mu(0)) < FP64_TOL
+        assert relerr(s.beta(0), m.beta(0)) < FP64_TOL, it
+        assert relerr(s.uhat(0), m.uhat(0)) < FP64_TOL, it
+        assert abs(lb - m.lambda_beta(0)[0]) / lb < FP64_TOL
+        s.update_prior(1, it)
+        m.update_prior(1, it)
+        # carry the GPU's state into the oracle so the next sweep starts from identical inputs
+        m.set("beta", 0, s.beta(0))
+        m.set("uhat", 0, s.uhat(0))
+        m.set("lambda_beta", 0, [lb])
+        for mode in (0, 1):
+            mu, Lam, _ = s.hyper(mode)
+            m.set("mu", mode, mu)
+            m.set("Lambda", mode, Lam)
+
+
+def test_macau_side_sweeps_fp64_match_oracle(oracle_parts):
+    # At the default tolerance (1e-6) block-CG's output is defined only to about the tolerance:
+    # the oracle itself moves by ~1e-7 when its reduction order changes.  Full sweeps are
+    # therefore compared at 1e-5 (CG-bounded), with identical iteration counts.
+    w = workloads.macau_side(scale=0.02, seed=5)
+    K, alpha, seed = 8, 1.0, 77
+    s = gpu_sampler(w, K, alpha, seed, lambda_beta=5.0, tol=1e-6)
+    m = oracle_model(w, K, alpha, seed, lambda_beta=5.0, tol=1e-6)
+    oracle_parts(gpu_cg_parts(w["side"][3][1]))
+    for it in range(3):
+        s.sweep(it, eval=True)
+        assert m.sweep(it, 10) == 0
+        for mode in (0, 1):
+            assert relerr(s.latents(mode), m.latents(mode)) < 1e-5, (it, mode)
+        assert relerr(s.beta(0), m.beta(0)) < 1e-5, it
+        assert relerr(s.uhat(0), m.uhat(0)) < 1e-5, it
+        lbo, iters = m.lambda_beta(0)
+        assert abs(s.hyper(0)[2] - lbo) / lbo < 1e-5
+        assert abs(s.stats()["cg_iters"][0] - int(iters)) <= 1
+
+
+FIX = json.loads((Path(__file__).parent / "golden" / "reference_tests_cpp.json").read_text())
+
+
+def _case(name):
+    env = {}
+    for st in FIX["cases"][name]["statements"]:
+        if st["kind"] == "array":
+            env[st["name"]] = np.array(st["values"])
+        elif st["kind"] == "matrix" and st["name"] not in env:
+            env[st["name"]] = np.array(st["values"]).reshape(st["shape"])
+    return env
+
+
+@pytest.mark.parametrize("name", ["SparseFeat/solve_blockcg", "SparseFeat/solve_blockcg_1_0",
+                                  "linop/solve_blockcg_dense"])
+@pytest.mark.parametrize("compute", [_lib.MG_COMPUTE_FP64, _lib.MG_COMPUTE_MIXED])
+def test_blockcg_golden_on_gpu(name, compute):  # tests.cpp:123-207
+    env = _case(name)
+    r = env["rows"].astype(np.int32)
+    c = env["cols"].astype(np.int32)
+    B = np.asfortranarray(env["B"])
+    if name.endswith("_1_0"):  # blocksize 1: every RHS solved on its own
+        X = np.vstack([_lib.blockcg_raw(r, c, None, (6, 4), B[i:i + 1], 0.5, 1e-6, compute)[0]
+                       for i in range(B.shape[0])])
+        it = 0
+    else:
+        X, it, _ = _lib.blockcg_raw(r, c, None, (6, 4), B, 0.5, 1e-6, compute)
+    np.testing.assert_allclose(X, env["X_true"], rtol=2e-5, atol=2e-6)
+    if name == "SparseFeat/solve_blockcg":
+        assert it <= 4
+
+
+@pytest.mark.parametrize("tol,bar", [(1e-12, FP64_TOL), (1e-6, 1e-5)])
+def test_blockcg_matches_oracle_fp64(oracle_parts, tol, bar):
+    # 32 right-hand sides over a Zipf-degree binary F.  At tol 1e-6 the solve is only defined to
+    # about the tolerance (the oracle moves by ~1.5e-7 between reduction orders), so that case
+    # is bounded by the CG tolerance; at tol 1e-12 the FP64 bar applies.
+    w = workloads.macau_side(scale=0.05, seed=6)
+    fr, fc, _, shp = w["side"]
+    F = sp.coo_matrix((np.ones(len(fr)), (fr, fc)), shape=shp)
+    rng = np.random.default_rng(1)
+    B = rng.normal(size=(32, shp[1]))
+    oracle_parts(gpu_cg_parts(shp[1]))
+    Xo, ito = orc.blockcg(orc.Csr.from_scipy(F, True), orc.Csr.from_scipy(F.T, True), 3.0, B.T,
+                          tol, 32, 8)
+    X, it, _ = _lib.blockcg_raw(fr, fc, None, shp, B, 3.0, tol, _lib.MG_COMPUTE_FP64)
+    assert abs(it - ito) <= 1
+    assert relerr(X.T, Xo) < bar
+
+
+def test_blockcg_fp32_with_fp64_residual_replacement():
+    w = workloads.macau_side(scale=0.05, seed=6)
+    fr, fc, _, shp = w["side"]
+    F = sp.coo_matrix((np.ones(len(fr)), (fr, fc)), shape=shp)
+    rng = np.random.default_rng(1)
+    B = rng.normal(size=(32, shp[1]))
+    Xd, itd, _ = _lib.blockcg_raw(fr, fc, None, shp, B, 3.0, 1e-6, _lib.MG_COMPUTE_FP64)
+    Xf, itf, _ = _lib.blockcg_raw(fr, fc, None, shp, B, 3.0, 1e-6, _lib.MG_COMPUTE_MIXED)
+    A = (F.T @ F).toarray() + 3.0 * np.eye(shp[1])
+    res = np.linalg.norm(A @ Xf.T - B.T, axis=0) / np.linalg.norm(B.T, axis=0)
+    assert res.max() < 1e-5
+    assert relerr(Xf, Xd) < 1e-5
+    assert itf <= 2 * itd
+
+
+def test_mixed_row_sampler_within_tolerance():
+    rng = np.random.default_rng(8)
+    K = 32
+    w = small_uniform(seed=3, nrow=500, ncol=300, nobs=20000)
+    s = gpu_sampler(w, K, 2.0, seed=1, compute=_lib.MG_COMPUTE_MIXED)
+    V = rng.normal(scale=0.3, size=(w["shape"][1], K))
+    s.set_latents(1, V)
+    mu, Lam, _ = s.hyper(0)
+    z = rng.normal(size=(w["shape"][0], K))
+    s.sample_latents(0, 0, z)
+    Y = train_matrix(w)
+    want, _ = orc.sample_latents(K, orc.Csr.from_scipy(Y), V, s.mean_value(), 2.0, mu, Lam, z=z)
+    assert relerr(s.latents(0), want) < MIXED_SAMPLE_TOL
+
+
+def test_cholesky_failure_is_reported_and_context_survives():
+    w = small_uniform(seed=4)
+    K = 6
+    s = gpu_sampler(w, K, 1.0, seed=1)
+    s.set_hyper(0, np.zeros(K), -10.0 * np.eye(K))
+    with pytest.raises(_lib.CholeskyError, match="Cholesky Decomposition failed"):
+        s.sample_latents(0, 0)
+    s.init()
+    s.sweep(0)
+    assert np.isfinite(s.latents(0)).all()
+
+
+def test_eval_rmse_golden_on_gpu():  # tests.cpp:552-591 through mg_eval
+    w = dict(rows=np.array([0], np.int32), cols=np.array([0], np.int32), vals=np.array([2.0]),
+             trows=np.array([0], np.int32), tcols=np.array([0], np.int32),
+             tvals=np.array([4.5]), shape=(1, 1))
+    s = gpu_sampler(w, 2, 1.0, seed=0)
+    steps = [([1.0, 0.0], [1.0, 0.0], 3.0, 0.0, 1.5, 1.5),
+             ([2.0, 0.0], [1.0, 0.0], 3.5, 0.5, 0.5, 1.0),
+             ([2.0, 0.0], [3.0, 0.0], 5.0, 14.0, 3.5, 0.5)]
+    for n, (u, v, pred, var, r1, ravg) in enumerate(steps):
+        s.set_latents(0, np.array([u]))
+        s.set_latents(1, np.array([v]))
+        s.eval(n)
+        got_r, got_r1 = s.rmse()
+        assert got_r1 == pytest.approx(r1) and got_r == pytest.approx(ravg)
+        assert s.predictions()[0] == pytest.approx(pred)
+    s.set_samples(0, 3)
+    assert s.stds()[0] == pytest.approx(np.sqrt(14.0 / 2))

@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark of the Gibbs-sweep hot path: sweeps/s of BPMF at K = 32 on the synthetic
+138,000 x 27,000 matrix with 20M power-law observations (alpha = 2), mixed-precision batched
+sampler vs the FP64 sampler, both on one B200, with the CPU oracle timed beside them.
+
+A step is one Gibbs sweep (sample both modes, update both Normal-Wishart priors; test-set
+evaluation excluded from the timed region and reported separately).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is the mixed-precision sweep rate with the data already resident in HBM, timed with CUDA
+events on the library's stream; `e2e` is the same metric through the C ABI with host buffers
+(data upload and CSR build, per-sweep RMSE read-back and the final prediction read-back inside
+the timed region).  `--impl reference` times the CPU oracle (FP64 restatement of the reference,
+OpenMP on all host cores).  Under torchrun each rank runs an independent chain on its own GPU.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gibbs sweeps/s at K=32: mixed-prec batched vs FP64 plain, equal test RMSE"
+UNIT = "sweeps/s"
+K_LATENT = 32
+ALPHA = 2.0
+PROFILE_SUMMARY = ROOT / "profiles" / "k_sample_mixed_bpmf_powerlaw_k32.txt"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = full size)")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0,
+                    help="budget of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="sweeps of the e2e run (0: = steps)")
+    ap.add_argument("--only", choices=["all", "mixed", "fp64"], default="all",
+                    help="profiling runs: time one sampler and print its phase times only")
+    return ap.parse_args()
+
+
+def workload(scale, seed):
+    from macau_b200 import workloads
+    return workloads.bpmf_powerlaw(seed=seed, scale=scale)
+
+
+def config_dict(w, args, n):
+    return {"workload": w["name"], "K": K_LATENT, "alpha": ALPHA,
+            "holdout": "10% random", "rows": w["shape"][0], "cols": w["shape"][1],
+            "ntrain": int(len(w["vals"])), "ntest": int(len(w["tvals"])),
+            "parallelism": f"independent chains x{n}" if n > 1 else "single GPU",
+            "l2": "inputs larger than L2 (per sweep the two CSR streams are >=290 MB)",
+            "eval": "excluded from the timed sweeps"}
+
+
+# ------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id=None):
+        self.bus_id = (bus_id or "").lower()
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 10:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        time.sleep(0.2)
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = self.rows
+        if self.bus_id:
+            mine = [r for r in rows if self.bus_id.endswith(r[1].lower()[-12:]) or
+                    r[1].lower().endswith(self.bus_id[-12:])]
+            rows = mine or rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[4]) for r in rows
+                                                         if r[4].replace(".", "").isdigit())
+                if any(r[4].replace(".", "").isdigit() for r in rows) else None}
+
+
+# ------------------------------------------------------------------------ helpers
+def make_sampler(w, compute, seed, device, burnin=10 ** 6, nsamples=1):
+    from macau_b200 import _lib
+    s = _lib.Sampler(K_LATENT, ALPHA, seed=seed, compute=compute, device=device)
+    s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
+    s.set_relation_data_test(w["trows"], w["tcols"], w["tvals"], w["shape"])
+    s.set_samples(burnin, nsamples)
+    s.init()
+    return s
+
+
+def sampler_bytes(st, w, compute, mode):
+    """Algorithmic bytes of one latent-sampler launch (mode 0 = rows, 1 = columns): the CSR
+    stream, the task list, one compulsory read of the other factor and the latent writes."""
+    KP = 32
+    N = w["shape"][mode]
+    No = w["shape"][1 - mode]
+    nnz = st["nnz"][mode]
+    tasks = st["ntasks"][mode] * 32
+    if compute == "mixed":
+        return nnz * 8 + tasks + No * KP * 2 + N * KP * (4 + 2)
+    return nnz * (4 + 8) + tasks + No * KP * 8 + N * KP * 8
+
+
+def sampler_flops(w, st, mode):
+    """Algorithmic flops of one sampler launch: lower-triangle Gram (K(K+1) per entry), the
+    right-hand side (2K per entry), Cholesky + two solves + Lambda mu per row."""
+    K = K_LATENT
+    N = w["shape"][mode]
+    return st["nnz"][mode] * (K * (K + 1) + 2 * K) + N * (K ** 3 / 3 + 6 * K * K)
+
+
+def read_traffic():
+    """DRAM bytes per sampler launch from the committed ncu summary (one capture), if any."""
+    try:
+        for line in PROFILE_SUMMARY.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def peaks():
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+def cpu_baseline(w, budget_s, sweeps_max):
+    """Times the CPU oracle (FP64 restatement, all host cores) on full sweeps of the same data."""
+    from oracle import oracle as orc
+    from tests.gpu_helpers import oracle_model
+    cores = orc.set_threads(os.cpu_count() or 1)
+    m = oracle_model(w, K_LATENT, ALPHA, 0)
+    t0 = time.perf_counter()
+    m.sweep(0, 10 ** 6)
+    t1 = time.perf_counter() - t0
+    n = int(max(1, min(sweeps_max, math.floor(budget_s / max(t1, 1e-9)) - 1)))
+    t0 = time.perf_counter()
+    for i in range(n):
+        m.sweep(1 + i, 10 ** 6)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} full FP64 sweeps (after 1 untimed) of {w['name']}, K=32"}
+
+
+# ------------------------------------------------------------------------ arms
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = workload(args.scale, 2)
+    from oracle import oracle as orc
+    from tests.gpu_helpers import oracle_model
+    cores = orc.set_threads(os.cpu_count() or 1)
+    m = oracle_model(w, K_LATENT, ALPHA, 0)
+    for i in range(args.warmup):
+        m.sweep(i, 10 ** 6)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        m.sweep(args.warmup + i, 10 ** 6)
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded power-law stand-in, no dataset read)",
+            "config": config_dict(w, args, 1), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full FP64 sweeps after {args.warmup} warm-up"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    from macau_b200 import _lib
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    import torch
+    bus = None
+    try:
+        props = torch.cuda.get_device_properties(local)
+        bus = getattr(props, "pci_bus_id", None)
+        if isinstance(bus, int):
+            bus = "%02x:00" % bus
+    except Exception:
+        pass
+
+    w = workload(args.scale, 2)
+    seed = 1000 + rank
+    K, W = args.steps, args.warmup
+    if args.only != "all":
+        comp = _lib.MG_COMPUTE_MIXED if args.only == "mixed" else _lib.MG_COMPUTE_FP64
+        s = make_sampler(w, comp, seed, local)
+        s.time_sweeps(0, max(W, 1), eval=False)
+        t, _ = s.time_sweeps(W, K, eval=False)
+        _, ph = s.time_sweeps(W + K, K, eval=False, phase_events=True)
+        print(json.dumps({"only": args.only, "workload": w["name"], "ms_per_step": t / K * 1e3,
+                          "phase_ms": [x / K * 1e3 for x in ph], "stats": s.stats()}), flush=True)
+        s.close()
+        return 0
+    # ---- mixed-precision batched sampler: headline value ----
+    mx = make_sampler(w, _lib.MG_COMPUTE_MIXED, seed, local)
+    mx.time_sweeps(0, max(W, 1), eval=False)
+    barrier()
+    with ClockSampler(bus) as clk:
+        t_mx, _ = mx.time_sweeps(W, K, eval=False)
+    t_mx = max_over_ranks(t_mx)
+    st_mx = mx.stats()
+    kernels_per_sweep = st_mx["kernel_launches"] / max(1, st_mx["sweeps"])
+    # per-kernel durations for the roofline (same kernels, un-captured, events between phases)
+    _, ph = mx.time_sweeps(W + K, min(K, 50), eval=False, phase_events=True)
+    nph = min(K, 50)
+    # test RMSE after the chain continues with evaluation (posterior mean over 20 sweeps)
+    mx.set_samples(W + K + nph, 20)
+    mx.sweeps(W + K + nph, 20, eval=True)
+    rmse_mx = mx.rmse()[0]
+    retries = st_mx["retries"]
+    mx.close()
+    # ---- FP64 plain sampler ----
+    fp = make_sampler(w, _lib.MG_COMPUTE_FP64, seed, local)
+    fp.time_sweeps(0, max(W, 1), eval=False)
+    barrier()
+    t_fp, _ = fp.time_sweeps(W, K, eval=False)
+    t_fp = max_over_ranks(t_fp)
+    _, ph_fp = fp.time_sweeps(W + K, min(K, 20), eval=False, phase_events=True)
+    fp.set_samples(W + K + min(K, 20), 20)
+    fp.sweeps(W + K + min(K, 20), 20, eval=True)
+    rmse_fp = fp.rmse()[0]
+    st_fp = fp.stats()
+    fp.close()
+    # ---- e2e through the C ABI with host buffers ----
+    E = args.e2e_steps or K
+    barrier()
+    h2d0, d2h0 = st_fp["h2d_bytes"], st_fp["d2h_bytes"]
+    t0 = time.perf_counter()
+    s = _lib.Sampler(K_LATENT, ALPHA, seed=seed, compute=_lib.MG_COMPUTE_MIXED, device=local)
+    s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
+    s.set_relation_data_test(w["trows"], w["tcols"], w["tvals"], w["shape"])
+    s.set_samples(0, E)
+    s.init()
+    for i in range(E):
+        s.sweep(i, eval=True)
+        s.rmse()
+    preds = s.predictions()
+    t_e2e = time.perf_counter() - t0
+    st_e = s.stats()
+    s.close()
+    t_e2e = max_over_ranks(t_e2e)
+    h2d = st_e["h2d_bytes"] - h2d0
+    d2h = st_e["d2h_bytes"] - d2h0
+    del preds
+
+    # ---- roofline of the dominant kernel (latent sampler, both modes) ----
+    hbm, tflops, src = peaks()
+    b = sampler_bytes(st_mx, w, "mixed", 0) + sampler_bytes(st_mx, w, "mixed", 1)
+    t_launch = (ph[0] + ph[1]) / (2 * nph)     # mean seconds per sampler launch
+    achieved = b / 2 / t_launch / 1e9
+    traffic = read_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
+                "kernel": "k_sample (latent sampler, mixed), mean of the two modes",
+                "algorithmic_bytes_per_launch": b / 2,
+                "gram_tflops": (sampler_flops(w, st_mx, 0) + sampler_flops(w, st_mx, 1))
+                / (ph[0] + ph[1]) * nph / 1e12,
+                "gram_tflops_peak_bf16": tflops}
+    v_mx = world * K / t_mx
+    v_fp = world * K / t_fp
+    line = {"metric": METRIC, "value": v_mx, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": t_mx / K * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16-gram/f32-chol/f64-hyper",
+            "data": "synthetic (seeded power-law stand-in, no dataset read)",
+            "config": config_dict(w, args, world),
+            "fp64_value": v_fp, "fp64_ms_per_step": t_fp / K * 1e3,
+            "mixed_over_fp64": v_mx / v_fp,
+            "test_rmse": {"mixed": rmse_mx, "fp64": rmse_fp,
+                          "note": "posterior mean of 20 evaluated sweeps after the timed ones"},
+            "phase_ms": {"mixed": [x / nph * 1e3 for x in ph],
+                         "fp64": [x / min(K, 20) * 1e3 for x in ph_fp],
+                         "order": ["sample0", "sample1", "prior0", "prior1", "eval"]},
+            "retries_fp64_refactor": retries,
+            "gpu_launches": int(round(kernels_per_sweep * K)),
+            "clocks": clk.summary(), "roofline": roofline,
+            "e2e": {"value": world * E / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d / E,
+                    "d2h_bytes_per_step": d2h / E,
+                    "timed": "C-ABI run: data upload + CSR build, init, sweeps with eval and "
+                             "RMSE read-back, final predictions read-back"}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds, 50)
+        line["mixed_over_cpu"] = v_mx / line["cpu_baseline"]["value"]
+        line["fp64_over_cpu"] = v_fp / line["cpu_baseline"]["value"]
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

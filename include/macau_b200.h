@@ -61,6 +61,11 @@ typedef struct mg_stats {
   int64_t rows_sampled[2];  /* rows sampled, per mode (cumulative) */
   int cg_iters[2];          /* block-CG iterations of the last beta update, per mode */
   int graph_captured;       /* 1 when sweeps replay a captured CUDA graph */
+  int64_t kernel_launches;  /* kernels launched by sweeps / phases since mg_init */
+  int64_t h2d_bytes;        /* host->device bytes copied by the library (process total) */
+  int64_t d2h_bytes;        /* device->host bytes copied by the library (process total) */
+  int64_t ntasks[2];        /* latent-sampler work items per mode (rows + split parts) */
+  int64_t nnz[2];           /* training entries per mode after duplicate summing */
 } mg_stats;
 
 /* Context lifetime.  Replaces `make_macau_fixed(2, K, precision)` (macau.cpp:214-220) plus
@@ -104,6 +109,15 @@ int mg_sweep(mg_ctx* ctx, int iter, int eval);
 /* `count` consecutive sweeps starting at `first_iter` without returning to the caller in
  * between (no per-sweep host synchronisation). */
 int mg_sweeps(mg_ctx* ctx, int first_iter, int count, int eval);
+
+/* Device time of `count` sweeps starting at `first_iter`, measured with CUDA events on the
+ * context's stream (benchmark support; no reference counterpart).  With phase_events = 0 the
+ * sweeps run as they would in mg_sweeps (captured graph when possible) and *total_seconds
+ * receives the elapsed time; with phase_events = 1 they run un-captured with events between
+ * phases and phase_seconds[0..4] receives the summed time of sample mode 0, sample mode 1,
+ * update prior 0, update prior 1, evaluation. */
+int mg_time_sweeps(mg_ctx* ctx, int first_iter, int count, int eval, int phase_events,
+                   double* total_seconds, double* phase_seconds);
 
 /* MacauX::run (macau.cpp:94-148): mg_init, then burnin + nsamples sweeps with evaluation. */
 int mg_run(mg_ctx* ctx);

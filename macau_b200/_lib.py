@@ -38,7 +38,9 @@ class MgStats(C.Structure):
     _fields_ = [("sweeps", C.c_double), ("seconds_sample", C.c_double),
                 ("seconds_prior", C.c_double), ("seconds_eval", C.c_double),
                 ("retries", C.c_int64 * 2), ("rows_sampled", C.c_int64 * 2),
-                ("cg_iters", C.c_int * 2), ("graph_captured", C.c_int)]
+                ("cg_iters", C.c_int * 2), ("graph_captured", C.c_int),
+                ("kernel_launches", C.c_int64), ("h2d_bytes", C.c_int64),
+                ("d2h_bytes", C.c_int64), ("ntasks", C.c_int64 * 2), ("nnz", C.c_int64 * 2)]
 
 
 _p = C.c_void_p
@@ -58,6 +60,7 @@ _SIGS = {
     "mg_sweep": (_i, [_p, _i, _i]),
     "mg_sweeps": (_i, [_p, _i, _i, _i]),
     "mg_run": (_i, [_p]),
+    "mg_time_sweeps": (_i, [_p, _i, _i, _i, _i, _p, _p]),
     "mg_sample_latents": (_i, [_p, _i, _i, _p]),
     "mg_update_prior": (_i, [_p, _i, _i]),
     "mg_eval": (_i, [_p, _i]),
@@ -178,6 +181,15 @@ class Sampler:
     def sweeps(self, first, count, eval=True):
         self._chk(lib().mg_sweeps(self.h, int(first), int(count), int(bool(eval))))
 
+    def time_sweeps(self, first, count, eval=False, phase_events=False):
+        """Device seconds of `count` sweeps (CUDA events on the library stream); with
+        phase_events also the per-phase seconds [sample0, sample1, prior0, prior1, eval]."""
+        tot = np.zeros(1)
+        ph = np.zeros(5)
+        self._chk(lib().mg_time_sweeps(self.h, int(first), int(count), int(bool(eval)),
+                                       int(bool(phase_events)), ptr(tot), ptr(ph)))
+        return float(tot[0]), ph
+
     def run(self):
         self._chk(lib().mg_run(self.h))
 
@@ -254,7 +266,9 @@ class Sampler:
         self._chk(lib().mg_get_stats(self.h, C.byref(st)))
         return {"sweeps": st.sweeps, "retries": list(st.retries),
                 "rows_sampled": list(st.rows_sampled), "cg_iters": list(st.cg_iters),
-                "graph_captured": bool(st.graph_captured)}
+                "graph_captured": bool(st.graph_captured),
+                "kernel_launches": int(st.kernel_launches), "h2d_bytes": int(st.h2d_bytes),
+                "d2h_bytes": int(st.d2h_bytes), "ntasks": list(st.ntasks), "nnz": list(st.nnz)}
 
 
 def blockcg_raw(rows, cols, vals, shape, B, reg, tol, compute=MG_COMPUTE_FP64):

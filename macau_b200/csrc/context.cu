@@ -29,6 +29,10 @@
 namespace mg {
 namespace {
 
+// Host<->device byte counters of the current process (reported through mg_stats).
+long long g_h2d_bytes = 0;
+long long g_d2h_bytes = 0;
+
 template <typename T>
 struct DBuf {
   T* p = nullptr;
@@ -55,6 +59,7 @@ struct DBuf {
   void upload(const T* h, size_t count, cudaStream_t s) {
     alloc(count);
     if (count) MG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    g_h2d_bytes += (long long)(count * sizeof(T));
   }
 };
 
@@ -356,17 +361,19 @@ class Context {
     retries_[0] = retries_[1] = 0;
     rows_[0] = rows_[1] = 0;
     sweeps_done_ = 0;
+    launches_ = 0;
     t_sample_ = t_prior_ = t_eval_ = 0.0;
     drop_graphs();
     initialised_ = true;
   }
 
   // ---- phases ----
-  void sample(int mode, const double* znoise_dev) {
+  void sample(int mode, const double* znoise_dev, bool reset_queue = true) {
+    launches_ += 1;
     ModeData& md = md_[mode];
     Prior& p = prior_[mode];
     const int other = 1 - mode;
-    MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[mode], 0, sizeof(uint32_t), s_));
+    if (reset_queue) MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[mode], 0, sizeof(uint32_t), s_));
     SampleParams sp{};
     sp.tasks = md.tasks.p;
     sp.ntasks = md.ntasks;
@@ -403,6 +410,7 @@ class Context {
   void update_prior(int mode) {
     Prior& p = prior_[mode];
     const long long N = dims_[mode];
+    launches_ += p.macau ? 0 : 2;  // Macau launches are counted by kernels_in_cg below
     const int nb = stats_blocks(N);
     launch_stats(latents(mode), mixed_, p.macau ? p.uhat.p : nullptr, N, K_, KP_, KP_,
                  stat_partials_.p, nb, s_);
@@ -425,6 +433,8 @@ class Context {
                       mode, p.B.p, CP_, s_);
     p.cg_iters = p.cg.solve(p.F, p.Ft, 0.0, p.lambda_beta.p, p.B.p, CP_, K_, p.tol, p.beta.p,
                             CP_, ctl_.p, s_, mixed_);
+    // stats x2, NW, chol, tmp, spmm, noise, uhat spmm, lambda_beta + the CG's launches
+    launches_ += 9 + 6 + 8LL * p.cg_iters;
     // compute_uhat (linop.h:196-198): Uhat = beta F^T, one K-vector per row of F
     launch_spmm(p.F, p.beta.p, CP_, p.uhat.p, KP_, K_, false, s_);
     // sample_lambda_beta with the new beta and Lambda (latentprior.cpp:263)
@@ -435,6 +445,7 @@ class Context {
 
   void eval(int n_fixed) {
     if (ntest_ == 0) return;
+    launches_ += 2;
     launch_eval(trow_.p, tcol_.p, tval_.p, ntest_, latents(0), latents(1), mixed_, K_, KP_,
                 mean_, n_fixed, ctl_.p, pred_.p, pvar_.p, eval_partials_.p,
                 eval_blocks(ntest_), rmse_.p, s_);
@@ -442,18 +453,82 @@ class Context {
 
   bool graphable() const { return !prior_[0].macau && !prior_[1].macau; }
 
-  void sweep_body(bool do_eval) {
-    sample(0, nullptr);
-    sample(1, nullptr);
+  // One sweep; ev (optional, 6 events) brackets: sample 0 | sample 1 | prior 0 | prior 1 |
+  // eval + advance.
+  void sweep_body(bool do_eval, cudaEvent_t* ev = nullptr) {
+    MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[0], 0, 2 * sizeof(uint32_t), s_));
+    if (ev) MG_CUDA(cudaEventRecord(ev[0], s_));
+    sample(0, nullptr, false);
+    if (ev) MG_CUDA(cudaEventRecord(ev[1], s_));
+    sample(1, nullptr, false);
+    if (ev) MG_CUDA(cudaEventRecord(ev[2], s_));
     update_prior(0);
+    if (ev) MG_CUDA(cudaEventRecord(ev[3], s_));
     update_prior(1);
+    if (ev) MG_CUDA(cudaEventRecord(ev[4], s_));
     if (do_eval) eval(-1);
     launch_advance(ctl_.p, s_);
+    launches_ += 1;
+    if (ev) MG_CUDA(cudaEventRecord(ev[5], s_));
+  }
+
+  // Device time of `count` sweeps: total between two events on the library stream; with
+  // phase_events the sweeps run un-captured with events between phases and phase[0..4]
+  // receives the summed seconds of sample 0, sample 1, prior 0, prior 1, eval.
+  void time_sweeps(int first_iter, int count, bool do_eval, bool phase_events, double* total,
+                   double* phase) {
+    if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_init first");
+    if (!phase_events) {
+      // make sure the graph exists before the timed region
+      if (graphable() && use_graph_ && !graph_[do_eval ? 1 : 0]) {
+        sweeps(first_iter, 1, do_eval, true);
+        first_iter++;
+        count--;
+      }
+      MG_CUDA(cudaStreamSynchronize(s_));
+      MG_CUDA(cudaEventRecord(ev0_, s_));
+      sweeps(first_iter, count, do_eval, false);
+      MG_CUDA(cudaEventRecord(ev1_, s_));
+      MG_CUDA(cudaEventSynchronize(ev1_));
+      float ms = 0.f;
+      MG_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+      if (total) *total = ms * 1e-3;
+      check_status();
+      return;
+    }
+    std::vector<cudaEvent_t> ev((size_t)count * 6);
+    for (auto& e : ev) MG_CUDA(cudaEventCreate(&e));
+    try {
+      launch_set_sweep(ctl_.p, (uint32_t)first_iter, burnin_, s_);
+      for (int i = 0; i < count; i++) sweep_body(do_eval, ev.data() + 6 * (size_t)i);
+      rows_[0] += md_[0].N * count;
+      rows_[1] += md_[1].N * count;
+      sweeps_done_ += count;
+      MG_CUDA(cudaEventSynchronize(ev.back()));
+      double ph[5] = {0, 0, 0, 0, 0};
+      for (int i = 0; i < count; i++)
+        for (int q = 0; q < 5; q++) {
+          float ms = 0.f;
+          MG_CUDA(cudaEventElapsedTime(&ms, ev[6 * i + q], ev[6 * i + q + 1]));
+          ph[q] += ms * 1e-3;
+        }
+      float ms = 0.f;
+      MG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev.back()));
+      if (total) *total = ms * 1e-3;
+      if (phase)
+        for (int q = 0; q < 5; q++) phase[q] = ph[q];
+    } catch (...) {
+      for (auto& e : ev) cudaEventDestroy(e);
+      throw;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    check_status();
   }
 
   void check_status() {
     Ctl h;
     MG_CUDA(cudaMemcpyAsync(&h, ctl_.p, sizeof(Ctl), cudaMemcpyDeviceToHost, s_));
+    g_d2h_bytes += sizeof(Ctl);
     MG_CUDA(cudaStreamSynchronize(s_));
     retries_[0] = h.retries[0];
     retries_[1] = h.retries[1];
@@ -479,8 +554,11 @@ class Context {
         count--;
         cudaGraph_t g = nullptr;
         MG_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        const long long before = launches_;
         try {
           sweep_body(do_eval);
+          graph_kernels_[do_eval ? 1 : 0] = launches_ - before;
+          launches_ = before;
         } catch (...) {
           cudaStreamEndCapture(s_, &g);
           if (g) cudaGraphDestroy(g);
@@ -491,6 +569,7 @@ class Context {
         cudaGraphDestroy(g);
       }
       for (int i = 0; i < count; i++) MG_CUDA(cudaGraphLaunch(ge, s_));
+      launches_ += graph_kernels_[do_eval ? 1 : 0] * count;
     } else {
       for (int i = 0; i < count; i++) sweep_body(do_eval);
     }
@@ -546,12 +625,14 @@ class Context {
     if (mixed_) {
       std::vector<float> h((size_t)N * KP_);
       MG_CUDA(cudaMemcpyAsync(h.data(), lat32_[mode].p, h.size() * 4, cudaMemcpyDeviceToHost, s_));
+      g_d2h_bytes += (long long)h.size() * 4;
       MG_CUDA(cudaStreamSynchronize(s_));
       for (long long n = 0; n < N; n++)
         for (int k = 0; k < K_; k++) out[n * K_ + k] = h[n * KP_ + k];
     } else {
       MG_CUDA(cudaMemcpy2DAsync(out, K_ * 8, lat64_[mode].p, KP_ * 8, K_ * 8, N,
                                 cudaMemcpyDeviceToHost, s_));
+      g_d2h_bytes += (long long)N * K_ * 8;
       MG_CUDA(cudaStreamSynchronize(s_));
     }
   }
@@ -616,11 +697,13 @@ class Context {
       return;
     }
     MG_CUDA(cudaMemcpyAsync(r, rmse_.p, 16, cudaMemcpyDeviceToHost, s_));
+    g_d2h_bytes += 16;
     MG_CUDA(cudaStreamSynchronize(s_));
   }
   void get_predictions(double* out) {
     if (ntest_ == 0) return;
     MG_CUDA(cudaMemcpyAsync(out, pred_.p, ntest_ * 8, cudaMemcpyDeviceToHost, s_));
+    g_d2h_bytes += ntest_ * 8;
     MG_CUDA(cudaStreamSynchronize(s_));
   }
   // MacauX::getStds (macau.cpp:175-188)
@@ -631,6 +714,7 @@ class Context {
       return;
     }
     MG_CUDA(cudaMemcpyAsync(out, pvar_.p, ntest_ * 8, cudaMemcpyDeviceToHost, s_));
+    g_d2h_bytes += ntest_ * 8;
     MG_CUDA(cudaStreamSynchronize(s_));
     const double inorm = 1.0 / (nsamples_ - 1);
     for (long long i = 0; i < ntest_; i++) out[i] = std::sqrt(out[i] * inorm);
@@ -658,6 +742,13 @@ class Context {
     st->cg_iters[0] = prior_[0].cg_iters;
     st->cg_iters[1] = prior_[1].cg_iters;
     st->graph_captured = (graph_[0] || graph_[1]) ? 1 : 0;
+    st->kernel_launches = launches_;
+    st->h2d_bytes = g_h2d_bytes;
+    st->d2h_bytes = g_d2h_bytes;
+    st->ntasks[0] = md_[0].ntasks;
+    st->ntasks[1] = md_[1].ntasks;
+    st->nnz[0] = md_[0].nnz;
+    st->nnz[1] = md_[1].nnz;
   }
   void dims(int64_t* nrow, int64_t* ncol, int64_t* ntrain, int64_t* ntest, double* mean) {
     if (nrow) *nrow = dims_[0];
@@ -775,6 +866,8 @@ class Context {
   cudaGraphExec_t graph_[2] = {nullptr, nullptr};
   long long retries_[2] = {0, 0}, rows_[2] = {0, 0};
   long long sweeps_done_ = 0;
+  long long launches_ = 0;
+  long long graph_kernels_[2] = {0, 0};
   double t_sample_ = 0, t_prior_ = 0, t_eval_ = 0;
 };
 
@@ -872,6 +965,14 @@ int mg_sweep(mg_ctx* ctx, int iter, int eval) {
 int mg_sweeps(mg_ctx* ctx, int first_iter, int count, int eval) {
   if (count < 0) return MG_ERR_ARG;
   return guarded(ctx, [&](mg::Context& c) { c.sweeps(first_iter, count, eval != 0, true); });
+}
+
+int mg_time_sweeps(mg_ctx* ctx, int first_iter, int count, int eval, int phase_events,
+                   double* total_seconds, double* phase_seconds) {
+  if (count < 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) {
+    c.time_sweeps(first_iter, count, eval != 0, phase_events != 0, total_seconds, phase_seconds);
+  });
 }
 
 int mg_run(mg_ctx* ctx) {

@@ -79,6 +79,8 @@ _SIGS = {
     "mg_set_option": (_i, [_p, C.c_char_p, _i]),
     "mg_blockcg": (_i, [_p, _p, _p, _i64, _i, _i, _p, _i, _d, _d, _i, _p, C.POINTER(_i),
                         C.POINTER(_d)]),
+    "mg_normal_wishart_noalloc": (_i, [_p, _i64, _i, _i, _p, _d, _p, _i, C.c_uint64, C.c_uint32,
+                                       _i, _p, _p, _p, C.c_char_p, _i]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -55,11 +55,20 @@ struct Cfg {
   static constexpr int EV = 16 / sizeof(Elem);  // elements per 16-byte vector load
   static constexpr int VPR = KP / EV;           // vectors per gathered row
   static constexpr size_t kGath = sizeof(Acc) * kChunk * KP;
-  static constexpr size_t kMM = sizeof(double) * KP * LD;
+  // warp-per-row path: Gram tile (KP x LD, Acc) + L^T (KP x (KP+4)) or an FP64 L^T;
+  // multi-warp path: FP64 MM (KP x LD)
+  static constexpr size_t kMMw = sizeof(double) * KP * (KP + 4) > sizeof(Acc) * KP * (LD + KP + 4)
+                                     ? sizeof(double) * KP * (KP + 4)
+                                     : sizeof(Acc) * KP * (LD + KP + 4);
+  static constexpr size_t kMM = WPR == 1 ? (kMMw > sizeof(double) * KP * LD ? kMMw
+                                                                          : sizeof(double) * KP * LD)
+                                         : sizeof(double) * KP * LD;
   static constexpr size_t kWork = (kGath > kMM ? kGath : kMM);
   // work | cidx[kChunk] | cw[kChunk] (double) | rr[KP] (double) | mun[KP] | diag[KP] | bcast[4]
   static constexpr size_t kGroupBytes =
       kWork + sizeof(int) * kChunk + sizeof(double) * (kChunk + 3 * KP) + 16;
+  // CTA-wide Lambda + Lambda mu of the warp-per-row path
+  static constexpr size_t kCtaBytes = WPR == 1 ? sizeof(double) * (KP * (KP + 1) + KP) : 0;
   static_assert(TR >= 1 && TC >= 1 && GR * TR == KP && GC * TC == KP, "tile");
   static_assert(VPR >= 1, "vector width");
 };
@@ -124,15 +133,177 @@ __device__ void add_noise(const SampleParams& p, F* rr, int row, int K, int t, i
   gsync<T>(g);
 }
 
+__device__ __forceinline__ float wshfl(float v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ double wshfl(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+
+__device__ __forceinline__ float mrsqrt(float a) { return rsqrtf(a); }
+__device__ __forceinline__ double mrsqrt(double a) { return rsqrt(a); }
+
+// Vector load of 4 consecutive values from shared memory (16-byte aligned for float).
+template <typename F>
+struct Vec4 {
+  F v[4];
+};
+template <typename F>
+__device__ __forceinline__ Vec4<F> lds4(const F* p) {
+  Vec4<F> r;
+  if constexpr (sizeof(F) == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+  } else {
+    const double2 t0 = *reinterpret_cast<const double2*>(p);
+    const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
+    r.v[0] = t0.x; r.v[1] = t0.y; r.v[2] = t1.x; r.v[3] = t1.y;
+  }
+  return r;
+}
+
+// Warp Cholesky of the KP x KP matrix whose row i is held by lane i in a[] (lower triangle
+// used).  Right-looking over columns: entry (i, k) receives its updates in the order
+// j = 0, 1, ... and is then scaled by 1/L(k, k).  Column j of L is published to shared memory
+// (Lc row j, leading dimension ld, a multiple of 4) and read back as 4-wide broadcasts for the
+// trailing update.  rinv receives the lane's 1/L(i, i).  A pivot that is not positive, or
+// (mixed mode) falls below rel_floor times the original diagonal d0, fails the whole warp.
+// On success Lc holds L^T (row j = column j of L).
+template <typename F, int KP>
+__device__ __forceinline__ bool warp_factor(F (&a)[KP], F& rinv, int lane, double rel_floor,
+                                            F d0, F* Lc, int ld) {
+#pragma unroll
+  for (int j = 0; j < KP; j++) {
+    const F piv = wshfl(a[j], j);
+    const F dj = wshfl(d0, j);
+    if (!(piv > (F)0) || !((double)piv > rel_floor * (double)dj)) return false;
+    const F r = mrsqrt(piv);
+    if (lane == j) {
+      a[j] = piv * r;
+      rinv = r;
+    } else if (lane > j) {
+      a[j] = a[j] * r;
+    }
+    if (lane < KP) Lc[j * ld + lane] = a[j];
+    __syncwarp();
+#pragma unroll
+    for (int q = (j + 1) / 4; q < KP / 4; q++) {
+      const Vec4<F> c = lds4(Lc + j * ld + 4 * q);
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int k = 4 * q + u;
+        if (k > j && lane >= k) a[k] = mfma(-a[j], c.v[u], a[k]);
+      }
+    }
+  }
+  return true;
+}
+
+// y = L^{-1} rr (lane i holds rr_i and row i of L), rr += z, then x = L^{-T} rr with L^T read
+// from Lc (row j = column j of L).  Returns x_i in lane i.
+template <typename F, int KP>
+__device__ __forceinline__ F warp_solve(const F (&a)[KP], F rinv, F rr, int lane, const F* Lc,
+                                        int ld, const SampleParams& p, int row, int K,
+                                        uint32_t sweep) {
+#pragma unroll
+  for (int j = 0; j < KP; j++) {
+    if (lane == j) rr = rr * rinv;
+    const F yj = wshfl(rr, j);
+    if (lane > j) rr = mfma(-a[j], yj, rr);
+  }
+  if (p.znoise) {
+    if (lane < K) rr += (F)p.znoise[(size_t)row * K + lane];
+  } else {
+    double z0, z1;
+    normal_pair(p.seed, sweep, stream_id(kRowNoise, (uint32_t)p.mode), (uint32_t)row,
+                (uint32_t)(lane >> 1), &z0, &z1);
+    if (lane < K) rr += (F)((lane & 1) ? z1 : z0);
+  }
+#pragma unroll
+  for (int j = KP - 1; j >= 0; j--) {
+    if (lane == j) rr = rr * rinv;
+    const F xj = wshfl(rr, j);
+    if (lane < j) rr = mfma(-Lc[lane * ld + j], xj, rr);
+  }
+  __syncwarp();
+  return rr;
+}
+
+// Row i of MM = Lambda + alpha * G for lane i (padded rows / columns of the identity), with G
+// read from the Gram tile in shared memory (row-major, leading dimension ld).
+template <typename F, typename GT, int KP>
+__device__ __forceinline__ void warp_load_mm(F (&a)[KP], F& d0, const GT* Gs, int ld,
+                                             const double* Lam_s, double alpha, int lane, int K) {
+#pragma unroll
+  for (int j = 0; j < KP; j++) {
+    F v;
+    if (lane < K && j < K) {
+      if constexpr (sizeof(F) == 4)
+        v = (float)Lam_s[lane * (KP + 1) + j] + (float)alpha * (float)Gs[lane * ld + j];
+      else
+        v = Lam_s[lane * (KP + 1) + j] + alpha * (double)Gs[lane * ld + j];
+    } else {
+      v = (lane == j) ? (F)1 : (F)0;
+    }
+    a[j] = v;
+    if (j == lane) d0 = v;
+  }
+}
+
+// FP64 finish of one row by one warp: MM = Lambda + alpha * G from the Gram tile Gs, Cholesky,
+// solves and noise in FP64 (the FP64 path, and the retry of a row whose FP32 factor failed).
+// Kept out of line so the FP32 path's register budget does not pay for it.  Writes the row and
+// returns true, or returns false when the FP64 factor fails too.
+template <int KP, typename GT>
+__device__ __noinline__ bool warp_finish_f64(const GT* Gs, int ld, const double* Lam_s,
+                                             double rac_lm, const SampleParams& p, int row,
+                                             uint32_t sweep, unsigned char* work) {
+  const int lane = threadIdx.x & 31;
+  const int K = p.K;
+  double a[KP], d0 = 1.0, rinv = 1.0;
+  warp_load_mm<double, GT, KP>(a, d0, Gs, ld, Lam_s, p.alpha, lane, K);
+  __syncwarp();
+  double* Lc = reinterpret_cast<double*>(work);  // the Gram tile has been read into a[]
+  if (!warp_factor<double, KP>(a, rinv, lane, 0.0, d0, Lc, KP + 4)) return false;
+  const double x = warp_solve<double, KP>(a, rinv, rac_lm, lane, Lc, KP + 4, p, row, K, sweep);
+  if (lane < K) {
+    if (p.out_f64) {
+      p.out_f64[(size_t)row * KP + lane] = x;
+    } else {
+      p.out_f32[(size_t)row * KP + lane] = (float)x;
+      p.out_bf16[(size_t)row * KP + lane] = __float2bfloat16_rn((float)x);
+    }
+  }
+  return true;
+}
+
+// Minimum resident CTAs requested from the register allocator (warp-per-row instances: 16
+// warps per SM for FP32 Grams, 12 for FP64).
+template <int WPR, bool MIXED>
+constexpr int min_ctas() { return WPR == 1 ? (MIXED ? 4 : 3) : 1; }
+
 template <int KP, int WPR, int G, bool MIXED>
-__global__ void __launch_bounds__(32 * WPR * G) k_sample(const SampleParams p) {
+__global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_sample(const SampleParams p) {
   using C = Cfg<KP, WPR, MIXED>;
   using Acc = typename C::Acc;
   using Elem = typename C::Elem;
   constexpr int T = C::T, GR = C::GR, GC = C::GC, TR = C::TR, TC = C::TC, LD = C::LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int g = threadIdx.x / T, t = threadIdx.x % T;
-  unsigned char* base = smem_raw + (size_t)g * C::kGroupBytes;
+  unsigned char* base = smem_raw + C::kCtaBytes + (size_t)g * C::kGroupBytes;
+  // warp-per-row path: Lambda (row-major, ld KP+1) and, for BPMF, Lambda mu once per CTA
+  double* Lam_s = reinterpret_cast<double*>(smem_raw);
+  double* lmu_s = Lam_s + KP * (KP + 1);
+  if constexpr (WPR == 1) {
+    for (int e = threadIdx.x; e < KP * KP; e += blockDim.x) {
+      const int i = e / KP, j = e % KP;
+      Lam_s[i * (KP + 1) + j] = (i < p.K && j < p.K) ? p.Lambda[i + j * p.K] : 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x < KP) {
+      double sacc = 0.0;
+      if ((int)threadIdx.x < p.K)
+        for (int j = 0; j < p.K; j++) sacc += Lam_s[threadIdx.x * (KP + 1) + j] * p.mu[j];
+      lmu_s[threadIdx.x] = sacc;
+    }
+    __syncthreads();
+  }
   Acc* gath = reinterpret_cast<Acc*>(base);
   int* cidx = reinterpret_cast<int*>(base + C::kWork);
   double* cw = reinterpret_cast<double*>(cidx + kChunk);
@@ -256,6 +427,56 @@ __global__ void __launch_bounds__(32 * WPR * G) k_sample(const SampleParams p) {
 
     // ---- finish the row ----
     const int row = tk.row;
+    if constexpr (WPR == 1) {
+      // Gram tile -> shared memory (row-major, ld LD), then lane i owns row i of MM.
+      Acc* Gs = reinterpret_cast<Acc*>(base);
+#pragma unroll
+      for (int i = 0; i < TR; i++)
+#pragma unroll
+        for (int j = 0; j < TC; j++) Gs[(rt * TR + i) * LD + ct * TC + j] = acc[i][j];
+      __syncwarp();
+      const int lane = t;
+      const Acc rac = wshfl(racc, lane < KP ? lane : 0);  // rhs accumulator of component lane
+      double lm;
+      if (p.uhat) {  // Macau prior mean mu + Uhat[row]
+        const double mun = lane < K ? p.mu[lane] + p.uhat[(size_t)row * KP + lane] : 0.0;
+        lm = 0.0;
+        for (int j = 0; j < K; j++) {
+          const double mj = wshfl(mun, j);
+          if (lane < K) lm += Lam_s[lane * (KP + 1) + j] * mj;
+        }
+      } else {
+        lm = lane < KP ? lmu_s[lane] : 0.0;
+      }
+      bool ok = false;
+      if constexpr (MIXED) {
+        float a[KP], d0 = 1.f, rinv = 1.f;
+        warp_load_mm<float, float, KP>(a, d0, reinterpret_cast<const float*>(Gs), LD, Lam_s,
+                                       p.alpha, lane, K);
+        // L^T goes after the Gram tile, which must stay readable for an FP64 retry
+        float* Lc = reinterpret_cast<float*>(base) + KP * LD;
+        ok = warp_factor<float, KP>(a, rinv, lane, 0x1p-20, d0, Lc, KP + 4);
+        if (ok) {
+          const float x = warp_solve<float, KP>(a, rinv, (float)((double)rac + lm), lane, Lc,
+                                                KP + 4, p, row, K, sweep);
+          if (lane < K) {
+            p.out_f32[(size_t)row * KP + lane] = x;
+            p.out_bf16[(size_t)row * KP + lane] = __float2bfloat16_rn(x);
+          }
+        } else if (lane == 0) {
+          atomicAdd(&p.ctl->retries[p.mode], 1u);
+        }
+      }
+      if (!ok) {
+        ok = warp_finish_f64<KP, Acc>(Gs, LD, Lam_s, (double)rac + lm, p, row, sweep, base);
+        if (!ok && lane == 0) {
+          atomicOr(&p.ctl->status, kStatCholFail);
+          atomicCAS(&p.ctl->bad_row, -1, row);
+        }
+      }
+      __syncwarp();
+      continue;
+    }
     if (t < K) mun[t] = p.mu[t] + (p.uhat ? p.uhat[(size_t)row * KP + t] : 0.0);
     gsync<T>(g);
     double lmu = 0.0;
@@ -335,7 +556,7 @@ template <int KP, int WPR, int G, bool MIXED>
 void launch_t(const SampleParams& p, cudaStream_t s, int num_sms) {
   using C = Cfg<KP, WPR, MIXED>;
   auto kern = k_sample<KP, WPR, G, MIXED>;
-  const size_t smem = C::kGroupBytes * G;
+  const size_t smem = C::kCtaBytes + C::kGroupBytes * G;
   static int per_sm_cache[64] = {0};  // per template instance and device
   int dev = 0;
   MG_CUDA(cudaGetDevice(&dev));

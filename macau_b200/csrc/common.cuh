@@ -20,7 +20,8 @@ struct Ctl {
   int32_t burnin;         // eval: n = sweep < burnin ? 0 : sweep - burnin
   int32_t status;         // OR of MG_STATUS_* bits raised by kernels
   int32_t bad_row;        // first row whose factorisation failed (diagnostics)
-  uint32_t queue[8];      // work-queue heads of persistent kernels (reset before each launch)
+  uint32_t queue[8];      // work-queue heads of persistent kernels ([mode]: the row sampler of
+                          // that mode), reset before each sampling launch
   uint32_t retries[2];    // mixed mode: rows re-factorised in FP64, per mode
   uint32_t cg_iters[2];   // last block-CG iteration count, per mode
   uint32_t cg_done;       // block-CG convergence flag
@@ -51,6 +52,7 @@ struct SampleParams {
   const RowTask* tasks;
   int ntasks;
   int nrows;
+  int nother;                  // rows of the other factor (the BF16 copy holds one more, zero)
   int K;                       // true latent dimension (<= KP)
   const long long* rowptr;     // CSR of the rows being sampled
   const int* colidx;

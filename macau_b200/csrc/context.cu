@@ -6,10 +6,14 @@
 // Device data layout
 //   * Ratings: one CSR per mode (mode 0 = rows of Y, mode 1 = columns), int64 row pointers,
 //     int32 indices sorted ascending, duplicates summed (Eigen setFromTriplets semantics).
-//     Mixed mode adds a packed (index, (y - mean) * alpha as FP32) pair per entry.
+//     Mixed mode adds a packed (index, (y - mean) * alpha as FP32) pair per entry, and at
+//     K <= 32 a second copy for the tensor-core sampler in which every row starts on a
+//     16-entry (128-byte) boundary and is padded to a multiple of 16 entries with
+//     (N_other, 0) sentinels, so each k-block of a row is one aligned bulk copy.
 //   * Latents: N x KP, row n = the K-vector of entity n, zero padded to KP in {8,..,128}.
 //     FP64 mode keeps FP64; mixed mode keeps an FP32 master plus a BF16 copy that the other
-//     mode's sampler gathers.
+//     mode's sampler gathers; the BF16 copy has one extra all-zero row N, the target of the
+//     padding sentinels (the tensor-core sampler's TMA gathers read it as a zero vector).
 //   * Hyperparameters (mu, Lambda, lambda_beta) and the Macau link matrix stay on the device;
 //     a sweep needs no host round trip except the block-CG convergence check.
 #include <cuda_runtime.h>
@@ -62,6 +66,26 @@ struct DBuf {
     g_h2d_bytes += (long long)(count * sizeof(T));
   }
 };
+
+// cuTensorMapEncodeTiled, looked up through the runtime so that the library does not link
+// libcuda directly (it loads on machines without a driver, where it reports MG_ERR_NOGPU).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn tensor_map_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    MG_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault,
+                                             &q));
+    if (q != cudaDriverEntryPointSuccess || !f)
+      throw MgError(MG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  return fn;
+}
 
 struct HostCsr {
   std::vector<long long> ptr;
@@ -136,7 +160,45 @@ struct ModeData {
   DBuf<unsigned> split_cnt;
   int ntasks = 0, nsplit = 0, nslots = 0;
   long long max_len = 0;
+  // tensor-core sampler (mixed, KP = 32): 16-entry padded packed CSR and its task list, whose
+  // begin / len are positions in the padded array (len a multiple of 16)
+  DBuf<uint2> packed_tc;
+  DBuf<RowTask> tasks_tc;
+  DBuf<float> gram_tc;     // N Gram records (32 x 32 + 32 floats) written by k_gram_tc
+  DBuf<int2> sinfo_tc;     // per row {parts, scratch slot of part 0}
+  int ntasks_tc = 0, nsplit_tc = 0, nslots_tc = 0;
 };
+
+// Task list over rows with lengths len(r) = ptr[r+1] - ptr[r] (positions ptr[r]): rows longer
+// than `thr` are cut into near-equal parts whose boundaries are multiples of `align` entries
+// (relative to the row start); tasks sorted by descending length (stable).
+std::vector<RowTask> make_tasks(const std::vector<long long>& ptr, long long thr, int align,
+                                int& nsplit, int& nslots) {
+  const long long n = (long long)ptr.size() - 1;
+  std::vector<RowTask> tasks;
+  tasks.reserve(n + 16);
+  nsplit = 0;
+  nslots = 0;
+  for (long long r = 0; r < n; r++) {
+    const long long len = ptr[r + 1] - ptr[r];
+    if (len <= thr) {
+      tasks.push_back(RowTask{ptr[r], (int)r, (int)len, 0, 1, 0, 0});
+      continue;
+    }
+    const long long units = (len + align - 1) / align;
+    const int parts = (int)((len + thr - 1) / thr);
+    for (int q = 0; q < parts; q++) {
+      const long long b = std::min(len, align * (units * q / parts));
+      const long long e = std::min(len, align * (units * (q + 1) / parts));
+      tasks.push_back(RowTask{ptr[r] + b, (int)r, (int)(e - b), q, parts, nslots, nsplit});
+    }
+    nslots += parts;
+    nsplit++;
+  }
+  std::stable_sort(tasks.begin(), tasks.end(),
+                   [](const RowTask& a, const RowTask& b) { return a.len > b.len; });
+  return tasks;
+}
 
 struct Prior {
   bool macau = false;
@@ -312,7 +374,7 @@ class Context {
       const size_t n = (size_t)dims_[m] * KP_;
       if (mixed_) {
         lat32_[m].alloc_zero(n, s_);
-        lat16_[m].alloc_zero(n, s_);
+        lat16_[m].alloc_zero(n + KP_, s_);  // + the zero row N
         lat64_[m].reset();
       } else {
         lat64_[m].alloc_zero(n, s_);
@@ -363,8 +425,28 @@ class Context {
     sweeps_done_ = 0;
     launches_ = 0;
     t_sample_ = t_prior_ = t_eval_ = 0.0;
+    if (mixed_ && KP_ == 32) {
+      for (int m = 0; m < 2; m++) make_gather_map(m);
+    }
     drop_graphs();
     initialised_ = true;
+  }
+
+  // TMA map over the BF16 copy of the latents of `m`'s other mode: {32, N_other + 1} bf16
+  // (row N_other is the zero row), box of one 64-byte row, 64-byte swizzle (the tensor-core
+  // sampler's stage layout).
+  void make_gather_map(int m) {
+    const int other = 1 - m;
+    const cuuint64_t dims[2] = {32, (cuuint64_t)dims_[other] + 1};
+    const cuuint64_t strides[1] = {64};
+    const cuuint32_t box[2] = {32, 1};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = tensor_map_encoder()(
+        &tmap_[m], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)lat16_[other].p, dims, strides, box,
+        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+        CU_TENSOR_MAP_L2_PROMOTION_L2_64B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      throw MgError(MG_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   }
 
   // ---- phases ----
@@ -373,11 +455,12 @@ class Context {
     ModeData& md = md_[mode];
     Prior& p = prior_[mode];
     const int other = 1 - mode;
-    if (reset_queue) MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[mode], 0, sizeof(uint32_t), s_));
+    if (reset_queue) MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[0], 0, 8 * sizeof(uint32_t), s_));
     SampleParams sp{};
     sp.tasks = md.tasks.p;
     sp.ntasks = md.ntasks;
     sp.nrows = (int)md.N;
+    sp.nother = (int)dims_[other];
     sp.K = K_;
     sp.rowptr = md.ptr.p;
     sp.colidx = md.idx.p;
@@ -399,8 +482,17 @@ class Context {
     sp.mode = mode;
     sp.seed = cfg_.seed;
     sp.znoise = znoise_dev;
-    if (!(mixed_ && use_tc_ && launch_sample_tc(sp, KP_, s_, num_sms_)))
-      launch_sample(sp, KP_, mixed_, s_, num_sms_);
+    if (mixed_ && use_tc_ && KP_ == 32) {
+      SampleParams tp = sp;
+      tp.tasks = md.tasks_tc.p;
+      tp.ntasks = md.ntasks_tc;
+      tp.packed = md.packed_tc.p;
+      if (launch_sample_tc(tp, tmap_[mode], md.gram_tc.p, md.sinfo_tc.p, KP_, s_, num_sms_)) {
+        launches_ += 1;  // k_gram_tc + k_finish_tc
+        return;
+      }
+    }
+    launch_sample(sp, KP_, mixed_, s_, num_sms_);
   }
 
   const void* latents(int mode) const {
@@ -456,7 +548,7 @@ class Context {
   // One sweep; ev (optional, 6 events) brackets: sample 0 | sample 1 | prior 0 | prior 1 |
   // eval + advance.
   void sweep_body(bool do_eval, cudaEvent_t* ev = nullptr) {
-    MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[0], 0, 2 * sizeof(uint32_t), s_));
+    MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[0], 0, 8 * sizeof(uint32_t), s_));
     if (ev) MG_CUDA(cudaEventRecord(ev[0], s_));
     sample(0, nullptr, false);
     if (ev) MG_CUDA(cudaEventRecord(ev[1], s_));
@@ -801,40 +893,47 @@ class Context {
     const long long groups = (long long)num_sms_ * 16;
     long long thr = md.nnz / (2 * groups);
     thr = std::max(256LL, std::min(16384LL, thr));
-    std::vector<long long> order(md.N);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](long long a, long long b) {
-      return (h.ptr[a + 1] - h.ptr[a]) > (h.ptr[b + 1] - h.ptr[b]);
-    });
-    std::vector<RowTask> tasks;
-    tasks.reserve(md.N + 16);
-    int nsplit = 0, nslots = 0;
     md.max_len = 0;
-    for (long long r : order) {
-      const long long len = h.ptr[r + 1] - h.ptr[r];
-      md.max_len = std::max(md.max_len, len);
-      if (len <= thr) {
-        tasks.push_back(RowTask{h.ptr[r], (int)r, (int)len, 0, 1, 0, 0});
-        continue;
-      }
-      const int parts = (int)((len + thr - 1) / thr);
-      for (int q = 0; q < parts; q++) {
-        const long long b = h.ptr[r] + len * q / parts;
-        const long long e = h.ptr[r] + len * (q + 1) / parts;
-        tasks.push_back(RowTask{b, (int)r, (int)(e - b), q, parts, nslots, nsplit});
-      }
-      nslots += parts;
-      nsplit++;
-    }
-    // longest tasks first
-    std::stable_sort(tasks.begin(), tasks.end(),
-                     [](const RowTask& a, const RowTask& b) { return a.len > b.len; });
+    for (long long r = 0; r < md.N; r++) md.max_len = std::max(md.max_len, h.ptr[r + 1] - h.ptr[r]);
+    int nsplit = 0, nslots = 0;
+    std::vector<RowTask> tasks = make_tasks(h.ptr, thr, 1, nsplit, nslots);
     md.ntasks = (int)tasks.size();
     md.nsplit = nsplit;
     md.nslots = nslots;
     md.tasks.upload(tasks.data(), tasks.size(), s_);
+    if (mixed_ && KP_ == 32) {
+      // padded copy for the tensor-core sampler: rows at 16-entry boundaries, sentinel padding
+      const int other_n = (int)dims_[1 - m];
+      std::vector<long long> pptr(md.N + 1, 0);
+      for (long long r = 0; r < md.N; r++)
+        pptr[r + 1] = pptr[r] + (h.ptr[r + 1] - h.ptr[r] + 15) / 16 * 16;
+      std::vector<uint2> pk(std::max(1LL, pptr[md.N]), make_uint2((unsigned)other_n, 0u));
+      for (long long r = 0; r < md.N; r++)
+        for (long long e = h.ptr[r]; e < h.ptr[r + 1]; e++) {
+          const float w = (float)((h.val[e] - mean_) * cfg_.precision);
+          uint32_t bits;
+          std::memcpy(&bits, &w, 4);
+          pk[pptr[r] + (e - h.ptr[r])] = make_uint2((unsigned)h.idx[e], bits);
+        }
+      md.packed_tc.upload(pk.data(), pk.size(), s_);
+      const long long thr16 = (thr + 15) / 16 * 16;
+      int ns = 0, nsl = 0;
+      std::vector<RowTask> tt = make_tasks(pptr, thr16, 16, ns, nsl);
+      md.ntasks_tc = (int)tt.size();
+      md.nsplit_tc = ns;
+      md.nslots_tc = nsl;
+      md.tasks_tc.upload(tt.data(), tt.size(), s_);
+      std::vector<int2> si(std::max(1LL, md.N), make_int2(1, 0));
+      for (const RowTask& t : tt)
+        if (t.nparts > 1 && t.part == 0) si[t.row] = make_int2(t.nparts, t.slot);
+      md.sinfo_tc.upload(si.data(), si.size(), s_);
+      md.gram_tc.alloc((size_t)std::max(1LL, md.N) * (32 * 32 + 32));
+    }
     md.split_cnt.alloc_zero(std::max(1, nsplit), s_);
-    const size_t need = (size_t)std::max(md_[0].nslots, md_[1].nslots) * (KP_ * KP_ + KP_);
+    const size_t need =
+        (size_t)std::max(std::max(md_[0].nslots, md_[1].nslots),
+                         std::max(md_[0].nslots_tc, md_[1].nslots_tc)) *
+        (KP_ * KP_ + KP_);
     if (need > scratch_.n) scratch_.alloc(need);
     MG_CUDA(cudaStreamSynchronize(s_));
   }
@@ -856,6 +955,7 @@ class Context {
   DBuf<double> lat64_[2];
   DBuf<float> lat32_[2];
   DBuf<__nv_bfloat16> lat16_[2];
+  CUtensorMap tmap_[2];  // tensor-core sampler: gather maps over lat16_ of the other mode
   DBuf<double> scratch_, stat_partials_, nwbuf_;
   NwWork nw_{};
   DBuf<Ctl> ctl_;

@@ -1,10 +1,665 @@
-// Mixed-precision latent sampler with the row Grams on the tcgen05 tensor cores (placeholder:
-// the CUDA-core kernel in sample_kernels.cu is used until this path is enabled).
+// Mixed-precision latent sampler whose row Grams run on the tcgen05 tensor cores (KP = 32), in
+// two kernels: k_gram_tc accumulates every sampled row's Gram V^T V and right-hand side on the
+// tensor cores and stores them to HBM; k_finish_tc then finishes each row (Lambda + alpha G,
+// Cholesky, solves, noise) with one warp per row at full occupancy.
+//
+// k_gram_tc.  Four sampler rows ("a group") share each MMA.  For a k-block of 16 entries per
+// row, the TMA gathers the four rows' BF16 other-factor vectors (64 B each, tile::gather4 by CSR
+// column index, 64B swizzle) into one shared-memory stage of five SW64 MN-major column blocks
+// (32 elements wide, four K-atoms of 512 B each): block p holds row p's 32 latent values, block
+// 4 holds the rows' (y - mean) * alpha in elements 0..3.  Each gather4 fills k-rows 0..3 of one
+// K-atom (its destination stays on the 512-byte swizzle period); k-rows 4..7 stay zero, so a
+// stage carries 16 entries per row in K = 32 and two tcgen05.mma (M = 128, N = 160, K = 16, BF16
+// in, FP32 accumulate in TMEM) consume it.  Together they add
+//     D[32p + i][32q + j] += sum_k X_p[k][i] X_q[k][j],   D[32p + i][128 + q] += sum_k X_p[k][i] w_q[k]
+// whose diagonal blocks p == q are the four rows' Grams and whose column 128 + p is row p's
+// right-hand side sum v (y - mean) alpha (the off-diagonal blocks are not used).  D row r lives
+// in TMEM lane r, so the epilogue warp of quadrant p reads row p's Gram with one 32x32b load.
+//
+// The CSR stream is the padded packed array of the mode: each row's (column, weight) entries
+// start on a 16-entry boundary and are padded to a multiple of 16 with (N_other, 0) sentinels;
+// a sentinel gathers the zero row N_other of the BF16 factor.
+//
+// Warp roles (one CTA of 13 warps per SM, persistent):
+//   warps 0-7   producers: warp w fills column block r = w % 4 of the stages of the k-blocks
+//               with global index t = w / 4 (mod 2).  Each keeps its own ring of CSR k-blocks
+//               (16 lanes x one 8-byte cp.async per k-block, up to kCsr - 1 of its k-blocks
+//               ahead), stores row r's 16 weights and issues 4 gather4 loads per k-block (a row
+//               with no entries left zero-fills its block instead); a stage's "full" barrier
+//               counts its 4 producers and the gathered bytes.  One warp issuing TMA
+//               instructions is issue-bound (about 70-90 cycles per instruction), so the issue
+//               is spread over eight warps.
+//   warp 8      scheduler + MMA: takes 4 tasks per group from the work queue and publishes the
+//               group descriptor kAhead groups ahead of the MMAs (the task loads overlap the
+//               MMA waits); allocates TMEM (512 columns: three accumulators of 160 columns); one
+//               lane issues the MMAs, releases stages (tcgen05.commit -> "empty") and publishes
+//               finished accumulators (tcgen05.commit -> "acc full").
+//   warps 9-12  epilogue (warp w reads TMEM quadrant w % 4 = row slot): TMEM -> registers,
+//               release the accumulator, store the row's FP32 Gram and rhs to its Gram record
+//               (or, for a part of a split row, the FP64 partial to the part's scratch slot).
+// Every barrier wait is bounded by a clock budget; on expiry the CTA raises an abort flag, all
+// roles leave their loops, the MMA lane drains its MMAs, TMEM is freed and the status word
+// reports a timeout.
+//
+// k_finish_tc.  One warp per row: the Gram record (or the FP64 sum of the row's split parts, in
+// part order), then the FP32 warp Cholesky and solves of warp_finish.cuh with the FP64 retry.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "kernels.h"
+#include "rng.cuh"
+#include "warp_finish.cuh"
 
 namespace mg {
+namespace {
 
-bool launch_sample_tc(const SampleParams&, int, cudaStream_t, int) { return false; }
+constexpr int kRowSlots = 4;
+constexpr int kParity = 2;                          // producers per row slot
+constexpr int kProducers = kRowSlots * kParity;     // warps 0-7
+constexpr int kMmaWarp = kProducers;                // warp 8
+constexpr int kEpiWarp0 = kProducers + 1;           // warps 9-12
+constexpr int kTcThreads = (kProducers + 5) * 32;
+constexpr int kStages = 16;               // gather stages in flight (even: stage s has parity s % 2)
+constexpr int kBlockBytes = 4 * 512;      // one column block: 4 K-atoms x 512 B
+constexpr int kStageBytes = 5 * kBlockBytes;
+constexpr int kSlots = 3;                 // TMEM accumulators
+constexpr int kSlotCols = 160;            // columns of one accumulator (N = 160)
+constexpr int kCsr = 6;                   // CSR prefetch slots per producer (its k-blocks ahead)
+constexpr int kDesc = 48;                 // group descriptor ring
+constexpr int kAhead = 28;                // groups the scheduler publishes ahead of the MMAs
+constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
+constexpr int kGramRec = 32 * 32 + 32;    // Gram record: 32 x 32 row-major Gram, then the rhs
+static_assert(kStages % kParity == 0, "a stage's k-blocks all have the same parity");
+
+struct GroupDesc {
+  int row[4];
+  int len[4];
+  long long begin[4];
+  int part[4];
+  int nparts[4];
+  int slot[4];
+  int rkb[4];  // k-blocks of each row (its padded length / 16)
+  int nkb;     // k-blocks of the group (>= 1)
+  int stop;    // 1: no more work
+};
+
+// Descriptor ring invariants: the scheduler writes group g + kAhead while the MMAs work on group
+// g.  A producer reads descriptor g while it is at most kStages k-blocks (so at most kStages
+// groups) ahead of the MMAs, and the epilogue reads it before releasing the accumulator of
+// group g, which the MMAs need before group g + kSlots; the slot is rewritten for group
+// g + kDesc only when the MMAs reach g + kDesc - kAhead.
+static_assert(kAhead > kStages + 1 && kDesc - kAhead > kSlots + 1,
+              "descriptor ring too small for the lookahead");
+
+struct TcShared {
+  uint64_t full[kStages];      // 4 producer arrivals + the gathered bytes
+  uint64_t empty[kStages];     // tcgen05.commit
+  uint64_t acc_full[kSlots];
+  uint64_t acc_empty[kSlots];  // 4 epilogue warps
+  uint64_t drain;
+  uint64_t desc_full[kDesc];   // scheduler -> producers, MMA, epilogue
+  alignas(16) uint2 csr[kProducers][kCsr][16];  // prefetched CSR k-blocks, per producer
+  uint32_t tmem_base;
+  int abort;
+  GroupDesc desc[kDesc];
+};
+
+__device__ __forceinline__ uint32_t su32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(ok)
+      : "r"(su32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait on phase `parity`: false on timeout or when another role aborted.
+__device__ bool mbar_wait(uint64_t* b, uint32_t parity, TcShared* sh, Ctl* ctl) {
+  const long long t0 = clock64();
+  for (int i = 0;; i++) {
+    if (mbar_test(b, parity)) return true;
+    if (*(volatile int*)&sh->abort) return false;
+    if (i > 32) __nanosleep(128);
+    if (clock64() - t0 > kWaitCycles) {
+      atomicOr(&ctl->status, kStatTimeout);
+      *(volatile int*)&sh->abort = 1;
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes)
+               : "memory");
+}
+
+// TMA gather of 4 rows (y0..y3) of the 2-D tensor `tmap` (box: one 64-byte row) into shared
+// memory at `dst`, completing on `b`; an out-of-range row is filled with zeros.
+__device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap* tmap, int y0, int y1,
+                                            int y2, int y3, uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(0), "r"(y0), "r"(y1), "r"(y2), "r"(y3),
+      "r"(su32(b))
+      : "memory");
+}
+
+// 8-byte asynchronous copy global -> shared (LSU path), completed by cp.async.wait_group.
+__device__ __forceinline__ void cp8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(su32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// SW64 MN-major shared-memory matrix descriptor: MN-atom stride 2048 B (LBO), K-atom stride
+// 512 B (SBO), descriptor version 1, layout type 4 (64-byte swizzle).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(kBlockBytes >> 4) << 16) |
+         ((uint64_t)(512 >> 4) << 32) | (1ull << 46) | (4ull << 61);
+}
+
+// kind::f16 instruction descriptor: D FP32, A/B BF16, A/B MN-major, N = 160, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                            ((160u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(d_tmem), "l"(a), "l"(b), "r"(kIdesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* b) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   su32(b))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, "
+      "%29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
+  uint32_t r;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Byte offset of element (mn, j) of a stage, j = entry 0..15 of the row's k-block (bf16
+// elements; SW64 MN-major: 64 B per k-row, entry j in K-atom j / 4, k-row j % 4, 16-byte chunk
+// index XOR (k-row / 2) % 4).
+__device__ __forceinline__ uint32_t stage_off(int mn, int j) {
+  const int a = mn >> 5, e = mn & 31, c = e >> 3, b = j >> 2, r = j & 3;
+  return (uint32_t)(a * kBlockBytes + b * 512 + r * 64 + ((c ^ ((r >> 1) & 3)) << 4) +
+                    ((e & 7) << 1));
+}
+
+// Writes the descriptor of group g (tasks t0 .. t0 + 3; lanes 0-3 hold their task in `tk`,
+// valid when `has`) and publishes it.  Returns true for the stop group (t0 past the end).
+__device__ __forceinline__ bool publish_group(TcShared* sh, int g, int t0, int ntasks,
+                                              const RowTask& tk, bool has, int lane) {
+  GroupDesc& d = sh->desc[g % kDesc];
+  const bool stop = t0 >= ntasks;
+  int rkb = 0;
+  if (lane < 4) {
+    d.row[lane] = has ? tk.row : -1;
+    d.len[lane] = has ? tk.len : 0;
+    d.begin[lane] = has ? tk.begin : 0;
+    d.part[lane] = has ? tk.part : 0;
+    d.nparts[lane] = has ? tk.nparts : 1;
+    d.slot[lane] = has ? tk.slot : 0;
+    rkb = has ? tk.len >> 4 : 0;
+    d.rkb[lane] = rkb;
+  }
+  int nkb = rkb;
+#pragma unroll
+  for (int o = 1; o < 4; o <<= 1) nkb = max(nkb, __shfl_xor_sync(0xffffffffu, nkb, o));
+  nkb = __shfl_sync(0xffffffffu, nkb, 0);
+  if (lane == 0) {
+    d.nkb = stop ? 1 : max(nkb, 1);
+    d.stop = stop ? 1 : 0;
+  }
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&sh->desc_full[g % kDesc]);
+  return stop;
+}
+
+// A producer's position in the flattened (group, k-block) sequence, restricted to the k-blocks
+// of its parity: group g, k-block kb of it, global k-block index t.
+struct Cursor {
+  int g, kb, t;
+  int nkb, rkb;
+  long long beg;
+  bool stop, end;
+};
+
+// Reads group c.g's descriptor (waiting for it to be published).  False on timeout / abort.
+__device__ __forceinline__ bool cursor_load(Cursor& c, TcShared* sh, Ctl* ctl, int r) {
+  if (!mbar_wait(&sh->desc_full[c.g % kDesc], (uint32_t)((c.g / kDesc) & 1), sh, ctl)) return false;
+  const GroupDesc& d = sh->desc[c.g % kDesc];
+  c.nkb = d.nkb;
+  c.stop = d.stop != 0;
+  c.beg = d.begin[r];
+  c.rkb = d.rkb[r];
+  return true;
+}
+
+// Moves the cursor `step` k-blocks on (crossing group boundaries); c.end once it passes the
+// stop group.  False on timeout / abort.
+__device__ __forceinline__ bool cursor_advance(Cursor& c, int step, TcShared* sh, Ctl* ctl, int r) {
+  c.kb += step;
+  c.t += step;
+  while (c.kb >= c.nkb) {
+    if (c.stop) {
+      c.end = true;
+      return true;
+    }
+    c.kb -= c.nkb;
+    c.g++;
+    if (!cursor_load(c, sh, ctl, r)) return false;
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_gram_tc(const SampleParams p, const __grid_constant__ CUtensorMap tmap, float* gram) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // layout: stages (1024-aligned) | TcShared
+  unsigned char* stages = smem_raw;
+  TcShared* sh = reinterpret_cast<TcShared*>(stages + (size_t)kStages * kStageBytes);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // The stage layout and the TMA's 64-byte swizzle agree only on 1024-byte aligned stages.
+  if ((su32(stages) & 1023u) != 0) {
+    if (threadIdx.x == 0) atomicOr(&p.ctl->status, kStatTimeout);
+    return;
+  }
+
+  // ---- set-up ----
+  // zero the stages once: k-rows 4..7 of every K-atom and weight elements 4..31 stay zero
+  for (int e = threadIdx.x; e < kStages * kStageBytes / 16; e += blockDim.x)
+    reinterpret_cast<uint4*>(stages)[e] = make_uint4(0u, 0u, 0u, 0u);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; s++) {
+      mbar_init(&sh->full[s], kRowSlots);
+      mbar_init(&sh->empty[s], 1);
+    }
+    for (int s = 0; s < kSlots; s++) {
+      mbar_init(&sh->acc_full[s], 1);
+      mbar_init(&sh->acc_empty[s], 4);
+    }
+    mbar_init(&sh->drain, 1);
+    for (int d = 0; d < kDesc; d++) mbar_init(&sh->desc_full[d], 1);
+    sh->abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == kMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     su32(&sh->tmem_base)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh->tmem_base;
+
+  if (warp < kProducers) {
+    // ================= producer of row slot r, parity h =================
+    // CSR cursor `c` copies this producer's k-blocks up to kCsr - 1 ahead; gather cursor `q`
+    // fills column block r of their stages.
+    const int r = warp % kRowSlots, h = warp / kRowSlots;
+    Cursor c{0, 0, 0, 0, 0, 0, false, false};
+    bool ok = cursor_load(c, sh, p.ctl, r) && cursor_advance(c, h, sh, p.ctl, r);
+    Cursor q = c;
+    int issued = 0, gathered = 0;
+    while (ok && !q.end) {
+      // ---- top up the CSR prefetch ----
+      while (!c.end && issued - gathered < kCsr - 1) {
+        const int slot = issued % kCsr;
+        if (lane < 16 && !c.stop && c.kb < c.rkb)
+          cp8(&sh->csr[warp][slot][lane], p.packed + c.beg + 16LL * c.kb + lane);
+        cp_commit();  // one group per k-block, empty or not
+        issued++;
+        if (!cursor_advance(c, kParity, sh, p.ctl, r)) {
+          ok = false;
+          break;
+        }
+      }
+      if (!ok) break;
+      // ---- fill column block r of k-block q.t's stage ----
+      const int cslot = gathered % kCsr;
+      // the k-block's copy group is the oldest of the issued - gathered groups in flight
+      if (issued - gathered == kCsr - 1)
+        cp_wait<kCsr - 2>();
+      else
+        cp_wait<0>();
+      __syncwarp();
+      const int stage = q.t % kStages;
+      const uint32_t phase = (uint32_t)((q.t / kStages) & 1);
+      if (!mbar_wait(&sh->empty[stage], phase ^ 1, sh, p.ctl)) break;
+      const bool v = !q.stop && q.kb < q.rkb;
+      unsigned char* sbase = stages + (size_t)stage * kStageBytes;
+      unsigned char* blk = sbase + r * kBlockBytes;
+      if (v) {
+        const uint2 ent = sh->csr[warp][cslot][lane & 15];
+        if (lane < 16)
+          *reinterpret_cast<__nv_bfloat16*>(sbase + stage_off(128 + r, lane)) =
+              __float2bfloat16_rn(__uint_as_float(ent.y));
+        int y[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) y[u] = __shfl_sync(0xffffffffu, (int)ent.x, (4 * lane + u) & 15);
+        fence_proxy_async();  // the weights before the async proxy reads them
+        __syncwarp();
+        if (lane == 0) mbar_expect_tx(&sh->full[stage], 4u * 256u);
+        __syncwarp();
+        if (lane < 4)
+          tma_gather4(su32(blk + lane * 512), &tmap, y[0], y[1], y[2], y[3], &sh->full[stage]);
+      } else {
+        // no entries of row r in this k-block: zero k-rows 0..3 of its 4 K-atoms and its weights
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          const int i = lane + 32 * k;
+          *reinterpret_cast<uint4*>(blk + (i >> 4) * 512 + (i & 15) * 16) = make_uint4(0u, 0u, 0u, 0u);
+        }
+        if (lane < 16)
+          *reinterpret_cast<__nv_bfloat16*>(sbase + stage_off(128 + r, lane)) = __float2bfloat16_rn(0.f);
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sh->full[stage]);
+      }
+      gathered++;
+      if (!cursor_advance(q, kParity, sh, p.ctl, r)) break;
+      __syncwarp();
+    }
+    cp_wait<0>();
+  } else if (warp == kMmaWarp) {
+    // ================= scheduler + MMA issuer =================
+    int next_t0 = 0;  // lane 0: queue position of the next group to publish
+    if (lane == 0) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
+    int sched = 0;    // next group to publish
+    bool sched_done = false;
+    while (!sched_done && sched < kAhead) {
+      const int t0 = __shfl_sync(0xffffffffu, next_t0, 0);
+      if (lane == 0 && t0 < p.ntasks) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
+      RowTask tk{};
+      const bool has = lane < 4 && t0 + lane < p.ntasks;
+      if (has) tk = p.tasks[t0 + lane];
+      sched_done = publish_group(sh, sched, t0, p.ntasks, tk, has, lane);
+      sched++;
+    }
+    int stage = 0;
+    uint32_t phase = 0;
+    for (int g = 0;; g++) {
+      // start the task loads of the group published at the end of this iteration
+      int t0 = 0;
+      RowTask tk{};
+      bool has = false;
+      if (!sched_done) {
+        t0 = __shfl_sync(0xffffffffu, next_t0, 0);
+        if (lane == 0 && t0 < p.ntasks) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
+        has = lane < 4 && t0 + lane < p.ntasks;
+        if (has) tk = p.tasks[t0 + lane];
+      }
+      const int slot = g % kSlots;
+      if (g >= kSlots &&
+          !mbar_wait(&sh->acc_empty[slot], (uint32_t)(((g / kSlots) & 1) ^ 1), sh, p.ctl))
+        break;
+      tc_fence_after();
+      const uint32_t d_tmem = tmem + (uint32_t)(slot * kSlotCols);
+      const GroupDesc& d = sh->desc[g % kDesc];
+      const int nkb = d.nkb, stop = d.stop;
+      bool ok = true;
+      for (int kb = 0; kb < nkb; kb++) {
+        if (!mbar_wait(&sh->full[stage], phase, sh, p.ctl)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        if (lane == 0) {
+          const uint32_t sa = su32(stages + (size_t)stage * kStageBytes);
+          mma_bf16(d_tmem, smem_desc(sa), smem_desc(sa), kb > 0 ? 1u : 0u);
+          mma_bf16(d_tmem, smem_desc(sa + 1024), smem_desc(sa + 1024), 1u);
+          mma_commit(&sh->empty[stage]);
+        }
+        __syncwarp();
+        if (++stage == kStages) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+      if (!ok) break;
+      if (lane == 0) mma_commit(&sh->acc_full[slot]);
+      __syncwarp();
+      if (!sched_done) {
+        sched_done = publish_group(sh, sched, t0, p.ntasks, tk, has, lane);
+        sched++;
+      }
+      if (stop) break;
+    }
+    // drain: wait for every issued MMA before TMEM is released
+    if (lane == 0) {
+      mma_commit(&sh->drain);
+      const long long t0 = clock64();
+      while (!mbar_test(&sh->drain, 0) && clock64() - t0 < kWaitCycles) __nanosleep(128);
+    }
+    __syncwarp();
+  } else {
+    // ================= epilogue: accumulators -> Gram records =================
+    const int qd = warp & 3;  // TMEM quadrant = row slot of the group
+    for (int g = 0;; g++) {
+      const int slot = g % kSlots;
+      if (!mbar_wait(&sh->acc_full[slot], (uint32_t)((g / kSlots) & 1), sh, p.ctl)) break;
+      if (!mbar_wait(&sh->desc_full[g % kDesc], (uint32_t)((g / kDesc) & 1), sh, p.ctl)) break;
+      tc_fence_after();
+      const GroupDesc& d = sh->desc[g % kDesc];
+      const int stop = d.stop;
+      const int row = d.row[qd];
+      const int part = d.part[qd], nparts = d.nparts[qd], pslot = d.slot[qd];
+      float gr[32];
+      float rhs = 0.f;
+      if (!stop) {
+        const uint32_t lanes = (uint32_t)(32 * qd) << 16;
+        tmem_ld32(tmem + lanes + (uint32_t)(slot * kSlotCols + 32 * qd), gr);
+        rhs = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 128 + qd));
+        tmem_wait_ld();
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh->acc_empty[slot]);
+      if (stop) break;
+      if (row < 0) continue;
+      if (nparts > 1) {
+        double* sp = p.scratch + (size_t)(pslot + part) * kGramRec;
+#pragma unroll
+        for (int j = 0; j < 32; j++) sp[lane * 32 + j] = (double)gr[j];
+        sp[32 * 32 + lane] = (double)rhs;
+      } else {
+        float* gp = gram + (size_t)row * kGramRec;
+#pragma unroll
+        for (int j = 0; j < 32; j += 4)
+          *reinterpret_cast<float4*>(gp + lane * 32 + j) = make_float4(gr[j], gr[j + 1], gr[j + 2], gr[j + 3]);
+        gp[32 * 32 + lane] = rhs;
+      }
+    }
+  }
+  // ---- tear-down ----
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_finish_tc: one warp per row (rows warp, warp + total warps, ...).
+constexpr int kFinWarps = 8;
+constexpr int kLD = 33;                 // Gram tile leading dimension (floats)
+constexpr int kLc = 36;                 // L^T leading dimension
+constexpr int kFinWork = 32 * 36 * 8;   // per warp: FP32 Gram + L^T, or the FP64 retry's L^T
+
+__global__ void __launch_bounds__(kFinWarps * 32, 2)
+    k_finish_tc(const SampleParams p, const float* __restrict__ gram, const int2* __restrict__ sinfo) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  double* Lam_s = reinterpret_cast<double*>(fsm);
+  double* lmu_s = Lam_s + 32 * 33;
+  unsigned char* works = reinterpret_cast<unsigned char*>(lmu_s + 32);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int K = p.K;
+  const uint32_t sweep = p.ctl->sweep;
+  for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
+    const int i = e / 32, j = e % 32;
+    Lam_s[i * 33 + j] = (i < K && j < K) ? p.Lambda[i + j * K] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double s = 0.0;
+    if (lane < K)
+      for (int j = 0; j < K; j++) s += Lam_s[lane * 33 + j] * p.mu[j];
+    lmu_s[lane] = s;
+  }
+  __syncthreads();
+  unsigned char* work = works + (size_t)warp * kFinWork;
+  float* Gs = reinterpret_cast<float*>(work);
+  float* Lc = Gs + 32 * kLD;
+  const int stride = gridDim.x * kFinWarps;
+  for (int row = blockIdx.x * kFinWarps + warp; row < p.nrows; row += stride) {
+    const int2 si = sinfo[row];  // {parts, scratch slot of part 0}
+    double rhs;
+    if (si.x > 1) {
+      // sum the parts in part order, one entry at a time in FP64
+      const double* s0 = p.scratch + (size_t)si.y * kGramRec;
+#pragma unroll 4
+      for (int j = 0; j < 32; j++) {
+        double acc = 0.0;
+        for (int prt = 0; prt < si.x; prt++) acc += __ldcg(s0 + (size_t)prt * kGramRec + lane * 32 + j);
+        Gs[lane * kLD + j] = (float)acc;
+      }
+      double rs = 0.0;
+      for (int prt = 0; prt < si.x; prt++) rs += __ldcg(s0 + (size_t)prt * kGramRec + 32 * 32 + lane);
+      rhs = (double)(float)rs;
+    } else {
+      const float* gp = gram + (size_t)row * kGramRec;
+#pragma unroll
+      for (int j = 0; j < 32; j += 4) {
+        const float4 v = __ldcs(reinterpret_cast<const float4*>(gp + lane * 32 + j));
+        Gs[lane * kLD + j] = v.x;
+        Gs[lane * kLD + j + 1] = v.y;
+        Gs[lane * kLD + j + 2] = v.z;
+        Gs[lane * kLD + j + 3] = v.w;
+      }
+      rhs = (double)__ldcs(gp + 32 * 32 + lane);
+    }
+    double lm;
+    if (p.uhat) {
+      const double mun = lane < K ? p.mu[lane] + p.uhat[(size_t)row * 32 + lane] : 0.0;
+      lm = 0.0;
+      for (int j = 0; j < K; j++) {
+        const double mj = __shfl_sync(0xffffffffu, mun, j);
+        if (lane < K) lm += Lam_s[lane * 33 + j] * mj;
+      }
+    } else {
+      lm = lmu_s[lane];
+    }
+    __syncwarp();
+    float a[32], d0 = 1.f, rinv = 1.f;
+    const double z = row_noise(p, row, K, lane, sweep);
+    warp_load_mm<float, float, 32>(a, d0, Gs, kLD, Lam_s, p.alpha, lane, K);
+    bool ok = warp_factor<float, 32>(a, rinv, lane, 0x1p-20, d0, Lc, kLc);
+    if (ok) {
+      const float x = warp_solve<float, 32>(a, rinv, (float)(rhs + lm), lane, Lc, kLc, z);
+      if (lane < K) {
+        p.out_f32[(size_t)row * 32 + lane] = x;
+        p.out_bf16[(size_t)row * 32 + lane] = __float2bfloat16_rn(x);
+      }
+    } else {
+      if (lane == 0) atomicAdd(&p.ctl->retries[p.mode], 1u);
+      ok = warp_finish_f64<32, float>(Gs, kLD, Lam_s, rhs + lm, p, row, sweep, work);
+      if (!ok && lane == 0) {
+        atomicOr(&p.ctl->status, kStatCholFail);
+        atomicCAS(&p.ctl->bad_row, -1, row);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+size_t tc_smem_bytes() { return (size_t)kStages * kStageBytes + sizeof(TcShared); }
+
+bool launch_sample_tc(const SampleParams& p, const CUtensorMap& tmap, float* gram,
+                      const int2* sinfo, int KP, cudaStream_t s, int num_sms) {
+  if (KP != 32 || p.packed == nullptr) return false;
+  static bool configured[64] = {false};
+  int dev = 0;
+  MG_CUDA(cudaGetDevice(&dev));
+  const size_t smem = tc_smem_bytes();
+  const size_t fsmem = sizeof(double) * (32 * 33 + 32) + (size_t)kFinWarps * kFinWork;
+  if (!configured[dev & 63]) {
+    MG_CUDA(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MG_CUDA(cudaFuncSetAttribute(k_finish_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)fsmem));
+    configured[dev & 63] = true;
+  }
+  k_gram_tc<<<num_sms, kTcThreads, smem, s>>>(p, tmap, gram);
+  MG_CUDA(cudaGetLastError());
+  k_finish_tc<<<num_sms * 2, kFinWarps * 32, fsmem, s>>>(p, gram, sinfo);
+  MG_CUDA(cudaGetLastError());
+  return true;
+}
 
 }  // namespace mg

@@ -1,5 +1,6 @@
 // Host-side launch functions of the sm_100a kernels (one translation unit per kernel family).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -8,9 +9,15 @@ namespace mg {
 
 // ---- latent sampler (sample_kernels.cu, gram_tc.cu) ----
 void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, int num_sms);
-// Mixed-precision sampler whose Gram runs on the tcgen05 tensor cores (K = 32 only).  Returns
-// false when the configuration is not covered (caller falls back to the CUDA-core kernel).
-bool launch_sample_tc(const SampleParams& p, int KP, cudaStream_t s, int num_sms);
+// Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only): two
+// launches, k_gram_tc then k_finish_tc.  It reads the 16-entry padded packed CSR and its task
+// list (p.packed / p.tasks, built by the context) and gathers the other factor's BF16 rows
+// through `tmap` (2-D, {32, nother + 1} bf16, box {32, 1}, 64-byte swizzle; row nother is all
+// zeros).  `gram` holds nrows Gram records of 32 * 32 + 32 floats; sinfo[row] = {parts, scratch
+// slot of part 0} (parts > 1: the row's partial Grams go to p.scratch, 1056 doubles per slot).
+// Returns false when the configuration is not covered (caller uses the CUDA-core kernel).
+bool launch_sample_tc(const SampleParams& p, const CUtensorMap& tmap, float* gram,
+                      const int2* sinfo, int KP, cudaStream_t s, int num_sms);
 
 // ---- hyperprior / eval (hyper_kernels.cu) ----
 struct NwWork {

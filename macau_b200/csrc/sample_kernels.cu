@@ -23,16 +23,12 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "rng.cuh"
+#include "warp_finish.cuh"
 
 namespace mg {
 namespace {
 
 constexpr int kChunk = 32;  // gathered rows staged per step
-
-__device__ __forceinline__ float mfma(float a, float b, float c) { return fmaf(a, b, c); }
-__device__ __forceinline__ double mfma(double a, double b, double c) { return fma(a, b, c); }
-__device__ __forceinline__ float msqrt(float a) { return sqrtf(a); }
-__device__ __forceinline__ double msqrt(double a) { return sqrt(a); }
 
 template <int T>
 __device__ __forceinline__ void gsync(int g) {
@@ -133,146 +129,6 @@ __device__ void add_noise(const SampleParams& p, F* rr, int row, int K, int t, i
   gsync<T>(g);
 }
 
-__device__ __forceinline__ float wshfl(float v, int src) { return __shfl_sync(0xffffffffu, v, src); }
-__device__ __forceinline__ double wshfl(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
-
-__device__ __forceinline__ float mrsqrt(float a) { return rsqrtf(a); }
-__device__ __forceinline__ double mrsqrt(double a) { return rsqrt(a); }
-
-// Vector load of 4 consecutive values from shared memory (16-byte aligned for float).
-template <typename F>
-struct Vec4 {
-  F v[4];
-};
-template <typename F>
-__device__ __forceinline__ Vec4<F> lds4(const F* p) {
-  Vec4<F> r;
-  if constexpr (sizeof(F) == 4) {
-    const float4 t = *reinterpret_cast<const float4*>(p);
-    r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
-  } else {
-    const double2 t0 = *reinterpret_cast<const double2*>(p);
-    const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
-    r.v[0] = t0.x; r.v[1] = t0.y; r.v[2] = t1.x; r.v[3] = t1.y;
-  }
-  return r;
-}
-
-// Warp Cholesky of the KP x KP matrix whose row i is held by lane i in a[] (lower triangle
-// used).  Right-looking over columns: entry (i, k) receives its updates in the order
-// j = 0, 1, ... and is then scaled by 1/L(k, k).  Column j of L is published to shared memory
-// (Lc row j, leading dimension ld, a multiple of 4) and read back as 4-wide broadcasts for the
-// trailing update.  rinv receives the lane's 1/L(i, i).  A pivot that is not positive, or
-// (mixed mode) falls below rel_floor times the original diagonal d0, fails the whole warp.
-// On success Lc holds L^T (row j = column j of L).
-template <typename F, int KP>
-__device__ __forceinline__ bool warp_factor(F (&a)[KP], F& rinv, int lane, double rel_floor,
-                                            F d0, F* Lc, int ld) {
-#pragma unroll
-  for (int j = 0; j < KP; j++) {
-    const F piv = wshfl(a[j], j);
-    const F dj = wshfl(d0, j);
-    if (!(piv > (F)0) || !((double)piv > rel_floor * (double)dj)) return false;
-    const F r = mrsqrt(piv);
-    if (lane == j) {
-      a[j] = piv * r;
-      rinv = r;
-    } else if (lane > j) {
-      a[j] = a[j] * r;
-    }
-    if (lane < KP) Lc[j * ld + lane] = a[j];
-    __syncwarp();
-#pragma unroll
-    for (int q = (j + 1) / 4; q < KP / 4; q++) {
-      const Vec4<F> c = lds4(Lc + j * ld + 4 * q);
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int k = 4 * q + u;
-        if (k > j && lane >= k) a[k] = mfma(-a[j], c.v[u], a[k]);
-      }
-    }
-  }
-  return true;
-}
-
-// y = L^{-1} rr (lane i holds rr_i and row i of L), rr += z, then x = L^{-T} rr with L^T read
-// from Lc (row j = column j of L).  Returns x_i in lane i.
-template <typename F, int KP>
-__device__ __forceinline__ F warp_solve(const F (&a)[KP], F rinv, F rr, int lane, const F* Lc,
-                                        int ld, const SampleParams& p, int row, int K,
-                                        uint32_t sweep) {
-#pragma unroll
-  for (int j = 0; j < KP; j++) {
-    if (lane == j) rr = rr * rinv;
-    const F yj = wshfl(rr, j);
-    if (lane > j) rr = mfma(-a[j], yj, rr);
-  }
-  if (p.znoise) {
-    if (lane < K) rr += (F)p.znoise[(size_t)row * K + lane];
-  } else {
-    double z0, z1;
-    normal_pair(p.seed, sweep, stream_id(kRowNoise, (uint32_t)p.mode), (uint32_t)row,
-                (uint32_t)(lane >> 1), &z0, &z1);
-    if (lane < K) rr += (F)((lane & 1) ? z1 : z0);
-  }
-#pragma unroll
-  for (int j = KP - 1; j >= 0; j--) {
-    if (lane == j) rr = rr * rinv;
-    const F xj = wshfl(rr, j);
-    if (lane < j) rr = mfma(-Lc[lane * ld + j], xj, rr);
-  }
-  __syncwarp();
-  return rr;
-}
-
-// Row i of MM = Lambda + alpha * G for lane i (padded rows / columns of the identity), with G
-// read from the Gram tile in shared memory (row-major, leading dimension ld).
-template <typename F, typename GT, int KP>
-__device__ __forceinline__ void warp_load_mm(F (&a)[KP], F& d0, const GT* Gs, int ld,
-                                             const double* Lam_s, double alpha, int lane, int K) {
-#pragma unroll
-  for (int j = 0; j < KP; j++) {
-    F v;
-    if (lane < K && j < K) {
-      if constexpr (sizeof(F) == 4)
-        v = (float)Lam_s[lane * (KP + 1) + j] + (float)alpha * (float)Gs[lane * ld + j];
-      else
-        v = Lam_s[lane * (KP + 1) + j] + alpha * (double)Gs[lane * ld + j];
-    } else {
-      v = (lane == j) ? (F)1 : (F)0;
-    }
-    a[j] = v;
-    if (j == lane) d0 = v;
-  }
-}
-
-// FP64 finish of one row by one warp: MM = Lambda + alpha * G from the Gram tile Gs, Cholesky,
-// solves and noise in FP64 (the FP64 path, and the retry of a row whose FP32 factor failed).
-// Kept out of line so the FP32 path's register budget does not pay for it.  Writes the row and
-// returns true, or returns false when the FP64 factor fails too.
-template <int KP, typename GT>
-__device__ __noinline__ bool warp_finish_f64(const GT* Gs, int ld, const double* Lam_s,
-                                             double rac_lm, const SampleParams& p, int row,
-                                             uint32_t sweep, unsigned char* work) {
-  const int lane = threadIdx.x & 31;
-  const int K = p.K;
-  double a[KP], d0 = 1.0, rinv = 1.0;
-  warp_load_mm<double, GT, KP>(a, d0, Gs, ld, Lam_s, p.alpha, lane, K);
-  __syncwarp();
-  double* Lc = reinterpret_cast<double*>(work);  // the Gram tile has been read into a[]
-  if (!warp_factor<double, KP>(a, rinv, lane, 0.0, d0, Lc, KP + 4)) return false;
-  const double x = warp_solve<double, KP>(a, rinv, rac_lm, lane, Lc, KP + 4, p, row, K, sweep);
-  if (lane < K) {
-    if (p.out_f64) {
-      p.out_f64[(size_t)row * KP + lane] = x;
-    } else {
-      p.out_f32[(size_t)row * KP + lane] = (float)x;
-      p.out_bf16[(size_t)row * KP + lane] = __float2bfloat16_rn((float)x);
-    }
-  }
-  return true;
-}
-
 // Minimum resident CTAs requested from the register allocator (warp-per-row instances: 16
 // warps per SM for FP32 Grams, 12 for FP64).
 template <int WPR, bool MIXED>
@@ -316,11 +172,12 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
   const uint32_t sweep = p.ctl->sweep;
   const Elem* other = reinterpret_cast<const Elem*>(p.other);
 
+  const int ntasks = p.ntasks;
   for (;;) {
     if (t == 0) bcast[0] = (int)atomicAdd(&p.ctl->queue[p.qslot], 1u);
     gsync<T>(g);
     const int ti = bcast[0];
-    if (ti >= p.ntasks) break;
+    if (ti >= ntasks) break;
     const RowTask tk = p.tasks[ti];
     Acc acc[TR][TC];
 #pragma unroll
@@ -455,10 +312,11 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
                                        p.alpha, lane, K);
         // L^T goes after the Gram tile, which must stay readable for an FP64 retry
         float* Lc = reinterpret_cast<float*>(base) + KP * LD;
+        const double z = row_noise(p, row, K, lane, sweep);
         ok = warp_factor<float, KP>(a, rinv, lane, 0x1p-20, d0, Lc, KP + 4);
         if (ok) {
           const float x = warp_solve<float, KP>(a, rinv, (float)((double)rac + lm), lane, Lc,
-                                                KP + 4, p, row, K, sweep);
+                                                KP + 4, z);
           if (lane < K) {
             p.out_f32[(size_t)row * KP + lane] = x;
             p.out_bf16[(size_t)row * KP + lane] = __float2bfloat16_rn(x);

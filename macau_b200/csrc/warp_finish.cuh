@@ -1,0 +1,179 @@
+// Warp-level finish of one sampler row (K <= 32): lane i holds row i of MM = Lambda + alpha*G,
+// the warp factorises MM = L L^T, solves L y = rr, adds the row's N(0,1) draws and solves
+// L^T x = y (sample_latent_blas, latentprior.cpp:373-384).  Shared by the CUDA-core sampler
+// (sample_kernels.cu) and the tensor-core sampler (gram_tc.cu).
+#pragma once
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "rng.cuh"
+
+namespace mg {
+
+__device__ __forceinline__ float mfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double mfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float msqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ double msqrt(double a) { return sqrt(a); }
+
+__device__ __forceinline__ float wshfl(float v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ double wshfl(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+
+__device__ __forceinline__ float mrsqrt(float a) { return rsqrtf(a); }
+__device__ __forceinline__ double mrsqrt(double a) { return rsqrt(a); }
+
+// Vector load of 4 consecutive values from shared memory (16-byte aligned for float).
+template <typename F>
+struct Vec4 {
+  F v[4];
+};
+template <typename F>
+__device__ __forceinline__ Vec4<F> lds4(const F* p) {
+  Vec4<F> r;
+  if constexpr (sizeof(F) == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+  } else {
+    const double2 t0 = *reinterpret_cast<const double2*>(p);
+    const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
+    r.v[0] = t0.x; r.v[1] = t0.y; r.v[2] = t1.x; r.v[3] = t1.y;
+  }
+  return r;
+}
+
+// Warp Cholesky of the KP x KP matrix whose row i is held by lane i in a[] (lower triangle
+// used; d0 = the lane's diagonal entry).  Right-looking over columns: entry (i, k) receives its
+// updates in the order j = 0, 1, ... and is then scaled by 1/L(k, k).  The critical chain of a
+// column step stays in registers and shuffles: each lane keeps its own diagonal in `diag`, the
+// pivot lane forms 1/L(j, j) and shuffles it, and the next column's L(j+1, j) comes by
+// shuffle; columns j+2 onwards read L(k, j) from shared memory (column j published as Lc row j,
+// leading dimension ld, a multiple of 4) as 4-wide broadcasts, off the critical chain.  Every
+// update is the same fma with the same operands as a plain right-looking loop, so the factor
+// does not depend on this scheduling.  rinv receives the lane's 1/L(i, i).  A pivot that is not
+// positive, or falls below rel_floor times the original diagonal d0, fails the whole warp.  On
+// success Lc holds L^T (row j = column j of L).
+template <typename F, int KP>
+__device__ __forceinline__ bool warp_factor(F (&a)[KP], F& rinv, int lane, double rel_floor,
+                                            F d0, F* Lc, int ld) {
+  const F floor = (F)rel_floor * d0;
+  F diag = d0;
+  bool bad = false;
+#pragma unroll
+  for (int j = 0; j < KP; j++) {
+    if (lane == j) bad = !(diag > (F)0) || !(diag > floor);
+    const F r = wshfl(mrsqrt(diag), j);
+    if (lane == j) {
+      a[j] = diag * r;
+      rinv = r;
+    } else if (lane > j) {
+      a[j] = a[j] * r;
+    }
+    if (j + 1 < KP) {
+      const F lnext = wshfl(a[j], j + 1);  // L(j+1, j)
+      if (lane > j) diag = mfma(-a[j], a[j], diag);
+      if (lane > j + 1) a[j + 1] = mfma(-a[j], lnext, a[j + 1]);
+    }
+    if (lane < KP) Lc[j * ld + lane] = a[j];
+    __syncwarp();
+#pragma unroll
+    for (int q = (j + 2) / 4; q < KP / 4; q++) {
+      const Vec4<F> c = lds4(Lc + j * ld + 4 * q);
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int k = 4 * q + u;
+        if (k > j + 1 && lane > k) a[k] = mfma(-a[j], c.v[u], a[k]);
+      }
+    }
+  }
+  return !__any_sync(0xffffffffu, bad);
+}
+
+// y = L^{-1} rr (lane i holds rr_i and row i of L), rr += z, then x = L^{-T} rr with L^T read
+// from Lc (row j = column j of L).  Returns x_i in lane i.
+// The row's N(0,1) draw for component `lane` (0 beyond K): injected, or keyed by
+// (seed, sweep, mode, row).  Computed before the factorisation so its latency overlaps it.
+__device__ __forceinline__ double row_noise(const SampleParams& p, int row, int K, int lane,
+                                            uint32_t sweep) {
+  if (p.znoise) return lane < K ? p.znoise[(size_t)row * K + lane] : 0.0;
+  double z0, z1;
+  normal_pair(p.seed, sweep, stream_id(kRowNoise, (uint32_t)p.mode), (uint32_t)row,
+              (uint32_t)(lane >> 1), &z0, &z1);
+  return lane < K ? ((lane & 1) ? z1 : z0) : 0.0;
+}
+
+template <typename F, int KP>
+__device__ __forceinline__ F warp_solve(const F (&a)[KP], F rinv, F rr, int lane, const F* Lc,
+                                        int ld, double z) {
+#pragma unroll
+  for (int j = 0; j < KP; j++) {
+    if (lane == j) rr = rr * rinv;
+    const F yj = wshfl(rr, j);
+    if (lane > j) rr = mfma(-a[j], yj, rr);
+  }
+  rr += (F)z;
+#pragma unroll
+  for (int j = KP - 1; j >= 0; j--) {
+    if (lane == j) rr = rr * rinv;
+    const F xj = wshfl(rr, j);
+    if (lane < j) rr = mfma(-Lc[lane * ld + j], xj, rr);
+  }
+  __syncwarp();
+  return rr;
+}
+
+// Row i of MM = Lambda + alpha * G for lane i (padded rows / columns of the identity), with G
+// read from the Gram tile in shared memory (row-major, leading dimension ld).
+template <typename F, typename GT, int KP>
+__device__ __forceinline__ void warp_load_mm(F (&a)[KP], F& d0, const GT* Gs, int ld,
+                                             const double* Lam_s, double alpha, int lane, int K) {
+#pragma unroll
+  for (int j = 0; j < KP; j++) {
+    F v;
+    if (lane < K && j < K) {
+      if constexpr (sizeof(F) == 4)
+        v = (float)Lam_s[lane * (KP + 1) + j] + (float)alpha * (float)Gs[lane * ld + j];
+      else
+        v = Lam_s[lane * (KP + 1) + j] + alpha * (double)Gs[lane * ld + j];
+    } else {
+      v = (lane == j) ? (F)1 : (F)0;
+    }
+    a[j] = v;
+    if (j == lane) d0 = v;
+  }
+}
+
+// FP64 finish of one row by one warp: MM = Lambda + alpha * G from the Gram tile Gs, Cholesky,
+// solves and noise in FP64 (the FP64 path, and the retry of a row whose FP32 factor failed).
+// Kept out of line so the FP32 path's register budget does not pay for it.  Writes the row and
+// returns true, or returns false when the FP64 factor fails too.
+template <int KP, typename GT>
+__device__ __forceinline__ bool warp_finish_f64_body(const GT* Gs, int ld, const double* Lam_s,
+                                             double rac_lm, const SampleParams& p, int row,
+                                             uint32_t sweep, unsigned char* work) {
+  const int lane = threadIdx.x & 31;
+  const int K = p.K;
+  double a[KP], d0 = 1.0, rinv = 1.0;
+  const double z = row_noise(p, row, K, lane, sweep);
+  warp_load_mm<double, GT, KP>(a, d0, Gs, ld, Lam_s, p.alpha, lane, K);
+  __syncwarp();
+  double* Lc = reinterpret_cast<double*>(work);  // the Gram tile has been read into a[]
+  if (!warp_factor<double, KP>(a, rinv, lane, 0.0, d0, Lc, KP + 4)) return false;
+  const double x = warp_solve<double, KP>(a, rinv, rac_lm, lane, Lc, KP + 4, z);
+  if (lane < K) {
+    if (p.out_f64) {
+      p.out_f64[(size_t)row * KP + lane] = x;
+    } else {
+      p.out_f32[(size_t)row * KP + lane] = (float)x;
+      p.out_bf16[(size_t)row * KP + lane] = __float2bfloat16_rn((float)x);
+    }
+  }
+  return true;
+}
+
+template <int KP, typename GT>
+__device__ __noinline__ bool warp_finish_f64(const GT* Gs, int ld, const double* Lam_s,
+                                             double rac_lm, const SampleParams& p, int row,
+                                             uint32_t sweep, unsigned char* work) {
+  return warp_finish_f64_body<KP, GT>(Gs, ld, Lam_s, rac_lm, p, row, sweep, work);
+}
+
+}  // namespace mg

@@ -212,7 +212,7 @@ struct Prior {
   DBuf<double> fval, tval;
   DBuf<float> fvalf, tvalf;
   DevCsr F, Ft;
-  DBuf<double> beta, uhat, tmp, B, Lchol, lambda_beta, bb_partials;
+  DBuf<double> beta, uhat, tmp, B, Lchol, lambda_beta, bb_partials, bb_final;
   double lambda_beta0 = 5.0, tol = 1e-6;
   double lb_mu0 = 1.0, lb_nu0 = 1e-3;
   BlockCg cg;
@@ -401,11 +401,13 @@ class Context {
         p.Lchol.alloc_zero((size_t)K_ * K_, s_);
         p.lambda_beta.upload(&p.lambda_beta0, 1, s_);
         p.bb_partials.alloc((size_t)stats_blocks(p.nfeat) * (K_ + K_ * K_));
+        p.bb_final.alloc((size_t)(K_ + K_ * K_));
         p.cg.reserve(p.F.nrow, p.nfeat, 64, mixed_);
       }
     }
     const long long maxN = std::max(dims_[0], dims_[1]);
     stat_partials_.alloc((size_t)stats_blocks(maxN) * (K_ + K_ * K_));
+    stat_final_.alloc((size_t)(K_ + K_ * K_));
     nwbuf_.alloc(3 * (size_t)K_ + 4 * (size_t)K_ * K_);
     nw_.vec = nwbuf_.p;
     nw_.m0 = nwbuf_.p + 3 * K_;
@@ -502,21 +504,24 @@ class Context {
   void update_prior(int mode) {
     Prior& p = prior_[mode];
     const long long N = dims_[mode];
-    launches_ += p.macau ? 0 : 2;  // Macau launches are counted by kernels_in_cg below
+    launches_ += p.macau ? 0 : 3;  // Macau launches are counted by kernels_in_cg below
     const int nb = stats_blocks(N);
+    const int rec = K_ + K_ * K_;
     launch_stats(latents(mode), mixed_, p.macau ? p.uhat.p : nullptr, N, K_, KP_, KP_,
                  stat_partials_.p, nb, s_);
+    launch_reduce_parts(stat_partials_.p, nb, rec, stat_final_.p, s_);
     if (!p.macau) {  // BPMFPrior::update_prior (latentprior.cpp:79-81)
-      launch_normal_wishart(stat_partials_.p, nb, N, K_, p.mu0.p, p.b0, p.WI.p, p.df, nullptr,
-                            0, nullptr, nw_, ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
+      launch_normal_wishart(stat_final_.p, 1, N, K_, p.mu0.p, p.b0, p.WI.p, p.df, nullptr, 0,
+                            nullptr, nw_, ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
       return;
     }
     // MacauPrior::update_prior (latentprior.cpp:255-264)
     const int nbb = stats_blocks(p.nfeat);
     launch_stats(p.beta.p, false, nullptr, p.nfeat, K_, CP_, 0, p.bb_partials.p, nbb, s_);
-    launch_normal_wishart(stat_partials_.p, nb, N, K_, p.mu0.p, p.b0, p.WI.p,
-                          p.df + (int)p.nfeat, p.bb_partials.p, nbb, p.lambda_beta.p, nw_,
-                          ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
+    launch_reduce_parts(p.bb_partials.p, nbb, rec, p.bb_final.p, s_);
+    launch_normal_wishart(stat_final_.p, 1, N, K_, p.mu0.p, p.b0, p.WI.p, p.df + (int)p.nfeat,
+                          p.bb_final.p, 1, p.lambda_beta.p, nw_, ctl_.p, cfg_.seed, mode, p.mu.p,
+                          p.Lambda.p, s_);
     // sample_beta (latentprior.cpp:273-293)
     launch_small_chol(p.Lambda.p, K_, p.Lchol.p, ctl_.p, s_);
     launch_beta_rhs_tmp(latents(mode), mixed_, KP_, N, K_, p.Lchol.p, p.mu.p, ctl_.p, cfg_.seed,
@@ -525,14 +530,15 @@ class Context {
                       mode, p.B.p, CP_, s_);
     p.cg_iters = p.cg.solve(p.F, p.Ft, 0.0, p.lambda_beta.p, p.B.p, CP_, K_, p.tol, p.beta.p,
                             CP_, ctl_.p, s_, mixed_);
-    // stats x2, NW, chol, tmp, spmm, noise, uhat spmm, lambda_beta + the CG's launches
-    launches_ += 9 + 6 + 8LL * p.cg_iters;
+    // stats x3 (+ reductions), NW, chol, tmp, spmm, noise, uhat spmm, lambda_beta + the CG's
+    launches_ += 12 + 6 + 8LL * p.cg_iters;
     // compute_uhat (linop.h:196-198): Uhat = beta F^T, one K-vector per row of F
     launch_spmm(p.F, p.beta.p, CP_, p.uhat.p, KP_, K_, false, s_);
     // sample_lambda_beta with the new beta and Lambda (latentprior.cpp:263)
     launch_stats(p.beta.p, false, nullptr, p.nfeat, K_, CP_, 0, p.bb_partials.p, nbb, s_);
-    launch_lambda_beta(p.bb_partials.p, nbb, K_, p.nfeat, p.Lambda.p, p.lb_nu0, p.lb_mu0,
-                       ctl_.p, cfg_.seed, mode, p.lambda_beta.p, s_);
+    launch_reduce_parts(p.bb_partials.p, nbb, rec, p.bb_final.p, s_);
+    launch_lambda_beta(p.bb_final.p, 1, K_, p.nfeat, p.Lambda.p, p.lb_nu0, p.lb_mu0, ctl_.p,
+                       cfg_.seed, mode, p.lambda_beta.p, s_);
   }
 
   void eval(int n_fixed) {
@@ -956,7 +962,7 @@ class Context {
   DBuf<float> lat32_[2];
   DBuf<__nv_bfloat16> lat16_[2];
   CUtensorMap tmap_[2];  // tensor-core sampler: gather maps over lat16_ of the other mode
-  DBuf<double> scratch_, stat_partials_, nwbuf_;
+  DBuf<double> scratch_, stat_partials_, stat_final_, nwbuf_;
   NwWork nw_{};
   DBuf<Ctl> ctl_;
   DBuf<int> trow_, tcol_;

@@ -3,6 +3,10 @@
 //   k_stats           per-block partial sums of x and x x^T over the rows of a latent matrix
 //                     (optionally x = U - Uhat, the Macau residual of latentprior.cpp:257);
 //                     FP64 accumulation from FP64 or FP32 latents.
+//   k_stats32         the same for K <= 32 with 4 x 4 register tiles of the outer product (four
+//                     row groups per block, summed in group order at the end).
+//   k_nw32            k_normal_wishart for K <= 32: shared-memory matrices, warp-register
+//                     Cholesky factors (warp_finish.cuh) and a warp-parallel triangular inverse.
 //   k_normal_wishart  one CTA: reduces the partials in block order (deterministic), then
 //                     CondNormalWishart -> NormalWishart -> Wishart/WishartUnit -> MvNormal_prec
 //                     (mvnormal.cpp:169-184, 217-287, 314-336) in FP64 with keyed draws.
@@ -12,6 +16,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "rng.cuh"
+#include "warp_finish.cuh"
 
 namespace mg {
 namespace {
@@ -326,10 +331,280 @@ __global__ void k_set_sweep(Ctl* ctl, uint32_t sweep, int burnin) {
 
 __global__ void k_advance(Ctl* ctl) { ctl->sweep += 1u; }
 
+// Column sums and outer-product sums of rows r0 .. r1 - 1 of (U - Uhat) for K <= 32: thread t
+// owns the 4 x 4 tile (4 (t % 64) / 8 .., 4 (t % 8) ..) for the rows of row group t / 64 (every
+// fourth staged row); the four groups are summed in group order at the end.  The next 32 rows
+// are loaded into registers while the current ones are multiplied (double-buffered staging).
+template <typename T>
+__device__ __forceinline__ void stats_load(const T* U, const double* Uhat, long long b0, int cnt,
+                                           int K, int stride, int uhat_stride, int t,
+                                           double (&nx)[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int e = t + kStatThreads * q, r = e >> 5, k = e & 31;
+    double x = 0.0;
+    if (r < cnt && k < K) {
+      x = (double)U[(b0 + r) * stride + k];
+      if (Uhat) x -= Uhat[(b0 + r) * uhat_stride + k];
+    }
+    nx[q] = x;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kStatThreads)
+    k_stats32(const T* __restrict__ U, const double* __restrict__ Uhat, long long N, int K,
+              int stride, int uhat_stride, long long rows_per_block, double* __restrict__ partials) {
+  static_assert(kStatRows * 32 == 4 * kStatThreads, "four staged values per thread");
+  __shared__ __align__(16) double xs[2][kStatRows][36];
+  __shared__ double red[3][64][17];
+  const int KK = K * K;
+  const int t = threadIdx.x, tile = t & 63, rg = t >> 6;
+  const int ti = tile >> 3, tj = tile & 7;
+  const long long r0 = (long long)blockIdx.x * rows_per_block;
+  const long long r1 = min(N, r0 + rows_per_block);
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+  double su = 0.0;
+  double nx[4];
+  stats_load(U, Uhat, r0, (int)max(0LL, min((long long)kStatRows, r1 - r0)), K, stride,
+             uhat_stride, t, nx);
+  int buf = 0;
+  for (long long b0 = r0; b0 < r1; b0 += kStatRows) {
+    const int cnt = (int)min((long long)kStatRows, r1 - b0);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = t + kStatThreads * q;
+      xs[buf][e >> 5][e & 31] = nx[q];
+    }
+    __syncthreads();
+    const long long nb0 = b0 + kStatRows;
+    if (nb0 < r1)
+      stats_load(U, Uhat, nb0, (int)min((long long)kStatRows, r1 - nb0), K, stride, uhat_stride,
+                 t, nx);
+    if (t < K)
+      for (int r = 0; r < cnt; r++) su += xs[buf][r][t];
+#pragma unroll 2
+    for (int r = rg; r < kStatRows; r += 4) {
+      const double2 i01 = *reinterpret_cast<const double2*>(&xs[buf][r][4 * ti]);
+      const double2 i23 = *reinterpret_cast<const double2*>(&xs[buf][r][4 * ti + 2]);
+      const double2 j01 = *reinterpret_cast<const double2*>(&xs[buf][r][4 * tj]);
+      const double2 j23 = *reinterpret_cast<const double2*>(&xs[buf][r][4 * tj + 2]);
+      const double xi[4] = {i01.x, i01.y, i23.x, i23.y}, xj[4] = {j01.x, j01.y, j23.x, j23.y};
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = fma(xi[a], xj[b], acc[a][b]);
+    }
+    buf ^= 1;
+  }
+  __syncthreads();
+  if (rg > 0)
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) red[rg - 1][tile][a * 4 + b] = acc[a][b];
+  __syncthreads();
+  double* out = partials + (size_t)blockIdx.x * (K + KK);
+  if (t < K) out[t] = su;
+  if (rg == 0) {
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const double v = ((acc[a][b] + red[0][tile][a * 4 + b]) + red[1][tile][a * 4 + b]) +
+                         red[2][tile][a * 4 + b];
+        const int i = 4 * ti + a, j = 4 * tj + b;
+        if (i < K && j < K) out[K + i + j * K] = v;
+      }
+  }
+}
+
+// Sums `nparts` partial records of `len` doubles in a fixed order: CTA c owns elements
+// 32 c .. 32 c + 31; warp w adds partials w, w + 8, ... in order, then the 8 warp sums are added
+// in warp order.  out = one record.
+__global__ void __launch_bounds__(256)
+    k_reduce_parts(const double* __restrict__ parts, int nparts, int len, double* __restrict__ out) {
+  __shared__ double ws[8][33];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = blockIdx.x * 32 + lane;
+  double s = 0.0;
+  if (e < len) {
+#pragma unroll 8
+    for (int b = warp; b < nparts; b += 8) s += parts[(size_t)b * len + e];
+  }
+  ws[warp][lane] = s;
+  __syncthreads();
+  if (warp == 0 && e < len) {
+    double t = ws[0][lane];
+#pragma unroll
+    for (int w = 1; w < 8; w++) t += ws[w][lane];
+    out[e] = t;
+  }
+}
+
+// CondNormalWishart -> NormalWishart -> MvNormal_prec (mvnormal.cpp:169-184, 217-287, 314-336)
+// for K <= 32 in one CTA of 256 threads, matrices in shared memory (row-major, ld 33), same
+// draws as k_normal_wishart.  Two identities replace two of the reference's three Cholesky
+// factorisations (results agree to FP64 rounding):
+//   * chol(X^{-1}) = J M^{-T} J with M = chol(J X J), J the index reversal: one Cholesky of the
+//     reversed X (warp 0's registers, warp_factor) and one triangular inverse Y = M^{-1}
+//     (lane c solves M y = e_c), L(i, j) = Y(K-1-j, K-1-i);
+//   * Lambda = L c^T c L^T = B B^T with B = L c^T lower triangular with positive diagonal, so
+//     chol(kappa_c Lambda) = sqrt(kappa_c) B and mu = mu_c + B^{-T} z / sqrt(kappa_c).
+// The Bartlett factor c and z are drawn by warps 1-7 while warp 0 factorises.
+constexpr int kNwLd = 33;
+constexpr int kNwLc = 36;
+
+__global__ void __launch_bounds__(256)
+    k_nw32(const double* __restrict__ partials, int nparts, long long N, int K,
+           const double* __restrict__ mu0, double kappa, const double* __restrict__ T0, int nu,
+           const double* __restrict__ bb_partials, int bb_nparts,
+           const double* __restrict__ lambda_beta, Ctl* ctl, unsigned long long seed, int mode,
+           double* __restrict__ mu_out, double* __restrict__ Lambda_out) {
+  __shared__ double A[32 * kNwLd], Bm[32 * kNwLd], C[32 * kNwLd], D[32 * kNwLd];
+  __shared__ __align__(16) double Lc[32 * kNwLc];
+  __shared__ double NU[32], muc[32], m0[32], rl[32], zs[32];
+  __shared__ int flag;
+  const int t = threadIdx.x, lane = t & 31;
+  const int KK = K * K;
+  const uint32_t sweep = ctl->sweep;
+  // 1. reduce partials in block order: NU = sum x, A = S = sum x x^T; Bm = T.  Thread t sums
+  //    elements t + 256 q (q < 5) together so that its loads of one partial are in flight at once.
+  {
+    double sv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+    for (int b = 0; b < nparts; b++) {
+      const double* pb = partials + (size_t)b * (K + KK);
+#pragma unroll
+      for (int q = 0; q < 5; q++)
+        if (t + 256 * q < K + KK) sv[q] += pb[t + 256 * q];
+    }
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      const int e = t + 256 * q;
+      if (e < K) NU[e] = sv[q];
+      else if (e < K + KK) A[((e - K) % K) * kNwLd + (e - K) / K] = sv[q];
+    }
+  }
+  if (bb_partials) {  // T = WI + lambda_beta * beta beta^T  (latentprior.cpp:258-260)
+    const double lb = *lambda_beta;
+    double sv[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+    for (int b = 0; b < bb_nparts; b++) {
+      const double* pb = bb_partials + (size_t)b * (K + KK) + K;
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (t + 256 * q < KK) sv[q] += pb[t + 256 * q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = t + 256 * q;
+      if (e < KK) Bm[(e % K) * kNwLd + e / K] = T0[e] + lb * sv[q];
+    }
+  } else {
+    for (int e = t; e < KK; e += blockDim.x) Bm[(e % K) * kNwLd + e / K] = T0[e];
+  }
+  if (t < K) m0[t] = mu0[t];
+  __syncthreads();
+  const double kappa_c = kappa + (double)N;
+  const int nu_c = nu + (int)N;
+  if (t < K) muc[t] = (kappa * m0[t] + NU[t]) / kappa_c;
+  __syncthreads();
+  // 2. X = T + NS + kappa mu0 mu0^T - kappa_c mu_c mu_c^T   (into A)
+  for (int e = t; e < KK; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    A[i * kNwLd + j] =
+        Bm[i * kNwLd + j] + A[i * kNwLd + j] + kappa * m0[i] * m0[j] - kappa_c * muc[i] * muc[j];
+  }
+  __syncthreads();
+  if (t < 32) {
+    // 3a. M = chol(J X J), M^T rows into Lc
+    double a[32], d0 = 1.0, rinv = 1.0;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      a[j] = (lane < K && j < K) ? A[(K - 1 - lane) * kNwLd + (K - 1 - j)] : (lane == j ? 1.0 : 0.0);
+      if (j == lane) d0 = a[j];
+    }
+    const bool ok = warp_factor<double, 32>(a, rinv, lane, 0.0, d0, Lc, kNwLc);
+    if (lane == 0) flag = ok ? 1 : 0;
+    // 3b. Y = M^{-1}: lane c solves M y = e_c; Y(i, c) into D
+    if (ok) {
+      rl[lane] = rinv;
+      __syncwarp();
+      double y[32];
+#pragma unroll
+      for (int i = 0; i < 32; i++) {
+        double s = (lane == i) ? 1.0 : 0.0;
+#pragma unroll
+        for (int q = 0; q < i; q++) s = fma(-Lc[q * kNwLc + i], y[q], s);
+        y[i] = s * rl[i];
+      }
+#pragma unroll
+      for (int i = 0; i < 32; i++) D[i * kNwLd + lane] = y[i];
+    }
+  } else {
+    // 3c. Bartlett factor c (upper) into C: c_ii = sqrt(2 Gamma((nu_c - i)/2)), c_ij ~ N(0,1);
+    //     z for the mean draw
+    for (int e = t - 32; e < KK; e += blockDim.x - 32) {
+      const int i = e % K, j = e / K;
+      double v = 0.0;
+      if (i == j)
+        v = sqrt(2.0 * gamma_draw(seed, sweep, stream_id(kWishartDiag, mode), (uint32_t)i,
+                                  0.5 * (double)(nu_c - i)));
+      else if (j > i)
+        v = normal_draw(seed, sweep, stream_id(kWishartOff, mode), (uint32_t)i,
+                        (uint32_t)(j - i - 1));
+      C[i * kNwLd + j] = v;
+    }
+    if (t - 32 < K) zs[t - 32] = normal_draw(seed, sweep, stream_id(kMuDraw, mode), 0u, (uint32_t)(t - 32));
+  }
+  __syncthreads();
+  if (!flag) {
+    if (t == 0) atomicOr(&ctl->status, kStatHyperFail);
+    return;
+  }
+  // 4. L = chol(T_c) = chol(X^{-1}) into A: L(i, j) = Y(K-1-j, K-1-i), j <= i
+  for (int e = t; e < KK; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    A[i * kNwLd + j] = (j <= i) ? D[(K - 1 - j) * kNwLd + (K - 1 - i)] : 0.0;
+  }
+  __syncthreads();
+  // 5. B = L c^T (lower triangular): B(i, j) = sum_{q=j..i} L(i, q) c(j, q)
+  for (int e = t; e < KK; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    double s = 0.0;
+    for (int q = j; q <= i; q++) s += A[i * kNwLd + q] * C[j * kNwLd + q];
+    Bm[i * kNwLd + j] = (j <= i) ? s : 0.0;
+  }
+  __syncthreads();
+  // 6. Lambda = B B^T
+  for (int e = t; e < KK; e += blockDim.x) {
+    const int i = e % K, j = e / K;
+    const int m = min(i, j);
+    double s = 0.0;
+    for (int q = 0; q <= m; q++) s += Bm[i * kNwLd + q] * Bm[j * kNwLd + q];
+    Lambda_out[e] = s;
+  }
+  // 7. mu = mu_c + B^{-T} z / sqrt(kappa_c)
+  if (t < 32) {
+    double x = lane < K ? zs[lane] / sqrt(kappa_c) : 0.0;
+    for (int j = K - 1; j >= 0; j--) {
+      if (lane == j) x = x / Bm[j * kNwLd + j];
+      const double xj = __shfl_sync(0xffffffffu, x, j);
+      if (lane < j) x = fma(-Bm[j * kNwLd + lane], xj, x);
+    }
+    if (lane < K) mu_out[lane] = x + muc[lane];
+  }
+}
+
 }  // namespace
 
 int stats_blocks(long long N) {
-  long long b = (N + 511) / 512;
+  long long b = (N + 127) / 128;
   if (b > 1184) b = 1184;
   return (int)(b < 1 ? 1 : b);
 }
@@ -338,6 +613,16 @@ void launch_stats(const void* U, bool f32, const double* Uhat, long long N, int 
                   int uhat_stride, double* partials, int nblocks, cudaStream_t s) {
   if (K > 128) throw MgError(MG_ERR_ARG, "K > 128 is not supported");
   const long long rpb = (N + nblocks - 1) / nblocks;
+  if (K <= 32) {
+    if (f32)
+      k_stats32<float><<<nblocks, kStatThreads, 0, s>>>((const float*)U, Uhat, N, K, stride,
+                                                        uhat_stride, rpb, partials);
+    else
+      k_stats32<double><<<nblocks, kStatThreads, 0, s>>>((const double*)U, Uhat, N, K, stride,
+                                                         uhat_stride, rpb, partials);
+    MG_CUDA(cudaGetLastError());
+    return;
+  }
   const int per = (K * K + kStatThreads - 1) / kStatThreads;
 #define MG_STATS(P)                                                                         \
   if (per <= P) {                                                                           \
@@ -357,14 +642,23 @@ void launch_stats(const void* U, bool f32, const double* Uhat, long long N, int 
 #undef MG_STATS
 }
 
+void launch_reduce_parts(const double* parts, int nparts, int len, double* out, cudaStream_t s) {
+  k_reduce_parts<<<(len + 31) / 32, 256, 0, s>>>(parts, nparts, len, out);
+  MG_CUDA(cudaGetLastError());
+}
+
 void launch_normal_wishart(const double* partials, int nparts, long long N, int K,
                            const double* mu0, double kappa, const double* T0, int nu,
                            const double* bb_partials, int bb_nparts, const double* lambda_beta,
                            const NwWork& w, Ctl* ctl, unsigned long long seed, int mode,
                            double* mu_out, double* Lambda_out, cudaStream_t s) {
-  k_normal_wishart<<<1, 256, 0, s>>>(partials, nparts, N, K, mu0, kappa, T0, nu, bb_partials,
-                                     bb_nparts, lambda_beta, w, ctl, seed, mode, mu_out,
-                                     Lambda_out);
+  if (K <= 32)
+    k_nw32<<<1, 256, 0, s>>>(partials, nparts, N, K, mu0, kappa, T0, nu, bb_partials, bb_nparts,
+                             lambda_beta, ctl, seed, mode, mu_out, Lambda_out);
+  else
+    k_normal_wishart<<<1, 256, 0, s>>>(partials, nparts, N, K, mu0, kappa, T0, nu, bb_partials,
+                                       bb_nparts, lambda_beta, w, ctl, seed, mode, mu_out,
+                                       Lambda_out);
   MG_CUDA(cudaGetLastError());
 }
 

@@ -28,6 +28,8 @@ struct NwWork {
   double* m3;
 };
 int stats_blocks(long long N);
+// Sums `nparts` records of `len` doubles (stats partials) into one record, in a fixed order.
+void launch_reduce_parts(const double* parts, int nparts, int len, double* out, cudaStream_t s);
 void launch_stats(const void* U, bool f32, const double* Uhat, long long N, int K, int stride,
                   int uhat_stride, double* partials, int nblocks, cudaStream_t s);
 void launch_normal_wishart(const double* partials, int nparts, long long N, int K,

@@ -34,7 +34,7 @@ METRIC = "Gibbs sweeps/s at K=32: mixed-prec batched vs FP64 plain, equal test R
 UNIT = "sweeps/s"
 K_LATENT = 32
 ALPHA = 2.0
-PROFILE_SUMMARY = ROOT / "profiles" / "k_sample_mixed_bpmf_powerlaw_k32.txt"
+PROFILE_SUMMARY = ROOT / "profiles" / "k_gram_tc_bpmf_powerlaw_k32.md"
 
 
 def parse_args():
@@ -150,16 +150,9 @@ def sampler_bytes(st, w, compute, mode):
     return nnz * (4 + 8) + tasks + No * KP * 8 + N * KP * 8
 
 
-def sampler_flops(w, st, mode):
-    """Algorithmic flops of one sampler launch: lower-triangle Gram (K(K+1) per entry), the
-    right-hand side (2K per entry), Cholesky + two solves + Lambda mu per row."""
-    K = K_LATENT
-    N = w["shape"][mode]
-    return st["nnz"][mode] * (K * (K + 1) + 2 * K) + N * (K ** 3 / 3 + 6 * K * K)
-
-
 def read_traffic():
-    """DRAM bytes per sampler launch from the committed ncu summary (one capture), if any."""
+    """DRAM bytes per half-sweep of the sampler (k_gram_tc + k_finish_tc, mean of the two modes,
+    full size) from the committed ncu summary, if any."""
     try:
         for line in PROFILE_SUMMARY.read_text().splitlines():
             if line.startswith("dram_bytes_per_launch:"):
@@ -324,19 +317,27 @@ def run_ours(args):
     d2h = st_e["d2h_bytes"] - d2h0
     del preds
 
-    # ---- roofline of the dominant kernel (latent sampler, both modes) ----
+    # ---- roofline of the dominant step: the latent sampler (k_gram_tc + k_finish_tc) ----
     hbm, tflops, src = peaks()
     b = sampler_bytes(st_mx, w, "mixed", 0) + sampler_bytes(st_mx, w, "mixed", 1)
-    t_launch = (ph[0] + ph[1]) / (2 * nph)     # mean seconds per sampler launch
+    t_launch = (ph[0] + ph[1]) / (2 * nph)     # mean seconds per half-sweep of the sampler
     achieved = b / 2 / t_launch / 1e9
     traffic = read_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
-                "kernel": "k_sample (latent sampler, mixed), mean of the two modes",
-                "algorithmic_bytes_per_launch": b / 2,
-                "gram_tflops": (sampler_flops(w, st_mx, 0) + sampler_flops(w, st_mx, 1))
-                / (ph[0] + ph[1]) * nph / 1e12,
-                "gram_tflops_peak_bf16": tflops}
+                "kernel": "latent sampler half-sweep (k_gram_tc + k_finish_tc), mean of the two "
+                          "modes, CUDA events on the library stream",
+                "algorithmic_bytes_per_launch": b / 2}
+    if ph[5] > 0:
+        t_gram = (ph[5] + ph[6]) / (2 * nph)   # mean seconds per k_gram_tc launch
+        gflop = sum(st_mx["nnz"][m] * (K_LATENT * (K_LATENT + 1) + 2 * K_LATENT) for m in (0, 1)) / 2
+        gathered = sum(st_mx["nnz"][m] for m in (0, 1)) / 2 * K_LATENT * 2
+        roofline["gram_kernel"] = {
+            "name": "k_gram_tc", "ms_per_launch": t_gram * 1e3,
+            "share_of_sampler": (ph[5] + ph[6]) / (ph[0] + ph[1]),
+            "algorithmic_tflops": gflop / t_gram / 1e12, "tensor_peak_bf16": tflops,
+            "tensor_frac": gflop / t_gram / 1e12 / tflops,
+            "l2_gather_GBps": gathered / t_gram / 1e9}
     v_mx = world * K / t_mx
     v_fp = world * K / t_fp
     line = {"metric": METRIC, "value": v_mx, "unit": UNIT, "n_gpus": world, "steps": K,
@@ -350,7 +351,8 @@ def run_ours(args):
                           "note": "posterior mean of 20 evaluated sweeps after the timed ones"},
             "phase_ms": {"mixed": [x / nph * 1e3 for x in ph],
                          "fp64": [x / min(K, 20) * 1e3 for x in ph_fp],
-                         "order": ["sample0", "sample1", "prior0", "prior1", "eval"]},
+                         "order": ["sample0", "sample1", "prior0", "prior1", "eval",
+                                   "gram0", "gram1"]},
             "retries_fp64_refactor": retries,
             "gpu_launches": int(round(kernels_per_sweep * K)),
             "clocks": clk.summary(), "roofline": roofline,

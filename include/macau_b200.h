@@ -114,8 +114,9 @@ int mg_sweeps(mg_ctx* ctx, int first_iter, int count, int eval);
  * context's stream (benchmark support; no reference counterpart).  With phase_events = 0 the
  * sweeps run as they would in mg_sweeps (captured graph when possible) and *total_seconds
  * receives the elapsed time; with phase_events = 1 they run un-captured with events between
- * phases and phase_seconds[0..4] receives the summed time of sample mode 0, sample mode 1,
- * update prior 0, update prior 1, evaluation. */
+ * phases and phase_seconds[0..6] receives the summed time of sample mode 0, sample mode 1,
+ * update prior 0, update prior 1, evaluation, then the Gram kernel of the tensor-core sampler
+ * alone in mode 0 and mode 1 (0 when that sampler is not used). */
 int mg_time_sweeps(mg_ctx* ctx, int first_iter, int count, int eval, int phase_events,
                    double* total_seconds, double* phase_seconds);
 

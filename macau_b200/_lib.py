@@ -185,9 +185,10 @@ class Sampler:
 
     def time_sweeps(self, first, count, eval=False, phase_events=False):
         """Device seconds of `count` sweeps (CUDA events on the library stream); with
-        phase_events also the per-phase seconds [sample0, sample1, prior0, prior1, eval]."""
+        phase_events also the per-phase seconds [sample0, sample1, prior0, prior1, eval,
+        gram0, gram1] (gram: the tensor-core Gram kernel alone, 0 when not used)."""
         tot = np.zeros(1)
-        ph = np.zeros(5)
+        ph = np.zeros(7)
         self._chk(lib().mg_time_sweeps(self.h, int(first), int(count), int(bool(eval)),
                                        int(bool(phase_events)), ptr(tot), ptr(ph)))
         return float(tot[0]), ph

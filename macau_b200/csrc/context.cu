@@ -452,7 +452,8 @@ class Context {
   }
 
   // ---- phases ----
-  void sample(int mode, const double* znoise_dev, bool reset_queue = true) {
+  void sample(int mode, const double* znoise_dev, bool reset_queue = true,
+              cudaEvent_t mid = nullptr) {
     launches_ += 1;
     ModeData& md = md_[mode];
     Prior& p = prior_[mode];
@@ -489,7 +490,8 @@ class Context {
       tp.tasks = md.tasks_tc.p;
       tp.ntasks = md.ntasks_tc;
       tp.packed = md.packed_tc.p;
-      if (launch_sample_tc(tp, tmap_[mode], md.gram_tc.p, md.sinfo_tc.p, KP_, s_, num_sms_)) {
+      if (launch_sample_tc(tp, tmap_[mode], md.gram_tc.p, md.sinfo_tc.p, KP_, s_, num_sms_,
+                           mid)) {
         launches_ += 1;  // k_gram_tc + k_finish_tc
         return;
       }
@@ -551,14 +553,15 @@ class Context {
 
   bool graphable() const { return !prior_[0].macau && !prior_[1].macau; }
 
-  // One sweep; ev (optional, 6 events) brackets: sample 0 | sample 1 | prior 0 | prior 1 |
-  // eval + advance.
+  // One sweep; ev (optional, 8 events) brackets: sample 0 | sample 1 | prior 0 | prior 1 |
+  // eval + advance; ev[6], ev[7] end the tensor-core Gram kernel of mode 0, 1 (recorded only
+  // when that sampler runs).
   void sweep_body(bool do_eval, cudaEvent_t* ev = nullptr) {
     MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[0], 0, 8 * sizeof(uint32_t), s_));
     if (ev) MG_CUDA(cudaEventRecord(ev[0], s_));
-    sample(0, nullptr, false);
+    sample(0, nullptr, false, ev ? ev[6] : nullptr);
     if (ev) MG_CUDA(cudaEventRecord(ev[1], s_));
-    sample(1, nullptr, false);
+    sample(1, nullptr, false, ev ? ev[7] : nullptr);
     if (ev) MG_CUDA(cudaEventRecord(ev[2], s_));
     update_prior(0);
     if (ev) MG_CUDA(cudaEventRecord(ev[3], s_));
@@ -576,6 +579,12 @@ class Context {
   void time_sweeps(int first_iter, int count, bool do_eval, bool phase_events, double* total,
                    double* phase) {
     if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_init first");
+    if (count < 1) {
+      if (total) *total = 0.0;
+      if (phase)
+        for (int q = 0; q < 7; q++) phase[q] = 0.0;
+      return;
+    }
     if (!phase_events) {
       // make sure the graph exists before the timed region
       if (graphable() && use_graph_ && !graph_[do_eval ? 1 : 0]) {
@@ -594,27 +603,35 @@ class Context {
       check_status();
       return;
     }
-    std::vector<cudaEvent_t> ev((size_t)count * 6);
+    std::vector<cudaEvent_t> ev((size_t)count * 8);
     for (auto& e : ev) MG_CUDA(cudaEventCreate(&e));
     try {
       launch_set_sweep(ctl_.p, (uint32_t)first_iter, burnin_, s_);
-      for (int i = 0; i < count; i++) sweep_body(do_eval, ev.data() + 6 * (size_t)i);
+      for (int i = 0; i < count; i++) sweep_body(do_eval, ev.data() + 8 * (size_t)i);
       rows_[0] += md_[0].N * count;
       rows_[1] += md_[1].N * count;
       sweeps_done_ += count;
-      MG_CUDA(cudaEventSynchronize(ev.back()));
-      double ph[5] = {0, 0, 0, 0, 0};
-      for (int i = 0; i < count; i++)
+      const bool tc = mixed_ && use_tc_ && KP_ == 32;
+      MG_CUDA(cudaEventSynchronize(ev[8 * (size_t)(count - 1) + 5]));
+      double ph[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int i = 0; i < count; i++) {
+        const cudaEvent_t* e = ev.data() + 8 * (size_t)i;
         for (int q = 0; q < 5; q++) {
           float ms = 0.f;
-          MG_CUDA(cudaEventElapsedTime(&ms, ev[6 * i + q], ev[6 * i + q + 1]));
+          MG_CUDA(cudaEventElapsedTime(&ms, e[q], e[q + 1]));
           ph[q] += ms * 1e-3;
         }
+        for (int m = 0; tc && m < 2; m++) {
+          float ms = 0.f;
+          MG_CUDA(cudaEventElapsedTime(&ms, e[m], e[6 + m]));
+          ph[5 + m] += ms * 1e-3;
+        }
+      }
       float ms = 0.f;
-      MG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev.back()));
+      MG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[8 * (size_t)(count - 1) + 5]));
       if (total) *total = ms * 1e-3;
       if (phase)
-        for (int q = 0; q < 5; q++) phase[q] = ph[q];
+        for (int q = 0; q < 7; q++) phase[q] = ph[q];
     } catch (...) {
       for (auto& e : ev) cudaEventDestroy(e);
       throw;

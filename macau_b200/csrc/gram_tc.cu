@@ -642,7 +642,7 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
 size_t tc_smem_bytes() { return (size_t)kStages * kStageBytes + sizeof(TcShared); }
 
 bool launch_sample_tc(const SampleParams& p, const CUtensorMap& tmap, float* gram,
-                      const int2* sinfo, int KP, cudaStream_t s, int num_sms) {
+                      const int2* sinfo, int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
   if (KP != 32 || p.packed == nullptr) return false;
   static bool configured[64] = {false};
   int dev = 0;
@@ -657,6 +657,7 @@ bool launch_sample_tc(const SampleParams& p, const CUtensorMap& tmap, float* gra
   }
   k_gram_tc<<<num_sms, kTcThreads, smem, s>>>(p, tmap, gram);
   MG_CUDA(cudaGetLastError());
+  if (mid) MG_CUDA(cudaEventRecord(mid, s));
   k_finish_tc<<<num_sms * 2, kFinWarps * 32, fsmem, s>>>(p, gram, sinfo);
   MG_CUDA(cudaGetLastError());
   return true;

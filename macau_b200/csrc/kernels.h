@@ -16,8 +16,10 @@ void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, in
 // zeros).  `gram` holds nrows Gram records of 32 * 32 + 32 floats; sinfo[row] = {parts, scratch
 // slot of part 0} (parts > 1: the row's partial Grams go to p.scratch, 1056 doubles per slot).
 // Returns false when the configuration is not covered (caller uses the CUDA-core kernel).
+// `mid`, if given, is recorded between the two launches (per-kernel timing).
 bool launch_sample_tc(const SampleParams& p, const CUtensorMap& tmap, float* gram,
-                      const int2* sinfo, int KP, cudaStream_t s, int num_sms);
+                      const int2* sinfo, int KP, cudaStream_t s, int num_sms,
+                      cudaEvent_t mid = nullptr);
 
 // ---- hyperprior / eval (hyper_kernels.cu) ----
 struct NwWork {

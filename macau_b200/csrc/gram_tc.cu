@@ -556,13 +556,16 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
   extern __shared__ __align__(16) unsigned char fsm[];
   double* Lam_s = reinterpret_cast<double*>(fsm);
   double* lmu_s = Lam_s + 32 * 33;
-  unsigned char* works = reinterpret_cast<unsigned char*>(lmu_s + 32);
+  float* LamF = reinterpret_cast<float*>(lmu_s + 32);  // (float) Lambda, ld kLc
+  unsigned char* works = reinterpret_cast<unsigned char*>(LamF + 32 * kLc);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int K = p.K;
   const uint32_t sweep = p.ctl->sweep;
   for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
     const int i = e / 32, j = e % 32;
-    Lam_s[i * 33 + j] = (i < K && j < K) ? p.Lambda[i + j * K] : 0.0;
+    const double v = (i < K && j < K) ? p.Lambda[i + j * K] : 0.0;
+    Lam_s[i * 33 + j] = v;
+    LamF[i * kLc + j] = (float)v;
   }
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -572,6 +575,7 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
     lmu_s[lane] = s;
   }
   __syncthreads();
+  const float alpha_f = (float)p.alpha;
   unsigned char* work = works + (size_t)warp * kFinWork;
   float* Gs = reinterpret_cast<float*>(work);
   float* Lc = Gs + 32 * kLD;
@@ -579,6 +583,9 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
   for (int row = blockIdx.x * kFinWarps + warp; row < p.nrows; row += stride) {
     const int2 si = sinfo[row];  // {parts, scratch slot of part 0}
     double rhs;
+    float a[32], d0 = 1.f, rinv = 1.f;
+    const float* G;  // the row's FP32 Gram (record or shared staging), kept for an FP64 retry
+    int ldg;
     if (si.x > 1) {
       // sum the parts in part order, one entry at a time in FP64
       const double* s0 = p.scratch + (size_t)si.y * kGramRec;
@@ -591,17 +598,29 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
       double rs = 0.0;
       for (int prt = 0; prt < si.x; prt++) rs += __ldcg(s0 + (size_t)prt * kGramRec + 32 * 32 + lane);
       rhs = (double)(float)rs;
+      __syncwarp();
+      warp_load_mm<float, float, 32>(a, d0, Gs, kLD, Lam_s, p.alpha, lane, K);
+      G = Gs;
+      ldg = kLD;
     } else {
+      // lane i: row i of Lambda + alpha G straight from the record (same arithmetic as
+      // warp_load_mm: (float) Lambda + (float) alpha * G)
       const float* gp = gram + (size_t)row * kGramRec;
 #pragma unroll
       for (int j = 0; j < 32; j += 4) {
-        const float4 v = __ldcs(reinterpret_cast<const float4*>(gp + lane * 32 + j));
-        Gs[lane * kLD + j] = v.x;
-        Gs[lane * kLD + j + 1] = v.y;
-        Gs[lane * kLD + j + 2] = v.z;
-        Gs[lane * kLD + j + 3] = v.w;
+        const float4 v = __ldcg(reinterpret_cast<const float4*>(gp + lane * 32 + j));
+        const float4 l = *reinterpret_cast<const float4*>(LamF + lane * kLc + j);
+        const float g4[4] = {v.x, v.y, v.z, v.w}, l4[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int jj = j + u;
+          a[jj] = (lane < K && jj < K) ? l4[u] + alpha_f * g4[u] : (lane == jj ? 1.f : 0.f);
+          if (jj == lane) d0 = a[jj];
+        }
       }
-      rhs = (double)__ldcs(gp + 32 * 32 + lane);
+      rhs = (double)__ldcg(gp + 32 * 32 + lane);
+      G = gp;
+      ldg = 32;
     }
     double lm;
     if (p.uhat) {
@@ -614,10 +633,7 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
     } else {
       lm = lmu_s[lane];
     }
-    __syncwarp();
-    float a[32], d0 = 1.f, rinv = 1.f;
     const double z = row_noise(p, row, K, lane, sweep);
-    warp_load_mm<float, float, 32>(a, d0, Gs, kLD, Lam_s, p.alpha, lane, K);
     bool ok = warp_factor<float, 32>(a, rinv, lane, 0x1p-20, d0, Lc, kLc);
     if (ok) {
       const float x = warp_solve<float, 32>(a, rinv, (float)(rhs + lm), lane, Lc, kLc, z);
@@ -627,7 +643,7 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
       }
     } else {
       if (lane == 0) atomicAdd(&p.ctl->retries[p.mode], 1u);
-      ok = warp_finish_f64<32, float>(Gs, kLD, Lam_s, rhs + lm, p, row, sweep, work);
+      ok = warp_finish_f64<32, float>(G, ldg, Lam_s, rhs + lm, p, row, sweep, work);
       if (!ok && lane == 0) {
         atomicOr(&p.ctl->status, kStatCholFail);
         atomicCAS(&p.ctl->bad_row, -1, row);
@@ -648,7 +664,8 @@ bool launch_sample_tc(const SampleParams& p, const CUtensorMap& tmap, float* gra
   int dev = 0;
   MG_CUDA(cudaGetDevice(&dev));
   const size_t smem = tc_smem_bytes();
-  const size_t fsmem = sizeof(double) * (32 * 33 + 32) + (size_t)kFinWarps * kFinWork;
+  const size_t fsmem = sizeof(double) * (32 * 33 + 32) + sizeof(float) * 32 * kLc +
+                       (size_t)kFinWarps * kFinWork;
   if (!configured[dev & 63]) {
     MG_CUDA(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     MG_CUDA(cudaFuncSetAttribute(k_finish_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -48,9 +48,12 @@ __device__ __forceinline__ Vec4<F> lds4(const F* p) {
 // shuffle; columns j+2 onwards read L(k, j) from shared memory (column j published as Lc row j,
 // leading dimension ld, a multiple of 4) as 4-wide broadcasts, off the critical chain.  Every
 // update is the same fma with the same operands as a plain right-looking loop, so the factor
-// does not depend on this scheduling.  rinv receives the lane's 1/L(i, i).  A pivot that is not
-// positive, or falls below rel_floor times the original diagonal d0, fails the whole warp.  On
-// success Lc holds L^T (row j = column j of L).
+// does not depend on this scheduling.  Entries above a lane's diagonal are never read for the
+// factor or the solves, so the updates run unpredicated on every lane (the upper entries of a[]
+// and a[lane] itself receive values that are discarded; a[lane] is overwritten by L(i, i) in
+// its own step).  rinv receives the lane's 1/L(i, i).  A pivot that is not positive, or falls
+// below rel_floor times the original diagonal d0, fails the whole warp.  On success Lc holds
+// L^T (row j = column j of L; its entries above the diagonal are not meaningful).
 template <typename F, int KP>
 __device__ __forceinline__ bool warp_factor(F (&a)[KP], F& rinv, int lane, double rel_floor,
                                             F d0, F* Lc, int ld) {
@@ -61,16 +64,12 @@ __device__ __forceinline__ bool warp_factor(F (&a)[KP], F& rinv, int lane, doubl
   for (int j = 0; j < KP; j++) {
     if (lane == j) bad = !(diag > (F)0) || !(diag > floor);
     const F r = wshfl(mrsqrt(diag), j);
-    if (lane == j) {
-      a[j] = diag * r;
-      rinv = r;
-    } else if (lane > j) {
-      a[j] = a[j] * r;
-    }
+    if (lane == j) rinv = r;
+    a[j] = (lane == j ? diag : a[j]) * r;
     if (j + 1 < KP) {
       const F lnext = wshfl(a[j], j + 1);  // L(j+1, j)
       if (lane > j) diag = mfma(-a[j], a[j], diag);
-      if (lane > j + 1) a[j + 1] = mfma(-a[j], lnext, a[j + 1]);
+      a[j + 1] = mfma(-a[j], lnext, a[j + 1]);
     }
     if (lane < KP) Lc[j * ld + lane] = a[j];
     __syncwarp();
@@ -80,7 +79,7 @@ __device__ __forceinline__ bool warp_factor(F (&a)[KP], F& rinv, int lane, doubl
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const int k = 4 * q + u;
-        if (k > j + 1 && lane > k) a[k] = mfma(-a[j], c.v[u], a[k]);
+        if (k > j + 1) a[k] = mfma(-a[j], c.v[u], a[k]);
       }
     }
   }

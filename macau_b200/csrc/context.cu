@@ -265,15 +265,40 @@ class Context {
     for (long long e = 0; e < nnz; e++)
       if (r[e] < 0 || r[e] >= dims_[0] || c[e] < 0 || c[e] >= dims_[1])
         throw MgError(MG_ERR_ARG, "training index out of range");
-    HostCsr rows = coo_to_csr(r, c, vals, nnz, dims_[0], dims_[1]);
-    HostCsr cols = transpose(rows, dims_[0], dims_[1]);
-    // mean_value = Y.sum() / Y.nonZeros() over the column-major storage (sparsetensor.cpp:82)
+    // CSR of the rows and of the columns, built on the device (build_kernels.cu)
+    long long nu = 0;
+    {
+      DBuf<int> dr, dc;
+      DBuf<double> dv;
+      dr.upload(r, (size_t)nnz, s_);
+      dc.upload(c, (size_t)nnz, s_);
+      dv.upload(vals, (size_t)nnz, s_);
+      for (int m = 0; m < 2; m++) {
+        md_[m].ptr.alloc((size_t)dims_[m] + 1);
+        md_[m].idx.alloc((size_t)nnz);
+        md_[m].val.alloc((size_t)nnz);
+      }
+      nu = build_csr_pair(dr.p, dc.p, dv.p, nnz, dims_[0], dims_[1], md_[0].ptr.p, md_[0].idx.p,
+                          md_[0].val.p, md_[1].ptr.p, md_[1].idx.p, md_[1].val.p, s_);
+    }
+    // mean_value = Y.sum() / Y.nonZeros() over the column-major storage (sparsetensor.cpp:82):
+    // summed on the host in that order
+    std::vector<double> cval((size_t)nu);
+    std::vector<long long> p0((size_t)dims_[0] + 1), p1((size_t)dims_[1] + 1);
+    MG_CUDA(cudaMemcpyAsync(cval.data(), md_[1].val.p, sizeof(double) * nu,
+                            cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaMemcpyAsync(p0.data(), md_[0].ptr.p, sizeof(long long) * p0.size(),
+                            cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaMemcpyAsync(p1.data(), md_[1].ptr.p, sizeof(long long) * p1.size(),
+                            cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    g_d2h_bytes += (long long)(sizeof(double) * nu + sizeof(long long) * (p0.size() + p1.size()));
     double sum = 0.0;
-    for (double v : cols.val) sum += v;
-    ntrain_ = (long long)cols.val.size();
+    for (double v : cval) sum += v;
+    ntrain_ = nu;
     mean_ = sum / (double)ntrain_;
-    upload_mode(0, rows);
-    upload_mode(1, cols);
+    upload_mode(0, p0, nu);
+    upload_mode(1, p1, nu);
     drop_graphs();
     have_data_ = true;
     initialised_ = false;
@@ -894,22 +919,15 @@ class Context {
       }
   }
 
-  void upload_mode(int m, const HostCsr& h) {
+  // Derived layouts of mode m from its device CSR (md.ptr / idx / val, nnz entries) and a host
+  // copy of its row pointers: packed entries, task lists, the padded copy.
+  void upload_mode(int m, const std::vector<long long>& hptr, long long nnz) {
     ModeData& md = md_[m];
     md.N = dims_[m];
-    md.nnz = (long long)h.idx.size();
-    md.ptr.upload(h.ptr.data(), h.ptr.size(), s_);
-    md.idx.upload(h.idx.data(), h.idx.size(), s_);
-    md.val.upload(h.val.data(), h.val.size(), s_);
+    md.nnz = nnz;
     if (mixed_) {
-      std::vector<uint2> pk(md.nnz);
-      for (long long e = 0; e < md.nnz; e++) {
-        const float w = (float)((h.val[e] - mean_) * cfg_.precision);
-        uint32_t bits;
-        std::memcpy(&bits, &w, 4);
-        pk[e] = make_uint2((unsigned)h.idx[e], bits);
-      }
-      md.packed.upload(pk.data(), pk.size(), s_);
+      md.packed.alloc((size_t)std::max(1LL, nnz));
+      launch_pack(md.idx.p, md.val.p, nnz, mean_, cfg_.precision, md.packed.p, s_);
     }
     // Task list: rows sorted by descending length; rows above the split threshold are cut into
     // near-equal parts so that no task is much longer than the average work per row group.
@@ -917,9 +935,9 @@ class Context {
     long long thr = md.nnz / (2 * groups);
     thr = std::max(256LL, std::min(16384LL, thr));
     md.max_len = 0;
-    for (long long r = 0; r < md.N; r++) md.max_len = std::max(md.max_len, h.ptr[r + 1] - h.ptr[r]);
+    for (long long r = 0; r < md.N; r++) md.max_len = std::max(md.max_len, hptr[r + 1] - hptr[r]);
     int nsplit = 0, nslots = 0;
-    std::vector<RowTask> tasks = make_tasks(h.ptr, thr, 1, nsplit, nslots);
+    std::vector<RowTask> tasks = make_tasks(hptr, thr, 1, nsplit, nslots);
     md.ntasks = (int)tasks.size();
     md.nsplit = nsplit;
     md.nslots = nslots;
@@ -929,16 +947,14 @@ class Context {
       const int other_n = (int)dims_[1 - m];
       std::vector<long long> pptr(md.N + 1, 0);
       for (long long r = 0; r < md.N; r++)
-        pptr[r + 1] = pptr[r] + (h.ptr[r + 1] - h.ptr[r] + 15) / 16 * 16;
-      std::vector<uint2> pk(std::max(1LL, pptr[md.N]), make_uint2((unsigned)other_n, 0u));
-      for (long long r = 0; r < md.N; r++)
-        for (long long e = h.ptr[r]; e < h.ptr[r + 1]; e++) {
-          const float w = (float)((h.val[e] - mean_) * cfg_.precision);
-          uint32_t bits;
-          std::memcpy(&bits, &w, 4);
-          pk[pptr[r] + (e - h.ptr[r])] = make_uint2((unsigned)h.idx[e], bits);
-        }
-      md.packed_tc.upload(pk.data(), pk.size(), s_);
+        pptr[r + 1] = pptr[r] + (hptr[r + 1] - hptr[r] + 15) / 16 * 16;
+      {
+        DBuf<long long> dpptr;
+        dpptr.upload(pptr.data(), pptr.size(), s_);
+        md.packed_tc.alloc((size_t)std::max(1LL, pptr[md.N]));
+        launch_pad(md.ptr.p, dpptr.p, md.N, md.packed.p, (unsigned)other_n, md.packed_tc.p, s_);
+        MG_CUDA(cudaStreamSynchronize(s_));
+      }
       const long long thr16 = (thr + 15) / 16 * 16;
       int ns = 0, nsl = 0;
       std::vector<RowTask> tt = make_tasks(pptr, thr16, 16, ns, nsl);

@@ -258,29 +258,58 @@ __global__ void k_lambda_beta(const double* __restrict__ bb_partials, int nparts
 
 constexpr int kEvalThreads = 256;
 
-// One warp per test entry: lanes split the K-dot product (coalesced row reads), lane 0 does
-// the online mean / variance update of that entry.
+// Groups of eight lanes take eight consecutive test entries at a time: for each entry the
+// group reads the two latent rows with vector loads (lane l: elements 4l .. 4l + 3, + 32 j) and
+// sums the partial dots with three shuffles; lane j keeps entry j's prediction and then does
+// the online mean / variance update of eval_rmse (bpmfutils.h:86-114) for it, so the updates
+// and their pred / pvar / value accesses run on all eight lanes.  Per block, the squared errors
+// are summed in lane and group order into partials[2 * block .. + 1].
+template <typename T>
+__device__ __forceinline__ double dot4(const T* u, const T* v) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(u), b = *reinterpret_cast<const float4*>(v);
+    return (double)a.x * (double)b.x + (double)a.y * (double)b.y + (double)a.z * (double)b.z +
+           (double)a.w * (double)b.w;
+  } else {
+    const double2 a0 = *reinterpret_cast<const double2*>(u), a1 = *reinterpret_cast<const double2*>(u + 2);
+    const double2 b0 = *reinterpret_cast<const double2*>(v), b1 = *reinterpret_cast<const double2*>(v + 2);
+    return a0.x * b0.x + a0.y * b0.y + a1.x * b1.x + a1.y * b1.y;
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kEvalThreads)
     k_eval(const int* __restrict__ trow, const int* __restrict__ tcol,
            const double* __restrict__ tval, long long ntest, const T* __restrict__ U,
            const T* __restrict__ V, int K, int stride, double mean, int n_fixed, const Ctl* ctl,
            double* __restrict__ pred, double* __restrict__ pvar, double* __restrict__ partials) {
-  __shared__ double r1[kEvalThreads / 32], r2[kEvalThreads / 32];
+  constexpr int kGroups = kEvalThreads / 8;
+  __shared__ double r1[kGroups], r2[kGroups];
   int n = n_fixed;
   if (n < 0) n = ((int)ctl->sweep < ctl->burnin) ? 0 : (int)ctl->sweep - ctl->burnin;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int g = threadIdx.x >> 3, l = threadIdx.x & 7;
+  const unsigned mask = 0xffu << (8 * ((threadIdx.x & 31) >> 3));
   double se = 0.0, sea = 0.0;
-  const long long nw = (long long)gridDim.x * (kEvalThreads / 32);
-  for (long long t = (long long)blockIdx.x * (kEvalThreads / 32) + wid; t < ntest; t += nw) {
-    const T* v = V + (size_t)tcol[t] * stride;
-    const T* u = U + (size_t)trow[t] * stride;
-    double dot = 0.0;
-    for (int k = lane; k < K; k += 32) dot += (double)v[k] * (double)u[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
-    if (lane == 0) {
-      const double p = dot + mean;
+  const long long step = (long long)gridDim.x * kGroups * 8;
+  for (long long t0 = ((long long)blockIdx.x * kGroups + g) * 8; t0 < ntest; t0 += step) {
+    const long long t = t0 + l;  // this lane's entry
+    const bool own = t < ntest;
+    const int r = own ? trow[t] : 0, c = own ? tcol[t] : 0;
+    double mydot = 0.0;
+#pragma unroll 2
+    for (int j = 0; j < 8; j++) {
+      const int rj = __shfl_sync(mask, r, j, 8), cj = __shfl_sync(mask, c, j, 8);
+      const T* u = U + (size_t)rj * stride;
+      const T* v = V + (size_t)cj * stride;
+      double dot = 0.0;
+      for (int k0 = 4 * l; k0 < K; k0 += 32) dot += dot4<T>(u + k0, v + k0);
+      dot += __shfl_xor_sync(mask, dot, 4, 8);
+      dot += __shfl_xor_sync(mask, dot, 2, 8);
+      dot += __shfl_xor_sync(mask, dot, 1, 8);
+      if (l == j) mydot = dot;
+    }
+    if (own) {
+      const double p = mydot + mean;
       const double y = tval[t];
       se += (y - p) * (y - p);
       double pavg;
@@ -295,14 +324,23 @@ __global__ void __launch_bounds__(kEvalThreads)
       pred[t] = pavg;
     }
   }
-  if (lane == 0) {
-    r1[wid] = se;
-    r2[wid] = sea;
+  // group sums in lane order
+#pragma unroll
+  for (int q = 1; q < 8; q++) {
+    const double a1 = __shfl_sync(mask, se, q, 8), b1 = __shfl_sync(mask, sea, q, 8);
+    if (l == 0) {
+      se += a1;
+      sea += b1;
+    }
+  }
+  if (l == 0) {
+    r1[g] = se;
+    r2[g] = sea;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     double a = 0.0, b = 0.0;
-    for (int q = 0; q < kEvalThreads / 32; q++) {
+    for (int q = 0; q < kGroups; q++) {
       a += r1[q];
       b += r2[q];
     }
@@ -311,14 +349,21 @@ __global__ void __launch_bounds__(kEvalThreads)
   }
 }
 
+// One warp: lane q sums partials q, q + 32, ... in order, then a fixed shuffle tree.
 __global__ void k_eval_finish(const double* partials, int nparts, long long ntest,
                               double* rmse) {
-  if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
-    for (int q = 0; q < nparts; q++) {
-      a += partials[2 * q];
-      b += partials[2 * q + 1];
-    }
+  const int lane = threadIdx.x & 31;
+  double a = 0.0, b = 0.0;
+  for (int q = lane; q < nparts; q += 32) {
+    a += partials[2 * q];
+    b += partials[2 * q + 1];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if (lane == 0) {
     rmse[0] = sqrt(b / (double)ntest);  // posterior-mean RMSE (rmse_test)
     rmse[1] = sqrt(a / (double)ntest);  // single-sample RMSE (rmse_test_onesample)
   }
@@ -671,8 +716,8 @@ void launch_lambda_beta(const double* bb_partials, int nparts, int K, long long 
 }
 
 int eval_blocks(long long ntest) {
-  long long b = (ntest + kEvalThreads / 32 - 1) / (kEvalThreads / 32);
-  if (b > 592) b = 592;
+  long long b = (ntest + kEvalThreads - 1) / kEvalThreads;
+  if (b > 1184) b = 1184;
   return (int)(b < 1 ? 1 : b);
 }
 

@@ -7,6 +7,20 @@
 
 namespace mg {
 
+// ---- data layout construction (build_kernels.cu) ----
+// COO (device) -> CSR of the rows and CSR of the columns, indices ascending, duplicates summed
+// in input order.  Output arrays hold nnz entries (capacity); returns the unique count.
+long long build_csr_pair(const int* d_r, const int* d_c, const double* d_v, long long nnz,
+                         long long nrow, long long ncol, long long* row_ptr, int* row_idx,
+                         double* row_val, long long* col_ptr, int* col_idx, double* col_val,
+                         cudaStream_t s);
+// out[e] = {idx[e], float bits of (val[e] - mean) * alpha}
+void launch_pack(const int* idx, const double* val, long long n, double mean, double alpha,
+                 uint2* out, cudaStream_t s);
+// Row r of `packed` (ptr) copied to pptr[r] and padded to pptr[r + 1] with {sentinel, 0}.
+void launch_pad(const long long* ptr, const long long* pptr, long long nrows, const uint2* packed,
+                unsigned sentinel, uint2* out, cudaStream_t s);
+
 // ---- latent sampler (sample_kernels.cu, gram_tc.cu) ----
 void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, int num_sms);
 // Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only): two

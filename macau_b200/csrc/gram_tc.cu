@@ -29,14 +29,16 @@
 //               counts its 4 producers and the gathered bytes.  One warp issuing TMA
 //               instructions is issue-bound (about 70-90 cycles per instruction), so the issue
 //               is spread over eight warps.
-//   warp 8      scheduler + MMA: takes 4 tasks per group from the work queue and publishes the
-//               group descriptor kAhead groups ahead of the MMAs (the task loads overlap the
-//               MMA waits); allocates TMEM (512 columns: three accumulators of 160 columns); one
-//               lane issues the MMAs, releases stages (tcgen05.commit -> "empty") and publishes
+//   warp 8      MMA: allocates TMEM (512 columns: three accumulators of 160 columns); one lane
+//               issues the MMAs, releases stages (tcgen05.commit -> "empty") and publishes
 //               finished accumulators (tcgen05.commit -> "acc full").
 //   warps 9-12  epilogue (warp w reads TMEM quadrant w % 4 = row slot): TMEM -> registers,
 //               release the accumulator, store the row's FP32 Gram and rhs to its Gram record
-//               (or, for a part of a split row, the FP64 partial to the part's scratch slot).
+//               (or, for a part of a split row, the FP64 partial to the part's scratch slot),
+//               and release the group's descriptor slot ("desc free").
+//   warp 13     scheduler: takes 4 tasks per group from the work queue and publishes the group
+//               descriptors into a ring of kDesc slots as far ahead as the ring allows, so that
+//               the queue atomics and task loads stay off the MMA warp.
 // Every barrier wait is bounded by a clock budget; on expiry the CTA raises an abort flag, all
 // roles leave their loops, the MMA lane drains its MMAs, TMEM is freed and the status word
 // reports a timeout.
@@ -59,7 +61,8 @@ constexpr int kParity = 2;                          // producers per row slot
 constexpr int kProducers = kRowSlots * kParity;     // warps 0-7
 constexpr int kMmaWarp = kProducers;                // warp 8
 constexpr int kEpiWarp0 = kProducers + 1;           // warps 9-12
-constexpr int kTcThreads = (kProducers + 5) * 32;
+constexpr int kSchedWarp = kProducers + 5;           // warp 13
+constexpr int kTcThreads = (kProducers + 6) * 32;
 constexpr int kStages = 16;               // gather stages in flight (even: stage s has parity s % 2)
 constexpr int kBlockBytes = 4 * 512;      // one column block: 4 K-atoms x 512 B
 constexpr int kStageBytes = 5 * kBlockBytes;
@@ -67,7 +70,6 @@ constexpr int kSlots = 3;                 // TMEM accumulators
 constexpr int kSlotCols = 160;            // columns of one accumulator (N = 160)
 constexpr int kCsr = 6;                   // CSR prefetch slots per producer (its k-blocks ahead)
 constexpr int kDesc = 48;                 // group descriptor ring
-constexpr int kAhead = 28;                // groups the scheduler publishes ahead of the MMAs
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
 constexpr int kGramRec = 32 * 32 + 32;    // Gram record: 32 x 32 row-major Gram, then the rhs
 static_assert(kStages % kParity == 0, "a stage's k-blocks all have the same parity");
@@ -84,13 +86,11 @@ struct GroupDesc {
   int stop;    // 1: no more work
 };
 
-// Descriptor ring invariants: the scheduler writes group g + kAhead while the MMAs work on group
-// g.  A producer reads descriptor g while it is at most kStages k-blocks (so at most kStages
-// groups) ahead of the MMAs, and the epilogue reads it before releasing the accumulator of
-// group g, which the MMAs need before group g + kSlots; the slot is rewritten for group
-// g + kDesc only when the MMAs reach g + kDesc - kAhead.
-static_assert(kAhead > kStages + 1 && kDesc - kAhead > kSlots + 1,
-              "descriptor ring too small for the lookahead");
+// Descriptor ring: the scheduler rewrites slot g % kDesc for group g + kDesc only after the
+// epilogue released group g ("desc free"), and the producers, the MMA lane and the epilogue all
+// read a group's descriptor before the epilogue releases it.  The ring must cover the groups
+// the producers run ahead of the MMAs (at most kStages + kCsr k-blocks) and the accumulators.
+static_assert(kDesc > kStages + 2 * kCsr + kSlots, "descriptor ring too small");
 
 struct TcShared {
   uint64_t full[kStages];      // 4 producer arrivals + the gathered bytes
@@ -99,6 +99,7 @@ struct TcShared {
   uint64_t acc_empty[kSlots];  // 4 epilogue warps
   uint64_t drain;
   uint64_t desc_full[kDesc];   // scheduler -> producers, MMA, epilogue
+  uint64_t desc_free[kDesc];   // epilogue (4 warps) -> scheduler
   alignas(16) uint2 csr[kProducers][kCsr][16];  // prefetched CSR k-blocks, per producer
   uint32_t tmem_base;
   int abort;
@@ -340,7 +341,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(&sh->acc_empty[s], 4);
     }
     mbar_init(&sh->drain, 1);
-    for (int d = 0; d < kDesc; d++) mbar_init(&sh->desc_full[d], 1);
+    for (int d = 0; d < kDesc; d++) {
+      mbar_init(&sh->desc_full[d], 1);
+      mbar_init(&sh->desc_free[d], 4);
+    }
     sh->abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -426,37 +430,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     cp_wait<0>();
   } else if (warp == kMmaWarp) {
-    // ================= scheduler + MMA issuer =================
-    int next_t0 = 0;  // lane 0: queue position of the next group to publish
-    if (lane == 0) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
-    int sched = 0;    // next group to publish
-    bool sched_done = false;
-    while (!sched_done && sched < kAhead) {
-      const int t0 = __shfl_sync(0xffffffffu, next_t0, 0);
-      if (lane == 0 && t0 < p.ntasks) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
-      RowTask tk{};
-      const bool has = lane < 4 && t0 + lane < p.ntasks;
-      if (has) tk = p.tasks[t0 + lane];
-      sched_done = publish_group(sh, sched, t0, p.ntasks, tk, has, lane);
-      sched++;
-    }
+    // ================= MMA issuer =================
     int stage = 0;
     uint32_t phase = 0;
     for (int g = 0;; g++) {
-      // start the task loads of the group published at the end of this iteration
-      int t0 = 0;
-      RowTask tk{};
-      bool has = false;
-      if (!sched_done) {
-        t0 = __shfl_sync(0xffffffffu, next_t0, 0);
-        if (lane == 0 && t0 < p.ntasks) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
-        has = lane < 4 && t0 + lane < p.ntasks;
-        if (has) tk = p.tasks[t0 + lane];
-      }
       const int slot = g % kSlots;
       if (g >= kSlots &&
           !mbar_wait(&sh->acc_empty[slot], (uint32_t)(((g / kSlots) & 1) ^ 1), sh, p.ctl))
         break;
+      if (!mbar_wait(&sh->desc_full[g % kDesc], (uint32_t)((g / kDesc) & 1), sh, p.ctl)) break;
       tc_fence_after();
       const uint32_t d_tmem = tmem + (uint32_t)(slot * kSlotCols);
       const GroupDesc& d = sh->desc[g % kDesc];
@@ -483,10 +465,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       if (!ok) break;
       if (lane == 0) mma_commit(&sh->acc_full[slot]);
       __syncwarp();
-      if (!sched_done) {
-        sched_done = publish_group(sh, sched, t0, p.ntasks, tk, has, lane);
-        sched++;
-      }
       if (stop) break;
     }
     // drain: wait for every issued MMA before TMEM is released
@@ -496,6 +474,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       while (!mbar_test(&sh->drain, 0) && clock64() - t0 < kWaitCycles) __nanosleep(128);
     }
     __syncwarp();
+  } else if (warp == kSchedWarp) {
+    // ================= scheduler =================
+    int next_t0 = 0;  // lane 0: queue position of the next group
+    if (lane == 0) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
+    for (int g = 0;; g++) {
+      if (g >= kDesc && !mbar_wait(&sh->desc_free[g % kDesc],
+                                   (uint32_t)(((g / kDesc) - 1) & 1), sh, p.ctl))
+        break;
+      const int t0 = __shfl_sync(0xffffffffu, next_t0, 0);
+      if (lane == 0 && t0 < p.ntasks) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
+      const bool has = lane < 4 && t0 + lane < p.ntasks;
+      const RowTask tk = p.tasks[min(t0 + lane, p.ntasks - 1)];
+      if (publish_group(sh, g, t0, p.ntasks, tk, has, lane)) break;
+    }
   } else {
     // ================= epilogue: accumulators -> Gram records =================
     const int qd = warp & 3;  // TMEM quadrant = row slot of the group
@@ -508,6 +500,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const int stop = d.stop;
       const int row = d.row[qd];
       const int part = d.part[qd], nparts = d.nparts[qd], pslot = d.slot[qd];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh->desc_free[g % kDesc]);
       float gr[32];
       float rhs = 0.f;
       if (!stop) {

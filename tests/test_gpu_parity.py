@@ -269,6 +269,60 @@ def test_mixed_row_sampler_within_tolerance():
     assert relerr(s.latents(0), want) < MIXED_SAMPLE_TOL
 
 
+def heavy_rows_workload(rng, nrow=64, ncol=4000):
+    """Rows 0, 7, 14, ... have 3,900 entries (split into parts by the samplers); the others 1-59."""
+    r, c = [], []
+    for i in range(nrow):
+        n = 3900 if i % 7 == 0 else rng.integers(1, 60)
+        cols = rng.choice(ncol, size=n, replace=False)
+        r += [i] * n
+        c += list(cols)
+    r = np.array(r, np.int32)
+    c = np.array(c, np.int32)
+    return dict(rows=r, cols=c, vals=rng.normal(3.0, 1.0, size=len(r)), shape=(nrow, ncol))
+
+
+@pytest.mark.parametrize("tensor_cores", [1, 0])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_mixed_row_sampler_split_heavy_rows(tensor_cores, mode):
+    # mixed precision at K = 32 through the tensor-core sampler (Gram records, split parts summed
+    # by the finish kernel) and through the CUDA-core sampler, against the FP64 oracle
+    rng = np.random.default_rng(19 + mode)
+    K = 32
+    w = heavy_rows_workload(rng)
+    s = gpu_sampler(w, K, 1.5, seed=3, compute=_lib.MG_COMPUTE_MIXED)
+    s.set_option("tensor_core_gram", tensor_cores)
+    other = 1 - mode
+    Vo = rng.normal(scale=0.3, size=(w["shape"][other], K))
+    s.set_latents(other, Vo)
+    z = rng.normal(size=(w["shape"][mode], K))
+    mu, Lam, _ = s.hyper(mode)
+    s.sample_latents(mode, 0, z)
+    Y = train_matrix(w)
+    R = orc.Csr.from_scipy(Y if mode == 0 else Y.T)
+    want, _ = orc.sample_latents(K, R, Vo, s.mean_value(), 1.5, mu, Lam, z=z)
+    assert relerr(s.latents(mode), want) < MIXED_SAMPLE_TOL
+
+
+@pytest.mark.parametrize("K", [10, 32, 64])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_mixed_row_sampler_keyed_draws(K, mode):
+    # keyed draws (no injection): the mixed samplers draw the same z as the FP64 oracle
+    rng = np.random.default_rng(K + 7 * mode)
+    w = small_uniform(seed=5, nrow=400, ncol=250, nobs=15000)
+    s = gpu_sampler(w, K, 2.0, seed=4242, compute=_lib.MG_COMPUTE_MIXED)
+    other = 1 - mode
+    Vo = rng.normal(scale=0.3, size=(w["shape"][other], K))
+    s.set_latents(other, Vo)
+    mu, Lam, _ = s.hyper(mode)
+    s.sample_latents(mode, 9)
+    Y = train_matrix(w)
+    R = orc.Csr.from_scipy(Y if mode == 0 else Y.T)
+    want, _ = orc.sample_latents(K, R, Vo, s.mean_value(), 2.0, mu, Lam, seed=4242, sweep=9,
+                                 mode=mode)
+    assert relerr(s.latents(mode), want) < MIXED_SAMPLE_TOL
+
+
 def test_cholesky_failure_is_reported_and_context_survives():
     w = small_uniform(seed=4)
     K = 6

@@ -22,13 +22,16 @@
 //
 // Warp roles (one CTA of 13 warps per SM, persistent):
 //   warps 0-7   producers: warp w fills column block r = w % 4 of the stages of the k-blocks
-//               with global index t = w / 4 (mod 2).  Each keeps its own ring of CSR k-blocks
-//               (16 lanes x one 8-byte cp.async per k-block, up to kCsr - 1 of its k-blocks
-//               ahead), stores row r's 16 weights and issues 4 gather4 loads per k-block (a row
-//               with no entries left zero-fills its block instead); a stage's "full" barrier
-//               counts its 4 producers and the gathered bytes.  One warp issuing TMA
-//               instructions is issue-bound (about 70-90 cycles per instruction), so the issue
-//               is spread over eight warps.
+//               with global index t = w / 4 (mod 2): per k-block it takes row r's 16 CSR
+//               entries from the CSR ring of its parity, stores the 16 weights and issues 4
+//               gather4 loads (a row with no entries left zero-fills its block instead); a
+//               stage's "full" barrier counts its 4 producers and the gathered bytes.  One warp
+//               issuing TMA instructions is issue-bound (about 70-90 cycles per instruction),
+//               so the issue is spread over eight warps.
+//   warps 14-15 CSR loaders, one per k-block parity: walk the group descriptors and, up to kCsr
+//               k-blocks of their parity ahead, copy each k-block's four 128-byte row segments
+//               with one 16-byte cp.async per lane into the ring, with a meta record (stage
+//               index, valid rows, stop / end) for the producers.
 //   warp 8      MMA: allocates TMEM (512 columns: three accumulators of 160 columns); one lane
 //               issues the MMAs, releases stages (tcgen05.commit -> "empty") and publishes
 //               finished accumulators (tcgen05.commit -> "acc full").
@@ -62,13 +65,14 @@ constexpr int kProducers = kRowSlots * kParity;     // warps 0-7
 constexpr int kMmaWarp = kProducers;                // warp 8
 constexpr int kEpiWarp0 = kProducers + 1;           // warps 9-12
 constexpr int kSchedWarp = kProducers + 5;           // warp 13
-constexpr int kTcThreads = (kProducers + 6) * 32;
+constexpr int kCsrWarp0 = kProducers + 6;            // warps 14-15
+constexpr int kTcThreads = (kProducers + 8) * 32;
 constexpr int kStages = 16;               // gather stages in flight (even: stage s has parity s % 2)
 constexpr int kBlockBytes = 4 * 512;      // one column block: 4 K-atoms x 512 B
 constexpr int kStageBytes = 5 * kBlockBytes;
 constexpr int kSlots = 3;                 // TMEM accumulators
 constexpr int kSlotCols = 160;            // columns of one accumulator (N = 160)
-constexpr int kCsr = 6;                   // CSR prefetch slots per producer (its k-blocks ahead)
+constexpr int kCsr = 8;                   // CSR ring slots per parity (k-blocks of that parity ahead)
 constexpr int kDesc = 48;                 // group descriptor ring
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
 constexpr int kGramRec = 32 * 32 + 32;    // Gram record: 32 x 32 row-major Gram, then the rhs
@@ -90,7 +94,10 @@ struct GroupDesc {
 // epilogue released group g ("desc free"), and the producers, the MMA lane and the epilogue all
 // read a group's descriptor before the epilogue releases it.  The ring must cover the groups
 // the producers run ahead of the MMAs (at most kStages + kCsr k-blocks) and the accumulators.
-static_assert(kDesc > kStages + 2 * kCsr + kSlots, "descriptor ring too small");
+static_assert(kDesc > kStages + kParity * kCsr + kSlots, "descriptor ring too small");
+
+constexpr int kMetaStop = 16;  // meta flag: the stop group's k-block (nothing valid)
+constexpr int kMetaEnd = 32;   // meta flag: no more k-blocks of this parity
 
 struct TcShared {
   uint64_t full[kStages];      // 4 producer arrivals + the gathered bytes
@@ -100,7 +107,10 @@ struct TcShared {
   uint64_t drain;
   uint64_t desc_full[kDesc];   // scheduler -> producers, MMA, epilogue
   uint64_t desc_free[kDesc];   // epilogue (4 warps) -> scheduler
-  alignas(16) uint2 csr[kProducers][kCsr][16];  // prefetched CSR k-blocks, per producer
+  uint64_t csr_full[kParity][kCsr];   // 32 cp.async completions + the loader's meta arrive
+  uint64_t csr_empty[kParity][kCsr];  // the 4 producers of the parity are done with the slot
+  int2 meta[kParity][kCsr];           // {global k-block index t, valid-row bits | kStop | kEnd}
+  alignas(16) uint2 csr[kParity][kCsr][4][16];  // CSR entries of one k-block: [row slot][16]
   uint32_t tmem_base;
   int abort;
   GroupDesc desc[kDesc];
@@ -162,14 +172,16 @@ __device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap* tma
       : "memory");
 }
 
-// 8-byte asynchronous copy global -> shared (LSU path), completed by cp.async.wait_group.
-__device__ __forceinline__ void cp8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(su32(dst)), "l"(src) : "memory");
+// Waits for every cp.async of this thread.
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// 16-byte asynchronous copy global -> shared (L2 only).
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(su32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+// Arrive on `b` once every earlier cp.async of this thread has completed (the barrier's count
+// includes this arrival).
+__device__ __forceinline__ void cp_arrive_noinc(uint64_t* b) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(su32(b)) : "memory");
 }
 
 __device__ __forceinline__ void fence_proxy_async() {
@@ -345,6 +357,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(&sh->desc_full[d], 1);
       mbar_init(&sh->desc_free[d], 4);
     }
+    for (int h = 0; h < kParity; h++)
+      for (int c = 0; c < kCsr; c++) {
+        mbar_init(&sh->csr_full[h][c], 33);
+        mbar_init(&sh->csr_empty[h][c], kRowSlots);
+      }
     sh->abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -362,49 +379,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
   if (warp < kProducers) {
     // ================= producer of row slot r, parity h =================
-    // CSR cursor `c` copies this producer's k-blocks up to kCsr - 1 ahead; gather cursor `q`
-    // fills column block r of their stages.
     const int r = warp % kRowSlots, h = warp / kRowSlots;
-    Cursor c{0, 0, 0, 0, 0, 0, false, false};
-    bool ok = cursor_load(c, sh, p.ctl, r) && cursor_advance(c, h, sh, p.ctl, r);
-    Cursor q = c;
-    int issued = 0, gathered = 0;
-    while (ok && !q.end) {
-      // ---- top up the CSR prefetch ----
-      while (!c.end && issued - gathered < kCsr - 1) {
-        const int slot = issued % kCsr;
-        if (lane < 16 && !c.stop && c.kb < c.rkb)
-          cp8(&sh->csr[warp][slot][lane], p.packed + c.beg + 16LL * c.kb + lane);
-        cp_commit();  // one group per k-block, empty or not
-        issued++;
-        if (!cursor_advance(c, kParity, sh, p.ctl, r)) {
-          ok = false;
-          break;
-        }
-      }
-      if (!ok) break;
-      // ---- fill column block r of k-block q.t's stage ----
-      const int cslot = gathered % kCsr;
-      // the k-block's copy group is the oldest of the issued - gathered groups in flight
-      if (issued - gathered == kCsr - 1)
-        cp_wait<kCsr - 2>();
-      else
-        cp_wait<0>();
+    for (int i = 0;; i++) {
+      const int slot = i % kCsr;
+      if (!mbar_wait(&sh->csr_full[h][slot], (uint32_t)((i / kCsr) & 1), sh, p.ctl)) break;
+      const int2 m = sh->meta[h][slot];
+      if (m.y & kMetaEnd) break;
+      const bool v = (m.y >> r) & 1;
+      const uint2 ent = sh->csr[h][slot][r][lane & 15];
+      const int stage = m.x % kStages;
+      const uint32_t phase = (uint32_t)((m.x / kStages) & 1);
+      int y[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) y[u] = __shfl_sync(0xffffffffu, (int)ent.x, (4 * lane + u) & 15);
       __syncwarp();
-      const int stage = q.t % kStages;
-      const uint32_t phase = (uint32_t)((q.t / kStages) & 1);
+      if (lane == 0) mbar_arrive(&sh->csr_empty[h][slot]);  // the entries are in registers
       if (!mbar_wait(&sh->empty[stage], phase ^ 1, sh, p.ctl)) break;
-      const bool v = !q.stop && q.kb < q.rkb;
       unsigned char* sbase = stages + (size_t)stage * kStageBytes;
       unsigned char* blk = sbase + r * kBlockBytes;
       if (v) {
-        const uint2 ent = sh->csr[warp][cslot][lane & 15];
         if (lane < 16)
           *reinterpret_cast<__nv_bfloat16*>(sbase + stage_off(128 + r, lane)) =
               __float2bfloat16_rn(__uint_as_float(ent.y));
-        int y[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) y[u] = __shfl_sync(0xffffffffu, (int)ent.x, (4 * lane + u) & 15);
         fence_proxy_async();  // the weights before the async proxy reads them
         __syncwarp();
         if (lane == 0) mbar_expect_tx(&sh->full[stage], 4u * 256u);
@@ -415,8 +411,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // no entries of row r in this k-block: zero k-rows 0..3 of its 4 K-atoms and its weights
 #pragma unroll
         for (int k = 0; k < 2; k++) {
-          const int i = lane + 32 * k;
-          *reinterpret_cast<uint4*>(blk + (i >> 4) * 512 + (i & 15) * 16) = make_uint4(0u, 0u, 0u, 0u);
+          const int e = lane + 32 * k;
+          *reinterpret_cast<uint4*>(blk + (e >> 4) * 512 + (e & 15) * 16) = make_uint4(0u, 0u, 0u, 0u);
         }
         if (lane < 16)
           *reinterpret_cast<__nv_bfloat16*>(sbase + stage_off(128 + r, lane)) = __float2bfloat16_rn(0.f);
@@ -424,11 +420,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(&sh->full[stage]);
       }
-      gathered++;
-      if (!cursor_advance(q, kParity, sh, p.ctl, r)) break;
       __syncwarp();
     }
-    cp_wait<0>();
   } else if (warp == kMmaWarp) {
     // ================= MMA issuer =================
     int stage = 0;
@@ -488,6 +481,35 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const RowTask tk = p.tasks[min(t0 + lane, p.ntasks - 1)];
       if (publish_group(sh, g, t0, p.ntasks, tk, has, lane)) break;
     }
+  } else if (warp >= kCsrWarp0) {
+    // ================= CSR loader of parity h =================
+    // lane l copies entries 2 (l % 8) .. + 1 of row slot l / 8's k-block
+    const int h = warp - kCsrWarp0, rs = lane >> 3, c2 = 2 * (lane & 7);
+    Cursor c{0, 0, 0, 0, 0, 0, false, false};
+    bool ok = cursor_load(c, sh, p.ctl, rs) && cursor_advance(c, h, sh, p.ctl, rs);
+    for (int i = 0; ok; i++) {
+      const int slot = i % kCsr;
+      if (i >= kCsr &&
+          !mbar_wait(&sh->csr_empty[h][slot], (uint32_t)(((i / kCsr) - 1) & 1), sh, p.ctl))
+        break;
+      const bool v = !c.end && !c.stop && c.kb < c.rkb;
+      if (v) cp16(&sh->csr[h][slot][rs][c2], p.packed + c.beg + 16LL * c.kb + c2);
+      cp_arrive_noinc(&sh->csr_full[h][slot]);
+      const unsigned vm = __ballot_sync(0xffffffffu, v);
+      if (lane == 0) {
+        int flags = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) flags |= ((vm >> (8 * q)) & 1u) << q;
+        if (c.end) flags = kMetaEnd;
+        else if (c.stop) flags |= kMetaStop;
+        sh->meta[h][slot] = make_int2(c.t, flags);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh->csr_full[h][slot]);
+      if (c.end) break;
+      ok = cursor_advance(c, kParity, sh, p.ctl, rs);
+    }
+    cp_wait_all();
   } else {
     // ================= epilogue: accumulators -> Gram records =================
     const int qd = warp & 3;  // TMEM quadrant = row slot of the group

@@ -140,19 +140,40 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait on phase `parity`: false on timeout or when another role aborted.
-__device__ bool mbar_wait(uint64_t* b, uint32_t parity, TcShared* sh, Ctl* ctl) {
+// Like mbar_test, but a thread whose phase is not complete may be suspended by the hardware
+// for up to `ns` nanoseconds while it waits, instead of returning at once (no issue slots are
+// spent while suspended).
+__device__ __forceinline__ bool mbar_test_suspend(uint64_t* b, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(ok)
+      : "r"(su32(b)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Slow path of mbar_wait: suspended tries of up to 20 us, the abort flag and the clock budget
+// checked between them.
+__device__ __noinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, TcShared* sh, Ctl* ctl) {
   const long long t0 = clock64();
-  for (int i = 0;; i++) {
-    if (mbar_test(b, parity)) return true;
+  for (;;) {
+    if (mbar_test_suspend(b, parity, 20000u)) return true;
     if (*(volatile int*)&sh->abort) return false;
-    if (i > 32) __nanosleep(128);
     if (clock64() - t0 > kWaitCycles) {
       atomicOr(&ctl->status, kStatTimeout);
       *(volatile int*)&sh->abort = 1;
       return false;
     }
   }
+}
+
+// Bounded wait on phase `parity`: false on timeout or when another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, TcShared* sh, Ctl* ctl) {
+  if (mbar_test(b, parity)) return true;
+  return mbar_wait_slow(b, parity, sh, ctl);
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
@@ -380,27 +401,27 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (warp < kProducers) {
     // ================= producer of row slot r, parity h =================
     const int r = warp % kRowSlots, h = warp / kRowSlots;
+    const uint32_t woff = stage_off(128 + r, lane & 15);  // this lane's weight in a stage
     for (int i = 0;; i++) {
       const int slot = i % kCsr;
       if (!mbar_wait(&sh->csr_full[h][slot], (uint32_t)((i / kCsr) & 1), sh, p.ctl)) break;
       const int2 m = sh->meta[h][slot];
       if (m.y & kMetaEnd) break;
       const bool v = (m.y >> r) & 1;
-      const uint2 ent = sh->csr[h][slot][r][lane & 15];
+      // lane l < 16: entry l's weight; lane l < 4: the columns of entries 4l .. 4l + 3
+      const float w = __uint_as_float(sh->csr[h][slot][r][lane & 15].y);
+      const uint4 c01 = *reinterpret_cast<const uint4*>(&sh->csr[h][slot][r][4 * (lane & 3)]);
+      const uint4 c23 = *reinterpret_cast<const uint4*>(&sh->csr[h][slot][r][4 * (lane & 3) + 2]);
+      const int y[4] = {(int)c01.x, (int)c01.z, (int)c23.x, (int)c23.z};
       const int stage = m.x % kStages;
       const uint32_t phase = (uint32_t)((m.x / kStages) & 1);
-      int y[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) y[u] = __shfl_sync(0xffffffffu, (int)ent.x, (4 * lane + u) & 15);
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh->csr_empty[h][slot]);  // the entries are in registers
       if (!mbar_wait(&sh->empty[stage], phase ^ 1, sh, p.ctl)) break;
       unsigned char* sbase = stages + (size_t)stage * kStageBytes;
       unsigned char* blk = sbase + r * kBlockBytes;
       if (v) {
-        if (lane < 16)
-          *reinterpret_cast<__nv_bfloat16*>(sbase + stage_off(128 + r, lane)) =
-              __float2bfloat16_rn(__uint_as_float(ent.y));
+        if (lane < 16) *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = __float2bfloat16_rn(w);
         fence_proxy_async();  // the weights before the async proxy reads them
         __syncwarp();
         if (lane == 0) mbar_expect_tx(&sh->full[stage], 4u * 256u);
@@ -414,8 +435,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const int e = lane + 32 * k;
           *reinterpret_cast<uint4*>(blk + (e >> 4) * 512 + (e & 15) * 16) = make_uint4(0u, 0u, 0u, 0u);
         }
-        if (lane < 16)
-          *reinterpret_cast<__nv_bfloat16*>(sbase + stage_off(128 + r, lane)) = __float2bfloat16_rn(0.f);
+        if (lane < 16) *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = __float2bfloat16_rn(0.f);
         fence_proxy_async();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sh->full[stage]);
@@ -469,17 +489,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncwarp();
   } else if (warp == kSchedWarp) {
     // ================= scheduler =================
-    int next_t0 = 0;  // lane 0: queue position of the next group
-    if (lane == 0) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
+    // lane 0 keeps four queue claims in flight (q[0] oldest); the next group's tasks are
+    // loaded while the current group is published
+    int q[4] = {0, 0, 0, 0};
+    if (lane == 0) {
+#pragma unroll
+      for (int j = 0; j < 4; j++) q[j] = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
+    }
+    int t_cur = __shfl_sync(0xffffffffu, q[0], 0);
+    RowTask tk_cur = p.tasks[min(t_cur + lane, p.ntasks - 1)];
     for (int g = 0;; g++) {
       if (g >= kDesc && !mbar_wait(&sh->desc_free[g % kDesc],
                                    (uint32_t)(((g / kDesc) - 1) & 1), sh, p.ctl))
         break;
-      const int t0 = __shfl_sync(0xffffffffu, next_t0, 0);
-      if (lane == 0 && t0 < p.ntasks) next_t0 = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
-      const bool has = lane < 4 && t0 + lane < p.ntasks;
-      const RowTask tk = p.tasks[min(t0 + lane, p.ntasks - 1)];
-      if (publish_group(sh, g, t0, p.ntasks, tk, has, lane)) break;
+      if (lane == 0) {
+        q[0] = q[1];
+        q[1] = q[2];
+        q[2] = q[3];
+        if (t_cur < p.ntasks) q[3] = (int)atomicAdd(&p.ctl->queue[p.qslot], 4u);
+      }
+      const int t_nxt = __shfl_sync(0xffffffffu, q[0], 0);
+      const RowTask tk_nxt = p.tasks[min(t_nxt + lane, p.ntasks - 1)];
+      const bool has = lane < 4 && t_cur + lane < p.ntasks;
+      if (publish_group(sh, g, t_cur, p.ntasks, tk_cur, has, lane)) break;
+      t_cur = t_nxt;
+      tk_cur = tk_nxt;
     }
   } else if (warp >= kCsrWarp0) {
     // ================= CSR loader of parity h =================

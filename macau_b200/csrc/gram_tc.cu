@@ -67,13 +67,13 @@ constexpr int kEpiWarp0 = kProducers + 1;           // warps 9-12
 constexpr int kSchedWarp = kProducers + 5;           // warp 13
 constexpr int kCsrWarp0 = kProducers + 6;            // warps 14-15
 constexpr int kTcThreads = (kProducers + 8) * 32;
-constexpr int kStages = 16;               // gather stages in flight (even: stage s has parity s % 2)
-constexpr int kBlockBytes = 4 * 512;      // one column block: 4 K-atoms x 512 B
+constexpr int kStages = 32;               // gather stages in flight (even: stage s has parity s % 2)
+constexpr int kBlockBytes = 2 * 512;      // one column block: 2 K-atoms x 512 B
 constexpr int kStageBytes = 5 * kBlockBytes;
 constexpr int kSlots = 3;                 // TMEM accumulators
 constexpr int kSlotCols = 160;            // columns of one accumulator (N = 160)
 constexpr int kCsr = 8;                   // CSR ring slots per parity (k-blocks of that parity ahead)
-constexpr int kDesc = 48;                 // group descriptor ring
+constexpr int kDesc = 64;                 // group descriptor ring
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
 constexpr int kGramRec = 32 * 32 + 32;    // Gram record: 32 x 32 row-major Gram, then the rhs
 static_assert(kStages % kParity == 0, "a stage's k-blocks all have the same parity");
@@ -272,10 +272,10 @@ __device__ __forceinline__ void tmem_wait_ld() {
 }
 
 // Byte offset of element (mn, j) of a stage, j = entry 0..15 of the row's k-block (bf16
-// elements; SW64 MN-major: 64 B per k-row, entry j in K-atom j / 4, k-row j % 4, 16-byte chunk
+// elements; SW64 MN-major: 64 B per k-row, entry j in K-atom j / 8, k-row j % 8, 16-byte chunk
 // index XOR (k-row / 2) % 4).
 __device__ __forceinline__ uint32_t stage_off(int mn, int j) {
-  const int a = mn >> 5, e = mn & 31, c = e >> 3, b = j >> 2, r = j & 3;
+  const int a = mn >> 5, e = mn & 31, c = e >> 3, b = j >> 3, r = j & 7;
   return (uint32_t)(a * kBlockBytes + b * 512 + r * 64 + ((c ^ ((r >> 1) & 3)) << 4) +
                     ((e & 7) << 1));
 }
@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     reinterpret_cast<uint4*>(stages)[e] = make_uint4(0u, 0u, 0u, 0u);
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; s++) {
-      mbar_init(&sh->full[s], kRowSlots);
+      mbar_init(&sh->full[s], kRowSlots * 33);  // per producer: 32 copy completions + 1
       mbar_init(&sh->empty[s], 1);
     }
     for (int s = 0; s < kSlots; s++) {
@@ -400,48 +400,37 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
   if (warp < kProducers) {
     // ================= producer of row slot r, parity h =================
+    // lane l copies 16-byte chunk l % 4 of the rows of entries l / 4 and l / 4 + 8
     const int r = warp % kRowSlots, h = warp / kRowSlots;
+    const int ch = lane & 3, e0 = lane >> 2;
     const uint32_t woff = stage_off(128 + r, lane & 15);  // this lane's weight in a stage
+    const uint32_t o0 = stage_off(32 * r + 8 * ch, e0), o1 = stage_off(32 * r + 8 * ch, e0 + 8);
+    const __nv_bfloat16* V = reinterpret_cast<const __nv_bfloat16*>(p.other);
+    const unsigned sentinel = (unsigned)p.nother;  // the zero row of the BF16 factor
     for (int i = 0;; i++) {
       const int slot = i % kCsr;
       if (!mbar_wait(&sh->csr_full[h][slot], (uint32_t)((i / kCsr) & 1), sh, p.ctl)) break;
       const int2 m = sh->meta[h][slot];
       if (m.y & kMetaEnd) break;
       const bool v = (m.y >> r) & 1;
-      // lane l < 16: entry l's weight; lane l < 4: the columns of entries 4l .. 4l + 3
-      const float w = __uint_as_float(sh->csr[h][slot][r][lane & 15].y);
-      const uint4 c01 = *reinterpret_cast<const uint4*>(&sh->csr[h][slot][r][4 * (lane & 3)]);
-      const uint4 c23 = *reinterpret_cast<const uint4*>(&sh->csr[h][slot][r][4 * (lane & 3) + 2]);
-      const int y[4] = {(int)c01.x, (int)c01.z, (int)c23.x, (int)c23.z};
+      const unsigned col0 = v ? sh->csr[h][slot][r][e0].x : sentinel;
+      const unsigned col1 = v ? sh->csr[h][slot][r][e0 + 8].x : sentinel;
+      const float w = v ? __uint_as_float(sh->csr[h][slot][r][lane & 15].y) : 0.f;
       const int stage = m.x % kStages;
       const uint32_t phase = (uint32_t)((m.x / kStages) & 1);
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh->csr_empty[h][slot]);  // the entries are in registers
       if (!mbar_wait(&sh->empty[stage], phase ^ 1, sh, p.ctl)) break;
       unsigned char* sbase = stages + (size_t)stage * kStageBytes;
-      unsigned char* blk = sbase + r * kBlockBytes;
-      if (v) {
-        if (lane < 16) *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = __float2bfloat16_rn(w);
-        fence_proxy_async();  // the weights before the async proxy reads them
-        __syncwarp();
-        if (lane == 0) mbar_expect_tx(&sh->full[stage], 4u * 256u);
-        __syncwarp();
-        if (lane < 4)
-          tma_gather4(su32(blk + lane * 512), &tmap, y[0], y[1], y[2], y[3], &sh->full[stage]);
-      } else {
-        // no entries of row r in this k-block: zero k-rows 0..3 of its 4 K-atoms and its weights
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-          const int e = lane + 32 * k;
-          *reinterpret_cast<uint4*>(blk + (e >> 4) * 512 + (e & 15) * 16) = make_uint4(0u, 0u, 0u, 0u);
-        }
-        if (lane < 16) *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = __float2bfloat16_rn(0.f);
-        fence_proxy_async();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sh->full[stage]);
-      }
+      cp16(sbase + o0, V + (size_t)col0 * 32 + 8 * ch);
+      cp16(sbase + o1, V + (size_t)col1 * 32 + 8 * ch);
+      cp_arrive_noinc(&sh->full[stage]);
+      if (lane < 16) *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = __float2bfloat16_rn(w);
+      fence_proxy_async();  // the weights before the async proxy reads them
       __syncwarp();
+      if (lane == 0) mbar_arrive(&sh->full[stage]);
     }
+    cp_wait_all();
   } else if (warp == kMmaWarp) {
     // ================= MMA issuer =================
     int stage = 0;
@@ -462,11 +451,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           ok = false;
           break;
         }
+        fence_proxy_async();  // the stage's cp.async data before the tensor cores read it
         tc_fence_after();
         if (lane == 0) {
           const uint32_t sa = su32(stages + (size_t)stage * kStageBytes);
           mma_bf16(d_tmem, smem_desc(sa), smem_desc(sa), kb > 0 ? 1u : 0u);
-          mma_bf16(d_tmem, smem_desc(sa + 1024), smem_desc(sa + 1024), 1u);
           mma_commit(&sh->empty[stage]);
         }
         __syncwarp();

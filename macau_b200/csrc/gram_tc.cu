@@ -204,6 +204,11 @@ __device__ __forceinline__ void cp16(void* dst, const void* src) {
 __device__ __forceinline__ void cp_arrive_noinc(uint64_t* b) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(su32(b)) : "memory");
 }
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -366,7 +371,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     reinterpret_cast<uint4*>(stages)[e] = make_uint4(0u, 0u, 0u, 0u);
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; s++) {
-      mbar_init(&sh->full[s], kRowSlots * 33);  // per producer: 32 copy completions + 1
+      mbar_init(&sh->full[s], kRowSlots);  // one arrive per producer (after its copies landed)
       mbar_init(&sh->empty[s], 1);
     }
     for (int s = 0; s < kSlots; s++) {
@@ -400,14 +405,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
   if (warp < kProducers) {
     // ================= producer of row slot r, parity h =================
-    // lane l copies 16-byte chunk l % 4 of the rows of entries l / 4 and l / 4 + 8
+    // lane l copies 16-byte chunk l % 4 of the rows of entries l / 4 and l / 4 + 8.  A k-block's
+    // copies form one cp.async group; kLag k-blocks later the producer waits for that group,
+    // fences the async proxy (its copies and weights before the tensor cores read them) and
+    // arrives on the stage's "full" barrier.
+    constexpr int kLag = 1;
     const int r = warp % kRowSlots, h = warp / kRowSlots;
     const int ch = lane & 3, e0 = lane >> 2;
     const uint32_t woff = stage_off(128 + r, lane & 15);  // this lane's weight in a stage
     const uint32_t o0 = stage_off(32 * r + 8 * ch, e0), o1 = stage_off(32 * r + 8 * ch, e0 + 8);
     const __nv_bfloat16* V = reinterpret_cast<const __nv_bfloat16*>(p.other);
     const unsigned sentinel = (unsigned)p.nother;  // the zero row of the BF16 factor
-    for (int i = 0;; i++) {
+    int pend[kLag + 1];  // stages of the k-blocks whose arrive is pending (ring by i % (kLag + 1))
+    int npend = 0, i = 0;
+    for (;; i++) {
       const int slot = i % kCsr;
       if (!mbar_wait(&sh->csr_full[h][slot], (uint32_t)((i / kCsr) & 1), sh, p.ctl)) break;
       const int2 m = sh->meta[h][slot];
@@ -424,13 +435,37 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       unsigned char* sbase = stages + (size_t)stage * kStageBytes;
       cp16(sbase + o0, V + (size_t)col0 * 32 + 8 * ch);
       cp16(sbase + o1, V + (size_t)col1 * 32 + 8 * ch);
-      cp_arrive_noinc(&sh->full[stage]);
+      cp_commit();
       if (lane < 16) *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = __float2bfloat16_rn(w);
-      fence_proxy_async();  // the weights before the async proxy reads them
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&sh->full[stage]);
+#pragma unroll
+      for (int q = 0; q <= kLag; q++)
+        if (q == i % (kLag + 1)) pend[q] = stage;
+      if (++npend > kLag) {
+        // the k-block of kLag iterations ago: its copies have landed (kLag groups may remain)
+        cp_wait_group<kLag>();
+        fence_proxy_async();
+        __syncwarp();
+        const int qo = (i + 1) % (kLag + 1);
+        int so = 0;
+#pragma unroll
+        for (int q = 0; q <= kLag; q++)
+          if (q == qo) so = pend[q];
+        if (lane == 0) mbar_arrive(&sh->full[so]);
+        npend--;
+      }
     }
+    // the pending k-blocks, oldest first
     cp_wait_all();
+    fence_proxy_async();
+    __syncwarp();
+    for (int k = npend; k > 0; k--) {
+      const int qo = (i - k + 3 * (kLag + 1)) % (kLag + 1);
+      int so = 0;
+#pragma unroll
+      for (int q = 0; q <= kLag; q++)
+        if (q == qo) so = pend[q];
+      if (lane == 0) mbar_arrive(&sh->full[so]);
+    }
   } else if (warp == kMmaWarp) {
     // ================= MMA issuer =================
     int stage = 0;
@@ -451,7 +486,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           ok = false;
           break;
         }
-        fence_proxy_async();  // the stage's cp.async data before the tensor cores read it
         tc_fence_after();
         if (lane == 0) {
           const uint32_t sa = su32(stages + (size_t)stage * kStageBytes);

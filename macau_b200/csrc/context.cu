@@ -13,7 +13,7 @@
 //   * Latents: N x KP, row n = the K-vector of entity n, zero padded to KP in {8,..,128}.
 //     FP64 mode keeps FP64; mixed mode keeps an FP32 master plus a BF16 copy that the other
 //     mode's sampler gathers; the BF16 copy has one extra all-zero row N, the target of the
-//     padding sentinels (the tensor-core sampler's TMA gathers read it as a zero vector).
+//     padding sentinels (the tensor-core sampler's gathers read it as a zero vector).
 //   * Hyperparameters (mu, Lambda, lambda_beta) and the Macau link matrix stay on the device;
 //     a sweep needs no host round trip except the block-CG convergence check.
 #include <cuda_runtime.h>
@@ -66,26 +66,6 @@ struct DBuf {
     g_h2d_bytes += (long long)(count * sizeof(T));
   }
 };
-
-// cuTensorMapEncodeTiled, looked up through the runtime so that the library does not link
-// libcuda directly (it loads on machines without a driver, where it reports MG_ERR_NOGPU).
-using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiledFn tensor_map_encoder() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    MG_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault,
-                                             &q));
-    if (q != cudaDriverEntryPointSuccess || !f)
-      throw MgError(MG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    fn = reinterpret_cast<EncodeTiledFn>(f);
-  }
-  return fn;
-}
 
 struct HostCsr {
   std::vector<long long> ptr;
@@ -452,29 +432,10 @@ class Context {
     sweeps_done_ = 0;
     launches_ = 0;
     t_sample_ = t_prior_ = t_eval_ = 0.0;
-    if (mixed_ && KP_ == 32) {
-      for (int m = 0; m < 2; m++) make_gather_map(m);
-    }
     drop_graphs();
     initialised_ = true;
   }
 
-  // TMA map over the BF16 copy of the latents of `m`'s other mode: {32, N_other + 1} bf16
-  // (row N_other is the zero row), box of one 64-byte row, 64-byte swizzle (the tensor-core
-  // sampler's stage layout).
-  void make_gather_map(int m) {
-    const int other = 1 - m;
-    const cuuint64_t dims[2] = {32, (cuuint64_t)dims_[other] + 1};
-    const cuuint64_t strides[1] = {64};
-    const cuuint32_t box[2] = {32, 1};
-    const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = tensor_map_encoder()(
-        &tmap_[m], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)lat16_[other].p, dims, strides, box,
-        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
-        CU_TENSOR_MAP_L2_PROMOTION_L2_64B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS)
-      throw MgError(MG_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-  }
 
   // ---- phases ----
   void sample(int mode, const double* znoise_dev, bool reset_queue = true,
@@ -515,8 +476,7 @@ class Context {
       tp.tasks = md.tasks_tc.p;
       tp.ntasks = md.ntasks_tc;
       tp.packed = md.packed_tc.p;
-      if (launch_sample_tc(tp, tmap_[mode], md.gram_tc.p, md.sinfo_tc.p, KP_, s_, num_sms_,
-                           mid)) {
+      if (launch_sample_tc(tp, md.gram_tc.p, md.sinfo_tc.p, KP_, s_, num_sms_, mid)) {
         launches_ += 1;  // k_gram_tc + k_finish_tc
         return;
       }
@@ -994,7 +954,6 @@ class Context {
   DBuf<double> lat64_[2];
   DBuf<float> lat32_[2];
   DBuf<__nv_bfloat16> lat16_[2];
-  CUtensorMap tmap_[2];  // tensor-core sampler: gather maps over lat16_ of the other mode
   DBuf<double> scratch_, stat_partials_, stat_final_, nwbuf_;
   NwWork nw_{};
   DBuf<Ctl> ctl_;

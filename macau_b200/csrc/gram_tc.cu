@@ -4,34 +4,31 @@
 // Cholesky, solves, noise) with one warp per row at full occupancy.
 //
 // k_gram_tc.  Four sampler rows ("a group") share each MMA.  For a k-block of 16 entries per
-// row, the TMA gathers the four rows' BF16 other-factor vectors (64 B each, tile::gather4 by CSR
-// column index, 64B swizzle) into one shared-memory stage of five SW64 MN-major column blocks
-// (32 elements wide, four K-atoms of 512 B each): block p holds row p's 32 latent values, block
-// 4 holds the rows' (y - mean) * alpha in elements 0..3.  Each gather4 fills k-rows 0..3 of one
-// K-atom (its destination stays on the 512-byte swizzle period); k-rows 4..7 stay zero, so a
-// stage carries 16 entries per row in K = 32 and two tcgen05.mma (M = 128, N = 160, K = 16, BF16
-// in, FP32 accumulate in TMEM) consume it.  Together they add
+// row, the producers gather the four rows' BF16 other-factor vectors (64 B each, by CSR column
+// index) with 16-byte cp.async copies into one shared-memory stage of five SW64 MN-major column
+// blocks (32 elements wide, two K-atoms of 8 k-rows x 64 B): block p holds row p's 32 latent
+// values, block 4 holds the rows' (y - mean) * alpha in elements 0..3.  One tcgen05.mma
+// (M = 128, N = 160, K = 16, BF16 in, FP32 accumulate in TMEM) per stage adds
 //     D[32p + i][32q + j] += sum_k X_p[k][i] X_q[k][j],   D[32p + i][128 + q] += sum_k X_p[k][i] w_q[k]
 // whose diagonal blocks p == q are the four rows' Grams and whose column 128 + p is row p's
 // right-hand side sum v (y - mean) alpha (the off-diagonal blocks are not used).  D row r lives
 // in TMEM lane r, so the epilogue warp of quadrant p reads row p's Gram with one 32x32b load.
+// (A TMA tile::gather4 variant of the producers was measured slower: a gather4 of 64-byte rows
+// into a 64B-swizzled stage must start on the 512-byte swizzle period, which leaves half of each
+// K-atom empty and doubles the MMAs, and each warp issues one TMA instruction per ~70-90 cycles.)
 //
 // The CSR stream is the padded packed array of the mode: each row's (column, weight) entries
 // start on a 16-entry boundary and are padded to a multiple of 16 with (N_other, 0) sentinels;
-// a sentinel gathers the zero row N_other of the BF16 factor.
+// a sentinel gathers the zero row N_other of the BF16 factor, and so does a row slot with no
+// entries left in a k-block.
 //
-// Warp roles (one CTA of 13 warps per SM, persistent):
+// Warp roles (one CTA of 16 warps per SM, persistent):
 //   warps 0-7   producers: warp w fills column block r = w % 4 of the stages of the k-blocks
 //               with global index t = w / 4 (mod 2): per k-block it takes row r's 16 CSR
-//               entries from the CSR ring of its parity, stores the 16 weights and issues 4
-//               gather4 loads (a row with no entries left zero-fills its block instead); a
-//               stage's "full" barrier counts its 4 producers and the gathered bytes.  One warp
-//               issuing TMA instructions is issue-bound (about 70-90 cycles per instruction),
-//               so the issue is spread over eight warps.
-//   warps 14-15 CSR loaders, one per k-block parity: walk the group descriptors and, up to kCsr
-//               k-blocks of their parity ahead, copy each k-block's four 128-byte row segments
-//               with one 16-byte cp.async per lane into the ring, with a meta record (stage
-//               index, valid rows, stop / end) for the producers.
+//               entries from the CSR ring of its parity, issues two 16-byte cp.async per lane
+//               (lane l: chunk l % 4 of entries l / 4 and l / 4 + 8) as one commit group and
+//               stores the 16 weights; one k-block later it waits for that group, fences the
+//               async proxy and arrives on the stage's "full" barrier (4 arrivals per stage).
 //   warp 8      MMA: allocates TMEM (512 columns: three accumulators of 160 columns); one lane
 //               issues the MMAs, releases stages (tcgen05.commit -> "empty") and publishes
 //               finished accumulators (tcgen05.commit -> "acc full").
@@ -39,16 +36,19 @@
 //               release the accumulator, store the row's FP32 Gram and rhs to its Gram record
 //               (or, for a part of a split row, the FP64 partial to the part's scratch slot),
 //               and release the group's descriptor slot ("desc free").
-//   warp 13     scheduler: takes 4 tasks per group from the work queue and publishes the group
-//               descriptors into a ring of kDesc slots as far ahead as the ring allows, so that
-//               the queue atomics and task loads stay off the MMA warp.
+//   warp 13     scheduler: takes 4 tasks per group from the work queue (four claims in flight)
+//               and publishes the group descriptors into a ring of kDesc slots as far ahead as
+//               the ring allows, so that the queue atomics and task loads stay off the MMA warp.
+//   warps 14-15 CSR loaders, one per k-block parity: walk the group descriptors and, up to kCsr
+//               k-blocks of their parity ahead, copy each k-block's four 128-byte row segments
+//               with one 16-byte cp.async per lane into the ring, with a meta record (stage
+//               index, valid rows, stop / end) for the producers.
 // Every barrier wait is bounded by a clock budget; on expiry the CTA raises an abort flag, all
 // roles leave their loops, the MMA lane drains its MMAs, TMEM is freed and the status word
 // reports a timeout.
 //
 // k_finish_tc.  One warp per row: the Gram record (or the FP64 sum of the row's split parts, in
 // part order), then the FP32 warp Cholesky and solves of warp_finish.cuh with the FP64 retry.
-#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -174,23 +174,6 @@ __device__ __noinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, TcShar
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, TcShared* sh, Ctl* ctl) {
   if (mbar_test(b, parity)) return true;
   return mbar_wait_slow(b, parity, sh, ctl);
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes)
-               : "memory");
-}
-
-// TMA gather of 4 rows (y0..y3) of the 2-D tensor `tmap` (box: one 64-byte row) into shared
-// memory at `dst`, completing on `b`; an out-of-range row is filled with zeros.
-__device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap* tmap, int y0, int y1,
-                                            int y2, int y3, uint64_t* b) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(0), "r"(y0), "r"(y1), "r"(y2), "r"(y3),
-      "r"(su32(b))
-      : "memory");
 }
 
 // Waits for every cp.async of this thread.
@@ -353,13 +336,13 @@ __device__ __forceinline__ bool cursor_advance(Cursor& c, int step, TcShared* sh
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-    k_gram_tc(const SampleParams p, const __grid_constant__ CUtensorMap tmap, float* gram) {
+    k_gram_tc(const SampleParams p, float* gram) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // layout: stages (1024-aligned) | TcShared
   unsigned char* stages = smem_raw;
   TcShared* sh = reinterpret_cast<TcShared*>(stages + (size_t)kStages * kStageBytes);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // The stage layout and the TMA's 64-byte swizzle agree only on 1024-byte aligned stages.
+  // The stage descriptors' 64-byte swizzle pattern assumes 1024-byte aligned stages.
   if ((su32(stages) & 1023u) != 0) {
     if (threadIdx.x == 0) atomicOr(&p.ctl->status, kStatTimeout);
     return;
@@ -730,7 +713,7 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
 
 size_t tc_smem_bytes() { return (size_t)kStages * kStageBytes + sizeof(TcShared); }
 
-bool launch_sample_tc(const SampleParams& p, const CUtensorMap& tmap, float* gram,
+bool launch_sample_tc(const SampleParams& p, float* gram,
                       const int2* sinfo, int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
   if (KP != 32 || p.packed == nullptr) return false;
   static bool configured[64] = {false};
@@ -745,7 +728,7 @@ bool launch_sample_tc(const SampleParams& p, const CUtensorMap& tmap, float* gra
                                  (int)fsmem));
     configured[dev & 63] = true;
   }
-  k_gram_tc<<<num_sms, kTcThreads, smem, s>>>(p, tmap, gram);
+  k_gram_tc<<<num_sms, kTcThreads, smem, s>>>(p, gram);
   MG_CUDA(cudaGetLastError());
   if (mid) MG_CUDA(cudaEventRecord(mid, s));
   k_finish_tc<<<num_sms * 2, kFinWarps * 32, fsmem, s>>>(p, gram, sinfo);

@@ -1,6 +1,5 @@
 // Host-side launch functions of the sm_100a kernels (one translation unit per kernel family).
 #pragma once
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -25,15 +24,14 @@ void launch_pad(const long long* ptr, const long long* pptr, long long nrows, co
 void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, int num_sms);
 // Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only): two
 // launches, k_gram_tc then k_finish_tc.  It reads the 16-entry padded packed CSR and its task
-// list (p.packed / p.tasks, built by the context) and gathers the other factor's BF16 rows
-// through `tmap` (2-D, {32, nother + 1} bf16, box {32, 1}, 64-byte swizzle; row nother is all
-// zeros).  `gram` holds nrows Gram records of 32 * 32 + 32 floats; sinfo[row] = {parts, scratch
-// slot of part 0} (parts > 1: the row's partial Grams go to p.scratch, 1056 doubles per slot).
-// Returns false when the configuration is not covered (caller uses the CUDA-core kernel).
-// `mid`, if given, is recorded between the two launches (per-kernel timing).
-bool launch_sample_tc(const SampleParams& p, const CUtensorMap& tmap, float* gram,
-                      const int2* sinfo, int KP, cudaStream_t s, int num_sms,
-                      cudaEvent_t mid = nullptr);
+// list (p.packed / p.tasks, built by the context) and gathers the other factor's BF16 rows from
+// p.other, whose row nother is all zeros (the padding sentinel).  `gram` holds nrows Gram
+// records of 32 * 32 + 32 floats; sinfo[row] = {parts, scratch slot of part 0} (parts > 1: the
+// row's partial Grams go to p.scratch, 1056 doubles per slot).  Returns false when the
+// configuration is not covered (caller uses the CUDA-core kernel).  `mid`, if given, is
+// recorded between the two launches (per-kernel timing).
+bool launch_sample_tc(const SampleParams& p, float* gram, const int2* sinfo, int KP,
+                      cudaStream_t s, int num_sms, cudaEvent_t mid = nullptr);
 
 // ---- hyperprior / eval (hyper_kernels.cu) ----
 struct NwWork {

@@ -188,6 +188,54 @@ def cpu_baseline(w, budget_s, sweeps_max):
             "sample": f"{n} full FP64 sweeps (after 1 untimed) of {w['name']}, K=32"}
 
 
+class Ranks:
+    """The multi-process plumbing of a run: one process per GPU, launched by torchrun (RANK,
+    LOCAL_RANK, WORLD_SIZE, MASTER_* in the environment).  Each rank runs an independent chain
+    (seed 1000 + rank); timings are taken as the maximum over ranks and whole-job rates count
+    every rank's work.  backend "nccl" with device "cuda:<local rank>" on GPUs; the CPU tests
+    use "gloo" with device "cpu"."""
+
+    def __init__(self, backend="nccl", device=None, timeout_s=600):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = device if device is not None else f"cuda:{self.local}"
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            if self.device.startswith("cuda"):
+                import torch
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def chain_seed(self):
+        return 1000 + self.rank
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.dist is None:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def rate(self, units_per_rank, seconds_max):
+        """Whole-job rate: every rank processed `units_per_rank` within `seconds_max`."""
+        return self.world * units_per_rank / seconds_max
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 # ------------------------------------------------------------------------ arms
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -219,28 +267,9 @@ def run_reference(args):
 
 def run_ours(args):
     from macau_b200 import _lib
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl")
+    world, rank, local = ranks.world, ranks.rank, ranks.local
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     import torch
     bus = None
@@ -253,7 +282,7 @@ def run_ours(args):
         pass
 
     w = workload(args.scale, 2)
-    seed = 1000 + rank
+    seed = ranks.chain_seed()
     K, W = args.steps, args.warmup
     if args.only != "all":
         comp = _lib.MG_COMPUTE_MIXED if args.only == "mixed" else _lib.MG_COMPUTE_FP64
@@ -264,6 +293,7 @@ def run_ours(args):
         print(json.dumps({"only": args.only, "workload": w["name"], "ms_per_step": t / K * 1e3,
                           "phase_ms": [x / K * 1e3 for x in ph], "stats": s.stats()}), flush=True)
         s.close()
+        ranks.close()
         return 0
     # ---- mixed-precision batched sampler: headline value ----
     mx = make_sampler(w, _lib.MG_COMPUTE_MIXED, seed, local)
@@ -338,8 +368,8 @@ def run_ours(args):
             "algorithmic_tflops": gflop / t_gram / 1e12, "tensor_peak_bf16": tflops,
             "tensor_frac": gflop / t_gram / 1e12 / tflops,
             "l2_gather_GBps": gathered / t_gram / 1e9}
-    v_mx = world * K / t_mx
-    v_fp = world * K / t_fp
+    v_mx = ranks.rate(K, t_mx)
+    v_fp = ranks.rate(K, t_fp)
     line = {"metric": METRIC, "value": v_mx, "unit": UNIT, "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": t_mx / K * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16-gram/f32-chol/f64-hyper",
@@ -356,7 +386,7 @@ def run_ours(args):
             "retries_fp64_refactor": retries,
             "gpu_launches": int(round(kernels_per_sweep * K)),
             "clocks": clk.summary(), "roofline": roofline,
-            "e2e": {"value": world * E / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d / E,
+            "e2e": {"value": ranks.rate(E, t_e2e), "unit": UNIT, "h2d_bytes_per_step": h2d / E,
                     "d2h_bytes_per_step": d2h / E,
                     "timed": "C-ABI run: data upload + CSR build, init, sweeps with eval and "
                              "RMSE read-back, final predictions read-back"}}
@@ -366,9 +396,7 @@ def run_ours(args):
         line["fp64_over_cpu"] = v_fp / line["cpu_baseline"]["value"]
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 

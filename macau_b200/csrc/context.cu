@@ -145,7 +145,7 @@ struct ModeData {
   DBuf<uint2> packed_tc;
   DBuf<RowTask> tasks_tc;
   DBuf<float> gram_tc;     // N Gram records (32 x 32 + 32 floats) written by k_gram_tc
-  DBuf<int2> sinfo_tc;     // per row {parts, scratch slot of part 0}
+  DBuf<int4> split_tc;     // split rows {row, parts, scratch slot of part 0, 0}
   int ntasks_tc = 0, nsplit_tc = 0, nslots_tc = 0;
 };
 
@@ -476,8 +476,9 @@ class Context {
       tp.tasks = md.tasks_tc.p;
       tp.ntasks = md.ntasks_tc;
       tp.packed = md.packed_tc.p;
-      if (launch_sample_tc(tp, md.gram_tc.p, md.sinfo_tc.p, KP_, s_, num_sms_, mid)) {
-        launches_ += 1;  // k_gram_tc + k_finish_tc
+      if (launch_sample_tc(tp, md.gram_tc.p, md.split_tc.p, md.nsplit_tc, KP_, s_, num_sms_,
+                           mid)) {
+        launches_ += 1 + (md.nsplit_tc > 0 ? 1 : 0);  // k_gram_tc (+ k_sum_parts) + k_finish_tc
         return;
       }
     }
@@ -922,10 +923,11 @@ class Context {
       md.nsplit_tc = ns;
       md.nslots_tc = nsl;
       md.tasks_tc.upload(tt.data(), tt.size(), s_);
-      std::vector<int2> si(std::max(1LL, md.N), make_int2(1, 0));
+      std::vector<int4> sr;
       for (const RowTask& t : tt)
-        if (t.nparts > 1 && t.part == 0) si[t.row] = make_int2(t.nparts, t.slot);
-      md.sinfo_tc.upload(si.data(), si.size(), s_);
+        if (t.nparts > 1 && t.part == 0) sr.push_back(make_int4(t.row, t.nparts, t.slot, 0));
+      std::sort(sr.begin(), sr.end(), [](const int4& a, const int4& b) { return a.x < b.x; });
+      md.split_tc.upload(sr.data(), sr.size(), s_);
       md.gram_tc.alloc((size_t)std::max(1LL, md.N) * (32 * 32 + 32));
     }
     md.split_cnt.alloc_zero(std::max(1, nsplit), s_);

@@ -603,18 +603,44 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ---------------------------------------------------------------------------------------------
 // k_finish_tc: one warp per row (rows warp, warp + total warps, ...).
 constexpr int kFinWarps = 8;
-constexpr int kLD = 33;                 // Gram tile leading dimension (floats)
 constexpr int kLc = 36;                 // L^T leading dimension
-constexpr int kFinWork = 32 * 36 * 8;   // per warp: FP32 Gram + L^T, or the FP64 retry's L^T
+constexpr int kFinWork = 32 * 36 * 8;   // per warp: two FP32 L^T (one per half), or the FP64
+                                        // retry's L^T
 
+// k_sum_parts: one warp per split row: its parts' FP64 partial Grams summed in part order, one
+// entry at a time, and rounded once into the row's FP32 Gram record (lane i: Gram row i).
+__global__ void __launch_bounds__(256)
+    k_sum_parts(const double* __restrict__ scratch, const int4* __restrict__ split_rows,
+                int nsplit, float* __restrict__ gram) {
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nsplit) return;
+  const int4 sr = split_rows[w];  // {row, parts, scratch slot of part 0, unused}
+  const double* s0 = scratch + (size_t)sr.z * kGramRec;
+  float* gp = gram + (size_t)sr.x * kGramRec;
+  for (int j = 0; j < 32; j++) {
+    double acc = 0.0;
+    for (int prt = 0; prt < sr.y; prt++) acc += __ldcg(s0 + (size_t)prt * kGramRec + lane * 32 + j);
+    gp[lane * 32 + j] = (float)acc;
+  }
+  double rs = 0.0;
+  for (int prt = 0; prt < sr.y; prt++) rs += __ldcg(s0 + (size_t)prt * kGramRec + 32 * 32 + lane);
+  gp[32 * 32 + lane] = (float)rs;
+}
+
+// k_finish_tc: one warp per two rows (rows 2q, 2q + 1 for q = warp, warp + total warps, ...),
+// half-warp h finishing row 2q + h with the pair routines of warp_finish.cuh from the row's
+// Gram record (split rows: written by k_sum_parts).  A half whose FP32 factorisation fails is
+// redone in FP64 by the whole warp.
 __global__ void __launch_bounds__(kFinWarps * 32, 2)
-    k_finish_tc(const SampleParams p, const float* __restrict__ gram, const int2* __restrict__ sinfo) {
+    k_finish_tc(const SampleParams p, const float* __restrict__ gram) {
   extern __shared__ __align__(16) unsigned char fsm[];
   double* Lam_s = reinterpret_cast<double*>(fsm);
   double* lmu_s = Lam_s + 32 * 33;
   float* LamF = reinterpret_cast<float*>(lmu_s + 32);  // (float) Lambda, ld kLc
   unsigned char* works = reinterpret_cast<unsigned char*>(LamF + 32 * kLc);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int h = lane >> 4, l = lane & 15;
   const int K = p.K;
   const uint32_t sweep = p.ctl->sweep;
   for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
@@ -633,76 +659,87 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
   __syncthreads();
   const float alpha_f = (float)p.alpha;
   unsigned char* work = works + (size_t)warp * kFinWork;
-  float* Gs = reinterpret_cast<float*>(work);
-  float* Lc = Gs + 32 * kLD;
+  float* Lc = reinterpret_cast<float*>(work) + h * 32 * kLc;  // this half's L^T
+  const int c_lo = l, c_hi = l + 16;                        // this lane's two components
   const int stride = gridDim.x * kFinWarps;
-  for (int row = blockIdx.x * kFinWarps + warp; row < p.nrows; row += stride) {
-    const int2 si = sinfo[row];  // {parts, scratch slot of part 0}
-    double rhs;
-    float a[32], d0 = 1.f, rinv = 1.f;
-    const float* G;  // the row's FP32 Gram (record or shared staging), kept for an FP64 retry
-    int ldg;
-    if (si.x > 1) {
-      // sum the parts in part order, one entry at a time in FP64
-      const double* s0 = p.scratch + (size_t)si.y * kGramRec;
-#pragma unroll 4
-      for (int j = 0; j < 32; j++) {
-        double acc = 0.0;
-        for (int prt = 0; prt < si.x; prt++) acc += __ldcg(s0 + (size_t)prt * kGramRec + lane * 32 + j);
-        Gs[lane * kLD + j] = (float)acc;
-      }
-      double rs = 0.0;
-      for (int prt = 0; prt < si.x; prt++) rs += __ldcg(s0 + (size_t)prt * kGramRec + 32 * 32 + lane);
-      rhs = (double)(float)rs;
-      __syncwarp();
-      warp_load_mm<float, float, 32>(a, d0, Gs, kLD, Lam_s, p.alpha, lane, K);
-      G = Gs;
-      ldg = kLD;
-    } else {
-      // lane i: row i of Lambda + alpha G straight from the record (same arithmetic as
-      // warp_load_mm: (float) Lambda + (float) alpha * G)
-      const float* gp = gram + (size_t)row * kGramRec;
+  for (int q = blockIdx.x * kFinWarps + warp; 2 * q < p.nrows; q += stride) {
+    const int row = 2 * q + h;
+    const bool have = row < p.nrows;  // the second half of a last odd pair only follows along
+    const int rw = have ? row : 2 * q;
+    const float* gp = gram + (size_t)rw * kGramRec;
+    // rows c_lo (columns 0..15) and c_hi (columns 0..31) of Lambda + alpha G: (float) Lambda +
+    // (float) alpha * G, the identity beyond K
+    float lo[16], hi[32], d0_lo = 1.f, d0_hi = 1.f;
 #pragma unroll
-      for (int j = 0; j < 32; j += 4) {
-        const float4 v = __ldcg(reinterpret_cast<const float4*>(gp + lane * 32 + j));
-        const float4 l = *reinterpret_cast<const float4*>(LamF + lane * kLc + j);
-        const float g4[4] = {v.x, v.y, v.z, v.w}, l4[4] = {l.x, l.y, l.z, l.w};
+    for (int j = 0; j < 16; j += 4) {
+      const float4 v = __ldcg(reinterpret_cast<const float4*>(gp + c_lo * 32 + j));
+      const float4 m = *reinterpret_cast<const float4*>(LamF + c_lo * kLc + j);
+      const float g4[4] = {v.x, v.y, v.z, v.w}, m4[4] = {m.x, m.y, m.z, m.w};
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int jj = j + u;
-          a[jj] = (lane < K && jj < K) ? l4[u] + alpha_f * g4[u] : (lane == jj ? 1.f : 0.f);
-          if (jj == lane) d0 = a[jj];
-        }
+      for (int u = 0; u < 4; u++) {
+        const int jj = j + u;
+        lo[jj] = (c_lo < K && jj < K) ? m4[u] + alpha_f * g4[u] : (c_lo == jj ? 1.f : 0.f);
+        if (jj == c_lo) d0_lo = lo[jj];
       }
-      rhs = (double)__ldcg(gp + 32 * 32 + lane);
-      G = gp;
-      ldg = 32;
     }
-    double lm;
+#pragma unroll
+    for (int j = 0; j < 32; j += 4) {
+      const float4 v = __ldcg(reinterpret_cast<const float4*>(gp + c_hi * 32 + j));
+      const float4 m = *reinterpret_cast<const float4*>(LamF + c_hi * kLc + j);
+      const float g4[4] = {v.x, v.y, v.z, v.w}, m4[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int jj = j + u;
+        hi[jj] = (c_hi < K && jj < K) ? m4[u] + alpha_f * g4[u] : (c_hi == jj ? 1.f : 0.f);
+        if (jj == c_hi) d0_hi = hi[jj];
+      }
+    }
+    // rhs + Lambda mu (Macau: mu + Uhat[row]) of the two components, in FP64
+    double rl_lo = (double)__ldcg(gp + 32 * 32 + c_lo), rl_hi = (double)__ldcg(gp + 32 * 32 + c_hi);
     if (p.uhat) {
-      const double mun = lane < K ? p.mu[lane] + p.uhat[(size_t)row * 32 + lane] : 0.0;
-      lm = 0.0;
+      double m_lo = 0.0, m_hi = 0.0;
       for (int j = 0; j < K; j++) {
-        const double mj = __shfl_sync(0xffffffffu, mun, j);
-        if (lane < K) lm += Lam_s[lane * 33 + j] * mj;
+        const double mj = p.mu[j] + p.uhat[(size_t)rw * 32 + j];
+        if (c_lo < K) m_lo += Lam_s[c_lo * 33 + j] * mj;
+        if (c_hi < K) m_hi += Lam_s[c_hi * 33 + j] * mj;
       }
+      rl_lo += m_lo;
+      rl_hi += m_hi;
     } else {
-      lm = lmu_s[lane];
+      rl_lo += lmu_s[c_lo];
+      rl_hi += lmu_s[c_hi];
     }
-    const double z = row_noise(p, row, K, lane, sweep);
-    bool ok = warp_factor<float, 32>(a, rinv, lane, 0x1p-20, d0, Lc, kLc);
-    if (ok) {
-      const float x = warp_solve<float, 32>(a, rinv, (float)(rhs + lm), lane, Lc, kLc, z);
-      if (lane < K) {
-        p.out_f32[(size_t)row * 32 + lane] = x;
-        p.out_bf16[(size_t)row * 32 + lane] = __float2bfloat16_rn(x);
+    const float z_lo = (float)comp_noise(p, rw, K, c_lo, sweep);
+    const float z_hi = (float)comp_noise(p, rw, K, c_hi, sweep);
+    float rinv_lo = 1.f, rinv_hi = 1.f;
+    const bool ok = pair_factor(lo, hi, rinv_lo, rinv_hi, l, d0_lo, d0_hi, Lc, kLc);
+    float x_lo = (float)rl_lo, x_hi = (float)rl_hi;
+    pair_solve(lo, hi, rinv_lo, rinv_hi, x_lo, x_hi, l, Lc, kLc, z_lo, z_hi);
+    if (ok && have) {
+      if (c_lo < K) {
+        p.out_f32[(size_t)row * 32 + c_lo] = x_lo;
+        p.out_bf16[(size_t)row * 32 + c_lo] = __float2bfloat16_rn(x_lo);
       }
-    } else {
+      if (c_hi < K) {
+        p.out_f32[(size_t)row * 32 + c_hi] = x_hi;
+        p.out_bf16[(size_t)row * 32 + c_hi] = __float2bfloat16_rn(x_hi);
+      }
+    }
+    // FP64 retry of a failed half by the whole warp (lane = component)
+    const unsigned okm = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+    for (int hf = 0; hf < 2; hf++) {
+      const int rf = 2 * q + hf;
+      if (((okm >> (16 * hf)) & 1u) || rf >= p.nrows) continue;
+      const int src = 16 * hf + (lane & 15);
+      const double v_lo = __shfl_sync(0xffffffffu, rl_lo, src);
+      const double v_hi = __shfl_sync(0xffffffffu, rl_hi, src);
       if (lane == 0) atomicAdd(&p.ctl->retries[p.mode], 1u);
-      ok = warp_finish_f64<32, float>(G, ldg, Lam_s, rhs + lm, p, row, sweep, work);
-      if (!ok && lane == 0) {
+      const bool ok2 = warp_finish_f64<32, float>(gram + (size_t)rf * kGramRec, 32, Lam_s,
+                                                  lane < 16 ? v_lo : v_hi, p, rf, sweep, work);
+      if (!ok2 && lane == 0) {
         atomicOr(&p.ctl->status, kStatCholFail);
-        atomicCAS(&p.ctl->bad_row, -1, row);
+        atomicCAS(&p.ctl->bad_row, -1, rf);
       }
     }
     __syncwarp();
@@ -713,8 +750,8 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
 
 size_t tc_smem_bytes() { return (size_t)kStages * kStageBytes + sizeof(TcShared); }
 
-bool launch_sample_tc(const SampleParams& p, float* gram,
-                      const int2* sinfo, int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
+bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
+                      int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
   if (KP != 32 || p.packed == nullptr) return false;
   static bool configured[64] = {false};
   int dev = 0;
@@ -731,7 +768,11 @@ bool launch_sample_tc(const SampleParams& p, float* gram,
   k_gram_tc<<<num_sms, kTcThreads, smem, s>>>(p, gram);
   MG_CUDA(cudaGetLastError());
   if (mid) MG_CUDA(cudaEventRecord(mid, s));
-  k_finish_tc<<<num_sms * 2, kFinWarps * 32, fsmem, s>>>(p, gram, sinfo);
+  if (nsplit > 0) {
+    k_sum_parts<<<(nsplit + 7) / 8, 256, 0, s>>>(p.scratch, split_rows, nsplit, gram);
+    MG_CUDA(cudaGetLastError());
+  }
+  k_finish_tc<<<num_sms * 2, kFinWarps * 32, fsmem, s>>>(p, gram);
   MG_CUDA(cudaGetLastError());
   return true;
 }

@@ -22,16 +22,17 @@ void launch_pad(const long long* ptr, const long long* pptr, long long nrows, co
 
 // ---- latent sampler (sample_kernels.cu, gram_tc.cu) ----
 void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, int num_sms);
-// Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only): two
-// launches, k_gram_tc then k_finish_tc.  It reads the 16-entry padded packed CSR and its task
-// list (p.packed / p.tasks, built by the context) and gathers the other factor's BF16 rows from
-// p.other, whose row nother is all zeros (the padding sentinel).  `gram` holds nrows Gram
-// records of 32 * 32 + 32 floats; sinfo[row] = {parts, scratch slot of part 0} (parts > 1: the
-// row's partial Grams go to p.scratch, 1056 doubles per slot).  Returns false when the
-// configuration is not covered (caller uses the CUDA-core kernel).  `mid`, if given, is
-// recorded between the two launches (per-kernel timing).
-bool launch_sample_tc(const SampleParams& p, float* gram, const int2* sinfo, int KP,
-                      cudaStream_t s, int num_sms, cudaEvent_t mid = nullptr);
+// Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only):
+// k_gram_tc, then (if nsplit > 0) k_sum_parts, then k_finish_tc.  It reads the 16-entry padded
+// packed CSR and its task list (p.packed / p.tasks, built by the context) and gathers the other
+// factor's BF16 rows from p.other, whose row nother is all zeros (the padding sentinel).
+// `gram` holds nrows Gram records of 32 * 32 + 32 floats; split_rows lists the nsplit rows
+// whose Grams are split into parts, as {row, parts, scratch slot of part 0, 0} (their partial
+// Grams go to p.scratch, 1056 doubles per slot).  Returns false when the configuration is not
+// covered (caller uses the CUDA-core kernel).  `mid`, if given, is recorded after k_gram_tc
+// (per-kernel timing).
+bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
+                      int KP, cudaStream_t s, int num_sms, cudaEvent_t mid = nullptr);
 
 // ---- hyperprior / eval (hyper_kernels.cu) ----
 struct NwWork {

@@ -119,6 +119,108 @@ __device__ __forceinline__ F warp_solve(const F (&a)[KP], F rinv, F rr, int lane
   return rr;
 }
 
+// ---- Two rows per warp (K <= 32, FP32): half-warp h factorises matrix h; lane l of the half holds
+// rows l ("lo", columns 0..15, all a row l < 16 has in its lower triangle) and l + 16 ("hi",
+// columns 0..31).  Every entry receives the same fma with the same operands, in the same
+// order, as in warp_factor / warp_solve, so the results are identical; each column step's
+// shuffles, rsqrt and barrier serve both matrices, and the short rows spend no instructions on
+// the upper triangle.
+
+__device__ __forceinline__ float hshfl(float v, int src) {
+  return __shfl_sync(0xffffffffu, v, src, 16);
+}
+
+// The N(0,1) draw of component c (0 beyond K) of `row`: injected, or keyed by
+// (seed, sweep, mode, row) exactly like row_noise.
+__device__ __forceinline__ double comp_noise(const SampleParams& p, int row, int K, int c,
+                                             uint32_t sweep) {
+  if (p.znoise) return c < K ? p.znoise[(size_t)row * K + c] : 0.0;
+  double z0, z1;
+  normal_pair(p.seed, sweep, stream_id(kRowNoise, (uint32_t)p.mode), (uint32_t)row,
+              (uint32_t)(c >> 1), &z0, &z1);
+  return c < K ? ((c & 1) ? z1 : z0) : 0.0;
+}
+
+// Factorises this half's matrix; Lc (this half's, leading dimension ld, a multiple of 4)
+// receives L^T.  Returns the half's verdict (pivot positive and above 2^-20 of its original
+// diagonal, as warp_factor with rel_floor 2^-20).
+__device__ __forceinline__ bool pair_factor(float (&lo)[16], float (&hi)[32], float& rinv_lo,
+                                            float& rinv_hi, int l, float d0_lo, float d0_hi,
+                                            float* Lc, int ld) {
+  const float fl_lo = 0x1p-20f * d0_lo, fl_hi = 0x1p-20f * d0_hi;
+  float dg_lo = d0_lo, dg_hi = d0_hi;
+  bool bad = false;
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    const int o = j & 15;  // the lane of the half that owns row j
+    const float dj = j < 16 ? dg_lo : dg_hi;
+    if (l == o) bad |= !(dj > 0.f) || !(dj > (j < 16 ? fl_lo : fl_hi));
+    const float r = hshfl(rsqrtf(dj), o);
+    if (l == o) {
+      if (j < 16) rinv_lo = r;
+      else rinv_hi = r;
+    }
+    if (j < 16) lo[j] = (l == j ? dg_lo : lo[j]) * r;
+    hi[j] = (l + 16 == j ? dg_hi : hi[j]) * r;
+    if (j + 1 < 32) {
+      const float ln = hshfl(j + 1 < 16 ? lo[j] : hi[j], (j + 1) & 15);  // L(j+1, j)
+      if (j < 16 && l > j) dg_lo = fmaf(-lo[j], lo[j], dg_lo);
+      if (l + 16 > j) dg_hi = fmaf(-hi[j], hi[j], dg_hi);
+      if (j + 1 < 16) lo[j + 1] = fmaf(-lo[j], ln, lo[j + 1]);
+      hi[j + 1] = fmaf(-hi[j], ln, hi[j + 1]);
+    }
+    if (j < 16) Lc[j * ld + l] = lo[j];
+    Lc[j * ld + l + 16] = hi[j];
+    __syncwarp();
+#pragma unroll
+    for (int q = (j + 2) / 4; q < 8; q++) {
+      const Vec4<float> c = lds4(Lc + j * ld + 4 * q);
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int k = 4 * q + u;
+        if (k > j + 1) {
+          if (k < 16) lo[k] = fmaf(-lo[j], c.v[u], lo[k]);
+          hi[k] = fmaf(-hi[j], c.v[u], hi[k]);
+        }
+      }
+    }
+  }
+  const unsigned b = __ballot_sync(0xffffffffu, bad);
+  return (b & (0xffffu << (16 * ((threadIdx.x & 31) >> 4)))) == 0u;
+}
+
+// y = L^{-1} b, y += z, x = L^{-T} y for this half's rows (r_lo, r_hi: b in, x out).
+__device__ __forceinline__ void pair_solve(const float (&lo)[16], const float (&hi)[32],
+                                           float rinv_lo, float rinv_hi, float& r_lo,
+                                           float& r_hi, int l, const float* Lc, int ld,
+                                           float z_lo, float z_hi) {
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    const int o = j & 15;
+    if (l == o) {
+      if (j < 16) r_lo = r_lo * rinv_lo;
+      else r_hi = r_hi * rinv_hi;
+    }
+    const float yj = hshfl(j < 16 ? r_lo : r_hi, o);
+    if (j < 16 && l > j) r_lo = fmaf(-lo[j], yj, r_lo);
+    if (l + 16 > j) r_hi = fmaf(-hi[j], yj, r_hi);
+  }
+  r_lo += z_lo;
+  r_hi += z_hi;
+#pragma unroll
+  for (int j = 31; j >= 0; j--) {
+    const int o = j & 15;
+    if (l == o) {
+      if (j < 16) r_lo = r_lo * rinv_lo;
+      else r_hi = r_hi * rinv_hi;
+    }
+    const float xj = hshfl(j < 16 ? r_lo : r_hi, o);
+    if (l < j) r_lo = fmaf(-Lc[l * ld + j], xj, r_lo);
+    if (l + 16 < j) r_hi = fmaf(-Lc[(l + 16) * ld + j], xj, r_hi);
+  }
+  __syncwarp();
+}
+
 // Row i of MM = Lambda + alpha * G for lane i (padded rows / columns of the identity), with G
 // read from the Gram tile in shared memory (row-major, leading dimension ld).
 template <typename F, typename GT, int KP>

@@ -69,7 +69,8 @@ typedef struct mg_stats {
 } mg_stats;
 
 /* Context lifetime.  Replaces `make_macau_fixed(2, K, precision)` (macau.cpp:214-220) plus
- * MacauX construction; only fixed Gaussian noise on a 2-mode matrix is supported. */
+ * MacauX construction on a 2-mode matrix; mg_set_noise_adaptive switches the noise model to
+ * AdaptiveGaussianNoise. */
 int mg_create(mg_ctx** out, const mg_config* cfg);
 void mg_destroy(mg_ctx* ctx);
 const char* mg_last_error(const mg_ctx* ctx);
@@ -129,6 +130,25 @@ int mg_run(mg_ctx* ctx);
  * `z` optionally injects the K x N standard normals of the row sampler (NULL = keyed draws). */
 int mg_sample_latents(mg_ctx* ctx, int mode, int iter, const double* z);
 int mg_update_prior(mg_ctx* ctx, int mode, int iter);
+
+/* Adaptive Gaussian noise in place of the fixed precision of mg_config: replaces
+ * `make_macau_adaptive(2, K, sn_init, sn_max)` (macau.cpp:222-228, called by macau.pyx:391-392
+ * with sn_init = 1 for precision="adaptive").  AdaptiveGaussianNoise::init
+ * (noisemodels.cpp:14-33) at mg_init: var_total = mean squared deviation of the training values
+ * from their mean (1 when not positive or NaN), alpha = (sn_init + 1) / var_total, cap
+ * alpha_max = (sn_max + 1) / var_total.  Each sweep then redraws alpha after the priors
+ * (AdaptiveGaussianNoise::update, noisemodels.cpp:55-81).  Call before mg_init; it undoes a
+ * previous mg_init. */
+int mg_set_noise_adaptive(mg_ctx* ctx, double sn_init, double sn_max);
+
+/* AdaptiveGaussianNoise::update (noisemodels.cpp:55-81) with the draw of sweep `iter`: alpha ~
+ * Gamma(1/2 + nnz/2, rate var_total/2 + SSE/2) capped at alpha_max, SSE the squared training
+ * residuals under the current latents.  A no-op under fixed noise. */
+int mg_update_noise(mg_ctx* ctx, int iter);
+
+/* out[0] = current noise precision alpha, out[1] = alpha_max (the fixed precision under fixed
+ * noise), out[2] = var_total of the training values. */
+int mg_get_noise(mg_ctx* ctx, double* out);
 
 /* FixedGaussianNoise::evalModel -> eval_rmse (noisemodels.cpp:161-166, bpmfutils.h:86-114). */
 int mg_eval(mg_ctx* ctx, int n);

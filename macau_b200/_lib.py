@@ -64,6 +64,9 @@ _SIGS = {
     "mg_sample_latents": (_i, [_p, _i, _i, _p]),
     "mg_update_prior": (_i, [_p, _i, _i]),
     "mg_eval": (_i, [_p, _i]),
+    "mg_set_noise_adaptive": (_i, [_p, _d, _d]),
+    "mg_update_noise": (_i, [_p, _i]),
+    "mg_get_noise": (_i, [_p, _p]),
     "mg_get_latents": (_i, [_p, _i, _p]),
     "mg_set_latents": (_i, [_p, _i, _p]),
     "mg_get_hyper": (_i, [_p, _i, _p, _p, _p]),
@@ -202,6 +205,19 @@ class Sampler:
 
     def update_prior(self, mode, it):
         self._chk(lib().mg_update_prior(self.h, mode, int(it)))
+
+    def set_noise_adaptive(self, sn_init=1.0, sn_max=10.0):
+        """AdaptiveGaussianNoise(sn_init, sn_max) in place of the fixed precision (before init)."""
+        self._chk(lib().mg_set_noise_adaptive(self.h, float(sn_init), float(sn_max)))
+
+    def update_noise(self, it):
+        self._chk(lib().mg_update_noise(self.h, int(it)))
+
+    def noise(self):
+        """(alpha, alpha_max, var_total) of the noise model."""
+        out = np.zeros(3)
+        self._chk(lib().mg_get_noise(self.h, out.ctypes.data))
+        return tuple(float(x) for x in out)
 
     def eval(self, n):
         self._chk(lib().mg_eval(self.h, int(n)))

@@ -26,6 +26,8 @@ struct Ctl {
   uint32_t cg_iters[2];   // last block-CG iteration count, per mode
   uint32_t cg_done;       // block-CG convergence flag
   uint32_t pad[3];
+  double alpha;           // current noise precision (AdaptiveGaussianNoise::alpha); with fixed
+                          // noise it holds the fixed precision and the samplers ignore it
 };
 
 // Status bits raised on the device (the host maps them to MG_ERR_* codes and messages).
@@ -59,7 +61,9 @@ struct SampleParams {
   const double* vals;          // raw ratings (FP64 path)
   const uint2* packed;         // (column, centred rating as float bits) pairs (mixed path)
   double mean;
-  double alpha;
+  double alpha;                // fixed noise precision (FixedGaussianNoise::alpha)
+  const double* alpha_dev;     // adaptive noise: the precision on the device (&ctl->alpha),
+                               // and the packed weights then hold y - mean unscaled; null = fixed
   const void* other;           // other factor: double (FP64) or bf16 (mixed), row stride KP
   const double* Lambda;        // K x K
   const double* mu;            // K
@@ -75,6 +79,18 @@ struct SampleParams {
   unsigned long long seed;
   const double* znoise;        // optional injected N(0,1) draws (nrows x K), tests only
 };
+
+#ifdef __CUDACC__
+// Noise precision of a sampler launch: the device value under adaptive noise, else the fixed one.
+__device__ __forceinline__ double noise_alpha(const SampleParams& p) {
+  return p.alpha_dev ? *p.alpha_dev : p.alpha;
+}
+// Factor applied to a packed weight when it is read: packed weights carry the fixed alpha
+// already, and are (y - mean) alone under adaptive noise.
+__device__ __forceinline__ double packed_scale(const SampleParams& p) {
+  return p.alpha_dev ? *p.alpha_dev : 1.0;
+}
+#endif
 
 #define MG_CUDA(call)                                                                   \
   do {                                                                                  \

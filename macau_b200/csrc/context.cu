@@ -143,6 +143,7 @@ struct ModeData {
   // tensor-core sampler (mixed, KP = 32): 16-entry padded packed CSR and its task list, whose
   // begin / len are positions in the padded array (len a multiple of 16)
   DBuf<uint2> packed_tc;
+  DBuf<long long> pptr_tc;  // row pointers of the padded copy
   DBuf<RowTask> tasks_tc;
   DBuf<float> gram_tc;     // N Gram records (32 x 32 + 32 floats) written by k_gram_tc
   DBuf<int4> split_tc;     // split rows {row, parts, scratch slot of part 0, 0}
@@ -277,6 +278,11 @@ class Context {
     for (double v : cval) sum += v;
     ntrain_ = nu;
     mean_ = sum / (double)ntrain_;
+    // AdaptiveGaussianNoise::init (noisemodels.cpp:14-33): var_total over the same order
+    double se = 0.0;
+    for (double v : cval) se += (v - mean_) * (v - mean_);
+    var_total_ = se / (double)ntrain_;
+    if (var_total_ <= 0.0 || std::isnan(var_total_)) var_total_ = 1.0;
     upload_mode(0, p0, nu);
     upload_mode(1, p1, nu);
     drop_graphs();
@@ -425,6 +431,14 @@ class Context {
     }
     Ctl zero{};
     zero.bad_row = -1;
+    // AdaptiveGaussianNoise::init: alpha = (sn_init + 1) / var_total, alpha_max likewise
+    alpha_max_ = (sn_max_ + 1.0) / var_total_;
+    zero.alpha = adaptive_ ? (sn_init_ + 1.0) / var_total_ : cfg_.precision;
+    if (adaptive_) {
+      erow_.alloc((size_t)md_[0].nnz);
+      launch_entry_rows(md_[0].ptr.p, md_[0].N, md_[0].nnz, erow_.p, s_);
+      noise_partials_.alloc((size_t)eval_blocks(md_[0].nnz));
+    }
     MG_CUDA(cudaMemcpyAsync(ctl_.p, &zero, sizeof(Ctl), cudaMemcpyHostToDevice, s_));
     MG_CUDA(cudaStreamSynchronize(s_));
     retries_[0] = retries_[1] = 0;
@@ -457,6 +471,7 @@ class Context {
     sp.packed = md.packed.p;
     sp.mean = mean_;
     sp.alpha = cfg_.precision;
+    sp.alpha_dev = adaptive_ ? &ctl_.p->alpha : nullptr;
     sp.other = mixed_ ? (const void*)lat16_[other].p : (const void*)lat64_[other].p;
     sp.Lambda = p.Lambda.p;
     sp.mu = p.mu.p;
@@ -537,10 +552,53 @@ class Context {
                 eval_blocks(ntest_), rmse_.p, s_);
   }
 
+  // AdaptiveGaussianNoise::update (noisemodels.cpp:55-81); nothing under fixed noise.
+  void update_noise() {
+    if (!adaptive_) return;
+    launches_ += 2;
+    const ModeData& md = md_[0];
+    launch_noise_update(erow_.p, md.idx.p, md.val.p, md.nnz, latents(0), latents(1), mixed_, K_,
+                        KP_, mean_, var_total_, alpha_max_, noise_partials_.p,
+                        eval_blocks(md.nnz), ctl_.p, cfg_.seed, s_);
+  }
+
+  // Noise model before its first sweep: AdaptiveGaussianNoise(sn_init, sn_max) in place of
+  // FixedGaussianNoise(precision) (make_macau_adaptive, macau.cpp:222-228).
+  void set_noise_adaptive(double sn_init, double sn_max) {
+    if (!(sn_init >= 0.0) || !(sn_max >= 0.0) || !std::isfinite(sn_init) || !std::isfinite(sn_max))
+      throw MgError(MG_ERR_ARG, "sn_init and sn_max must be finite and non-negative");
+    adaptive_ = true;
+    sn_init_ = sn_init;
+    sn_max_ = sn_max;
+    if (have_data_) {
+      pack_mode(0);
+      pack_mode(1);
+      MG_CUDA(cudaStreamSynchronize(s_));
+    }
+    drop_graphs();
+    initialised_ = false;
+  }
+
+  // out[0] = current precision, out[1] = its cap (adaptive noise), out[2] = var_total
+  void get_noise(double* out) {
+    double a = cfg_.precision;
+    if (initialised_) {
+      Ctl h;
+      MG_CUDA(cudaMemcpyAsync(&h, ctl_.p, sizeof(Ctl), cudaMemcpyDeviceToHost, s_));
+      MG_CUDA(cudaStreamSynchronize(s_));
+      g_d2h_bytes += sizeof(Ctl);
+      a = h.alpha;
+    }
+    out[0] = a;
+    out[1] = adaptive_ ? (sn_max_ + 1.0) / var_total_ : cfg_.precision;
+    out[2] = var_total_;
+  }
+  bool adaptive() const { return adaptive_; }
+
   bool graphable() const { return !prior_[0].macau && !prior_[1].macau; }
 
   // One sweep; ev (optional, 8 events) brackets: sample 0 | sample 1 | prior 0 | prior 1 |
-  // eval + advance; ev[6], ev[7] end the tensor-core Gram kernel of mode 0, 1 (recorded only
+  // noise update + eval + advance; ev[6], ev[7] end the tensor-core Gram kernel of mode 0, 1 (recorded only
   // when that sampler runs).
   void sweep_body(bool do_eval, cudaEvent_t* ev = nullptr) {
     MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[0], 0, 8 * sizeof(uint32_t), s_));
@@ -553,6 +611,7 @@ class Context {
     if (ev) MG_CUDA(cudaEventRecord(ev[3], s_));
     update_prior(1);
     if (ev) MG_CUDA(cudaEventRecord(ev[4], s_));
+    update_noise();  // noise.update between the priors and the evaluation (macau.cpp:130-132)
     if (do_eval) eval(-1);
     launch_advance(ctl_.p, s_);
     launches_ += 1;
@@ -680,7 +739,11 @@ class Context {
   void run() {
     init();
     if (cfg_.verbose) {
-      printf("Noise precision: %f (fixed)\nSampling\n", cfg_.precision);
+      if (adaptive_)  // AdaptiveGaussianNoise::getInitStatus (noisemodels.h:75)
+        printf("Noise precision: adaptive (with max precision of %f)\nSampling\n",
+               (sn_max_ + 1.0) / var_total_);
+      else
+        printf("Noise precision: %f (fixed)\nSampling\n", cfg_.precision);
       fflush(stdout);
     }
     const int total = burnin_ + nsamples_;
@@ -694,9 +757,16 @@ class Context {
         get_rmse(r);
         const double took =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        printf("Iter %3d: RMSE: %.5f (1samp: %.5f)  U:[%1.2e, %1.2e]\tSide:[%s, %s] [took %0.1fs]\n",
+        // AdaptiveGaussianNoise::getStatus (noisemodels.h:77-79): "Prec:" + alpha to 2 digits
+        char prec[48] = "";
+        if (adaptive_) {
+          double nz[3];
+          get_noise(nz);
+          snprintf(prec, sizeof prec, "Prec:%.2g", nz[0]);
+        }
+        printf("Iter %3d: RMSE: %.5f (1samp: %.5f)  U:[%1.2e, %1.2e]\tSide:[%s, %s]%s [took %0.1fs]\n",
                i, r[0], r[1], latent_norm(0), latent_norm(1), link_norm_str(0).c_str(),
-               link_norm_str(1).c_str(), took);
+               link_norm_str(1).c_str(), prec, took);
         fflush(stdout);
       }
     }
@@ -886,10 +956,7 @@ class Context {
     ModeData& md = md_[m];
     md.N = dims_[m];
     md.nnz = nnz;
-    if (mixed_) {
-      md.packed.alloc((size_t)std::max(1LL, nnz));
-      launch_pack(md.idx.p, md.val.p, nnz, mean_, cfg_.precision, md.packed.p, s_);
-    }
+    if (mixed_) md.packed.alloc((size_t)std::max(1LL, nnz));
     // Task list: rows sorted by descending length; rows above the split threshold are cut into
     // near-equal parts so that no task is much longer than the average work per row group.
     const long long groups = (long long)num_sms_ * 16;
@@ -909,13 +976,8 @@ class Context {
       std::vector<long long> pptr(md.N + 1, 0);
       for (long long r = 0; r < md.N; r++)
         pptr[r + 1] = pptr[r] + (hptr[r + 1] - hptr[r] + 15) / 16 * 16;
-      {
-        DBuf<long long> dpptr;
-        dpptr.upload(pptr.data(), pptr.size(), s_);
-        md.packed_tc.alloc((size_t)std::max(1LL, pptr[md.N]));
-        launch_pad(md.ptr.p, dpptr.p, md.N, md.packed.p, (unsigned)other_n, md.packed_tc.p, s_);
-        MG_CUDA(cudaStreamSynchronize(s_));
-      }
+      md.pptr_tc.upload(pptr.data(), pptr.size(), s_);
+      md.packed_tc.alloc((size_t)std::max(1LL, pptr[md.N]));
       const long long thr16 = (thr + 15) / 16 * 16;
       int ns = 0, nsl = 0;
       std::vector<RowTask> tt = make_tasks(pptr, thr16, 16, ns, nsl);
@@ -936,7 +998,21 @@ class Context {
                          std::max(md_[0].nslots_tc, md_[1].nslots_tc)) *
         (KP_ * KP_ + KP_);
     if (need > scratch_.n) scratch_.alloc(need);
+    pack_mode(m);
     MG_CUDA(cudaStreamSynchronize(s_));
+  }
+
+  // Mixed mode: the packed (index, weight) entries of mode m and their padded copy.  The weights
+  // are (y - mean) * alpha under fixed noise and (y - mean) under adaptive noise, whose precision
+  // the samplers apply from the device as they read them.
+  void pack_mode(int m) {
+    ModeData& md = md_[m];
+    if (!mixed_) return;
+    launch_pack(md.idx.p, md.val.p, md.nnz, mean_, adaptive_ ? 1.0 : cfg_.precision,
+                md.packed.p, s_);
+    if (KP_ == 32)
+      launch_pad(md.ptr.p, md.pptr_tc.p, md.N, md.packed.p, (unsigned)dims_[1 - m],
+                 md.packed_tc.p, s_);
   }
 
   mg_config cfg_;
@@ -948,6 +1024,12 @@ class Context {
   long long dims_[2] = {0, 0};
   long long ntrain_ = 0, ntest_ = 0;
   double mean_ = 0.0;
+  // AdaptiveGaussianNoise (noisemodels.h:50-86): var_total of the training values, the cap of
+  // the precision, and sn_init / sn_max; the current precision lives in Ctl::alpha
+  bool adaptive_ = false;
+  double sn_init_ = 1.0, sn_max_ = 10.0, var_total_ = 1.0, alpha_max_ = 0.0;
+  DBuf<int> erow_;                // row of each mode-0 entry (residual sum of the noise update)
+  DBuf<double> noise_partials_;
   bool have_data_ = false, initialised_ = false;
   bool use_graph_ = true, use_tc_ = true;
   int burnin_ = 50, nsamples_ = 400;
@@ -1113,6 +1195,24 @@ int mg_update_prior(mg_ctx* ctx, int mode, int iter) {
     c.update_prior(mode);
     c.check_status();
   });
+}
+
+int mg_set_noise_adaptive(mg_ctx* ctx, double sn_init, double sn_max) {
+  return guarded(ctx, [&](mg::Context& c) { c.set_noise_adaptive(sn_init, sn_max); });
+}
+
+int mg_update_noise(mg_ctx* ctx, int iter) {
+  return guarded(ctx, [&](mg::Context& c) {
+    if (!c.initialised()) throw mg::MgError(MG_ERR_STATE, "call mg_init first");
+    mg::launch_set_sweep(c.ctl(), (uint32_t)iter, 0, c.stream());
+    c.update_noise();
+    c.check_status();
+  });
+}
+
+int mg_get_noise(mg_ctx* ctx, double* out) {
+  if (!out) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.get_noise(out); });
 }
 
 int mg_eval(mg_ctx* ctx, int n) {

@@ -399,6 +399,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t o0 = stage_off(32 * r + 8 * ch, e0), o1 = stage_off(32 * r + 8 * ch, e0 + 8);
     const __nv_bfloat16* V = reinterpret_cast<const __nv_bfloat16*>(p.other);
     const unsigned sentinel = (unsigned)p.nother;  // the zero row of the BF16 factor
+    const float wscale = (float)packed_scale(p);     // 1 unless the noise is adaptive
     int pend[kLag + 1];  // stages of the k-blocks whose arrive is pending (ring by i % (kLag + 1))
     int npend = 0, i = 0;
     for (;; i++) {
@@ -409,7 +410,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const bool v = (m.y >> r) & 1;
       const unsigned col0 = v ? sh->csr[h][slot][r][e0].x : sentinel;
       const unsigned col1 = v ? sh->csr[h][slot][r][e0 + 8].x : sentinel;
-      const float w = v ? __uint_as_float(sh->csr[h][slot][r][lane & 15].y) : 0.f;
+      const float w = v ? __uint_as_float(sh->csr[h][slot][r][lane & 15].y) * wscale : 0.f;
       const int stage = m.x % kStages;
       const uint32_t phase = (uint32_t)((m.x / kStages) & 1);
       __syncwarp();
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
     lmu_s[lane] = s;
   }
   __syncthreads();
-  const float alpha_f = (float)p.alpha;
+  const float alpha_f = (float)noise_alpha(p);
   unsigned char* work = works + (size_t)warp * kFinWork;
   float* Lc = reinterpret_cast<float*>(work) + h * 32 * kLc;  // this half's L^T
   const int c_lo = l, c_hi = l + 16;                        // this lane's two components

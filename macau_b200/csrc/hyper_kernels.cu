@@ -369,6 +369,95 @@ __global__ void k_eval_finish(const double* partials, int nparts, long long ntes
   }
 }
 
+// Row of every CSR entry (the inverse of the row pointers): entry e lies in the row r with
+// ptr[r] <= e < ptr[r + 1], found by binary search so that heavy rows cost no more than others.
+__global__ void k_entry_rows(const long long* __restrict__ ptr, long long nrows, long long nnz,
+                             int* __restrict__ erow) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride) {
+    long long lo = 0, hi = nrows;  // invariant: ptr[lo] <= e < ptr[hi]
+    while (hi - lo > 1) {
+      const long long mid = (lo + hi) >> 1;
+      if (ptr[mid] <= e) lo = mid;
+      else hi = mid;
+    }
+    erow[e] = (int)lo;
+  }
+}
+
+// Squared training residuals of AdaptiveGaussianNoise::update (noisemodels.cpp:55-72):
+// (U_i . V_j + mean - y)^2 over the entries (i = erow[e], j = col[e], y = val[e]).  Same
+// group layout as k_eval: eight lanes share the dot of one entry through vector loads and three
+// shuffles, lane l keeps entry t0 + l; the per-block sum goes to partials[block] in lane and
+// group order.
+template <typename T>
+__global__ void __launch_bounds__(kEvalThreads)
+    k_noise_sse(const int* __restrict__ erow, const int* __restrict__ col,
+                const double* __restrict__ val, long long nnz, const T* __restrict__ U,
+                const T* __restrict__ V, int K, int stride, double mean,
+                double* __restrict__ partials) {
+  constexpr int kGroups = kEvalThreads / 8;
+  __shared__ double r1[kGroups];
+  const int g = threadIdx.x >> 3, l = threadIdx.x & 7;
+  const unsigned mask = 0xffu << (8 * ((threadIdx.x & 31) >> 3));
+  double se = 0.0;
+  const long long step = (long long)gridDim.x * kGroups * 8;
+  for (long long t0 = ((long long)blockIdx.x * kGroups + g) * 8; t0 < nnz; t0 += step) {
+    const long long t = t0 + l;
+    const bool own = t < nnz;
+    const int r = own ? erow[t] : 0, c = own ? col[t] : 0;
+    double mydot = 0.0;
+#pragma unroll 2
+    for (int j = 0; j < 8; j++) {
+      const int rj = __shfl_sync(mask, r, j, 8), cj = __shfl_sync(mask, c, j, 8);
+      const T* u = U + (size_t)rj * stride;
+      const T* v = V + (size_t)cj * stride;
+      double dot = 0.0;
+      for (int k0 = 4 * l; k0 < K; k0 += 32) dot += dot4<T>(u + k0, v + k0);
+      dot += __shfl_xor_sync(mask, dot, 4, 8);
+      dot += __shfl_xor_sync(mask, dot, 2, 8);
+      dot += __shfl_xor_sync(mask, dot, 1, 8);
+      if (l == j) mydot = dot;
+    }
+    if (own) {
+      const double d = (mydot + mean) - val[t];
+      se += d * d;
+    }
+  }
+#pragma unroll
+  for (int q = 1; q < 8; q++) {
+    const double a1 = __shfl_sync(mask, se, q, 8);
+    if (l == 0) se += a1;
+  }
+  if (l == 0) r1[g] = se;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int q = 0; q < kGroups; q++) a += r1[q];
+    partials[blockIdx.x] = a;
+  }
+}
+
+// The precision draw of AdaptiveGaussianNoise::update (noisemodels.cpp:73-81), one warp: the
+// partial sums in a fixed order, then aN = a0 + nnz / 2, bN = b0 + sumsq / 2 with
+// (a0, b0) = (1/2, var_total / 2), alpha = Gamma(aN, 1) / bN capped at alpha_max, into ctl->alpha.
+__global__ void k_noise_draw(const double* __restrict__ partials, int nparts, long long nnz,
+                             double var_total, double alpha_max, Ctl* ctl,
+                             unsigned long long seed) {
+  const int lane = threadIdx.x & 31;
+  double a = 0.0;
+  for (int q = lane; q < nparts; q += 32) a += partials[q];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if (lane == 0) {
+    const double aN = 0.5 + (double)nnz / 2.0;
+    const double bN = 0.5 * var_total + a / 2.0;
+    double alpha = gamma_draw(seed, ctl->sweep, stream_id(kNoiseAlpha, 0u), 0u, aN) * (1.0 / bN);
+    if (alpha > alpha_max) alpha = alpha_max;
+    ctl->alpha = alpha;
+  }
+}
+
 __global__ void k_set_sweep(Ctl* ctl, uint32_t sweep, int burnin) {
   ctl->sweep = sweep;
   ctl->burnin = burnin;
@@ -735,6 +824,32 @@ void launch_eval(const int* trow, const int* tcol, const double* tval, long long
                                                     ctl, pred, pvar, partials);
   MG_CUDA(cudaGetLastError());
   k_eval_finish<<<1, 32, 0, s>>>(partials, nblocks, ntest, rmse);
+  MG_CUDA(cudaGetLastError());
+}
+
+void launch_entry_rows(const long long* ptr, long long nrows, long long nnz, int* erow,
+                       cudaStream_t s) {
+  if (nnz <= 0) return;
+  long long b = (nnz + 255) / 256;
+  if (b > 4736) b = 4736;
+  k_entry_rows<<<(int)b, 256, 0, s>>>(ptr, nrows, nnz, erow);
+  MG_CUDA(cudaGetLastError());
+}
+
+void launch_noise_update(const int* erow, const int* col, const double* val, long long nnz,
+                         const void* U, const void* V, bool f32, int K, int stride, double mean,
+                         double var_total, double alpha_max, double* partials, int nblocks,
+                         Ctl* ctl, unsigned long long seed, cudaStream_t s) {
+  if (f32)
+    k_noise_sse<float><<<nblocks, kEvalThreads, 0, s>>>(erow, col, val, nnz, (const float*)U,
+                                                        (const float*)V, K, stride, mean,
+                                                        partials);
+  else
+    k_noise_sse<double><<<nblocks, kEvalThreads, 0, s>>>(erow, col, val, nnz, (const double*)U,
+                                                         (const double*)V, K, stride, mean,
+                                                         partials);
+  MG_CUDA(cudaGetLastError());
+  k_noise_draw<<<1, 32, 0, s>>>(partials, nblocks, nnz, var_total, alpha_max, ctl, seed);
   MG_CUDA(cudaGetLastError());
 }
 

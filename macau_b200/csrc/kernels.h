@@ -60,6 +60,16 @@ void launch_eval(const int* trow, const int* tcol, const double* tval, long long
                  const void* U, const void* V, bool f32, int K, int stride, double mean,
                  int n_fixed, const Ctl* ctl, double* pred, double* pvar, double* partials,
                  int nblocks, double* rmse, cudaStream_t s);
+// Row index of every entry of a CSR (nnz entries, nrows rows).
+void launch_entry_rows(const long long* ptr, long long nrows, long long nnz, int* erow,
+                       cudaStream_t s);
+// AdaptiveGaussianNoise::update: squared residuals of the nnz training entries (erow / col /
+// val) under the latents U (rows) and V (columns), summed through `partials` (nblocks =
+// eval_blocks(nnz) doubles), then the capped Gamma draw of the precision into ctl->alpha.
+void launch_noise_update(const int* erow, const int* col, const double* val, long long nnz,
+                         const void* U, const void* V, bool f32, int K, int stride, double mean,
+                         double var_total, double alpha_max, double* partials, int nblocks,
+                         Ctl* ctl, unsigned long long seed, cudaStream_t s);
 void launch_set_sweep(Ctl* ctl, uint32_t sweep, int burnin, cudaStream_t s);
 void launch_advance(Ctl* ctl, cudaStream_t s);
 

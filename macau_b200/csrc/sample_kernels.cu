@@ -173,6 +173,8 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
   const Elem* other = reinterpret_cast<const Elem*>(p.other);
 
   const int ntasks = p.ntasks;
+  const double alpha = noise_alpha(p);
+  const double wscale = packed_scale(p);
   for (;;) {
     if (t == 0) bcast[0] = (int)atomicAdd(&p.ctl->queue[p.qslot], 1u);
     gsync<T>(g);
@@ -196,10 +198,10 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
           if constexpr (MIXED) {
             const uint2 pk = p.packed[b + e];
             c = (int)pk.x;
-            w = (double)__uint_as_float(pk.y);
+            w = (double)__uint_as_float(pk.y) * wscale;
           } else {
             c = p.colidx[b + e];
-            w = (p.vals[b + e] - p.mean) * p.alpha;
+            w = (p.vals[b + e] - p.mean) * alpha;
           }
         }
         cidx[e] = c;
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
       if constexpr (MIXED) {
         float a[KP], d0 = 1.f, rinv = 1.f;
         warp_load_mm<float, float, KP>(a, d0, reinterpret_cast<const float*>(Gs), LD, Lam_s,
-                                       p.alpha, lane, K);
+                                       alpha, lane, K);
         // L^T goes after the Gram tile, which must stay readable for an FP64 retry
         float* Lc = reinterpret_cast<float*>(base) + KP * LD;
         const double z = row_noise(p, row, K, lane, sweep);
@@ -346,7 +348,7 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
     if constexpr (MIXED) {
       float* M = reinterpret_cast<float*>(base);
       float* rr = reinterpret_cast<float*>(rrd);
-      const float af = (float)p.alpha;
+      const float af = (float)alpha;
 #pragma unroll
       for (int i = 0; i < TR; i++)
 #pragma unroll
@@ -382,7 +384,7 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
         for (int j = 0; j < TC; j++) {
           const int gi = rt * TR + i, gj = ct * TC + j;
           if (gi < K && gj <= gi) {
-            const double v = p.Lambda[gi + gj * K] + p.alpha * (double)acc[i][j];
+            const double v = p.Lambda[gi + gj * K] + alpha * (double)acc[i][j];
             M[gi * LD + gj] = v;
             if (gi == gj) diag[gi] = v;
           }

@@ -254,7 +254,7 @@ __device__ __forceinline__ bool warp_finish_f64_body(const GT* Gs, int ld, const
   const int K = p.K;
   double a[KP], d0 = 1.0, rinv = 1.0;
   const double z = row_noise(p, row, K, lane, sweep);
-  warp_load_mm<double, GT, KP>(a, d0, Gs, ld, Lam_s, p.alpha, lane, K);
+  warp_load_mm<double, GT, KP>(a, d0, Gs, ld, Lam_s, noise_alpha(p), lane, K);
   __syncwarp();
   double* Lc = reinterpret_cast<double*>(work);  // the Gram tile has been read into a[]
   if (!warp_factor<double, KP>(a, rinv, lane, 0.0, d0, Lc, KP + 4)) return false;

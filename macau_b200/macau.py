@@ -6,10 +6,11 @@
 include/macau_b200.h; there is no CPU fallback.
 
 Supported by the GPU sampler (the hot path): a 2-mode sparse matrix or 2-index-column
-DataFrame, fixed Gaussian noise (numeric ``precision``), BPMF priors and Macau priors with sparse
-or dense side information (block-CG; the reference switches to a direct FtF Cholesky solve when a
-side matrix has at most 10000 columns, macau.pyx:160, which solves the same system).  Tensors,
-``precision="adaptive"``/``"probit"`` and ``univariate=True`` raise ValueError.
+DataFrame, fixed Gaussian noise (numeric ``precision``) or adaptive Gaussian noise
+(``precision="adaptive"``), BPMF priors and Macau priors with sparse or dense side information
+(block-CG; the reference switches to a direct FtF Cholesky solve when a side matrix has at most
+10000 columns, macau.pyx:160, which solves the same system).  Tensors, ``precision="probit"``
+and ``univariate=True`` raise ValueError.
 
 Two keyword arguments are added: ``seed`` (key of all random draws; the reference is
 unseeded) and ``compute`` ("fp64" or "mixed"; default from the MACAU_GPU_PRECISION environment
@@ -219,12 +220,15 @@ def macau(Y,
       side       list of side information matrices (one per mode, None = no side info)
       lambda_beta  initial precision (regularization) for the link matrix
       num_latent   number of latent dimensions
-      precision    precision of observations of Y (a number: fixed Gaussian noise)
+      precision    precision of observations of Y:
+                   number     - fixed Gaussian noise
+                   "adaptive" - automatically learn precision (also "sample")
       burnin       number of Gibbs samples to drop (burn-in)
       nsamples     number of Gibbs samples to collect
       univariate   must be False (the univariate sampler is not on the GPU path)
       tol          error tolerance for conjugate gradient solver
-      sn_max       unused (adaptive precision is not on the GPU path)
+      sn_max       maximum signal-to-noise ratio for observation precision
+                   only used if precision="adaptive"
       save_prefix  prefix for model files or None if not saving the model
       verbose      whether to print output for each Gibbs iteration
       seed         key of all random draws (None: drawn from the OS)
@@ -242,10 +246,14 @@ def macau(Y,
                          (len(side), len(data.shape)))
     if len(data.shape) != 2:
         raise ValueError("Tensor data (%d modes) is not supported by the GPU sampler." % len(data.shape))
+    adaptive = False
     if isinstance(precision, str):
-        if precision in ("adaptive", "sample", "probit"):
-            raise ValueError("precision=%r is not supported by the GPU sampler (fixed Gaussian noise only)." % precision)
-        raise ValueError("Parameter 'precision' has to be either a number or \"adaptive\" for adaptive precision, or \"probit\" for binary matrices.")
+        if precision in ("adaptive", "sample"):  # make_macau_adaptive(Nmodes, D, 1.0, sn_max) (macau.pyx:391-392)
+            adaptive = True
+        elif precision == "probit":
+            raise ValueError("precision='probit' is not supported by the GPU sampler (Gaussian noise only).")
+        else:
+            raise ValueError("Parameter 'precision' has to be either a number or \"adaptive\" for adaptive precision, or \"probit\" for binary matrices.")
     if univariate:
         raise ValueError("The univariate sampler is not supported by the GPU sampler.")
     if save_prefix is not None and type(save_prefix) != str:
@@ -254,9 +262,11 @@ def macau(Y,
     if seed is None:
         seed = int.from_bytes(os.urandom(8), "little")
     D = int(np.int32(num_latent))
-    s = _lib.Sampler(D, float(precision), seed=seed, compute=_compute_mode(compute),
-                     verbose=False)
+    s = _lib.Sampler(D, 1.0 if adaptive else float(precision), seed=seed,
+                     compute=_compute_mode(compute), verbose=False)
     try:
+        if adaptive:
+            s.set_noise_adaptive(1.0, float(sn_max))
         s.set_relation_data(data.idxTrain[0], data.idxTrain[1], data.valTrain, data.shape)
         if len(data.valTest) > 0:
             s.set_relation_data_test(data.idxTest[0], data.idxTest[1], data.valTest, data.shape)
@@ -271,7 +281,10 @@ def macau(Y,
         s.set_samples(int(burnin), int(nsamples))
         s.init()
         if verbose:
-            print("Noise precision: %f (fixed)" % float(precision))
+            if adaptive:  # AdaptiveGaussianNoise::getInitStatus (noisemodels.h:75)
+                print("Noise precision: adaptive (with max precision of %f)" % s.noise()[1])
+            else:
+                print("Noise precision: %f (fixed)" % float(precision))
             print("Sampling")
         if save_prefix is not None:
             _write_csv(save_prefix + "-meanvalue.csv", [[s.mean_value()]])
@@ -287,8 +300,9 @@ def macau(Y,
                 r, r1 = s.rmse()
                 norms = [np.linalg.norm(s.latents(m)) for m in range(2)]
                 links = ["%1.2e" % np.linalg.norm(s.beta(m)) if s.nfeat[m] else "nan" for m in range(2)]
-                print("Iter %3d: RMSE: %.5f (1samp: %.5f)  U:[%1.2e, %1.2e]\tSide:[%s] [took %0.1fs]" %
-                      (i, r, r1, norms[0], norms[1], ", ".join(links), time.time() - t0))
+                prec = "Prec:%.2g" % s.noise()[0] if adaptive else ""  # noisemodels.h:77-79
+                print("Iter %3d: RMSE: %.5f (1samp: %.5f)  U:[%1.2e, %1.2e]\tSide:[%s]%s [took %0.1fs]" %
+                      (i, r, r1, norms[0], norms[1], ", ".join(links), prec, time.time() - t0))
                 sys.stdout.flush()
         rmse_test, _ = s.rmse()
         yhat = s.predictions()

@@ -16,6 +16,7 @@
 //                                   linop.cpp:37-57 (libfastsparse csr_A_mul_Bn restated as the
 //                                   plain CSR row loop)
 //   eval_rmse ..................... lib/macau-cpp/bpmfutils.h:86-114
+//   AdaptiveGaussianNoise ......... lib/macau-cpp/noisemodels.cpp:14-33 (init), 55-81 (update)
 //   MacauX::run sweep body ........ lib/macau-cpp/macau.cpp:110-147
 // Eigen 3.3.7 (LLT, triangular solves, inverse) is not in the reference tree; its operations are
 // restated as textbook left-looking Cholesky and substitution.  X.inverse() (mvnormal.cpp:326),
@@ -512,6 +513,9 @@ struct Model {
   const double* tval = nullptr;
   std::vector<double> pred, pred_var;
   double rmse = NAN, rmse1 = NAN;
+  // AdaptiveGaussianNoise (noisemodels.h:50-86); alpha above is its current precision
+  bool adaptive = false;
+  double var_total = 1.0, alpha_max = 0.0;
 };
 
 void init_prior(Prior& p, int K) {  // BPMFPrior::init / MacauPrior::init (latentprior.cpp:84-99)
@@ -598,6 +602,33 @@ int update_prior(Model& m, int mode, int iter) {
   return 0;
 }
 
+// AdaptiveGaussianNoise::update (noisemodels.cpp:55-81): the squared training residuals summed
+// over the columns of Y in storage order, then alpha ~ Gamma(aN, 1 / bN) capped at alpha_max,
+// with (a0, b0) = (1/2, var_total / 2), one prior sample of noise at the full variance.
+void update_noise(Model& m, int iter) {
+  if (!m.adaptive) return;
+  const Csr& C = m.Y[1];  // columns of Y: C.idx are row indices
+  const int K = m.K;
+  const double* U = m.lat[0].data();
+  const double* V = m.lat[1].data();
+  double sumsq = 0.0;
+  for (int j = 0; j < C.nrow; j++)
+    for (int64_t e = C.ptr[j]; e < C.ptr[j + 1]; e++) {
+      const double* u = U + (size_t)C.idx[e] * K;
+      const double* v = V + (size_t)j * K;
+      double dot = 0.0;
+      for (int k = 0; k < K; k++) dot += v[k] * u[k];
+      const double d = (dot + m.mean) - C.val[e];
+      sumsq += d * d;
+    }
+  const double nnz = (double)C.ptr[C.nrow];
+  const double aN = 0.5 + nnz / 2.0;
+  const double bN = 0.5 * m.var_total + sumsq / 2.0;
+  double a = gamma_draw(m.seed, (uint32_t)iter, stream_id(kNoiseAlpha, 0u), 0u, aN) * (1.0 / bN);
+  if (a > m.alpha_max) a = m.alpha_max;
+  m.alpha = a;
+}
+
 void eval_model(Model& m, int n) {
   if (m.ntest == 0) {
     m.rmse = NAN;
@@ -680,12 +711,37 @@ int orc_model_sweep(void* h, int iter, int burnin) {
     if (sample_mode(m, mode, iter)) return -1;
   for (int mode = 0; mode < 2; mode++)
     if (update_prior(m, mode, iter)) return -1;
+  update_noise(m, iter);
   eval_model(m, iter < burnin ? 0 : iter - burnin);
   return 0;
 }
 
+// AdaptiveGaussianNoise(sn_init, sn_max) + init (noisemodels.cpp:14-33, macau.cpp:222-228):
+// var_total = mean squared deviation of the training values from the mean (in column storage
+// order; 1 when not positive or NaN), alpha = (sn_init + 1) / var_total, alpha_max =
+// (sn_max + 1) / var_total.  Call after orc_model_set_train.
+void orc_model_set_noise_adaptive(void* h, double sn_init, double sn_max) {
+  Model& m = *static_cast<Model*>(h);
+  const Csr& C = m.Y[1];
+  const int64_t nnz = C.ptr[C.nrow];
+  double se = 0.0;
+  for (int64_t e = 0; e < nnz; e++) se += (C.val[e] - m.mean) * (C.val[e] - m.mean);
+  double vt = se / (double)nnz;
+  if (vt <= 0.0 || std::isnan(vt)) vt = 1.0;
+  m.adaptive = true;
+  m.var_total = vt;
+  m.alpha = (sn_init + 1.0) / vt;
+  m.alpha_max = (sn_max + 1.0) / vt;
+}
+
+int orc_model_update_noise(void* h, int iter) {
+  update_noise(*static_cast<Model*>(h), iter);
+  return 0;
+}
+
 // what: 0 latents (K x dim), 1 mu (K), 2 Lambda (K x K), 3 beta (K x nfeat), 4 Uhat (K x dim),
-//       5 [lambda_beta, cg_iters], 6 predictions, 7 predictions_var, 8 [rmse_avg, rmse_1samp]
+//       5 [lambda_beta, cg_iters], 6 predictions, 7 predictions_var, 8 [rmse_avg, rmse_1samp],
+//       9 [alpha, alpha_max, var_total] (noise precision)
 void orc_model_get(void* h, int what, int mode, double* out) {
   Model& m = *static_cast<Model*>(h);
   Prior& p = m.prior[mode];
@@ -699,11 +755,12 @@ void orc_model_get(void* h, int what, int mode, double* out) {
     case 6: std::copy(m.pred.begin(), m.pred.end(), out); break;
     case 7: std::copy(m.pred_var.begin(), m.pred_var.end(), out); break;
     case 8: out[0] = m.rmse; out[1] = m.rmse1; break;
+    case 9: out[0] = m.alpha; out[1] = m.alpha_max; out[2] = m.var_total; break;
     default: break;
   }
 }
 
-// what: 0 latents, 1 mu, 2 Lambda, 3 beta, 4 Uhat, 5 lambda_beta
+// what: 0 latents, 1 mu, 2 Lambda, 3 beta, 4 Uhat, 5 lambda_beta, 9 noise precision alpha
 void orc_model_set(void* h, int what, int mode, const double* in) {
   Model& m = *static_cast<Model*>(h);
   Prior& p = m.prior[mode];
@@ -714,6 +771,7 @@ void orc_model_set(void* h, int what, int mode, const double* in) {
     case 3: std::copy(in, in + p.beta.size(), p.beta.begin()); break;
     case 4: std::copy(in, in + p.Uhat.size(), p.Uhat.begin()); break;
     case 5: p.lambda_beta = in[0]; break;
+    case 9: m.alpha = in[0]; break;
     default: break;
   }
 }

@@ -15,7 +15,7 @@ _HERE = Path(__file__).resolve().parent
 LIB_PATH = _HERE / "_build" / "liboracle.so"
 
 PURPOSE = dict(row_noise=1, mvn_n=2, mvn_f=3, wishart_off=4, wishart_diag=5, mu_draw=6,
-               lambda_beta=7)
+               lambda_beta=7, noise_alpha=8)
 
 _d = C.c_double
 _i = C.c_int
@@ -58,6 +58,8 @@ def _load():
         "orc_model_eval": (None, [_p, _i]),
         "orc_model_sweep": (_i, [_p, _i, _i]),
         "orc_model_get": (None, [_p, _i, _i, _p]),
+        "orc_model_set_noise_adaptive": (None, [_p, _d, _d]),
+        "orc_model_update_noise": (_i, [_p, _i]),
         "orc_model_set": (None, [_p, _i, _i, _p]),
     }
     for name, (res, args) in sig.items():
@@ -256,6 +258,18 @@ class Model:
         lib().orc_model_set_side(self.h, mode, F.ncol, _ptr(F.ptr), _ptr(F.idx), _ptr(F.val),
                                  _ptr(Ft.ptr), _ptr(Ft.idx), _ptr(Ft.val), lambda_beta, tol)
 
+    def set_noise_adaptive(self, sn_init=1.0, sn_max=10.0):
+        """AdaptiveGaussianNoise(sn_init, sn_max) + init (noisemodels.cpp:14-33); after set_train."""
+        lib().orc_model_set_noise_adaptive(self.h, sn_init, sn_max)
+
+    def update_noise(self, it):
+        """AdaptiveGaussianNoise::update with the draw of sweep `it` (noisemodels.cpp:55-81)."""
+        return lib().orc_model_update_noise(self.h, it)
+
+    def noise(self):
+        """(alpha, alpha_max, var_total) of the noise model."""
+        return tuple(self._get(9, 0, (3,)))
+
     def sweep(self, it, burnin):
         return lib().orc_model_sweep(self.h, it, burnin)
 
@@ -303,5 +317,5 @@ class Model:
     def set(self, what, mode, arr):
         arr = f64(arr)
         self._keep.append(arr)
-        code = dict(latents=0, mu=1, Lambda=2, beta=3, uhat=4, lambda_beta=5)[what]
+        code = dict(latents=0, mu=1, Lambda=2, beta=3, uhat=4, lambda_beta=5, alpha=9)[what]
         lib().orc_model_set(self.h, code, mode, _ptr(arr))

@@ -32,6 +32,7 @@ enum Purpose : uint32_t {
   kWishartDiag = 5,   // WishartUnit chi via Gamma (mvnormal.cpp:223-224)
   kMuDraw = 6,        // NormalWishart: MvNormal_prec(kappa*Lambda, mu) (mvnormal.cpp:273)
   kLambdaBeta = 7,    // sample_lambda_beta: rgamma (latentprior.cpp:328-331)
+  kNoiseAlpha = 8,    // AdaptiveGaussianNoise::update: rgamma(aN, 1/bN) (noisemodels.cpp:75-78)
 };
 
 inline void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {

@@ -323,6 +323,101 @@ def test_mixed_row_sampler_keyed_draws(K, mode):
     assert relerr(s.latents(mode), want) < MIXED_SAMPLE_TOL
 
 
+# ---- adaptive Gaussian noise (AdaptiveGaussianNoise, noisemodels.cpp:14-33, 55-81) ----
+
+def adaptive_pair(w, K, seed, sn_max=10.0, compute=_lib.MG_COMPUTE_FP64, burnin=0, nsamples=1):
+    s = gpu_sampler(w, K, 1.0, seed, compute=compute, burnin=burnin, nsamples=nsamples,
+                    init=False)
+    s.set_noise_adaptive(1.0, sn_max)
+    s.init()
+    m = oracle_model(w, K, 1.0, seed)
+    m.set_noise_adaptive(1.0, sn_max)
+    return s, m
+
+
+@pytest.mark.parametrize("sn_max", [10.0, 0.05])
+def test_adaptive_noise_sweeps_fp64_match_oracle(sn_max):
+    # whole sweeps (samplers at the current precision, priors, precision redraw, eval); with
+    # sn_max = 0.05 the cap binds
+    w = workloads.bpmf_uniform(nrow=400, ncol=300, nobs=12000, seed=6)
+    K, seed, burnin = 10, 77, 4
+    s, m = adaptive_pair(w, K, seed, sn_max, burnin=burnin, nsamples=6)
+    a0, amax0, vt0 = m.noise()
+    a, amax, vt = s.noise()
+    assert abs(vt - vt0) <= 1e-12 * vt0 and abs(a - a0) <= 1e-12 * a0
+    assert abs(amax - amax0) <= 1e-12 * amax0
+    capped = 0
+    for it in range(10):
+        s.sweep(it, eval=True)
+        assert m.sweep(it, burnin) == 0
+        for mode in (0, 1):
+            assert relerr(s.latents(mode), m.latents(mode)) < 1e-8, (it, mode)
+            assert relerr(s.hyper(mode)[1], m.Lambda(mode)) < 1e-8
+        a, ao = s.noise()[0], m.noise()[0]
+        assert abs(a - ao) <= FP64_TOL * ao, (it, a, ao)
+        capped += ao == amax0
+        r, r1 = s.rmse()
+        ro, r1o = m.rmse()
+        assert abs(r - ro) < 1e-9 and abs(r1 - r1o) < 1e-9
+    assert (capped > 0) == (sn_max < 1.0)
+
+
+@pytest.mark.parametrize("compute", [_lib.MG_COMPUTE_FP64, _lib.MG_COMPUTE_MIXED])
+def test_adaptive_noise_update_matches_oracle(compute):
+    # the precision redraw alone from given latents (the mixed context keeps FP32 latents, so the
+    # oracle gets the same FP32 values)
+    rng = np.random.default_rng(31)
+    w = small_uniform(seed=8, nrow=500, ncol=350, nobs=25000)
+    K, seed = 32, 5
+    s, m = adaptive_pair(w, K, seed, compute=compute)
+    for it in (0, 3):
+        U = rng.normal(scale=0.4, size=(w["shape"][0], K))
+        V = rng.normal(scale=0.4, size=(w["shape"][1], K))
+        if compute == _lib.MG_COMPUTE_MIXED:
+            U = U.astype(np.float32).astype(np.float64)
+            V = V.astype(np.float32).astype(np.float64)
+        s.set_latents(0, U)
+        s.set_latents(1, V)
+        m.set("latents", 0, U)
+        m.set("latents", 1, V)
+        s.update_noise(it)
+        m.update_noise(it)
+        a, ao = s.noise()[0], m.noise()[0]
+        assert abs(a - ao) <= 1e-12 * ao, (it, a, ao)
+
+
+@pytest.mark.parametrize("compute,tensor_cores,K", [
+    (_lib.MG_COMPUTE_FP64, 0, 10),
+    (_lib.MG_COMPUTE_MIXED, 1, 32),
+    (_lib.MG_COMPUTE_MIXED, 0, 32),
+    (_lib.MG_COMPUTE_MIXED, 0, 10),
+])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_row_sampler_uses_device_precision(compute, tensor_cores, K, mode):
+    # after a redraw the samplers read the precision from the device (mixed: unscaled packed
+    # weights times that precision) and match the oracle sampled at the same alpha
+    rng = np.random.default_rng(40 + K + mode)
+    w = heavy_rows_workload(rng, nrow=80, ncol=3000)
+    s, _ = adaptive_pair(w, K, 12, compute=compute)
+    s.set_option("tensor_core_gram", tensor_cores)
+    s.set_latents(0, rng.normal(scale=0.3, size=(w["shape"][0], K)))
+    s.set_latents(1, rng.normal(scale=0.3, size=(w["shape"][1], K)))
+    s.update_noise(2)
+    alpha = s.noise()[0]
+    assert alpha > 0
+    other = 1 - mode
+    Vo = rng.normal(scale=0.3, size=(w["shape"][other], K))
+    s.set_latents(other, Vo)
+    z = rng.normal(size=(w["shape"][mode], K))
+    mu, Lam, _ = s.hyper(mode)
+    s.sample_latents(mode, 0, z)
+    Y = train_matrix(w)
+    R = orc.Csr.from_scipy(Y if mode == 0 else Y.T)
+    want, _ = orc.sample_latents(K, R, Vo, s.mean_value(), alpha, mu, Lam, z=z)
+    tol = FP64_TOL if compute == _lib.MG_COMPUTE_FP64 else MIXED_SAMPLE_TOL
+    assert relerr(s.latents(mode), want) < tol
+
+
 def test_cholesky_failure_is_reported_and_context_survives():
     w = small_uniform(seed=4)
     K = 6

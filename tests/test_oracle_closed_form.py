@@ -121,3 +121,73 @@ def test_model_runs_and_learns_small_bpmf():
         assert m.sweep(it, 30) == 0
     rmse, rmse1 = m.rmse()
     assert rmse < 0.6, rmse
+
+
+def test_adaptive_noise_matches_closed_form():
+    """AdaptiveGaussianNoise (noisemodels.cpp:14-33, 55-81): var_total, the initial and capped
+    precision, and the update's Gamma(aN, 1/bN) draw from the squared training residuals."""
+    rng = np.random.default_rng(11)
+    nrow, ncol, K, seed = 50, 40, 5, 99
+    Y = rand_csr(rng, nrow, ncol, 0.25).tocsc()
+    Y.sort_indices()
+    mean = Y.sum() / Y.nnz
+    m = orc.Model(K, 1.0, seed)
+    m.set_train(orc.Csr.from_scipy(Y), orc.Csr.from_scipy(Y.T), mean)
+    m.set_noise_adaptive(1.0, 10.0)
+    var_total = np.mean((Y.data - mean) ** 2)
+    alpha, alpha_max, vt = m.noise()
+    assert abs(vt - var_total) <= 1e-14 * var_total
+    assert abs(alpha - 2.0 / var_total) <= 1e-14 * alpha
+    assert abs(alpha_max - 11.0 / var_total) <= 1e-14 * alpha_max
+    U = rng.normal(scale=0.5, size=(nrow, K))
+    V = rng.normal(scale=0.5, size=(ncol, K))
+    m.set("latents", 0, U)
+    m.set("latents", 1, V)
+    m.update_noise(7)
+    Yc = Y.tocoo()
+    sse = np.sum((np.sum(U[Yc.row] * V[Yc.col], axis=1) + mean - Yc.data) ** 2)
+    aN = 0.5 + Y.nnz / 2.0
+    bN = 0.5 * var_total + sse / 2.0
+    want = min(orc.gamma(seed, 7, "noise_alpha", 0, 0, aN) / bN, alpha_max)
+    assert abs(m.noise()[0] - want) <= 1e-12 * want
+    # latents that fit Y exactly: the draw (about nnz / var_total) is capped at alpha_max
+    Yc = Y.tocoo()
+    a, b = rng.normal(size=nrow), rng.normal(size=ncol)
+    ab = a[Yc.row] * b[Yc.col]
+    Yx = sp.coo_matrix((ab + 3.0, (Yc.row, Yc.col)), shape=Y.shape).tocsc()
+    Yx.sort_indices()
+    mx = Yx.sum() / Yx.nnz
+    Ux = np.zeros((nrow, K))
+    Vx = np.zeros((ncol, K))
+    Ux[:, 0], Vx[:, 0] = a, b
+    Ux[:, 1], Vx[:, 1] = 1.0, -(mx - 3.0)
+    m2 = orc.Model(K, 1.0, seed)
+    m2.set_train(orc.Csr.from_scipy(Yx), orc.Csr.from_scipy(Yx.T), mx)
+    m2.set_noise_adaptive(1.0, 10.0)
+    m2.set("latents", 0, Ux)
+    m2.set("latents", 1, Vx)
+    m2.update_noise(0)
+    assert m2.noise()[0] == m2.noise()[1]
+
+
+def test_adaptive_noise_model_learns_noise_level():
+    """A full adaptive-noise run: the precision settles near 1 / noise variance (signal-to-noise
+    below sn_max), like AdaptiveGaussianNoise in MacauX::run (macau.cpp:110-147)."""
+    rng = np.random.default_rng(5)
+    nrow, ncol, K, sd = 150, 100, 4, 0.8
+    Ut = rng.normal(size=(nrow, 3))
+    Vt = rng.normal(size=(ncol, 3))
+    mask = rng.random((nrow, ncol)) < 0.4
+    r, c = np.nonzero(mask)
+    v = np.sum(Ut[r] * Vt[c], axis=1) + rng.normal(scale=sd, size=len(r))
+    Y = sp.coo_matrix((v, (r, c)), shape=(nrow, ncol)).tocsc()
+    Y.sort_indices()
+    m = orc.Model(K, 1.0, 3)
+    m.set_train(orc.Csr.from_scipy(Y), orc.Csr.from_scipy(Y.T), Y.sum() / Y.nnz)
+    m.set_noise_adaptive(1.0, 10.0)
+    alphas = []
+    for it in range(40):
+        assert m.sweep(it, 20) == 0
+        alphas.append(m.noise()[0])
+    a = np.mean(alphas[20:])
+    assert 0.7 / sd**2 < a < 1.5 / sd**2 and a < m.noise()[1], a

@@ -397,7 +397,7 @@ def test_row_sampler_uses_device_precision(compute, tensor_cores, K, mode):
     # after a redraw the samplers read the precision from the device (mixed: unscaled packed
     # weights times that precision) and match the oracle sampled at the same alpha
     rng = np.random.default_rng(40 + K + mode)
-    w = heavy_rows_workload(rng, nrow=80, ncol=3000)
+    w = heavy_rows_workload(rng, nrow=80)
     s, _ = adaptive_pair(w, K, 12, compute=compute)
     s.set_option("tensor_core_gram", tensor_cores)
     s.set_latents(0, rng.normal(scale=0.3, size=(w["shape"][0], K)))

@@ -335,11 +335,14 @@ def run_ours(args):
     s.set_relation_data_test(w["trows"], w["tcols"], w["tvals"], w["shape"])
     s.set_samples(0, E)
     s.init()
+    t1 = time.perf_counter()
     for i in range(E):
         s.sweep(i, eval=True)
         s.rmse()
+    t2 = time.perf_counter()
     preds = s.predictions()
     t_e2e = time.perf_counter() - t0
+    e2e_split = {"setup_s": t1 - t0, "sweeps_s": t2 - t1, "readback_s": t0 + t_e2e - t2}
     st_e = s.stats()
     s.close()
     t_e2e = max_over_ranks(t_e2e)
@@ -389,7 +392,8 @@ def run_ours(args):
             "e2e": {"value": ranks.rate(E, t_e2e), "unit": UNIT, "h2d_bytes_per_step": h2d / E,
                     "d2h_bytes_per_step": d2h / E,
                     "timed": "C-ABI run: data upload + CSR build, init, sweeps with eval and "
-                             "RMSE read-back, final predictions read-back"}}
+                             "RMSE read-back, final predictions read-back",
+                    "split_s": e2e_split}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds, 50)
         line["mixed_over_cpu"] = v_mx / line["cpu_baseline"]["value"]

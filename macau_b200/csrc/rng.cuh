@@ -31,6 +31,7 @@ enum Purpose : uint32_t {
   kMuDraw = 6,       // NormalWishart mean draw (mvnormal.cpp:273)
   kLambdaBeta = 7,   // lambda_beta Gamma draw (latentprior.cpp:328-331)
   kNoiseAlpha = 8,   // AdaptiveGaussianNoise precision Gamma draw (noisemodels.cpp:75-78)
+  kBetaOne = 9,      // univariate link-matrix draws, one per (feature, dim) (macauoneprior.cpp:241)
 };
 
 MG_HD uint32_t stream_id(uint32_t purpose, uint32_t mode) { return (purpose << 8) | mode; }

@@ -17,6 +17,9 @@
 //                                   plain CSR row loop)
 //   eval_rmse ..................... lib/macau-cpp/bpmfutils.h:86-114
 //   AdaptiveGaussianNoise ......... lib/macau-cpp/noisemodels.cpp:14-33 (init), 55-81 (update)
+//   MacauOnePrior (univariate) .... lib/macau-cpp/macauoneprior.cpp:16-39 (init), 41-95 (row
+//                                   sampler), 189-257 (mu/lambda, beta), 267-290 (lambda_beta);
+//                                   linop.cpp:374-401 (col_square_sum), linop.h:121-178
 //   MacauX::run sweep body ........ lib/macau-cpp/macau.cpp:110-147
 // Eigen 3.3.7 (LLT, triangular solves, inverse) is not in the reference tree; its operations are
 // restated as textbook left-looking Cholesky and substitution.  X.inverse() (mvnormal.cpp:326),
@@ -497,6 +500,11 @@ struct Prior {
   std::vector<double> Uhat, beta;
   double lambda_beta = 5.0, lb_mu0 = 1.0, lb_nu0 = 1e-3, tol = 1e-6;
   int cg_iters = 0;
+  // MacauOnePrior (macauoneprior.h:8-51): per-dimension precisions lambda = diag(Lambda) and
+  // lambda_beta, the squared column norms of F, and the Gamma hyperprior of lambda_beta
+  bool one = false;
+  std::vector<double> lb_one, colsq;
+  double lb_a0 = 0.1, lb_b0 = 0.1;
 };
 
 struct Model {
@@ -531,8 +539,55 @@ void init_prior(Prior& p, int K) {  // BPMFPrior::init / MacauPrior::init (laten
   p.df = K;
 }
 
+// MacauOnePrior::sample_latents (macauoneprior.cpp:41-95): per row, the coordinates are
+// resampled one after another, u_d ~ N(L_d / Q_d, 1 / Q_d) with Q_d = lambda_d + alpha sum v_d^2
+// and L_d = lambda_d (mu_d + Uhat_d) + alpha sum (y - (yhat - u_d v_d)) v_d, where yhat keeps the
+// row's predictions under the coordinates updated so far.  The normals are the row sampler's
+// keyed draws (kRowNoise, row, d).
+int sample_mode_one(Model& m, int mode, int iter) {
+  Prior& p = m.prior[mode];
+  const int other = 1 - mode;
+  const Csr& R = m.Y[mode];
+  const int K = m.K;
+  double* U = m.lat[mode].data();
+  const double* V = m.lat[other].data();
+  const double alpha = m.alpha;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int i = 0; i < R.nrow; i++) {
+    const int64_t b = R.ptr[i], n = R.ptr[i + 1] - b;
+    std::vector<double> yhat(n), Q(K);
+    double* u = U + (size_t)i * K;
+    for (int d = 0; d < K; d++) Q[d] = p.Lambda[d + (size_t)d * K];
+    for (int64_t e = 0; e < n; e++) {
+      const double* v = V + (size_t)R.idx[b + e] * K;
+      double dot = 0.0;
+      for (int d = 0; d < K; d++) {
+        Q[d] += alpha * (v[d] * v[d]);
+        dot += u[d] * v[d];
+      }
+      yhat[e] = m.mean + dot;
+    }
+    for (int d = 0; d < K; d++) {
+      const double z = normal_draw(m.seed, (uint32_t)iter, stream_id(kRowNoise, (uint32_t)mode),
+                                   (uint32_t)i, (uint32_t)d);
+      const double uid = u[d];
+      double L = p.Lambda[d + (size_t)d * K] * (p.mu[d] + p.Uhat[(size_t)i * K + d]);
+      for (int64_t e = 0; e < n; e++) {
+        const double vjd = V[(size_t)R.idx[b + e] * K + d];
+        L += alpha * (R.val[b + e] - (yhat[e] - uid * vjd)) * vjd;
+      }
+      const double var = 1.0 / Q[d];
+      u[d] = L * var + std::sqrt(var) * z;
+      const double delta = u[d] - uid;
+      for (int64_t e = 0; e < n; e++) yhat[e] += delta * V[(size_t)R.idx[b + e] * K + d];
+    }
+  }
+  return 0;
+}
+
 int sample_mode(Model& m, int mode, int iter) {
   Prior& p = m.prior[mode];
+  if (p.one) return sample_mode_one(m, mode, iter);
   const int other = 1 - mode;
   const Csr& R = m.Y[mode];
   return orc_sample_latents(m.K, R.nrow, R.ncol, R.ptr, R.idx, R.val, m.mean,
@@ -573,8 +628,73 @@ int sample_beta(Model& m, Prior& p, const std::vector<double>& U, int mode, int 
   return 0;
 }
 
+// MacauOnePrior::update_prior (macauoneprior.cpp:189-290): sample_mu_lambda (Normal-Wishart
+// of U - Uhat with mu0 = 0, kappa = 2, W = I, nu = K; lambda = diag Lambda), sample_beta (each
+// link coefficient in turn, features in order within blocks of four dimensions, with the
+// residual Z = U - mu - F beta kept current), compute_uhat, sample_lambda_beta (one Gamma per
+// dimension, keyed (kLambdaBeta, d)).
+int update_prior_one(Model& m, int mode, int iter) {
+  Prior& p = m.prior[mode];
+  const int K = m.K;
+  const std::vector<double>& U = m.lat[mode];
+  const int N = m.dims[mode];
+  std::vector<double> Ud((size_t)K * N), WI((size_t)K * K, 0.0), mu0(K, 0.0);
+  for (size_t t = 0; t < Ud.size(); t++) Ud[t] = U[t] - p.Uhat[t];
+  for (int d = 0; d < K; d++) WI[d + (size_t)d * K] = 1.0;
+  int st = orc_cond_normal_wishart(K, N, Ud.data(), mu0.data(), 2.0, WI.data(), K, m.seed,
+                                   (uint32_t)iter, (uint32_t)mode, p.mu.data(), p.Lambda.data());
+  if (st) return st;
+  // sample_beta (macauoneprior.cpp:216-257)
+  const int nF = p.nfeat;
+  std::vector<double> Z((size_t)N * K);  // Z[i * K + d]
+  for (int i = 0; i < N; i++)
+    for (int d = 0; d < K; d++)
+      Z[(size_t)i * K + d] = U[(size_t)i * K + d] - p.mu[d] - p.Uhat[(size_t)i * K + d];
+  const Csr& Ft = p.Ft;  // row f: the entries of column f of F
+#pragma omp parallel for schedule(static, 1)
+  for (int d0 = 0; d0 < K; d0 += 4) {
+    const int dc = std::min(4, K - d0);
+    for (int f = 0; f < nF; f++) {
+      double zx[4] = {0.0, 0.0, 0.0, 0.0}, delta[4];
+      for (int64_t e = Ft.ptr[f]; e < Ft.ptr[f + 1]; e++) {
+        const double v = Ft.val ? Ft.val[e] : 1.0;
+        for (int d = 0; d < dc; d++) zx[d] += v * Z[(size_t)Ft.idx[e] * K + d0 + d];
+      }
+      for (int d = 0; d < dc; d++) {
+        const int dx = d0 + d;
+        const double lam = p.Lambda[dx + (size_t)dx * K];
+        const double z = normal_draw(m.seed, (uint32_t)iter, stream_id(kBetaOne, (uint32_t)mode),
+                                     (uint32_t)f, (uint32_t)dx);
+        double& bf = p.beta[(size_t)f * K + dx];
+        const double A = p.lb_one[dx] + lam * p.colsq[f];
+        const double B = lam * (zx[d] + bf * p.colsq[f]);
+        const double Ainv = 1.0 / A;
+        const double bnew = B * Ainv + std::sqrt(Ainv) * z;
+        delta[d] = bf - bnew;
+        bf = bnew;
+      }
+      for (int64_t e = Ft.ptr[f]; e < Ft.ptr[f + 1]; e++) {
+        const double v = Ft.val ? Ft.val[e] : 1.0;
+        for (int d = 0; d < dc; d++) Z[(size_t)Ft.idx[e] * K + d0 + d] += v * delta[d];
+      }
+    }
+  }
+  csr_mul_bn(p.F, p.beta.data(), K, p.Uhat.data());  // compute_uhat
+  // sample_lambda_beta (macauoneprior.cpp:267-290)
+  const double a = p.lb_a0 + nF / 2.0;
+  for (int d = 0; d < K; d++) {
+    double ss = 0.0;
+    for (int f = 0; f < nF; f++) ss += p.beta[(size_t)f * K + d] * p.beta[(size_t)f * K + d];
+    const double b = p.lb_b0 + ss / 2.0;
+    p.lb_one[d] = gamma_draw(m.seed, (uint32_t)iter, stream_id(kLambdaBeta, (uint32_t)mode),
+                             (uint32_t)d, a) * (1.0 / b);
+  }
+  return 0;
+}
+
 int update_prior(Model& m, int mode, int iter) {
   Prior& p = m.prior[mode];
+  if (p.one) return update_prior_one(m, mode, iter);
   const int K = m.K;
   const std::vector<double>& U = m.lat[mode];
   const int N = m.dims[mode];
@@ -696,6 +816,28 @@ void orc_model_set_side(void* h, int mode, int nfeat, const int64_t* fptr, const
   p.tol = tol;
 }
 
+// MacauOnePrior<SparseFeat | SparseDoubleFeat>(K, F) + setLambdaBeta (macauoneprior.cpp:16-39,
+// macau.pyx:194-214): mu = 0, Lambda = 10 I, beta = Uhat = 0, lambda_beta = lambda_beta for every
+// dimension, colsq = squared column norms of F (the column counts when F is binary).
+void orc_model_set_side_one(void* h, int mode, int nfeat, const int64_t* fptr,
+                            const int32_t* fidx, const double* fval, const int64_t* tptr,
+                            const int32_t* tidx, const double* tval, double lambda_beta) {
+  Model& m = *static_cast<Model*>(h);
+  Prior& p = m.prior[mode];
+  const int N = m.dims[mode];
+  p.macau = false;
+  p.one = true;
+  p.nfeat = nfeat;
+  p.F = Csr{fptr, fidx, fval, N, nfeat};
+  p.Ft = Csr{tptr, tidx, tval, nfeat, N};
+  p.Uhat.assign((size_t)m.K * N, 0.0);
+  p.beta.assign((size_t)m.K * nfeat, 0.0);
+  p.lb_one.assign(m.K, lambda_beta);
+  p.colsq.assign(nfeat, 0.0);
+  for (int f = 0; f < nfeat; f++)
+    for (int64_t e = tptr[f]; e < tptr[f + 1]; e++) p.colsq[f] += tval ? tval[e] * tval[e] : 1.0;
+}
+
 int orc_model_sample_mode(void* h, int mode, int iter) {
   return sample_mode(*static_cast<Model*>(h), mode, iter);
 }
@@ -741,7 +883,8 @@ int orc_model_update_noise(void* h, int iter) {
 
 // what: 0 latents (K x dim), 1 mu (K), 2 Lambda (K x K), 3 beta (K x nfeat), 4 Uhat (K x dim),
 //       5 [lambda_beta, cg_iters], 6 predictions, 7 predictions_var, 8 [rmse_avg, rmse_1samp],
-//       9 [alpha, alpha_max, var_total] (noise precision)
+//       9 [alpha, alpha_max, var_total] (noise precision), 10 lambda_beta per dimension (K,
+//       univariate prior)
 void orc_model_get(void* h, int what, int mode, double* out) {
   Model& m = *static_cast<Model*>(h);
   Prior& p = m.prior[mode];
@@ -756,6 +899,7 @@ void orc_model_get(void* h, int what, int mode, double* out) {
     case 7: std::copy(m.pred_var.begin(), m.pred_var.end(), out); break;
     case 8: out[0] = m.rmse; out[1] = m.rmse1; break;
     case 9: out[0] = m.alpha; out[1] = m.alpha_max; out[2] = m.var_total; break;
+    case 10: std::copy(p.lb_one.begin(), p.lb_one.end(), out); break;
     default: break;
   }
 }
@@ -772,6 +916,7 @@ void orc_model_set(void* h, int what, int mode, const double* in) {
     case 4: std::copy(in, in + p.Uhat.size(), p.Uhat.begin()); break;
     case 5: p.lambda_beta = in[0]; break;
     case 9: m.alpha = in[0]; break;
+    case 10: std::copy(in, in + p.lb_one.size(), p.lb_one.begin()); break;
     default: break;
   }
 }

@@ -15,7 +15,7 @@ _HERE = Path(__file__).resolve().parent
 LIB_PATH = _HERE / "_build" / "liboracle.so"
 
 PURPOSE = dict(row_noise=1, mvn_n=2, mvn_f=3, wishart_off=4, wishart_diag=5, mu_draw=6,
-               lambda_beta=7, noise_alpha=8)
+               lambda_beta=7, noise_alpha=8, beta_one=9)
 
 _d = C.c_double
 _i = C.c_int
@@ -59,6 +59,7 @@ def _load():
         "orc_model_sweep": (_i, [_p, _i, _i]),
         "orc_model_get": (None, [_p, _i, _i, _p]),
         "orc_model_set_noise_adaptive": (None, [_p, _d, _d]),
+        "orc_model_set_side_one": (None, [_p, _i, _i, _p, _p, _p, _p, _p, _p, _d]),
         "orc_model_update_noise": (_i, [_p, _i]),
         "orc_model_set": (None, [_p, _i, _i, _p]),
     }
@@ -258,6 +259,18 @@ class Model:
         lib().orc_model_set_side(self.h, mode, F.ncol, _ptr(F.ptr), _ptr(F.idx), _ptr(F.val),
                                  _ptr(Ft.ptr), _ptr(Ft.idx), _ptr(Ft.val), lambda_beta, tol)
 
+    def set_side_one(self, mode, F, Ft, lambda_beta):
+        """MacauOnePrior (univariate sampler) with side information F for `mode`
+        (macauoneprior.cpp:16-39; binary F when built with binary=True)."""
+        self._keep += [F, Ft]
+        self.nfeat[mode] = F.ncol
+        lib().orc_model_set_side_one(self.h, mode, F.ncol, _ptr(F.ptr), _ptr(F.idx), _ptr(F.val),
+                                     _ptr(Ft.ptr), _ptr(Ft.idx), _ptr(Ft.val), lambda_beta)
+
+    def lambda_beta_one(self, mode):
+        """lambda_beta per dimension of a univariate prior (K,)."""
+        return self._get(10, mode, (self.K,))
+
     def set_noise_adaptive(self, sn_init=1.0, sn_max=10.0):
         """AdaptiveGaussianNoise(sn_init, sn_max) + init (noisemodels.cpp:14-33); after set_train."""
         lib().orc_model_set_noise_adaptive(self.h, sn_init, sn_max)
@@ -317,5 +330,6 @@ class Model:
     def set(self, what, mode, arr):
         arr = f64(arr)
         self._keep.append(arr)
-        code = dict(latents=0, mu=1, Lambda=2, beta=3, uhat=4, lambda_beta=5, alpha=9)[what]
+        code = dict(latents=0, mu=1, Lambda=2, beta=3, uhat=4, lambda_beta=5, alpha=9,
+                    lambda_beta_one=10)[what]
         lib().orc_model_set(self.h, code, mode, _ptr(arr))

@@ -33,6 +33,7 @@ enum Purpose : uint32_t {
   kMuDraw = 6,        // NormalWishart: MvNormal_prec(kappa*Lambda, mu) (mvnormal.cpp:273)
   kLambdaBeta = 7,    // sample_lambda_beta: rgamma (latentprior.cpp:328-331)
   kNoiseAlpha = 8,    // AdaptiveGaussianNoise::update: rgamma(aN, 1/bN) (noisemodels.cpp:75-78)
+  kBetaOne = 9,       // MacauOnePrior::sample_beta: bmrandn_single per feature (macauoneprior.cpp:241)
 };
 
 inline void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {

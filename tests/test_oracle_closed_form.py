@@ -191,3 +191,121 @@ def test_adaptive_noise_model_learns_noise_level():
         alphas.append(m.noise()[0])
     a = np.mean(alphas[20:])
     assert 0.7 / sd**2 < a < 1.5 / sd**2 and a < m.noise()[1], a
+
+
+def _one_model(rng, nrow, ncol, K, nfeat, seed, lambda_beta=5.0, binary=False):
+    Y = rand_csr(rng, nrow, ncol, 0.3).tocsc()
+    Y.sort_indices()
+    F = sp.random(nrow, nfeat, density=0.5, random_state=rng, format="csr")
+    if binary:
+        F.data[:] = 1.0
+    m = orc.Model(K, 1.5, seed)
+    m.set_train(orc.Csr.from_scipy(Y), orc.Csr.from_scipy(Y.T), Y.sum() / Y.nnz)
+    m.set_side_one(0, orc.Csr.from_scipy(F, binary), orc.Csr.from_scipy(F.T, binary), lambda_beta)
+    return m, Y, F
+
+
+def test_univariate_row_sampler_targets_the_gaussian_posterior():
+    """MacauOnePrior::sample_latents (macauoneprior.cpp:41-95) is a coordinate-wise Gibbs sweep
+    on a row's Gaussian posterior: with the other factor and the hyperparameters held fixed,
+    its chain's mean and covariance approach P^-1 b and P^-1, P = diag(lambda) + alpha V'V."""
+    rng = np.random.default_rng(21)
+    K, nrow, ncol = 3, 4, 12
+    m, Y, _ = _one_model(rng, nrow, ncol, K, 2, seed=8)
+    V = rng.normal(size=(ncol, K))
+    m.set("latents", 1, V)
+    mu = np.array([0.2, -0.1, 0.3])
+    m.set("mu", 0, mu)
+    lam = np.array([2.0, 3.0, 1.5])
+    m.set("Lambda", 0, np.diag(lam))
+    mean = Y.sum() / Y.nnz
+    Yr = Y.tocsr()
+    draws = []
+    for it in range(20000):
+        m.sample_mode(0, it)
+        draws.append(m.latents(0)[1].copy())
+    draws = np.array(draws[200:])
+    cols = Yr.indices[Yr.indptr[1]:Yr.indptr[2]]
+    vals = Yr.data[Yr.indptr[1]:Yr.indptr[2]]
+    Vr = V[cols]
+    P = np.diag(lam) + 1.5 * Vr.T @ Vr
+    b = lam * mu + 1.5 * Vr.T @ (vals - mean)
+    want_mean = np.linalg.solve(P, b)
+    want_cov = np.linalg.inv(P)
+    sd = np.sqrt(np.diag(want_cov))
+    assert np.all(np.abs(draws.mean(0) - want_mean) < 0.05 * sd + 0.01), (draws.mean(0), want_mean)
+    np.testing.assert_allclose(np.cov(draws.T), want_cov, atol=0.08 * sd.max() ** 2)
+
+
+def test_univariate_update_prior_matches_restatement():
+    """MacauOnePrior::update_prior (macauoneprior.cpp:189-290) against a numpy restatement on a
+    small case: Normal-Wishart of U - Uhat, the feature-by-feature link sampler, Uhat = F beta,
+    and the per-dimension lambda_beta draws."""
+    rng = np.random.default_rng(4)
+    K, nrow, ncol, nfeat, seed, it = 6, 30, 20, 5, 77, 3
+    for binary in (False, True):
+        m, Y, F = _one_model(rng, nrow, ncol, K, nfeat, seed, lambda_beta=2.5, binary=binary)
+        U = rng.normal(size=(nrow, K))
+        m.set("latents", 0, U)
+        beta0 = rng.normal(scale=0.3, size=(nfeat, K))
+        m.set("beta", 0, beta0)
+        Uhat0 = F @ beta0
+        m.set("uhat", 0, Uhat0)
+        lb = np.full(K, 2.5)
+        assert m.update_prior(0, it) == 0
+        mu, Lam, st = orc.cond_normal_wishart(U - Uhat0, np.zeros(K), 2.0, np.eye(K), K, seed=seed,
+                                              sweep=it, mode=0)
+        assert st == 0
+        np.testing.assert_allclose(m.mu(0), mu, rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(m.Lambda(0), Lam, rtol=1e-12, atol=1e-14)
+        lam = np.diag(Lam)
+        Fc = F.tocsc()
+        colsq = np.asarray(Fc.multiply(Fc).sum(axis=0)).ravel()
+        beta = beta0.copy()
+        Z = U - mu - Uhat0
+        for d0 in range(0, K, 4):
+            ds = range(d0, min(K, d0 + 4))
+            for f in range(nfeat):
+                rows = Fc.indices[Fc.indptr[f]:Fc.indptr[f + 1]]
+                v = Fc.data[Fc.indptr[f]:Fc.indptr[f + 1]]
+                for d in ds:
+                    zx = np.dot(v, Z[rows, d])
+                    A = lb[d] + lam[d] * colsq[f]
+                    B = lam[d] * (zx + beta[f, d] * colsq[f])
+                    z = orc.normal(seed, it, "beta_one", 0, f, d)
+                    new = B / A + np.sqrt(1.0 / A) * z
+                    Z[rows, d] += v * (beta[f, d] - new)
+                    beta[f, d] = new
+        np.testing.assert_allclose(m.beta(0), beta, rtol=1e-10, atol=1e-12)
+        np.testing.assert_allclose(m.uhat(0), F @ beta, rtol=1e-10, atol=1e-12)
+        a = 0.1 + nfeat / 2.0
+        want = [orc.gamma(seed, it, "lambda_beta", 0, d, a) / (0.1 + np.sum(beta[:, d] ** 2) / 2)
+                for d in range(K)]
+        np.testing.assert_allclose(m.lambda_beta_one(0), want, rtol=1e-10)
+
+
+def test_univariate_model_learns_small_matrix():
+    """A univariate chain (MacauOnePrior on the rows, BPMF on the columns) learns a low-rank
+    matrix about as well as the BPMF chain, like test_macau_univariate (test_macau.py:64-73)."""
+    rng = np.random.default_rng(3)
+    nrow, ncol, K = 120, 80, 4
+    Ut = rng.normal(size=(nrow, 3))
+    Vt = rng.normal(size=(ncol, 3))
+    Yfull = Ut @ Vt.T + rng.normal(scale=0.3, size=(nrow, ncol))
+    mask = rng.random((nrow, ncol)) < 0.3
+    r, c = np.nonzero(mask)
+    test = rng.random(len(r)) < 0.1
+    Ytr = sp.coo_matrix((Yfull[r[~test], c[~test]], (r[~test], c[~test])), shape=(nrow, ncol))
+    Yte = sp.csc_matrix((Yfull[r[test], c[test]], (r[test], c[test])), shape=(nrow, ncol))
+    Yte.sort_indices()
+    te = Yte.tocoo()
+    F = sp.csr_matrix(np.hstack([Ut + rng.normal(scale=0.5, size=Ut.shape), np.ones((nrow, 1))]))
+    m = orc.Model(K, 1.0 / 0.09, 5)
+    m.set_train(orc.Csr.from_scipy(Ytr), orc.Csr.from_scipy(Ytr.T), Ytr.tocsc().sum() / Ytr.nnz)
+    m.set_test(te.row, te.col, te.data)
+    m.set_side_one(0, orc.Csr.from_scipy(F), orc.Csr.from_scipy(F.T), 5.0)
+    for it in range(80):
+        assert m.sweep(it, 40) == 0
+    rmse, _ = m.rmse()
+    assert rmse < 0.6, rmse
+    assert np.linalg.norm(m.beta(0)) > 0.1

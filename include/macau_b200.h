@@ -95,6 +95,20 @@ int mg_set_side(mg_ctx* ctx, int mode, const int32_t* rows, const int32_t* cols,
                 const double* vals, int64_t nnz, int nrows, int nfeat, double lambda_beta,
                 double tol);
 
+/* Univariate side-information prior for `mode`: replaces `make_one_prior` (macau.pyx:194-214,
+ * used by macau(univariate=True)) -> MacauOnePrior<SparseFeat | SparseDoubleFeat>(K, F) +
+ * setLambdaBeta (macauoneprior.cpp:16-39, macauoneprior.h:47).  F is nrows x nfeat COO; vals ==
+ * NULL means binary.  Each sweep then redraws the mode's latents one coordinate at a time
+ * (macauoneprior.cpp:41-95) and its prior with sample_mu_lambda / sample_beta / compute_uhat /
+ * sample_lambda_beta (macauoneprior.cpp:189-290).  mg_get_hyper reports the mean of the K
+ * lambda_beta values, like getLinkLambda (macauoneprior.h:46). */
+int mg_set_side_univariate(mg_ctx* ctx, int mode, const int32_t* rows, const int32_t* cols,
+                           const double* vals, int64_t nnz, int nrows, int nfeat,
+                           double lambda_beta);
+
+/* The K per-dimension lambda_beta values of a univariate prior (MacauOnePrior::lambda_beta). */
+int mg_get_lambda_beta_univariate(mg_ctx* ctx, int mode, double* out);
+
 /* Macau::setSamples (macau.h:36). */
 int mg_set_samples(mg_ctx* ctx, int burnin, int nsamples);
 

@@ -65,6 +65,8 @@ _SIGS = {
     "mg_update_prior": (_i, [_p, _i, _i]),
     "mg_eval": (_i, [_p, _i]),
     "mg_set_noise_adaptive": (_i, [_p, _d, _d]),
+    "mg_set_side_univariate": (_i, [_p, _i, _p, _p, _p, _i64, _i, _i, _d]),
+    "mg_get_lambda_beta_univariate": (_i, [_p, _i, _p]),
     "mg_update_noise": (_i, [_p, _i]),
     "mg_get_noise": (_i, [_p, _p]),
     "mg_get_latents": (_i, [_p, _i, _p]),
@@ -170,6 +172,21 @@ class Sampler:
         self._chk(lib().mg_set_side(self.h, mode, ptr(rows), ptr(cols), ptr(vals), len(rows),
                                     int(shape[0]), int(shape[1]), float(lambda_beta), float(tol)))
         self.nfeat[mode] = int(shape[1])
+
+    def set_side_univariate(self, mode, rows, cols, vals, shape, lambda_beta):
+        """MacauOnePrior (univariate sampler) with side information for `mode`."""
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = None if vals is None else np.ascontiguousarray(vals, np.float64)
+        self._chk(lib().mg_set_side_univariate(self.h, mode, ptr(rows), ptr(cols), ptr(vals),
+                                               len(rows), int(shape[0]), int(shape[1]),
+                                               float(lambda_beta)))
+        self.nfeat[mode] = int(shape[1])
+
+    def lambda_beta_univariate(self, mode):
+        out = np.zeros(self.K)
+        self._chk(lib().mg_get_lambda_beta_univariate(self.h, mode, ptr(out)))
+        return out
 
     def set_samples(self, burnin, nsamples):
         self._chk(lib().mg_set_samples(self.h, int(burnin), int(nsamples)))

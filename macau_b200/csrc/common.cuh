@@ -78,6 +78,8 @@ struct SampleParams {
   int mode;                    // 0 = rows of Y, 1 = columns
   unsigned long long seed;
   const double* znoise;        // optional injected N(0,1) draws (nrows x K), tests only
+  int one;                     // univariate prior (MacauOnePrior): coordinate-wise draws from
+                               // the row's Gram with the precisions on Lambda's diagonal
 };
 
 #ifdef __CUDACC__

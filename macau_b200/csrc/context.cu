@@ -198,6 +198,15 @@ struct Prior {
   double lb_mu0 = 1.0, lb_nu0 = 1e-3;
   BlockCg cg;
   int cg_iters = 0;
+  // univariate prior (MacauOnePrior, macauoneprior.h:8-51): squared column norms of F, the
+  // per-dimension lambda_beta, and the feature levels of its link sampler (features sorted by
+  // level, lvl_ptr[l] .. lvl_ptr[l + 1] the features of level l)
+  bool one = false;
+  DBuf<double> colsq, lb_one;
+  DBuf<int> lvl_ptr, lvl_feat;
+  int nlevels = 0;
+  double lb_a0 = 0.1, lb_b0 = 0.1;
+  bool side() const { return macau || one; }
 };
 
 }  // namespace
@@ -322,8 +331,11 @@ class Context {
     drop_graphs();
   }
 
+  // univariate = false: MacauPrior<SparseDoubleFeat> (block-CG link solve); true: MacauOnePrior
+  // (macauoneprior.cpp:16-39), whose link sampler visits the features level by level.
   void set_side(int mode, const int32_t* rows, const int32_t* cols, const double* vals,
-                long long nnz, int nrows, int nfeat, double lambda_beta, double tol) {
+                long long nnz, int nrows, int nfeat, double lambda_beta, double tol,
+                bool univariate = false) {
     if (mode < 0 || mode > 1) throw MgError(MG_ERR_ARG, "mode must be 0 or 1");
     if (!have_data_) throw MgError(MG_ERR_STATE, "set the training data before side info");
     if (nrows != dims_[mode])
@@ -337,7 +349,8 @@ class Context {
     HostCsr t = transpose(f, nrows, nfeat);
     bool binary = true;
     for (double v : f.val) binary = binary && (v == 1.0);
-    p.macau = true;
+    p.macau = !univariate;
+    p.one = univariate;
     p.nfeat = nfeat;
     p.fptr.upload(f.ptr.data(), f.ptr.size(), s_);
     p.fidx.upload(f.idx.data(), f.idx.size(), s_);
@@ -368,6 +381,32 @@ class Context {
     p.Ft.nnz = p.F.nnz;
     p.lambda_beta0 = lambda_beta;
     p.tol = tol;
+    if (univariate) {
+      // col_square_sum (linop.cpp:374-401) and the feature levels: level(f) = 1 + the highest
+      // level of an earlier feature sharing a row with f (0 when none)
+      std::vector<double> cs(nfeat, 0.0);
+      std::vector<int> level(nfeat, 0), last(nrows, -1);
+      int nl = 0;
+      for (int f = 0; f < nfeat; f++) {
+        int lv = 0;
+        for (long long e = t.ptr[f]; e < t.ptr[f + 1]; e++) {
+          cs[f] += binary ? 1.0 : t.val[e] * t.val[e];
+          lv = std::max(lv, last[t.idx[e]] + 1);
+        }
+        for (long long e = t.ptr[f]; e < t.ptr[f + 1]; e++) last[t.idx[e]] = lv;
+        level[f] = lv;
+        nl = std::max(nl, lv + 1);
+      }
+      std::vector<int> lptr(nl + 1, 0), order(nfeat);
+      for (int f = 0; f < nfeat; f++) lptr[level[f] + 1]++;
+      for (int l = 0; l < nl; l++) lptr[l + 1] += lptr[l];
+      std::vector<int> fill(lptr.begin(), lptr.end() - 1);
+      for (int f = 0; f < nfeat; f++) order[fill[level[f]]++] = f;
+      p.colsq.upload(cs.data(), cs.size(), s_);
+      p.lvl_ptr.upload(lptr.data(), lptr.size(), s_);
+      p.lvl_feat.upload(order.data(), order.size(), s_);
+      p.nlevels = nl;
+    }
     MG_CUDA(cudaStreamSynchronize(s_));
     drop_graphs();
     initialised_ = false;
@@ -414,6 +453,13 @@ class Context {
         p.bb_partials.alloc((size_t)stats_blocks(p.nfeat) * (K_ + K_ * K_));
         p.bb_final.alloc((size_t)(K_ + K_ * K_));
         p.cg.reserve(p.F.nrow, p.nfeat, 64, mixed_);
+      }
+      if (p.one) {  // MacauOnePrior::init (macauoneprior.cpp:16-39) + setLambdaBeta
+        p.beta.alloc_zero((size_t)p.nfeat * CP_, s_);
+        p.uhat.alloc_zero((size_t)dims_[m] * KP_, s_);
+        p.tmp.alloc_zero((size_t)dims_[m] * CP_, s_);
+        std::vector<double> lb(K_, p.lambda_beta0);
+        p.lb_one.upload(lb.data(), lb.size(), s_);
       }
     }
     const long long maxN = std::max(dims_[0], dims_[1]);
@@ -475,7 +521,8 @@ class Context {
     sp.other = mixed_ ? (const void*)lat16_[other].p : (const void*)lat64_[other].p;
     sp.Lambda = p.Lambda.p;
     sp.mu = p.mu.p;
-    sp.uhat = p.macau ? p.uhat.p : nullptr;
+    sp.uhat = p.side() ? p.uhat.p : nullptr;
+    sp.one = p.one ? 1 : 0;
     sp.out_f64 = lat64_[mode].p;
     sp.out_f32 = lat32_[mode].p;
     sp.out_bf16 = lat16_[mode].p;
@@ -510,9 +557,24 @@ class Context {
     launches_ += p.macau ? 0 : 3;  // Macau launches are counted by kernels_in_cg below
     const int nb = stats_blocks(N);
     const int rec = K_ + K_ * K_;
-    launch_stats(latents(mode), mixed_, p.macau ? p.uhat.p : nullptr, N, K_, KP_, KP_,
+    launch_stats(latents(mode), mixed_, p.side() ? p.uhat.p : nullptr, N, K_, KP_, KP_,
                  stat_partials_.p, nb, s_);
     launch_reduce_parts(stat_partials_.p, nb, rec, stat_final_.p, s_);
+    if (p.one) {
+      // MacauOnePrior::update_prior (macauoneprior.cpp:189-194): sample_mu_lambda (Normal-Wishart
+      // of U - Uhat with mu0 = 0, kappa = 2, W0 = I, nu = K, the BPMF defaults), sample_beta,
+      // compute_uhat, sample_lambda_beta
+      launch_normal_wishart(stat_final_.p, 1, N, K_, p.mu0.p, p.b0, p.WI.p, p.df, nullptr, 0,
+                            nullptr, nw_, ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
+      launch_beta_one(p.Ft, p.colsq.p, p.lvl_ptr.p, p.lvl_feat.p, p.nlevels, latents(mode),
+                      mixed_, KP_, p.mu.p, p.uhat.p, KP_, p.Lambda.p, p.lb_one.p, K_, N, p.beta.p,
+                      CP_, p.tmp.p, CP_, ctl_.p, cfg_.seed, mode, s_);
+      launch_spmm(p.F, p.beta.p, CP_, p.uhat.p, KP_, K_, false, s_);
+      launch_lambda_beta_one(p.beta.p, CP_, p.nfeat, K_, p.lb_a0, p.lb_b0, ctl_.p, cfg_.seed,
+                             mode, p.lb_one.p, s_);
+      launches_ += 3;  // beta, spmm, lambda_beta (after the 3 of stats / reduce / NW)
+      return;
+    }
     if (!p.macau) {  // BPMFPrior::update_prior (latentprior.cpp:79-81)
       launch_normal_wishart(stat_final_.p, 1, N, K_, p.mu0.p, p.b0, p.WI.p, p.df, nullptr, 0,
                             nullptr, nw_, ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
@@ -780,7 +842,7 @@ class Context {
     return std::sqrt(s);
   }
   std::string link_norm_str(int mode) {
-    if (!prior_[mode].macau) return "nan";
+    if (!prior_[mode].side()) return "nan";
     std::vector<double> b((size_t)prior_[mode].nfeat * K_);
     get_beta(mode, b.data());
     double s = 0.0;
@@ -834,10 +896,27 @@ class Context {
     if (mu) MG_CUDA(cudaMemcpyAsync(mu, p.mu.p, K_ * 8, cudaMemcpyDeviceToHost, s_));
     if (Lambda)
       MG_CUDA(cudaMemcpyAsync(Lambda, p.Lambda.p, (size_t)K_ * K_ * 8, cudaMemcpyDeviceToHost, s_));
+    std::vector<double> lbv;
     if (lb) {
-      if (p.macau) MG_CUDA(cudaMemcpyAsync(lb, p.lambda_beta.p, 8, cudaMemcpyDeviceToHost, s_));
-      else *lb = NAN;
+      if (p.macau) {
+        MG_CUDA(cudaMemcpyAsync(lb, p.lambda_beta.p, 8, cudaMemcpyDeviceToHost, s_));
+      } else if (p.one && p.lb_one.p) {
+        lbv.resize(K_);
+        MG_CUDA(cudaMemcpyAsync(lbv.data(), p.lb_one.p, K_ * 8, cudaMemcpyDeviceToHost, s_));
+      } else {
+        *lb = NAN;
+      }
     }
+    MG_CUDA(cudaStreamSynchronize(s_));
+    // a univariate prior reports the mean over dimensions, like getLinkLambda (macauoneprior.h:46)
+    if (!lbv.empty()) *lb = std::accumulate(lbv.begin(), lbv.end(), 0.0) / K_;
+  }
+  // lambda_beta of each dimension of a univariate prior (K values)
+  void get_lambda_beta_one(int mode, double* out) {
+    Prior& p = prior_[mode];
+    if (!p.one) throw MgError(MG_ERR_STATE, "mode has no univariate prior");
+    if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_init first");
+    MG_CUDA(cudaMemcpyAsync(out, p.lb_one.p, K_ * 8, cudaMemcpyDeviceToHost, s_));
     MG_CUDA(cudaStreamSynchronize(s_));
   }
   void set_hyper(int mode, const double* mu, const double* Lambda, const double* lb) {
@@ -846,18 +925,21 @@ class Context {
     if (Lambda)
       MG_CUDA(cudaMemcpyAsync(p.Lambda.p, Lambda, (size_t)K_ * K_ * 8, cudaMemcpyHostToDevice, s_));
     if (lb && p.macau) MG_CUDA(cudaMemcpyAsync(p.lambda_beta.p, lb, 8, cudaMemcpyHostToDevice, s_));
+    std::vector<double> lbv(lb && p.one ? K_ : 0, lb ? *lb : 0.0);  // setLambdaBeta: every dim
+    if (!lbv.empty() && p.lb_one.p)
+      MG_CUDA(cudaMemcpyAsync(p.lb_one.p, lbv.data(), K_ * 8, cudaMemcpyHostToDevice, s_));
     MG_CUDA(cudaStreamSynchronize(s_));
   }
   void get_beta(int mode, double* out) {
     Prior& p = prior_[mode];
-    if (!p.macau) throw MgError(MG_ERR_STATE, "mode has no side information");
+    if (!p.side()) throw MgError(MG_ERR_STATE, "mode has no side information");
     MG_CUDA(cudaMemcpy2DAsync(out, K_ * 8, p.beta.p, CP_ * 8, K_ * 8, p.nfeat,
                               cudaMemcpyDeviceToHost, s_));
     MG_CUDA(cudaStreamSynchronize(s_));
   }
   void get_uhat(int mode, double* out) {
     Prior& p = prior_[mode];
-    if (!p.macau) throw MgError(MG_ERR_STATE, "mode has no side information");
+    if (!p.side()) throw MgError(MG_ERR_STATE, "mode has no side information");
     MG_CUDA(cudaMemcpy2DAsync(out, K_ * 8, p.uhat.p, KP_ * 8, K_ * 8, dims_[mode],
                               cudaMemcpyDeviceToHost, s_));
     MG_CUDA(cudaStreamSynchronize(s_));
@@ -1129,6 +1211,20 @@ int mg_set_side(mg_ctx* ctx, int mode, const int32_t* rows, const int32_t* cols,
   return guarded(ctx, [&](mg::Context& c) {
     c.set_side(mode, rows, cols, vals, nnz, nrows, nfeat, lambda_beta, tol);
   });
+}
+
+int mg_set_side_univariate(mg_ctx* ctx, int mode, const int32_t* rows, const int32_t* cols,
+                           const double* vals, int64_t nnz, int nrows, int nfeat,
+                           double lambda_beta) {
+  if ((nnz > 0 && (!rows || !cols)) || nfeat < 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) {
+    c.set_side(mode, rows, cols, vals, nnz, nrows, nfeat, lambda_beta, 1e-6, true);
+  });
+}
+
+int mg_get_lambda_beta_univariate(mg_ctx* ctx, int mode, double* out) {
+  if (mode < 0 || mode > 1 || !out) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.get_lambda_beta_one(mode, out); });
 }
 
 int mg_set_samples(mg_ctx* ctx, int burnin, int nsamples) {

@@ -747,6 +747,35 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
   }
 }
 
+// k_finish_one_tc: the univariate prior's finish (one_gs_warp) from the Gram records, one warp
+// per row (rows warp, warp + total warps, ...); lane d reads row d of the record.
+__global__ void __launch_bounds__(256)
+    k_finish_one_tc(const SampleParams p, const float* __restrict__ gram) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t sweep = p.ctl->sweep;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < p.nrows;
+       row += warps) {
+    const float* gp = gram + (size_t)row * kGramRec;
+    float g[32];
+#pragma unroll
+    for (int j = 0; j < 32; j += 4) {
+      const float4 v = __ldcg(reinterpret_cast<const float4*>(gp + lane * 32 + j));
+      g[j] = v.x;
+      g[j + 1] = v.y;
+      g[j + 2] = v.z;
+      g[j + 3] = v.w;
+    }
+    const double c = (double)__ldcg(gp + 32 * 32 + lane);
+    const double u0 = lane < p.K ? (double)p.out_f32[(size_t)row * 32 + lane] : 0.0;
+    const double un = one_gs_warp<32, float>(g, c, u0, p, row, sweep, lane);
+    if (lane < p.K) {
+      p.out_f32[(size_t)row * 32 + lane] = (float)un;
+      p.out_bf16[(size_t)row * 32 + lane] = __float2bfloat16_rn((float)un);
+    }
+  }
+}
+
 }  // namespace
 
 size_t tc_smem_bytes() { return (size_t)kStages * kStageBytes + sizeof(TcShared); }
@@ -773,7 +802,10 @@ bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows
     k_sum_parts<<<(nsplit + 7) / 8, 256, 0, s>>>(p.scratch, split_rows, nsplit, gram);
     MG_CUDA(cudaGetLastError());
   }
-  k_finish_tc<<<num_sms * 2, kFinWarps * 32, fsmem, s>>>(p, gram);
+  if (p.one)
+    k_finish_one_tc<<<num_sms * 8, 256, 0, s>>>(p, gram);
+  else
+    k_finish_tc<<<num_sms * 2, kFinWarps * 32, fsmem, s>>>(p, gram);
   MG_CUDA(cudaGetLastError());
   return true;
 }

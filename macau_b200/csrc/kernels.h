@@ -23,7 +23,7 @@ void launch_pad(const long long* ptr, const long long* pptr, long long nrows, co
 // ---- latent sampler (sample_kernels.cu, gram_tc.cu) ----
 void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, int num_sms);
 // Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only):
-// k_gram_tc, then (if nsplit > 0) k_sum_parts, then k_finish_tc.  It reads the 16-entry padded
+// k_gram_tc, then (if nsplit > 0) k_sum_parts, then k_finish_tc (k_finish_one_tc when p.one).  It reads the 16-entry padded
 // packed CSR and its task list (p.packed / p.tasks, built by the context) and gathers the other
 // factor's BF16 rows from p.other, whose row nother is all zeros (the padding sentinel).
 // `gram` holds nrows Gram records of 32 * 32 + 32 floats; split_rows lists the nsplit rows
@@ -87,6 +87,19 @@ struct DevCsr {
 // out[r, :ncomp] = sum_{e in row r} val_e * src[idx_e, :]   (csr_A_mul_Bn / A_mul_Bx<N>)
 void launch_spmm(const DevCsr& A, const void* src, int src_stride, void* dst, int dst_stride,
                  int ncomp, bool f32, cudaStream_t s);
+
+// Univariate prior (univariate_kernels.cu): MacauOnePrior::sample_beta over Ft (the columns of
+// F as CSR rows) with the feature levels lvl_ptr / lvl_feat, Z (N x zstride doubles) as
+// workspace; and sample_lambda_beta into lambda_beta[0 .. K).
+void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
+                     const int* lvl_feat, int nlevels, const void* U, bool f32, int ustride,
+                     const double* mu, const double* uhat, int hstride, const double* Lambda,
+                     const double* lambda_beta, int K, long long N, double* beta, int bstride,
+                     double* Z, int zstride, const Ctl* ctl, unsigned long long seed, int mode,
+                     cudaStream_t s);
+void launch_lambda_beta_one(const double* beta, int bstride, long long nfeat, int K, double a0,
+                            double b0, const Ctl* ctl, unsigned long long seed, int mode,
+                            double* lambda_beta, cudaStream_t s);
 
 // sample_beta pieces (latentprior.cpp:273-293)
 //   tmp[n] = U[n] + chol(Lambda)^{-T} z_n - mu      (n < N; z keyed (kMvnN, n))

@@ -296,6 +296,27 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
       __syncwarp();
       const int lane = t;
       const Acc rac = wshfl(racc, lane < KP ? lane : 0);  // rhs accumulator of component lane
+      if (p.one) {  // univariate prior: coordinate draws from the Gram (warp_finish.cuh)
+        Acc gr[KP];
+#pragma unroll
+        for (int j = 0; j < KP; j++) gr[j] = Gs[lane * LD + j];
+        double u0 = 0.0;
+        if (lane < K) {
+          if constexpr (MIXED) u0 = (double)p.out_f32[(size_t)row * KP + lane];
+          else u0 = p.out_f64[(size_t)row * KP + lane];
+        }
+        const double un = one_gs_warp<KP, Acc>(gr, (double)rac, u0, p, row, sweep, lane);
+        if (lane < K) {
+          if constexpr (MIXED) {
+            p.out_f32[(size_t)row * KP + lane] = (float)un;
+            p.out_bf16[(size_t)row * KP + lane] = __float2bfloat16_rn((float)un);
+          } else {
+            p.out_f64[(size_t)row * KP + lane] = un;
+          }
+        }
+        __syncwarp();
+        continue;
+      }
       double lm;
       if (p.uhat) {  // Macau prior mean mu + Uhat[row]
         const double mun = lane < K ? p.mu[lane] + p.uhat[(size_t)row * KP + lane] : 0.0;
@@ -335,6 +356,58 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
         }
       }
       __syncwarp();
+      continue;
+    }
+    if (p.one) {
+      // univariate prior, K > 32: the coordinate draws of one_gs_warp by the group; thread d
+      // owns coordinate d, G (full, FP64) in shared memory, the deltas broadcast through diag[]
+      double* M = reinterpret_cast<double*>(base);
+#pragma unroll
+      for (int i = 0; i < TR; i++)
+#pragma unroll
+        for (int j = 0; j < TC; j++) {
+          const int gi = rt * TR + i, gj = ct * TC + j;
+          if (gi < K && gj < K) M[gi * LD + gj] = (double)acc[i][j];
+        }
+      double u = 0.0;
+      if (t < K) {
+        if constexpr (MIXED) u = (double)p.out_f32[(size_t)row * KP + t];
+        else u = p.out_f64[(size_t)row * KP + t];
+        mun[t] = u;
+      }
+      gsync<T>(g);
+      const double alpha = noise_alpha(p);
+      double tt = 0.0, lam = 1.0, m = 0.0, z = 0.0;
+      const double c = (double)racc;
+      if (t < K) {
+        for (int j = 0; j < K; j++) tt = fma(M[t * LD + j], mun[j], tt);
+        lam = p.Lambda[t + t * K];
+        m = lam * (p.mu[t] + (p.uhat ? p.uhat[(size_t)row * KP + t] : 0.0));
+        z = p.znoise ? p.znoise[(size_t)row * K + t]
+                     : normal_draw(p.seed, sweep, stream_id(kRowNoise, (uint32_t)p.mode),
+                                   (uint32_t)row, (uint32_t)t);
+      }
+      for (int d = 0; d < K; d++) {
+        if (t == d) {
+          const double gdd = M[d * LD + d];
+          const double L = m + c - alpha * (tt - gdd * u);
+          const double var = 1.0 / (lam + alpha * gdd);
+          const double un = L * var + sqrt(var) * z;
+          diag[d] = un - u;
+          u = un;
+        }
+        gsync<T>(g);
+        if (t < K) tt = fma(M[t * LD + d], diag[d], tt);
+      }
+      if (t < K) {
+        if constexpr (MIXED) {
+          p.out_f32[(size_t)row * KP + t] = (float)u;
+          p.out_bf16[(size_t)row * KP + t] = __float2bfloat16_rn((float)u);
+        } else {
+          p.out_f64[(size_t)row * KP + t] = u;
+        }
+      }
+      gsync<T>(g);
       continue;
     }
     if (t < K) mun[t] = p.mu[t] + (p.uhat ? p.uhat[(size_t)row * KP + t] : 0.0);

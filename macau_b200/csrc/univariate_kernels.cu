@@ -1,0 +1,194 @@
+// Prior update of the univariate sampler (MacauOnePrior, macauoneprior.cpp:189-290): the link
+// matrix, one coefficient at a time, and the per-dimension lambda_beta.  The Normal-Wishart part
+// (sample_mu_lambda) and compute_uhat reuse the BPMF statistics kernels and the SpMM.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "rng.cuh"
+
+namespace mg {
+namespace {
+
+constexpr int kBetaThreads = 512;
+constexpr int kBetaWarps = kBetaThreads / 32;
+
+// One link coefficient per lane d < dc (dimension d0 + d) of feature f, sample_beta's update
+// (macauoneprior.cpp:243-252):
+//   A = lambda_beta_d + lambda_d colsq_f,   B = lambda_d (zx_d + beta_df colsq_f),
+//   beta_df <- B / A + z / sqrt(A),   delta_d = beta_df old - beta_df new.
+// zx, lam, lb are this lane's components; returns delta (0 for lanes >= dc).
+__device__ __forceinline__ double beta_coef(int lane, int dc, int d0, int f, double zx,
+                                            double lam, double lb, double cs, double* beta,
+                                            int bstride, unsigned long long seed, uint32_t sweep,
+                                            uint32_t st) {
+  if (lane >= dc) return 0.0;
+  const int dx = d0 + lane;
+  double* bp = beta + (size_t)f * bstride + dx;
+  const double b = *bp;
+  const double A = lb + lam * cs;
+  const double B = lam * (zx + b * cs);
+  const double Ainv = 1.0 / A;
+  const double bn = B * Ainv + sqrt(Ainv) * normal_draw(seed, sweep, st, (uint32_t)f, (uint32_t)dx);
+  *bp = bn;
+  return b - bn;
+}
+
+// sample_beta (macauoneprior.cpp:216-257) for the dimensions d0 .. d0 + 3 of block blockIdx.x.
+// Z = U - mu - Uhat (N x zstride, this block's four columns) is formed first; then the features
+// are visited level by level.  lvl_feat lists the features sorted by (level, index), where a
+// feature's level is one more than the highest level of an earlier feature sharing a row with
+// it, so the features of one level touch disjoint rows of Z and their updates commute: the
+// result equals the reference's feature-by-feature order.  A level with many features gives
+// one feature to each warp; a level with few gives each feature to the whole block.
+template <typename T>
+__global__ void __launch_bounds__(kBetaThreads)
+    k_beta_one(const long long* __restrict__ tptr, const int* __restrict__ tidx,
+               const double* __restrict__ tval, const double* __restrict__ colsq,
+               const int* __restrict__ lvl_ptr, const int* __restrict__ lvl_feat, int nlevels,
+               const T* __restrict__ U, int ustride, const double* __restrict__ mu,
+               const double* __restrict__ uhat, int hstride, const double* __restrict__ Lambda,
+               const double* __restrict__ lambda_beta, int K, long long N,
+               double* __restrict__ beta, int bstride, double* __restrict__ Z, int zstride,
+               const Ctl* ctl, unsigned long long seed, int mode) {
+  __shared__ double red[kBetaWarps][4];
+  __shared__ double dl[4];
+  const int d0 = blockIdx.x * 4, dc = min(4, K - d0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t sweep = ctl->sweep;
+  const uint32_t st = stream_id(kBetaOne, (uint32_t)mode);
+  // this lane's dimension d0 + lane (lanes 0 .. dc - 1 update the coefficients)
+  const double lam = lane < dc ? Lambda[(size_t)(d0 + lane) * (K + 1)] : 0.0;
+  const double lb = lane < dc ? lambda_beta[d0 + lane] : 1.0;
+  for (long long i = threadIdx.x; i < N; i += kBetaThreads)
+    for (int d = 0; d < dc; d++)
+      Z[i * zstride + d0 + d] =
+          (double)U[i * ustride + d0 + d] - mu[d0 + d] - uhat[i * hstride + d0 + d];
+  __syncthreads();
+  for (int L = 0; L < nlevels; L++) {
+    const int f0 = lvl_ptr[L], f1 = lvl_ptr[L + 1];
+    if (2 * (f1 - f0) >= kBetaWarps) {
+      for (int q = f0 + warp; q < f1; q += kBetaWarps) {
+        const int f = lvl_feat[q];
+        double zx[4] = {0.0, 0.0, 0.0, 0.0};
+        for (long long e = tptr[f] + lane; e < tptr[f + 1]; e += 32) {
+          const double v = tval ? tval[e] : 1.0;
+          const double* zr = Z + (size_t)tidx[e] * zstride + d0;
+#pragma unroll
+          for (int d = 0; d < 4; d++)
+            if (d < dc) zx[d] = fma(v, zr[d], zx[d]);
+        }
+#pragma unroll
+        for (int d = 0; d < 4; d++)
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) zx[d] += __shfl_xor_sync(0xffffffffu, zx[d], o);
+        double mine = 0.0;
+#pragma unroll
+        for (int d = 0; d < 4; d++)
+          if (lane == d) mine = zx[d];
+        const double my =
+            beta_coef(lane, dc, d0, f, mine, lam, lb, colsq[f], beta, bstride, seed, sweep, st);
+        double delta[4];
+#pragma unroll
+        for (int d = 0; d < 4; d++) delta[d] = __shfl_sync(0xffffffffu, my, d);
+        for (long long e = tptr[f] + lane; e < tptr[f + 1]; e += 32) {
+          const double v = tval ? tval[e] : 1.0;
+          double* zr = Z + (size_t)tidx[e] * zstride + d0;
+#pragma unroll
+          for (int d = 0; d < 4; d++)
+            if (d < dc) zr[d] = fma(v, delta[d], zr[d]);
+        }
+      }
+    } else {
+      for (int q = f0; q < f1; q++) {
+        const int f = lvl_feat[q];
+        double zx[4] = {0.0, 0.0, 0.0, 0.0};
+        for (long long e = tptr[f] + threadIdx.x; e < tptr[f + 1]; e += kBetaThreads) {
+          const double v = tval ? tval[e] : 1.0;
+          const double* zr = Z + (size_t)tidx[e] * zstride + d0;
+#pragma unroll
+          for (int d = 0; d < 4; d++)
+            if (d < dc) zx[d] = fma(v, zr[d], zx[d]);
+        }
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) zx[d] += __shfl_xor_sync(0xffffffffu, zx[d], o);
+          if (lane == 0) red[warp][d] = zx[d];
+        }
+        __syncthreads();
+        if (warp == 0) {
+          double s = 0.0;
+          if (lane < dc)
+            for (int w = 0; w < kBetaWarps; w++) s += red[w][lane];
+          const double my =
+              beta_coef(lane, dc, d0, f, s, lam, lb, colsq[f], beta, bstride, seed, sweep, st);
+          if (lane < 4) dl[lane] = my;
+        }
+        __syncthreads();
+        const double delta[4] = {dl[0], dl[1], dl[2], dl[3]};
+        for (long long e = tptr[f] + threadIdx.x; e < tptr[f + 1]; e += kBetaThreads) {
+          const double v = tval ? tval[e] : 1.0;
+          double* zr = Z + (size_t)tidx[e] * zstride + d0;
+#pragma unroll
+          for (int d = 0; d < 4; d++)
+            if (d < dc) zr[d] = fma(v, delta[d], zr[d]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// sample_lambda_beta (macauoneprior.cpp:267-290): lambda_beta_d ~ Gamma(a0 + nfeat / 2,
+// 1 / (b0 + sum_f beta_df^2 / 2)), one warp per dimension, keyed (kLambdaBeta, d).
+__global__ void k_lambda_beta_one(const double* __restrict__ beta, int bstride, long long nfeat,
+                                  int K, double a0, double b0, const Ctl* ctl,
+                                  unsigned long long seed, int mode,
+                                  double* __restrict__ lambda_beta) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double a = a0 + (double)nfeat / 2.0;
+  for (int d = warp; d < K; d += blockDim.x >> 5) {
+    double s = 0.0;
+    for (long long f = lane; f < nfeat; f += 32) {
+      const double b = beta[f * bstride + d];
+      s = fma(b, b, s);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0)
+      lambda_beta[d] = gamma_draw(seed, ctl->sweep, stream_id(kLambdaBeta, (uint32_t)mode),
+                                  (uint32_t)d, a) *
+                       (1.0 / (b0 + s / 2.0));
+  }
+}
+
+}  // namespace
+
+void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
+                     const int* lvl_feat, int nlevels, const void* U, bool f32, int ustride,
+                     const double* mu, const double* uhat, int hstride, const double* Lambda,
+                     const double* lambda_beta, int K, long long N, double* beta, int bstride,
+                     double* Z, int zstride, const Ctl* ctl, unsigned long long seed, int mode,
+                     cudaStream_t s) {
+  const int blocks = (K + 3) / 4;
+  if (f32)
+    k_beta_one<float><<<blocks, kBetaThreads, 0, s>>>(
+        Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const float*)U, ustride, mu,
+        uhat, hstride, Lambda, lambda_beta, K, N, beta, bstride, Z, zstride, ctl, seed, mode);
+  else
+    k_beta_one<double><<<blocks, kBetaThreads, 0, s>>>(
+        Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const double*)U, ustride, mu,
+        uhat, hstride, Lambda, lambda_beta, K, N, beta, bstride, Z, zstride, ctl, seed, mode);
+  MG_CUDA(cudaGetLastError());
+}
+
+void launch_lambda_beta_one(const double* beta, int bstride, long long nfeat, int K, double a0,
+                            double b0, const Ctl* ctl, unsigned long long seed, int mode,
+                            double* lambda_beta, cudaStream_t s) {
+  k_lambda_beta_one<<<1, 256, 0, s>>>(beta, bstride, nfeat, K, a0, b0, ctl, seed, mode,
+                                      lambda_beta);
+  MG_CUDA(cudaGetLastError());
+}
+
+}  // namespace mg

@@ -99,6 +99,47 @@ __device__ __forceinline__ double row_noise(const SampleParams& p, int row, int 
   return lane < K ? ((lane & 1) ? z1 : z0) : 0.0;
 }
 
+// Univariate finish of one row by a warp (MacauOnePrior::sample_latents,
+// macauoneprior.cpp:41-95).  Lane d holds row d of the row's Gram G = sum_e v_e v_e^T (g), the
+// rhs component c_d = sum_e w_e v_ed with w_e = alpha (y_e - mean), and the row's current value
+// u_d (0 beyond K).  The coordinates are redrawn in order d = 0 .. K-1 with t = G u kept current:
+//   L_d = lambda_d (mu_d + Uhat_d) + c_d - alpha (t_d - G_dd u_d),   Q_d = lambda_d + alpha G_dd,
+//   u_d <- L_d / Q_d + z_d / sqrt(Q_d),   t += G[:, d] (u_d new - u_d old),
+// lambda = diag(Lambda).  This is the reference's residual form with yhat_e = mean + v_e . u
+// expanded through G: the same L_d and Q_d in exact arithmetic, O(K^2) per row after the Gram.
+// Returns the new u for the lane.
+template <int KP, typename GT>
+__device__ __forceinline__ double one_gs_warp(const GT (&g)[KP], double c, double u,
+                                              const SampleParams& p, int row, uint32_t sweep,
+                                              int lane) {
+  const int K = p.K;
+  const double alpha = noise_alpha(p);
+  const bool on = lane < K;
+  const double lam = on ? p.Lambda[lane + lane * K] : 1.0;
+  const double m =
+      on ? lam * (p.mu[lane] + (p.uhat ? p.uhat[(size_t)row * KP + lane] : 0.0)) : 0.0;
+  const double z = row_noise(p, row, K, lane, sweep);
+  double t = 0.0;
+#pragma unroll
+  for (int j = 0; j < KP; j++) t = fma((double)g[j], __shfl_sync(0xffffffffu, u, j), t);
+#pragma unroll
+  for (int d = 0; d < KP; d++) {
+    if (d >= K) break;
+    double delta = 0.0;
+    if (lane == d) {
+      const double gdd = (double)g[d];
+      const double L = m + c - alpha * (t - gdd * u);
+      const double var = 1.0 / (lam + alpha * gdd);
+      const double un = L * var + sqrt(var) * z;
+      delta = un - u;
+      u = un;
+    }
+    delta = __shfl_sync(0xffffffffu, delta, d);
+    t = fma((double)g[d], delta, t);
+  }
+  return u;
+}
+
 template <typename F, int KP>
 __device__ __forceinline__ F warp_solve(const F (&a)[KP], F rinv, F rr, int lane, const F* Lc,
                                         int ld, double z) {

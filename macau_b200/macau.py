@@ -9,8 +9,9 @@ Supported by the GPU sampler (the hot path): a 2-mode sparse matrix or 2-index-c
 DataFrame, fixed Gaussian noise (numeric ``precision``) or adaptive Gaussian noise
 (``precision="adaptive"``), BPMF priors and Macau priors with sparse or dense side information
 (block-CG; the reference switches to a direct FtF Cholesky solve when a side matrix has at most
-10000 columns, macau.pyx:160, which solves the same system).  Tensors, ``precision="probit"``
-and ``univariate=True`` raise ValueError.
+10000 columns, macau.pyx:160, which solves the same system), and with ``univariate=True`` the
+univariate MacauOnePrior for sparse side information (macau.pyx:194-214).  Tensors and
+``precision="probit"`` raise ValueError.
 
 Two keyword arguments are added: ``seed`` (key of all random draws; the reference is
 unseeded) and ``compute`` ("fp64" or "mixed"; default from the MACAU_GPU_PRECISION environment
@@ -225,7 +226,7 @@ def macau(Y,
                    "adaptive" - automatically learn precision (also "sample")
       burnin       number of Gibbs samples to drop (burn-in)
       nsamples     number of Gibbs samples to collect
-      univariate   must be False (the univariate sampler is not on the GPU path)
+      univariate   whether to use univariate sampler (faster than standard sampler)
       tol          error tolerance for conjugate gradient solver
       sn_max       maximum signal-to-noise ratio for observation precision
                    only used if precision="adaptive"
@@ -254,10 +255,14 @@ def macau(Y,
             raise ValueError("precision='probit' is not supported by the GPU sampler (Gaussian noise only).")
         else:
             raise ValueError("Parameter 'precision' has to be either a number or \"adaptive\" for adaptive precision, or \"probit\" for binary matrices.")
-    if univariate:
-        raise ValueError("The univariate sampler is not supported by the GPU sampler.")
     if save_prefix is not None and type(save_prefix) != str:
         raise ValueError("Parameter 'save_prefix' has to be a string (str) or None.")
+    if univariate:  # make_one_prior accepts sparse matrices only (macau.pyx:194-198)
+        for sd in side:
+            if sd is None or (isinstance(sd, tuple) and sd == ()):
+                continue
+            if not _is_matrix(sd):
+                raise ValueError("Unsupported side information type: '%s'" % type(sd).__name__)
 
     if seed is None:
         seed = int.from_bytes(os.urandom(8), "little")
@@ -273,11 +278,16 @@ def macau(Y,
         for mode, sd in enumerate(side):
             if sd is None:
                 continue
+            if univariate and isinstance(sd, tuple) and sd == ():  # make_one_prior: () = none
+                continue
             r, c, v, shp = _side_coo(sd, data.shape[mode])
             if shp[0] != data.shape[mode]:
                 raise ValueError("Side information for mode %d has %d rows, expected %d." %
                                  (mode, shp[0], data.shape[mode]))
-            s.set_side(mode, r, c, v, shp, lambda_beta, tol)
+            if univariate:  # MacauOnePrior<SparseFeat | SparseDoubleFeat> (macau.pyx:194-214)
+                s.set_side_univariate(mode, r, c, v, shp, lambda_beta)
+            else:
+                s.set_side(mode, r, c, v, shp, lambda_beta, tol)
         s.set_samples(int(burnin), int(nsamples))
         s.init()
         if verbose:

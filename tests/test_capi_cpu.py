@@ -58,8 +58,8 @@ def test_python_api_validation_errors():
         macau_b200.macau(Y, verbose=False, side="x")
     with pytest.raises(ValueError):
         macau_b200.macau(Y, verbose=False, precision="probit")
-    with pytest.raises(ValueError):
-        macau_b200.macau(Y, verbose=False, univariate=True)
+    with pytest.raises(ValueError):  # make_one_prior takes sparse side information only
+        macau_b200.macau(Y, verbose=False, univariate=True, side=[np.zeros((10, 2)), None])
     with pytest.raises(TypeError):
         macau_b200.macau(np.zeros((3, 3)), verbose=False)
     with pytest.raises(ValueError):

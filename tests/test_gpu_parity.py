@@ -418,6 +418,123 @@ def test_row_sampler_uses_device_precision(compute, tensor_cores, K, mode):
     assert relerr(s.latents(mode), want) < tol
 
 
+# ---- univariate prior (MacauOnePrior, macauoneprior.cpp:41-95, 189-290) ----
+
+def side_matrix(rng, nrows, kind):
+    """'sparse': many features of a few rows each (the link sampler gives one feature per warp);
+    'dense': a few features sharing most rows (one feature at a time per block); 'binary'."""
+    if kind == "dense":
+        F = sp.random(nrows, 6, density=0.6, random_state=rng, format="csr")
+    else:
+        F = sp.random(nrows, 300, density=0.01, random_state=rng, format="csr")
+    if kind == "binary":
+        F.data[:] = 1.0
+    else:
+        F.data = rng.normal(size=F.nnz)
+    return F
+
+
+def univariate_pair(w, K, seed, mode, F, compute=_lib.MG_COMPUTE_FP64, lambda_beta=3.0,
+                    burnin=0, nsamples=1):
+    binary = bool(np.all(F.data == 1.0))
+    s = gpu_sampler(w, K, 1.5, seed, compute=compute, burnin=burnin, nsamples=nsamples,
+                    init=False)
+    Fc = F.tocoo()
+    s.set_side_univariate(mode, Fc.row, Fc.col, None if binary else Fc.data, F.shape, lambda_beta)
+    s.init()
+    m = oracle_model(w, K, 1.5, seed)
+    m.set_side_one(mode, orc.Csr.from_scipy(F, binary), orc.Csr.from_scipy(F.T, binary),
+                   lambda_beta)
+    return s, m
+
+
+@pytest.mark.parametrize("K", [10, 32, 64])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_univariate_row_sampler_fp64_matches_oracle(K, mode):
+    # coordinate draws from the Gram (warp finish at K <= 32, group finish at K = 64) against the
+    # oracle's residual form, from random current values and hyperparameters, keyed draws
+    rng = np.random.default_rng(K + 3 * mode)
+    w = heavy_rows_workload(rng, nrow=70)
+    F = side_matrix(rng, w["shape"][mode], "sparse")
+    s, m = univariate_pair(w, K, 321, mode, F)
+    for it in (0, 4):
+        Ut = rng.normal(scale=0.3, size=(w["shape"][mode], K))
+        Vo = rng.normal(scale=0.3, size=(w["shape"][1 - mode], K))
+        mu = rng.normal(scale=0.2, size=K)
+        Lam = random_spd(rng, K, 3.0)
+        s.set_latents(mode, Ut)
+        s.set_latents(1 - mode, Vo)
+        m.set("latents", mode, Ut)
+        m.set("latents", 1 - mode, Vo)
+        s.set_hyper(mode, mu, Lam, None)
+        m.set("mu", mode, mu)
+        m.set("Lambda", mode, Lam)
+        s.sample_latents(mode, it)
+        assert m.sample_mode(mode, it) == 0
+        assert relerr(s.latents(mode), m.latents(mode)) < FP64_TOL, it
+
+
+@pytest.mark.parametrize("kind", ["sparse", "dense", "binary"])
+def test_univariate_update_prior_fp64_matches_oracle(kind):
+    rng = np.random.default_rng(len(kind))
+    K, mode = 12, 0
+    w = small_uniform(seed=2, nrow=400, ncol=250, nobs=9000)
+    F = side_matrix(rng, w["shape"][mode], kind)
+    s, m = univariate_pair(w, K, 55, mode, F)
+    for it in (0, 1, 2):
+        U = rng.normal(scale=0.5, size=(w["shape"][mode], K))
+        s.set_latents(mode, U)
+        m.set("latents", mode, U)
+        s.update_prior(mode, it)
+        assert m.update_prior(mode, it) == 0
+        mu, Lam, lb_mean = s.hyper(mode)
+        assert relerr(mu, m.mu(mode)) < FP64_TOL
+        assert relerr(Lam, m.Lambda(mode)) < FP64_TOL
+        assert relerr(s.beta(mode), m.beta(mode)) < FP64_TOL, it
+        assert relerr(s.uhat(mode), m.uhat(mode)) < FP64_TOL
+        lb = s.lambda_beta_univariate(mode)
+        assert relerr(lb, m.lambda_beta_one(mode)) < FP64_TOL
+        assert abs(lb_mean - lb.mean()) <= 1e-12 * lb.mean()
+
+
+def test_univariate_sweeps_fp64_match_oracle():
+    # whole sweeps: univariate prior on the rows (dense side), BPMF on the columns, evaluation
+    rng = np.random.default_rng(77)
+    w = workloads.bpmf_uniform(nrow=400, ncol=300, nobs=12000, seed=9)
+    K, seed, burnin = 8, 2026, 4
+    F = side_matrix(rng, w["shape"][0], "dense")
+    s, m = univariate_pair(w, K, seed, 0, F, burnin=burnin, nsamples=6)
+    for it in range(10):
+        s.sweep(it, eval=True)
+        assert m.sweep(it, burnin) == 0
+        for mode in (0, 1):
+            assert relerr(s.latents(mode), m.latents(mode)) < 1e-8, (it, mode)
+        assert relerr(s.beta(0), m.beta(0)) < 1e-8
+        r, r1 = s.rmse()
+        ro, r1o = m.rmse()
+        assert abs(r - ro) < 1e-9 and abs(r1 - r1o) < 1e-9
+    np.testing.assert_allclose(s.predictions(), m.predictions(), rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("tensor_cores,K", [(1, 32), (0, 32), (0, 10)])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_univariate_row_sampler_mixed_within_tolerance(tensor_cores, K, mode):
+    rng = np.random.default_rng(90 + K + mode)
+    w = heavy_rows_workload(rng, nrow=70)
+    F = side_matrix(rng, w["shape"][mode], "sparse")
+    s, m = univariate_pair(w, K, 8, mode, F, compute=_lib.MG_COMPUTE_MIXED)
+    s.set_option("tensor_core_gram", tensor_cores)
+    Ut = rng.normal(scale=0.3, size=(w["shape"][mode], K)).astype(np.float32).astype(np.float64)
+    Vo = rng.normal(scale=0.3, size=(w["shape"][1 - mode], K)).astype(np.float32).astype(np.float64)
+    s.set_latents(mode, Ut)
+    s.set_latents(1 - mode, Vo)
+    m.set("latents", mode, Ut)
+    m.set("latents", 1 - mode, Vo)
+    s.sample_latents(mode, 3)
+    assert m.sample_mode(mode, 3) == 0
+    assert relerr(s.latents(mode), m.latents(mode)) < MIXED_SAMPLE_TOL
+
+
 def test_cholesky_failure_is_reported_and_context_survives():
     w = small_uniform(seed=4)
     K = 6

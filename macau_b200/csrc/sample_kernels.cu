@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
       if (p.one) {  // univariate prior: coordinate draws from the Gram (warp_finish.cuh)
         Acc gr[KP];
 #pragma unroll
-        for (int j = 0; j < KP; j++) gr[j] = Gs[lane * LD + j];
+        for (int j = 0; j < KP; j++) gr[j] = lane < K ? Gs[lane * LD + j] : (Acc)0;
         double u0 = 0.0;
         if (lane < K) {
           if constexpr (MIXED) u0 = (double)p.out_f32[(size_t)row * KP + lane];

@@ -69,6 +69,126 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------- SpMM over a work split (DevCsr::tasks) ----------------
+// One warp per task (a whole row, or one part of a long row).  Entries are read four at a time
+// (independent gathers in flight) and added in CSR order.  A part stores its FP64 partial row in
+// A.parts; the last part of a row to finish (arrival counter) adds the parts in part order and
+// writes the row.  Whole rows give the same sums as k_spmm.
+template <typename V, int NRP>
+__global__ void __launch_bounds__(256)
+    k_spmm_split(const DevCsr A, const V* __restrict__ src, int sstride, V* __restrict__ dst,
+                 int dstride, int ncomp, const V* __restrict__ add, int astride, double reg,
+                 const double* __restrict__ reg_dev) {
+  constexpr int C = NRP / 32;
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  const bool weighted = sizeof(V) == 8 ? A.val != nullptr : A.valf != nullptr;
+  for (int ti = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); ti < A.ntasks; ti += nw) {
+    const RowTask tk = A.tasks[ti];
+    V acc[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) acc[c] = (V)0;
+    const long long b = tk.begin, e = tk.begin + tk.len;
+    long long q = b;
+    for (; q + 4 <= e; q += 4) {
+      const V* s0 = src + (size_t)A.idx[q] * sstride;
+      const V* s1 = src + (size_t)A.idx[q + 1] * sstride;
+      const V* s2 = src + (size_t)A.idx[q + 2] * sstride;
+      const V* s3 = src + (size_t)A.idx[q + 3] * sstride;
+      V w0 = (V)1, w1 = (V)1, w2 = (V)1, w3 = (V)1;
+      if (weighted) {
+        if constexpr (sizeof(V) == 8) {
+          w0 = (V)A.val[q]; w1 = (V)A.val[q + 1]; w2 = (V)A.val[q + 2]; w3 = (V)A.val[q + 3];
+        } else {
+          w0 = (V)A.valf[q]; w1 = (V)A.valf[q + 1]; w2 = (V)A.valf[q + 2]; w3 = (V)A.valf[q + 3];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < C; c++) {
+        const int k = lane + 32 * c;
+        if (k < ncomp) {
+          const V x0 = s0[k], x1 = s1[k], x2 = s2[k], x3 = s3[k];
+          if (weighted) {
+            acc[c] += x0 * w0;
+            acc[c] += x1 * w1;
+            acc[c] += x2 * w2;
+            acc[c] += x3 * w3;
+          } else {
+            acc[c] += x0;
+            acc[c] += x1;
+            acc[c] += x2;
+            acc[c] += x3;
+          }
+        }
+      }
+    }
+    for (; q < e; q++) {
+      const V* s0 = src + (size_t)A.idx[q] * sstride;
+      V w0 = (V)1;
+      if (weighted) {
+        if constexpr (sizeof(V) == 8) w0 = (V)A.val[q];
+        else w0 = (V)A.valf[q];
+      }
+#pragma unroll
+      for (int c = 0; c < C; c++) {
+        const int k = lane + 32 * c;
+        if (k < ncomp) acc[c] += weighted ? s0[k] * w0 : s0[k];
+      }
+    }
+    const V r = (V)(reg_dev ? *reg_dev : reg);
+    if (tk.nparts == 1) {
+#pragma unroll
+      for (int c = 0; c < C; c++) {
+        const int k = lane + 32 * c;
+        if (k < ncomp) {
+          V o = acc[c];
+          if (add) o += r * add[(size_t)tk.row * astride + k];
+          dst[(size_t)tk.row * dstride + k] = o;
+        }
+      }
+      continue;
+    }
+    double* pp = A.parts + (size_t)(tk.slot + tk.part) * 64;
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+      const int k = lane + 32 * c;
+      if (k < ncomp) pp[k] = (double)acc[c];
+    }
+    __threadfence();
+    __syncwarp();
+    unsigned last = 0;
+    if (lane == 0) last = atomicAdd(&A.split_cnt[tk.split], 1u) == (unsigned)(tk.nparts - 1);
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) continue;
+    __threadfence();
+    const double* p0 = A.parts + (size_t)tk.slot * 64;
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+      const int k = lane + 32 * c;
+      if (k < ncomp) {
+        double t = 0.0;
+        for (int pt = 0; pt < tk.nparts; pt++) t += __ldcg(p0 + (size_t)pt * 64 + k);
+        V o = (V)t;
+        if (add) o += r * add[(size_t)tk.row * astride + k];
+        dst[(size_t)tk.row * dstride + k] = o;
+      }
+    }
+    if (lane == 0) A.split_cnt[tk.split] = 0u;
+  }
+}
+
+// Sum of `nparts` records of `len` doubles in record order (the order of sum_part), one thread
+// per entry: out[e] = ((parts[0][e] + parts[1][e]) + ...).
+__global__ void __launch_bounds__(128)
+    k_sum_records(const double* __restrict__ parts, int nparts, int len, double* __restrict__ out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= len) return;
+  double s = 0.0;
+#pragma unroll 8
+  for (int b = 0; b < nparts; b++) s += parts[(size_t)b * len + e];
+  out[e] = s;
+}
+
 // ---------------- per-block partial of sum_f a_f b_f^T (NRP x NRP, full) ----------------
 template <typename V, int NRP>
 __global__ void __launch_bounds__(kOuterThreads)
@@ -473,6 +593,12 @@ int outer_blocks(long long nrow) {
   return (int)(b < 1 ? 1 : b);
 }
 
+// The partials' sum in block order into `out` (the 1-CTA solves then read one record).
+void sum_records(const double* parts, int nparts, int len, double* out, cudaStream_t s) {
+  k_sum_records<<<(len + 127) / 128, 128, 0, s>>>(parts, nparts, len, out);
+  MG_CUDA(cudaGetLastError());
+}
+
 template <typename V, int NRP>
 void outer(const V* A, const V* B, long long nrow, double* partials, int nb, cudaStream_t s) {
   const long long rpb = (nrow + nb - 1) / nb;
@@ -483,6 +609,12 @@ void outer(const V* A, const V* B, long long nrow, double* partials, int nb, cud
 template <typename V, int NRP>
 void spmm_t(const DevCsr& A, const V* src, int sstride, V* dst, int dstride, int ncomp,
             const V* add, int astride, double reg, const double* reg_dev, cudaStream_t s) {
+  if (A.tasks) {
+    k_spmm_split<V, NRP><<<grid_for(A.ntasks, 8), 256, 0, s>>>(A, src, sstride, dst, dstride,
+                                                                ncomp, add, astride, reg, reg_dev);
+    MG_CUDA(cudaGetLastError());
+    return;
+  }
   k_spmm<V, NRP><<<grid_for(A.nrow, 8), 256, 0, s>>>(A.ptr, A.idx, A.val, A.valf, A.nrow, src,
                                                       sstride, dst, dstride, ncomp, add,
                                                       astride, reg, reg_dev);
@@ -497,6 +629,7 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
             volatile int* flag_host) {
   const long long nfeat = Ft.nrow;
   const int nb = outer_blocks(nfeat);
+  double* reduced = partials + (size_t)296 * 64 * 64;
   const int eg = grid_for(nfeat * NRP, 256);
   // Bn <- B padded to NRP columns, then the RHS norms from diag(B B^T)
   MG_CUDA(cudaMemcpy2DAsync(Bn, NRP * sizeof(double), B, bstride * sizeof(double),
@@ -505,13 +638,15 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
     MG_CUDA(cudaMemset2DAsync(Bn + n, NRP * sizeof(double), 0, (NRP - n) * sizeof(double),
                               nfeat, s));
   outer<double, NRP>(Bn, Bn, nfeat, partials, nb, s);
-  k_cg_norms<<<1, 64, 0, s>>>(partials, nb, NRP, n, small);
+  sum_records(partials, nb, NRP * NRP, reduced, s);
+  k_cg_norms<<<1, 64, 0, s>>>(reduced, 1, NRP, n, small);
   MG_CUDA(cudaGetLastError());
   k_cg_init<V><<<eg, 256, 0, s>>>(Bn, NRP, nfeat, n, NRP, small, R, P, Xd,
                                   sizeof(V) == 4 ? Bn : nullptr);
   MG_CUDA(cudaGetLastError());
   outer<V, NRP>(R, R, nfeat, partials, nb, s);
-  k_cg_rtr<<<1, 256, 0, s>>>(partials, nb, NRP, n, small);
+  sum_records(partials, nb, NRP * NRP, reduced, s);
+  k_cg_rtr<<<1, 256, 0, s>>>(reduced, 1, NRP, n, small);
   MG_CUDA(cudaGetLastError());
   const double tolsq = tol * tol;
   int iter = 0;
@@ -520,7 +655,8 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
     spmm_t<V, NRP>(F, P, NRP, inner, NRP, n, nullptr, 0, 0.0, nullptr, s);
     spmm_t<V, NRP>(Ft, inner, NRP, KPm, NRP, n, P, NRP, reg, reg_dev, s);
     outer<V, NRP>(P, KPm, nfeat, partials, nb, s);
-    k_cg_solve_a<<<1, 64, 0, s>>>(partials, nb, NRP, n, small, ctl);
+    sum_records(partials, nb, NRP * NRP, reduced, s);
+    k_cg_solve_a<<<1, 64, 0, s>>>(reduced, 1, NRP, n, small, ctl);
     MG_CUDA(cudaGetLastError());
     k_cg_update<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, P, KPm, R, Xd);
     MG_CUDA(cudaGetLastError());
@@ -531,7 +667,8 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
       MG_CUDA(cudaGetLastError());
     }
     outer<V, NRP>(R, R, nfeat, partials, nb, s);
-    k_cg_solve_psi<<<1, 64, 0, s>>>(partials, nb, NRP, n, tolsq, small, ctl, flag_dev);
+    sum_records(partials, nb, NRP * NRP, reduced, s);
+    k_cg_solve_psi<<<1, 64, 0, s>>>(reduced, 1, NRP, n, tolsq, small, ctl, flag_dev);
     MG_CUDA(cudaGetLastError());
     MG_CUDA(cudaStreamSynchronize(s));
     if (*flag_host) break;
@@ -616,7 +753,7 @@ void BlockCg::reserve(long long nrow, long long nfeat, int max_rhs, bool f32) {
     MG_CUDA(cudaMalloc(&innerd_, 8 * nrow * NRP));
   }
   MG_CUDA(cudaMalloc(&small_, sizeof(double) * (5 * kSq + 256)));
-  MG_CUDA(cudaMalloc(&partials_, sizeof(double) * 296 * 64 * 64));
+  MG_CUDA(cudaMalloc(&partials_, sizeof(double) * 297 * 64 * 64));  // 296 partials + their sum
   MG_CUDA(cudaHostAlloc(&flag_host_, sizeof(int), cudaHostAllocMapped));
 }
 

@@ -181,6 +181,28 @@ std::vector<RowTask> make_tasks(const std::vector<long long>& ptr, long long thr
   return tasks;
 }
 
+// Work split of a CSR for the side-information SpMMs (k_spmm_split): rows longer than
+// max(256, nnz / (64 warps per SM)) entries are cut into parts, so the long feature columns of a
+// Zipf-distributed F do not serialise on one warp.
+struct SpmmSplit {
+  DBuf<RowTask> tasks;
+  DBuf<unsigned> cnt;
+  DBuf<double> parts;
+  void build(const std::vector<long long>& ptr, int num_sms, cudaStream_t s, DevCsr& A) {
+    const long long nnz = ptr.empty() ? 0 : ptr.back();
+    const long long thr = std::max(256LL, nnz / ((long long)num_sms * 64));
+    int nsplit = 0, nslots = 0;
+    std::vector<RowTask> t = make_tasks(ptr, thr, 1, nsplit, nslots);
+    tasks.upload(t.data(), t.size(), s);
+    cnt.alloc_zero(std::max(1, nsplit), s);
+    parts.alloc((size_t)std::max(1, nslots) * 64);
+    A.tasks = tasks.p;
+    A.ntasks = (int)t.size();
+    A.split_cnt = cnt.p;
+    A.parts = parts.p;
+  }
+};
+
 struct Prior {
   bool macau = false;
   DBuf<double> mu, Lambda, WI, mu0;
@@ -193,6 +215,7 @@ struct Prior {
   DBuf<double> fval, tval;
   DBuf<float> fvalf, tvalf;
   DevCsr F, Ft;
+  SpmmSplit fsplit, tsplit;
   DBuf<double> beta, uhat, tmp, B, Lchol, lambda_beta, bb_partials, bb_final;
   double lambda_beta0 = 5.0, tol = 1e-6;
   double lb_mu0 = 1.0, lb_nu0 = 1e-3;
@@ -379,6 +402,8 @@ class Context {
     p.Ft.nrow = nfeat;
     p.Ft.ncol = nrows;
     p.Ft.nnz = p.F.nnz;
+    p.fsplit.build(f.ptr, num_sms_, s_, p.F);
+    p.tsplit.build(t.ptr, num_sms_, s_, p.Ft);
     p.lambda_beta0 = lambda_beta;
     p.tol = tol;
     if (univariate) {
@@ -1404,6 +1429,11 @@ int mg_blockcg(const int32_t* rows, const int32_t* cols, const double* vals, int
     mg::DevCsr F, Ft;
     F.ptr = fp.p; F.idx = fi.p; F.nrow = nrows; F.ncol = nfeat; F.nnz = (long long)f.idx.size();
     Ft.ptr = tp.p; Ft.idx = ti.p; Ft.nrow = nfeat; Ft.ncol = nrows; Ft.nnz = F.nnz;
+    int nsm = 148;
+    MG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    mg::SpmmSplit fs, ts;
+    fs.build(f.ptr, nsm, s, F);
+    ts.build(t.ptr, nsm, s, Ft);
     if (vals) {
       fv.upload(f.val.data(), f.val.size(), s);
       tv.upload(t.val.data(), t.val.size(), s);

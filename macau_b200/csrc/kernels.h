@@ -82,6 +82,13 @@ struct DevCsr {
   long long nrow = 0;
   long long ncol = 0;
   long long nnz = 0;
+  // optional work split of the SpMMs over this CSR (built by make_spmm_split): rows sorted by
+  // length, rows longer than the threshold in parts whose FP64 partial rows go to `parts`
+  // (64 doubles per slot) and are summed in part order by the last part to finish
+  const RowTask* tasks = nullptr;
+  int ntasks = 0;
+  unsigned* split_cnt = nullptr;  // arrival counters of split rows (zero between launches)
+  double* parts = nullptr;
 };
 
 // out[r, :ncomp] = sum_{e in row r} val_e * src[idx_e, :]   (csr_A_mul_Bn / A_mul_Bx<N>)

@@ -20,6 +20,8 @@ namespace mg {
 namespace {
 
 constexpr int kReplaceEvery = 20;
+constexpr int kCgBatch = 8;         // CG iterations queued between host convergence checks
+constexpr int kMaxCgIter = 100000;  // iteration cap (the breakdown flag ends a run earlier)
 constexpr int kOuterThreads = 256;
 constexpr int kOuterRows = 32;
 
@@ -32,7 +34,9 @@ __global__ void __launch_bounds__(256)
     k_spmm(const long long* __restrict__ ptr, const int* __restrict__ idx,
            const double* __restrict__ val, const float* __restrict__ valf, long long nrow,
            const V* __restrict__ src, int sstride, V* __restrict__ dst, int dstride, int ncomp,
-           const V* __restrict__ add, int astride, double reg, const double* __restrict__ reg_dev) {
+           const V* __restrict__ add, int astride, double reg, const double* __restrict__ reg_dev,
+           const uint32_t* __restrict__ done) {
+  if (done && *done) return;
   constexpr int C = NRP / 32;
   const int lane = threadIdx.x & 31;
   const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
@@ -78,7 +82,8 @@ template <typename V, int NRP>
 __global__ void __launch_bounds__(256)
     k_spmm_split(const DevCsr A, const V* __restrict__ src, int sstride, V* __restrict__ dst,
                  int dstride, int ncomp, const V* __restrict__ add, int astride, double reg,
-                 const double* __restrict__ reg_dev) {
+                 const double* __restrict__ reg_dev, const uint32_t* __restrict__ done) {
+  if (done && *done) return;
   constexpr int C = NRP / 32;
   const int lane = threadIdx.x & 31;
   const int nw = gridDim.x * (blockDim.x >> 5);
@@ -180,9 +185,10 @@ __global__ void __launch_bounds__(256)
 // Sum of `nparts` records of `len` doubles in record order (the order of sum_part), one thread
 // per entry: out[e] = ((parts[0][e] + parts[1][e]) + ...).
 __global__ void __launch_bounds__(128)
-    k_sum_records(const double* __restrict__ parts, int nparts, int len, double* __restrict__ out) {
+    k_sum_records(const double* __restrict__ parts, int nparts, int len, double* __restrict__ out,
+                  const uint32_t* __restrict__ done) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= len) return;
+  if (e >= len || (done && *done)) return;
   double s = 0.0;
 #pragma unroll 8
   for (int b = 0; b < nparts; b++) s += parts[(size_t)b * len + e];
@@ -193,7 +199,9 @@ __global__ void __launch_bounds__(128)
 template <typename V, int NRP>
 __global__ void __launch_bounds__(kOuterThreads)
     k_outer(const V* __restrict__ A, const V* __restrict__ B, int stride, long long nrow,
-            long long rows_per_block, double* __restrict__ partials) {
+            long long rows_per_block, double* __restrict__ partials,
+            const uint32_t* __restrict__ done) {
+  if (done && *done) return;
   constexpr int PER = NRP * NRP / kOuterThreads;  // 4 or 16
   __shared__ double as[kOuterRows * NRP], bs[kOuterRows * NRP];
   const long long r0 = (long long)blockIdx.x * rows_per_block;
@@ -291,8 +299,10 @@ __global__ void k_cg_norms(const double* partials, int nparts, int NRP, int n, d
 // R = P = B * inorms (V), X = 0, Bn = B * inorms (FP64, for residual replacement)
 template <typename V>
 __global__ void k_cg_init(const double* __restrict__ B, int bstride, long long nfeat, int n,
-                          int NRP, const double* small, V* R, V* P, double* X, double* Bn) {
+                          int NRP, const double* small, V* R, V* P, double* X, double* Bn,
+                          Ctl* ctl) {
   SmallView v(const_cast<double*>(small));
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cg_done = 0u;  // the iterations' skip flag
   const long long total = nfeat * NRP;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
@@ -307,9 +317,32 @@ __global__ void k_cg_init(const double* __restrict__ B, int bstride, long long n
   }
 }
 
+// Out = (M^{-T} M^{-1} Rhs)^T for the n columns of Rhs, M the lower Cholesky factor in v.M
+// (leading dimension 64): thread c solves column c through Ys (shared, 64 x 65), forward then
+// backward substitution in the order of the reference's llt().solve.
+__device__ void cta_chol_solve_cols(const double* M, const double* Rhs, int n, double* Out,
+                                    double (*Ys)[65]) {
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    for (int i = 0; i < n; i++) Ys[i][c] = Rhs[i + c * 64];
+    for (int i = 0; i < n; i++) {
+      double s = Ys[i][c];
+      for (int p = 0; p < i; p++) s -= M[i + p * 64] * Ys[p][c];
+      Ys[i][c] = s / M[i + i * 64];
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double s = Ys[i][c];
+      for (int p = i + 1; p < n; p++) s -= M[p + i * 64] * Ys[p][c];
+      Ys[i][c] = s / M[i + i * 64];
+    }
+    for (int i = 0; i < n; i++) Out[c + i * 64] = Ys[i][c];
+  }
+}
+
 // A = (chol(PtKP) \ RtR)^T  (linop.h:286-289); PtKP from the lower triangle of sum P KP^T.
 __global__ void k_cg_solve_a(const double* partials, int nparts, int NRP, int n, double* small,
                              Ctl* ctl) {
+  if (ctl->cg_done) return;
+  __shared__ double Ys[64][65];
   SmallView v(small);
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int i = e % n, j = e / n;
@@ -318,26 +351,14 @@ __global__ void k_cg_solve_a(const double* partials, int nparts, int NRP, int n,
   cta_chol_n(v.M, n, 64);  // a failed pivot is not an error in the reference either
   __syncthreads();
   // columns c of RtR solved: Y = L^{-T} L^{-1} RtR ; A(c, i) = Y(i, c)
-  for (int c = threadIdx.x; c < n; c += blockDim.x) {
-    double y[64];
-    for (int i = 0; i < n; i++) y[i] = v.RtR[i + c * 64];
-    for (int i = 0; i < n; i++) {
-      double s = y[i];
-      for (int p = 0; p < i; p++) s -= v.M[i + p * 64] * y[p];
-      y[i] = s / v.M[i + i * 64];
-    }
-    for (int i = n - 1; i >= 0; i--) {
-      double s = y[i];
-      for (int p = i + 1; p < n; p++) s -= v.M[p + i * 64] * y[p];
-      y[i] = s / v.M[i + i * 64];
-    }
-    for (int i = 0; i < n; i++) v.A[c + i * 64] = y[i];
-  }
+  cta_chol_solve_cols(v.M, v.RtR, n, v.A, Ys);
 }
 
 // RtR2 = sum R R^T; converged = all diag < tol^2; Psi = (chol(RtR) \ RtR2)^T; RtR <- RtR2.
 __global__ void k_cg_solve_psi(const double* partials, int nparts, int NRP, int n, double tolsq,
-                               double* small, Ctl* ctl, int* flag_out) {
+                               double* small, Ctl* ctl, int* flag_out, int iter) {
+  if (ctl->cg_done) return;
+  __shared__ double Ys[64][65];
   SmallView v(small);
   __shared__ int conv;
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
@@ -370,26 +391,16 @@ __global__ void k_cg_solve_psi(const double* partials, int nparts, int NRP, int 
   if (threadIdx.x == 0) {
     v.flags[0] = conv;
     ctl->cg_done = (uint32_t)conv;
-    if (flag_out) *flag_out = conv;
+    if (flag_out && conv) {  // [1]: the iteration that converged, then [0]: done
+      flag_out[1] = iter;
+      __threadfence_system();
+      flag_out[0] = 1;
+    }
   }
   if (conv) return;
   cta_chol_n(v.M, n, 64);
   __syncthreads();
-  for (int c = threadIdx.x; c < n; c += blockDim.x) {
-    double y[64];
-    for (int i = 0; i < n; i++) y[i] = v.RtR2[i + c * 64];
-    for (int i = 0; i < n; i++) {
-      double s = y[i];
-      for (int p = 0; p < i; p++) s -= v.M[i + p * 64] * y[p];
-      y[i] = s / v.M[i + i * 64];
-    }
-    for (int i = n - 1; i >= 0; i--) {
-      double s = y[i];
-      for (int p = i + 1; p < n; p++) s -= v.M[p + i * 64] * y[p];
-      y[i] = s / v.M[i + i * 64];
-    }
-    for (int i = 0; i < n; i++) v.Psi[c + i * 64] = y[i];
-  }
+  cta_chol_solve_cols(v.M, v.RtR2, n, v.Psi, Ys);
   __syncthreads();
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int i = e % n, j = e / n;
@@ -411,7 +422,9 @@ __device__ __forceinline__ V bcast_comp(const V (&x)[C], int k) {
 template <typename V, int NRP>
 __global__ void __launch_bounds__(256)
     k_cg_update(long long nfeat, int n, const double* small, const V* __restrict__ P,
-                const V* __restrict__ KPm, V* __restrict__ R, double* __restrict__ X) {
+                const V* __restrict__ KPm, V* __restrict__ R, double* __restrict__ X,
+                const uint32_t* __restrict__ done) {
+  if (*done) return;
   constexpr int C = NRP / 32;
   __shared__ double As[64 * 64];
   SmallView v(const_cast<double*>(small));
@@ -456,7 +469,8 @@ __global__ void __launch_bounds__(256)
 template <typename V, int NRP>
 __global__ void __launch_bounds__(256)
     k_cg_pupdate(long long nfeat, int n, const double* small, const V* __restrict__ R,
-                 V* __restrict__ P) {
+                 V* __restrict__ P, const uint32_t* __restrict__ done) {
+  if (*done) return;
   constexpr int C = NRP / 32;
   __shared__ double Ps[64 * 64];
   SmallView v(const_cast<double*>(small));
@@ -491,7 +505,9 @@ __global__ void __launch_bounds__(256)
 // R = Bn - KX (FP64 residual replacement, rounded to V)
 template <typename V>
 __global__ void k_cg_resid(long long total, int NRP, int n, const double* __restrict__ Bn,
-                           const double* __restrict__ KX, V* __restrict__ R) {
+                           const double* __restrict__ KX, V* __restrict__ R,
+                           const uint32_t* __restrict__ done) {
+  if (*done) return;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(e % NRP);
@@ -594,30 +610,33 @@ int outer_blocks(long long nrow) {
 }
 
 // The partials' sum in block order into `out` (the 1-CTA solves then read one record).
-void sum_records(const double* parts, int nparts, int len, double* out, cudaStream_t s) {
-  k_sum_records<<<(len + 127) / 128, 128, 0, s>>>(parts, nparts, len, out);
+void sum_records(const double* parts, int nparts, int len, double* out, cudaStream_t s,
+                 const uint32_t* done = nullptr) {
+  k_sum_records<<<(len + 127) / 128, 128, 0, s>>>(parts, nparts, len, out, done);
   MG_CUDA(cudaGetLastError());
 }
 
 template <typename V, int NRP>
-void outer(const V* A, const V* B, long long nrow, double* partials, int nb, cudaStream_t s) {
+void outer(const V* A, const V* B, long long nrow, double* partials, int nb, cudaStream_t s,
+           const uint32_t* done = nullptr) {
   const long long rpb = (nrow + nb - 1) / nb;
-  k_outer<V, NRP><<<nb, kOuterThreads, 0, s>>>(A, B, NRP, nrow, rpb, partials);
+  k_outer<V, NRP><<<nb, kOuterThreads, 0, s>>>(A, B, NRP, nrow, rpb, partials, done);
   MG_CUDA(cudaGetLastError());
 }
 
 template <typename V, int NRP>
 void spmm_t(const DevCsr& A, const V* src, int sstride, V* dst, int dstride, int ncomp,
-            const V* add, int astride, double reg, const double* reg_dev, cudaStream_t s) {
+            const V* add, int astride, double reg, const double* reg_dev, cudaStream_t s,
+            const uint32_t* done = nullptr) {
   if (A.tasks) {
-    k_spmm_split<V, NRP><<<grid_for(A.ntasks, 8), 256, 0, s>>>(A, src, sstride, dst, dstride,
-                                                                ncomp, add, astride, reg, reg_dev);
+    k_spmm_split<V, NRP><<<grid_for(A.ntasks, 8), 256, 0, s>>>(
+        A, src, sstride, dst, dstride, ncomp, add, astride, reg, reg_dev, done);
     MG_CUDA(cudaGetLastError());
     return;
   }
   k_spmm<V, NRP><<<grid_for(A.nrow, 8), 256, 0, s>>>(A.ptr, A.idx, A.val, A.valf, A.nrow, src,
                                                       sstride, dst, dstride, ncomp, add,
-                                                      astride, reg, reg_dev);
+                                                      astride, reg, reg_dev, done);
   MG_CUDA(cudaGetLastError());
 }
 
@@ -642,38 +661,47 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
   k_cg_norms<<<1, 64, 0, s>>>(reduced, 1, NRP, n, small);
   MG_CUDA(cudaGetLastError());
   k_cg_init<V><<<eg, 256, 0, s>>>(Bn, NRP, nfeat, n, NRP, small, R, P, Xd,
-                                  sizeof(V) == 4 ? Bn : nullptr);
+                                  sizeof(V) == 4 ? Bn : nullptr, ctl);
   MG_CUDA(cudaGetLastError());
   outer<V, NRP>(R, R, nfeat, partials, nb, s);
   sum_records(partials, nb, NRP * NRP, reduced, s);
   k_cg_rtr<<<1, 256, 0, s>>>(reduced, 1, NRP, n, small);
   MG_CUDA(cudaGetLastError());
   const double tolsq = tol * tol;
-  int iter = 0;
   const int fg = grid_for(nfeat, 8);
-  for (iter = 0; iter < 100000; iter++) {
-    spmm_t<V, NRP>(F, P, NRP, inner, NRP, n, nullptr, 0, 0.0, nullptr, s);
-    spmm_t<V, NRP>(Ft, inner, NRP, KPm, NRP, n, P, NRP, reg, reg_dev, s);
-    outer<V, NRP>(P, KPm, nfeat, partials, nb, s);
-    sum_records(partials, nb, NRP * NRP, reduced, s);
-    k_cg_solve_a<<<1, 64, 0, s>>>(reduced, 1, NRP, n, small, ctl);
-    MG_CUDA(cudaGetLastError());
-    k_cg_update<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, P, KPm, R, Xd);
-    MG_CUDA(cudaGetLastError());
-    if (sizeof(V) == 4 && (iter + 1) % kReplaceEvery == 0) {
-      spmm_t<double, NRP>(F, Xd, NRP, innerd, NRP, n, nullptr, 0, 0.0, nullptr, s);
-      spmm_t<double, NRP>(Ft, innerd, NRP, KX, NRP, n, Xd, NRP, reg, reg_dev, s);
-      k_cg_resid<V><<<eg, 256, 0, s>>>(nfeat * NRP, NRP, n, Bn, KX, R);
+  // Iterations are queued kCgBatch at a time and the host reads the convergence flag between
+  // batches; once k_cg_solve_psi has set ctl->cg_done, every later kernel of the batch returns
+  // at once, so the result is that of stopping at the converged iteration.
+  const uint32_t* done = &ctl->cg_done;
+  int iter = 0;
+  while (iter < kMaxCgIter) {
+    for (int b = 0; b < kCgBatch && iter < kMaxCgIter; b++, iter++) {
+      spmm_t<V, NRP>(F, P, NRP, inner, NRP, n, nullptr, 0, 0.0, nullptr, s, done);
+      spmm_t<V, NRP>(Ft, inner, NRP, KPm, NRP, n, P, NRP, reg, reg_dev, s, done);
+      outer<V, NRP>(P, KPm, nfeat, partials, nb, s, done);
+      sum_records(partials, nb, NRP * NRP, reduced, s, done);
+      k_cg_solve_a<<<1, 64, 0, s>>>(reduced, 1, NRP, n, small, ctl);
+      MG_CUDA(cudaGetLastError());
+      k_cg_update<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, P, KPm, R, Xd, done);
+      MG_CUDA(cudaGetLastError());
+      if (sizeof(V) == 4 && (iter + 1) % kReplaceEvery == 0) {
+        spmm_t<double, NRP>(F, Xd, NRP, innerd, NRP, n, nullptr, 0, 0.0, nullptr, s, done);
+        spmm_t<double, NRP>(Ft, innerd, NRP, KX, NRP, n, Xd, NRP, reg, reg_dev, s, done);
+        k_cg_resid<V><<<eg, 256, 0, s>>>(nfeat * NRP, NRP, n, Bn, KX, R, done);
+        MG_CUDA(cudaGetLastError());
+      }
+      outer<V, NRP>(R, R, nfeat, partials, nb, s, done);
+      sum_records(partials, nb, NRP * NRP, reduced, s, done);
+      k_cg_solve_psi<<<1, 64, 0, s>>>(reduced, 1, NRP, n, tolsq, small, ctl, flag_dev, iter);
+      MG_CUDA(cudaGetLastError());
+      k_cg_pupdate<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, R, P, done);
       MG_CUDA(cudaGetLastError());
     }
-    outer<V, NRP>(R, R, nfeat, partials, nb, s);
-    sum_records(partials, nb, NRP * NRP, reduced, s);
-    k_cg_solve_psi<<<1, 64, 0, s>>>(reduced, 1, NRP, n, tolsq, small, ctl, flag_dev);
-    MG_CUDA(cudaGetLastError());
     MG_CUDA(cudaStreamSynchronize(s));
-    if (*flag_host) break;
-    k_cg_pupdate<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, R, P);
-    MG_CUDA(cudaGetLastError());
+    if (flag_host[0]) {
+      iter = flag_host[1];
+      break;
+    }
   }
   k_cg_finish<<<grid_for(nfeat * n, 256), 256, 0, s>>>(nfeat, NRP, n, small, Xd, Xout, xstride);
   MG_CUDA(cudaGetLastError());
@@ -754,7 +782,7 @@ void BlockCg::reserve(long long nrow, long long nfeat, int max_rhs, bool f32) {
   }
   MG_CUDA(cudaMalloc(&small_, sizeof(double) * (5 * kSq + 256)));
   MG_CUDA(cudaMalloc(&partials_, sizeof(double) * 297 * 64 * 64));  // 296 partials + their sum
-  MG_CUDA(cudaHostAlloc(&flag_host_, sizeof(int), cudaHostAllocMapped));
+  MG_CUDA(cudaHostAlloc(&flag_host_, 2 * sizeof(int), cudaHostAllocMapped));  // done, iteration
 }
 
 void BlockCg::release() {
@@ -774,7 +802,8 @@ int BlockCg::core(const DevCsr& F, const DevCsr& Ft, double reg, const double* r
                   Ctl* ctl, cudaStream_t s, bool f32) {
   int* flag_dev = nullptr;
   MG_CUDA(cudaHostGetDevicePointer((void**)&flag_dev, flag_host_, 0));
-  *flag_host_ = 0;
+  flag_host_[0] = 0;
+  flag_host_[1] = 0;
   if (f32) {
     if (n <= 32)
       return cg_core<float, 32>(F, Ft, reg, reg_dev, B, bstride, n, tol, X, xstride, ctl, s,

@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "rng.cuh"
+#include "warp_finish.cuh"
 
 namespace mg {
 namespace {
@@ -317,33 +318,94 @@ __global__ void k_cg_init(const double* __restrict__ B, int bstride, long long n
   }
 }
 
-// Out = (M^{-T} M^{-1} Rhs)^T for the n columns of Rhs, M the lower Cholesky factor in v.M
-// (leading dimension 64): thread c solves column c through Ys (shared, 64 x 65), forward then
-// backward substitution in the order of the reference's llt().solve.
-__device__ void cta_chol_solve_cols(const double* M, const double* Rhs, int n, double* Out,
-                                    double (*Ys)[65]) {
+// Out(c, i) = (M^{-T} M^{-1} Rhs)(i, c) for the n columns of Rhs, M the lower Cholesky factor
+// in v.M (leading dimension 64): thread c solves column c, forward then backward substitution in
+// the order of the reference's llt().solve.  The general path (n > 32, or a failed pivot).
+__device__ void cta_chol_solve_cols(const double* M, const double* Rhs, int n, double* Out) {
   for (int c = threadIdx.x; c < n; c += blockDim.x) {
-    for (int i = 0; i < n; i++) Ys[i][c] = Rhs[i + c * 64];
+    double y[64];
+    for (int i = 0; i < n; i++) y[i] = Rhs[i + c * 64];
     for (int i = 0; i < n; i++) {
-      double s = Ys[i][c];
-      for (int p = 0; p < i; p++) s -= M[i + p * 64] * Ys[p][c];
-      Ys[i][c] = s / M[i + i * 64];
+      double s = y[i];
+      for (int p = 0; p < i; p++) s -= M[i + p * 64] * y[p];
+      y[i] = s / M[i + i * 64];
     }
     for (int i = n - 1; i >= 0; i--) {
-      double s = Ys[i][c];
-      for (int p = i + 1; p < n; p++) s -= M[p + i * 64] * Ys[p][c];
-      Ys[i][c] = s / M[i + i * 64];
+      double s = y[i];
+      for (int p = i + 1; p < n; p++) s -= M[p + i * 64] * y[p];
+      y[i] = s / M[i + i * 64];
     }
-    for (int i = 0; i < n; i++) Out[c + i * 64] = Ys[i][c];
+    for (int i = 0; i < n; i++) Out[c + i * 64] = y[i];
   }
 }
 
+constexpr int kSolveThreads = 256;
+constexpr int kLcLd = 36;
+
+// The same solves for n <= 32 with the factor in registers: warp 0 factorises the SPD matrix Ms
+// (lower triangle, padded with the identity beyond n) by warp_factor, publishing L^T in Lc;
+// then warp w solves columns w, w + 8, ...: lane i holds L(i, j) for j <= i and L(j, i) for
+// j > i and runs each substitution as 32 shuffle steps.  Returns false, with Out untouched, when
+// a pivot is not positive (the caller then takes the general path).
+__device__ bool warp_chol_solve(const double (*Ms)[33], double* Lc, const double* Rhs, int n,
+                                double* Out, int* okf) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) {
+    double a[32], rinv = 1.0, d0 = 1.0;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      double x;
+      if (lane < n && j < n) x = j <= lane ? Ms[lane][j] : Ms[j][lane];
+      else x = lane == j ? 1.0 : 0.0;
+      a[j] = x;
+      if (j == lane) d0 = x;
+    }
+    const bool ok = warp_factor<double, 32>(a, rinv, lane, 0.0, d0, Lc, kLcLd);
+    if (lane == 0) *okf = ok ? 1 : 0;
+  }
+  __syncthreads();
+  if (!*okf) return false;
+  double m[32], dinv = 1.0;
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    m[j] = j <= lane ? Lc[j * kLcLd + lane] : Lc[lane * kLcLd + j];
+    if (j == lane) dinv = 1.0 / m[j];
+  }
+  for (int c = warp; c < n; c += kSolveThreads / 32) {
+    double y = lane < n ? Rhs[lane + c * 64] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      if (lane == j) y *= dinv;
+      const double yj = __shfl_sync(0xffffffffu, y, j);
+      if (lane > j) y = fma(-m[j], yj, y);
+    }
+#pragma unroll
+    for (int j = 31; j >= 0; j--) {
+      if (lane == j) y *= dinv;
+      const double xj = __shfl_sync(0xffffffffu, y, j);
+      if (lane < j) y = fma(-m[j], xj, y);
+    }
+    if (lane < n) Out[c + lane * 64] = y;
+  }
+  return true;
+}
+
 // A = (chol(PtKP) \ RtR)^T  (linop.h:286-289); PtKP from the lower triangle of sum P KP^T.
-__global__ void k_cg_solve_a(const double* partials, int nparts, int NRP, int n, double* small,
-                             Ctl* ctl) {
+__global__ void __launch_bounds__(kSolveThreads, 1)
+    k_cg_solve_a(const double* partials, int nparts, int NRP, int n, double* small, Ctl* ctl) {
   if (ctl->cg_done) return;
-  __shared__ double Ys[64][65];
+  __shared__ double Ms[32][33];
+  __shared__ __align__(16) double Lc[32 * kLcLd];
+  __shared__ int okf;
   SmallView v(small);
+  if (n <= 32) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int i = e % n, j = e / n;
+      if (i >= j) Ms[i][j] = sum_part(partials, nparts, NRP, i, j);
+    }
+    __syncthreads();
+    if (warp_chol_solve(Ms, Lc, v.RtR, n, v.A, &okf)) return;
+  }
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int i = e % n, j = e / n;
     if (i >= j) v.M[i + j * 64] = sum_part(partials, nparts, NRP, i, j);  // P(i) . KP(j)
@@ -351,14 +413,17 @@ __global__ void k_cg_solve_a(const double* partials, int nparts, int NRP, int n,
   cta_chol_n(v.M, n, 64);  // a failed pivot is not an error in the reference either
   __syncthreads();
   // columns c of RtR solved: Y = L^{-T} L^{-1} RtR ; A(c, i) = Y(i, c)
-  cta_chol_solve_cols(v.M, v.RtR, n, v.A, Ys);
+  cta_chol_solve_cols(v.M, v.RtR, n, v.A);
 }
 
 // RtR2 = sum R R^T; converged = all diag < tol^2; Psi = (chol(RtR) \ RtR2)^T; RtR <- RtR2.
-__global__ void k_cg_solve_psi(const double* partials, int nparts, int NRP, int n, double tolsq,
-                               double* small, Ctl* ctl, int* flag_out, int iter) {
+__global__ void __launch_bounds__(kSolveThreads, 1)
+    k_cg_solve_psi(const double* partials, int nparts, int NRP, int n, double tolsq,
+                   double* small, Ctl* ctl, int* flag_out, int iter) {
   if (ctl->cg_done) return;
-  __shared__ double Ys[64][65];
+  __shared__ double Ms[32][33];
+  __shared__ __align__(16) double Lc[32 * kLcLd];
+  __shared__ int okf;
   SmallView v(small);
   __shared__ int conv;
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
@@ -383,10 +448,6 @@ __global__ void k_cg_solve_psi(const double* partials, int nparts, int NRP, int 
       atomicOr(&ctl->status, kStatCgFail);
     }
   }
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    const int i = e % n, j = e / n;
-    v.M[i + j * 64] = v.RtR[i + j * 64];
-  }
   __syncthreads();
   if (threadIdx.x == 0) {
     v.flags[0] = conv;
@@ -398,9 +459,24 @@ __global__ void k_cg_solve_psi(const double* partials, int nparts, int NRP, int 
     }
   }
   if (conv) return;
-  cta_chol_n(v.M, n, 64);
-  __syncthreads();
-  cta_chol_solve_cols(v.M, v.RtR2, n, v.Psi, Ys);
+  bool fast = false;
+  if (n <= 32) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int i = e % n, j = e / n;
+      if (i >= j) Ms[i][j] = v.RtR[i + j * 64];
+    }
+    __syncthreads();
+    fast = warp_chol_solve(Ms, Lc, v.RtR2, n, v.Psi, &okf);
+  }
+  if (!fast) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int i = e % n, j = e / n;
+      v.M[i + j * 64] = v.RtR[i + j * 64];
+    }
+    cta_chol_n(v.M, n, 64);
+    __syncthreads();
+    cta_chol_solve_cols(v.M, v.RtR2, n, v.Psi);
+  }
   __syncthreads();
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int i = e % n, j = e / n;
@@ -680,7 +756,7 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
       spmm_t<V, NRP>(Ft, inner, NRP, KPm, NRP, n, P, NRP, reg, reg_dev, s, done);
       outer<V, NRP>(P, KPm, nfeat, partials, nb, s, done);
       sum_records(partials, nb, NRP * NRP, reduced, s, done);
-      k_cg_solve_a<<<1, 64, 0, s>>>(reduced, 1, NRP, n, small, ctl);
+      k_cg_solve_a<<<1, kSolveThreads, 0, s>>>(reduced, 1, NRP, n, small, ctl);
       MG_CUDA(cudaGetLastError());
       k_cg_update<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, P, KPm, R, Xd, done);
       MG_CUDA(cudaGetLastError());
@@ -692,7 +768,8 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
       }
       outer<V, NRP>(R, R, nfeat, partials, nb, s, done);
       sum_records(partials, nb, NRP * NRP, reduced, s, done);
-      k_cg_solve_psi<<<1, 64, 0, s>>>(reduced, 1, NRP, n, tolsq, small, ctl, flag_dev, iter);
+      k_cg_solve_psi<<<1, kSolveThreads, 0, s>>>(reduced, 1, NRP, n, tolsq, small, ctl, flag_dev,
+                                                 iter);
       MG_CUDA(cudaGetLastError());
       k_cg_pupdate<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, R, P, done);
       MG_CUDA(cudaGetLastError());

@@ -183,54 +183,103 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Sum of `nparts` records of `len` doubles in record order (the order of sum_part), one thread
-// per entry: out[e] = ((parts[0][e] + parts[1][e]) + ...).
-__global__ void __launch_bounds__(128)
+// Sum of `nparts` records of `len` doubles: eight lanes per entry, lane l adding records
+// l, l + 8, ... in order, then a fixed xor tree over the eight lanes (deterministic).
+__global__ void __launch_bounds__(256)
     k_sum_records(const double* __restrict__ parts, int nparts, int len, double* __restrict__ out,
                   const uint32_t* __restrict__ done) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= len || (done && *done)) return;
+  if (done && *done) return;
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 3, l = threadIdx.x & 7;
   double s = 0.0;
-#pragma unroll 8
-  for (int b = 0; b < nparts; b++) s += parts[(size_t)b * len + e];
-  out[e] = s;
+  if (g < len)
+#pragma unroll 4
+    for (int b = l; b < nparts; b += 8) s += parts[(size_t)b * len + g];
+  s += __shfl_xor_sync(0xffffffffu, s, 4, 8);
+  s += __shfl_xor_sync(0xffffffffu, s, 2, 8);
+  s += __shfl_xor_sync(0xffffffffu, s, 1, 8);
+  if (l == 0 && g < len) out[g] = s;
 }
 
 // ---------------- per-block partial of sum_f a_f b_f^T (NRP x NRP, full) ----------------
+// Rows staged 32 at a time in shared memory (the next 32 prefetched into registers); each thread
+// accumulates a 4 x 4 tile (i in 4 ti .., j in 4 tj ..) over the rows of its row group (every
+// G-th staged row; G = 4 for NRP = 32, 1 for NRP = 64), and the groups' tiles are added in group
+// order at the end.  partials[block][i + j * NRP] = sum over the block's rows of a_i b_j.
 template <typename V, int NRP>
-__global__ void __launch_bounds__(kOuterThreads)
+__global__ void __launch_bounds__(kOuterThreads, 2)
     k_outer(const V* __restrict__ A, const V* __restrict__ B, int stride, long long nrow,
             long long rows_per_block, double* __restrict__ partials,
             const uint32_t* __restrict__ done) {
   if (done && *done) return;
-  constexpr int PER = NRP * NRP / kOuterThreads;  // 4 or 16
-  __shared__ double as[kOuterRows * NRP], bs[kOuterRows * NRP];
+  constexpr int T4 = NRP / 4, TILES = T4 * T4, G = kOuterThreads / TILES;
+  constexpr int LD = NRP + 4, PRE = kOuterRows * NRP / kOuterThreads;  // staged values / thread
+  static_assert(G >= 1 && TILES * G == kOuterThreads, "tile layout");
+  __shared__ __align__(16) double as[kOuterRows][LD], bs[kOuterRows][LD];
+  __shared__ double red[G > 1 ? G - 1 : 1][G > 1 ? TILES : 1][16];
+  const int t = threadIdx.x, tile = t % TILES, rg = t / TILES;
+  const int ti = tile / T4, tj = tile % T4;
   const long long r0 = (long long)blockIdx.x * rows_per_block;
   const long long r1 = min(nrow, r0 + rows_per_block);
-  double acc[PER];
+  double acc[4][4];
 #pragma unroll
-  for (int q = 0; q < PER; q++) acc[q] = 0.0;
-  for (long long b = r0; b < r1; b += kOuterRows) {
-    const int cnt = (int)min((long long)kOuterRows, r1 - b);
+  for (int x = 0; x < 4; x++)
+#pragma unroll
+    for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
+  double na[PRE], nb[PRE];
+  auto fetch = [&](long long b0) {
+#pragma unroll
+    for (int q = 0; q < PRE; q++) {
+      const int e = t + kOuterThreads * q, rr = e / NRP, k = e % NRP;
+      const bool in = b0 + rr < r1;
+      na[q] = in ? (double)A[(b0 + rr) * stride + k] : 0.0;
+      nb[q] = in ? (double)B[(b0 + rr) * stride + k] : 0.0;
+    }
+  };
+  fetch(r0);
+  for (long long b0 = r0; b0 < r1; b0 += kOuterRows) {
+    const int cnt = (int)min((long long)kOuterRows, r1 - b0);
     __syncthreads();
-    for (int e = threadIdx.x; e < cnt * NRP; e += kOuterThreads) {
-      const int rr = e / NRP, k = e % NRP;
-      as[e] = (double)A[(b + rr) * stride + k];
-      bs[e] = (double)B[(b + rr) * stride + k];
+#pragma unroll
+    for (int q = 0; q < PRE; q++) {
+      const int e = t + kOuterThreads * q;
+      as[e / NRP][e % NRP] = na[q];
+      bs[e / NRP][e % NRP] = nb[q];
     }
     __syncthreads();
+    if (b0 + kOuterRows < r1) fetch(b0 + kOuterRows);
+    for (int r = rg; r < cnt; r += G) {
+      const double2 i01 = *reinterpret_cast<const double2*>(&as[r][4 * ti]);
+      const double2 i23 = *reinterpret_cast<const double2*>(&as[r][4 * ti + 2]);
+      const double2 j01 = *reinterpret_cast<const double2*>(&bs[r][4 * tj]);
+      const double2 j23 = *reinterpret_cast<const double2*>(&bs[r][4 * tj + 2]);
+      const double xi[4] = {i01.x, i01.y, i23.x, i23.y}, xj[4] = {j01.x, j01.y, j23.x, j23.y};
 #pragma unroll
-    for (int q = 0; q < PER; q++) {
-      const int ent = threadIdx.x + q * kOuterThreads;
-      const int i = ent % NRP, j = ent / NRP;  // entry (i, j) = sum a_i b_j
-      double s = acc[q];
-      for (int rr = 0; rr < cnt; rr++) s += as[rr * NRP + i] * bs[rr * NRP + j];
-      acc[q] = s;
+      for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y] = fma(xi[x], xj[y], acc[x][y]);
     }
   }
+  if constexpr (G > 1) {
+    if (rg > 0)
 #pragma unroll
-  for (int q = 0; q < PER; q++)
-    partials[(size_t)blockIdx.x * NRP * NRP + threadIdx.x + q * kOuterThreads] = acc[q];
+      for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) red[rg - 1][tile][x * 4 + y] = acc[x][y];
+    __syncthreads();
+  }
+  if (rg == 0) {
+    double* out = partials + (size_t)blockIdx.x * NRP * NRP;
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+      for (int y = 0; y < 4; y++) {
+        double v = acc[x][y];
+        if constexpr (G > 1)
+#pragma unroll
+          for (int g = 0; g < G - 1; g++) v += red[g][tile][x * 4 + y];
+        out[(4 * ti + x) + (4 * tj + y) * NRP] = v;
+      }
+  }
 }
 
 // Sum of the block partials of entry (i, j), i,j < n.
@@ -484,96 +533,84 @@ __global__ void __launch_bounds__(kSolveThreads, 1)
   }
 }
 
-// Broadcast of component k of a feature row held as lane-distributed registers.
-template <typename V, int C>
-__device__ __forceinline__ V bcast_comp(const V (&x)[C], int k) {
-  V out = (V)0;
-#pragma unroll
-  for (int c = 0; c < C; c++)
-    if ((k >> 5) == c) out = __shfl_sync(0xffffffffu, x[c], k & 31);
-  return out;
+// Row updates of the block-CG as small tiled products with the n x n matrix M (A or Psi, in
+// shared memory, M[i + k * 64]):
+//   UPDATE (linop.h:292-300):   X[f] += M P[f],  R[f] -= M KP[f]
+//   PUPDATE (linop.h:319-326):  P[f] = R[f] + M P[f]
+// A block takes 32 feature rows, staged k-major in shared memory; thread (trow, tcol) owns rows
+// 2 trow, 2 trow + 1 and components tcol * CI .. + CI - 1, and sums over k in order with fma.
+constexpr int kRowTile = 32;
+constexpr size_t rows_smem(int NRP, bool update) {
+  return sizeof(double) * ((size_t)NRP * NRP + (update ? 2 : 1) * (size_t)NRP * (kRowTile + 2));
 }
-
-// X += A P ; R -= A KP  (linop.h:292-300), warp per feature; A (n x n) in shared memory.
-template <typename V, int NRP>
+template <typename V, int NRP, bool UPDATE>
 __global__ void __launch_bounds__(256)
-    k_cg_update(long long nfeat, int n, const double* small, const V* __restrict__ P,
-                const V* __restrict__ KPm, V* __restrict__ R, double* __restrict__ X,
-                const uint32_t* __restrict__ done) {
+    k_cg_rows(long long nfeat, int n, const double* small, const V* __restrict__ P,
+              const V* __restrict__ KPm, V* __restrict__ R, double* __restrict__ X,
+              V* __restrict__ Pout, const uint32_t* __restrict__ done) {
   if (*done) return;
-  constexpr int C = NRP / 32;
-  __shared__ double As[64 * 64];
+  constexpr int CI = NRP / 16;  // components per thread: 2 or 4
+  extern __shared__ __align__(16) double dsm[];  // Ms | Pt | Qt (rows_smem bytes)
+  double(*Ms)[NRP] = reinterpret_cast<double(*)[NRP]>(dsm);  // Ms[k][i] = M(i, k)
+  double(*Pt)[kRowTile + 2] = reinterpret_cast<double(*)[kRowTile + 2]>(dsm + NRP * NRP);
+  double(*Qt)[kRowTile + 2] = Pt + NRP;
   SmallView v(const_cast<double*>(small));
-  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) As[e] = v.A[e];
+  const double* M = UPDATE ? v.A : v.Psi;
+  for (int e = threadIdx.x; e < NRP * NRP; e += blockDim.x) {
+    const int i = e % NRP, k = e / NRP;
+    Ms[k][i] = (i < n && k < n) ? M[i + k * 64] : 0.0;
+  }
+  const long long f0 = (long long)blockIdx.x * kRowTile;
+  for (int e = threadIdx.x; e < kRowTile * NRP; e += blockDim.x) {
+    const int r = e / NRP, k = e % NRP;
+    const bool in = f0 + r < nfeat;
+    Pt[k][r] = in ? (double)P[(f0 + r) * NRP + k] : 0.0;
+    if constexpr (UPDATE) Qt[k][r] = in ? (double)KPm[(f0 + r) * NRP + k] : 0.0;
+  }
   __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long f = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); f < nfeat;
-       f += nw) {
-    V p[C], kp[C];
+  const int tcol = threadIdx.x % 16, trow = threadIdx.x / 16;
+  double sp[2][CI], sq[2][CI];
 #pragma unroll
-    for (int c = 0; c < C; c++) {
-      p[c] = P[f * NRP + lane + 32 * c];
-      kp[c] = KPm[f * NRP + lane + 32 * c];
-    }
-    double sx[C], sr[C];
+  for (int x = 0; x < 2; x++)
 #pragma unroll
-    for (int c = 0; c < C; c++) sx[c] = sr[c] = 0.0;
-    for (int k = 0; k < n; k++) {
-      const double pk = (double)bcast_comp<V, C>(p, k);
-      const double kk = (double)bcast_comp<V, C>(kp, k);
+    for (int y = 0; y < CI; y++) sp[x][y] = sq[x][y] = 0.0;
+  for (int k = 0; k < n; k++) {
+    const double2 pr = *reinterpret_cast<const double2*>(&Pt[k][2 * trow]);
+    double m[CI];
 #pragma unroll
-      for (int c = 0; c < C; c++) {
-        const int i = lane + 32 * c;
-        const double a = (i < n) ? As[i + k * 64] : 0.0;
-        sx[c] += a * pk;
-        sr[c] += a * kk;
-      }
+    for (int y = 0; y < CI; y += 2) {
+      const double2 mm = *reinterpret_cast<const double2*>(&Ms[k][CI * tcol + y]);
+      m[y] = mm.x;
+      m[y + 1] = mm.y;
     }
 #pragma unroll
-    for (int c = 0; c < C; c++) {
-      const int i = lane + 32 * c;
-      if (i < n) {
-        X[f * NRP + i] += sx[c];
-        R[f * NRP + i] = (V)((double)R[f * NRP + i] - sr[c]);
+    for (int y = 0; y < CI; y++) {
+      sp[0][y] = fma(m[y], pr.x, sp[0][y]);
+      sp[1][y] = fma(m[y], pr.y, sp[1][y]);
+    }
+    if constexpr (UPDATE) {
+      const double2 qr = *reinterpret_cast<const double2*>(&Qt[k][2 * trow]);
+#pragma unroll
+      for (int y = 0; y < CI; y++) {
+        sq[0][y] = fma(m[y], qr.x, sq[0][y]);
+        sq[1][y] = fma(m[y], qr.y, sq[1][y]);
       }
     }
   }
-}
-
-// P = R + Psi P  (linop.h:319-326)
-template <typename V, int NRP>
-__global__ void __launch_bounds__(256)
-    k_cg_pupdate(long long nfeat, int n, const double* small, const V* __restrict__ R,
-                 V* __restrict__ P, const uint32_t* __restrict__ done) {
-  if (*done) return;
-  constexpr int C = NRP / 32;
-  __shared__ double Ps[64 * 64];
-  SmallView v(const_cast<double*>(small));
-  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) Ps[e] = v.Psi[e];
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long f = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); f < nfeat;
-       f += nw) {
-    V p[C];
 #pragma unroll
-    for (int c = 0; c < C; c++) p[c] = P[f * NRP + lane + 32 * c];
-    double s[C];
+  for (int x = 0; x < 2; x++) {
+    const long long f = f0 + 2 * trow + x;
+    if (f >= nfeat) continue;
 #pragma unroll
-    for (int c = 0; c < C; c++) s[c] = 0.0;
-    for (int k = 0; k < n; k++) {
-      const double pk = (double)bcast_comp<V, C>(p, k);
-#pragma unroll
-      for (int c = 0; c < C; c++) {
-        const int i = lane + 32 * c;
-        s[c] += (i < n ? Ps[i + k * 64] : 0.0) * pk;
+    for (int y = 0; y < CI; y++) {
+      const int i = CI * tcol + y;
+      if (i >= n) continue;
+      if constexpr (UPDATE) {
+        X[f * NRP + i] += sp[x][y];
+        R[f * NRP + i] = (V)((double)R[f * NRP + i] - sq[x][y]);
+      } else {
+        Pout[f * NRP + i] = (V)((double)R[f * NRP + i] + sp[x][y]);
       }
-    }
-#pragma unroll
-    for (int c = 0; c < C; c++) {
-      const int i = lane + 32 * c;
-      if (i < n) P[f * NRP + i] = (V)((double)R[f * NRP + i] + s[c]);
     }
   }
 }
@@ -688,7 +725,7 @@ int outer_blocks(long long nrow) {
 // The partials' sum in block order into `out` (the 1-CTA solves then read one record).
 void sum_records(const double* parts, int nparts, int len, double* out, cudaStream_t s,
                  const uint32_t* done = nullptr) {
-  k_sum_records<<<(len + 127) / 128, 128, 0, s>>>(parts, nparts, len, out, done);
+  k_sum_records<<<(len * 8 + 255) / 256, 256, 0, s>>>(parts, nparts, len, out, done);
   MG_CUDA(cudaGetLastError());
 }
 
@@ -744,7 +781,21 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
   k_cg_rtr<<<1, 256, 0, s>>>(reduced, 1, NRP, n, small);
   MG_CUDA(cudaGetLastError());
   const double tolsq = tol * tol;
-  const int fg = grid_for(nfeat, 8);
+  const int rg = (int)((nfeat + kRowTile - 1) / kRowTile);
+  {
+    static bool configured[64] = {false};
+    int dev = 0;
+    MG_CUDA(cudaGetDevice(&dev));
+    if (!configured[dev & 63]) {
+      MG_CUDA(cudaFuncSetAttribute(k_cg_rows<V, NRP, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)rows_smem(NRP, true)));
+      MG_CUDA(cudaFuncSetAttribute(k_cg_rows<V, NRP, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)rows_smem(NRP, false)));
+      configured[dev & 63] = true;
+    }
+  }
   // Iterations are queued kCgBatch at a time and the host reads the convergence flag between
   // batches; once k_cg_solve_psi has set ctl->cg_done, every later kernel of the batch returns
   // at once, so the result is that of stopping at the converged iteration.
@@ -758,7 +809,8 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
       sum_records(partials, nb, NRP * NRP, reduced, s, done);
       k_cg_solve_a<<<1, kSolveThreads, 0, s>>>(reduced, 1, NRP, n, small, ctl);
       MG_CUDA(cudaGetLastError());
-      k_cg_update<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, P, KPm, R, Xd, done);
+      k_cg_rows<V, NRP, true><<<rg, 256, rows_smem(NRP, true), s>>>(nfeat, n, small, P, KPm, R,
+                                                                    Xd, nullptr, done);
       MG_CUDA(cudaGetLastError());
       if (sizeof(V) == 4 && (iter + 1) % kReplaceEvery == 0) {
         spmm_t<double, NRP>(F, Xd, NRP, innerd, NRP, n, nullptr, 0, 0.0, nullptr, s, done);
@@ -771,7 +823,8 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
       k_cg_solve_psi<<<1, kSolveThreads, 0, s>>>(reduced, 1, NRP, n, tolsq, small, ctl, flag_dev,
                                                  iter);
       MG_CUDA(cudaGetLastError());
-      k_cg_pupdate<V, NRP><<<fg, 256, 0, s>>>(nfeat, n, small, R, P, done);
+      k_cg_rows<V, NRP, false><<<rg, 256, rows_smem(NRP, false), s>>>(nfeat, n, small, P, nullptr,
+                                                                       R, nullptr, P, done);
       MG_CUDA(cudaGetLastError());
     }
     MG_CUDA(cudaStreamSynchronize(s));

@@ -188,9 +188,14 @@ int mg_get_stds(mg_ctx* ctx, double* out);
 int mg_get_test_data(mg_ctx* ctx, double* out);
 int mg_get_stats(mg_ctx* ctx, mg_stats* out);
 
-/* Switches of the implementation (no reference counterpart; defaults 1):
- *   "graph"            replay captured CUDA graphs for sweeps without host-side decisions
- *   "tensor_core_gram" mixed mode: run the K = 32 row Grams on the tcgen05 tensor cores */
+/* Switches of the implementation (no reference counterpart):
+ *   "graph"            (default 1) replay captured CUDA graphs for sweeps without host-side
+ *                      decisions
+ *   "tensor_core_gram" (default 1) mixed mode: run the K = 32 row Grams on the tcgen05 tensor
+ *                      cores
+ *   "cg_fp32"          (default 0) mixed mode: run the Macau block-CG in FP32 with an FP64
+ *                      residual replacement every 20 iterations instead of FP64; set before
+ *                      mg_init */
 int mg_set_option(mg_ctx* ctx, const char* name, int value);
 
 /* macau.blockcg(X, B, reg, tol) (macau.pyx:67-91 -> solve_blockcg, linop.h:229-343) on the GPU:

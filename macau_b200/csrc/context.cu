@@ -477,7 +477,7 @@ class Context {
         p.lambda_beta.upload(&p.lambda_beta0, 1, s_);
         p.bb_partials.alloc((size_t)stats_blocks(p.nfeat) * (K_ + K_ * K_));
         p.bb_final.alloc((size_t)(K_ + K_ * K_));
-        p.cg.reserve(p.F.nrow, p.nfeat, 64, mixed_);
+        p.cg.reserve(p.F.nrow, p.nfeat, 64, cg_f32_);
       }
       if (p.one) {  // MacauOnePrior::init (macauoneprior.cpp:16-39) + setLambdaBeta
         p.beta.alloc_zero((size_t)p.nfeat * CP_, s_);
@@ -619,9 +619,10 @@ class Context {
     launch_beta_rhs_b(p.Ft, p.tmp.p, CP_, K_, p.Lchol.p, p.lambda_beta.p, ctl_.p, cfg_.seed,
                       mode, p.B.p, CP_, s_);
     p.cg_iters = p.cg.solve(p.F, p.Ft, 0.0, p.lambda_beta.p, p.B.p, CP_, K_, p.tol, p.beta.p,
-                            CP_, ctl_.p, s_, mixed_);
+                            CP_, ctl_.p, s_, cg_f32_);
     // stats x3 (+ reductions), NW, chol, tmp, spmm, noise, uhat spmm, lambda_beta + the CG's
-    launches_ += 12 + 6 + 8LL * p.cg_iters;
+    // (set-up, then 10 per iteration)
+    launches_ += 12 + 6 + 10LL * p.cg_iters;
     // compute_uhat (linop.h:196-198): Uhat = beta F^T, one K-vector per row of F
     launch_spmm(p.F, p.beta.p, CP_, p.uhat.p, KP_, K_, false, s_);
     // sample_lambda_beta with the new beta and Lambda (latentprior.cpp:263)
@@ -1045,6 +1046,7 @@ class Context {
   bool initialised() const { return initialised_; }
   void set_use_graph(bool b) { use_graph_ = b; drop_graphs(); }
   void set_use_tc(bool b) { use_tc_ = b; drop_graphs(); }
+  void set_cg_f32(bool b) { cg_f32_ = b && mixed_; }
 
   std::string err;
 
@@ -1139,6 +1141,10 @@ class Context {
   DBuf<double> noise_partials_;
   bool have_data_ = false, initialised_ = false;
   bool use_graph_ = true, use_tc_ = true;
+  // Block-CG in FP32 with FP64 residual replacement (mixed mode, option "cg_fp32").  Off by
+  // default: at tol 1e-6 the FP32 iteration needs about 1.5x the iterations of FP64, which
+  // costs more than its halved gather traffic saves.
+  bool cg_f32_ = false;
   int burnin_ = 50, nsamples_ = 400;
   ModeData md_[2];
   Prior prior_[2];
@@ -1400,6 +1406,7 @@ int mg_set_option(mg_ctx* ctx, const char* name, int value) {
     const std::string n(name);
     if (n == "graph") c.set_use_graph(value != 0);
     else if (n == "tensor_core_gram") c.set_use_tc(value != 0);
+    else if (n == "cg_fp32") c.set_cg_f32(value != 0);
     else throw mg::MgError(MG_ERR_ARG, "unknown option " + n);
   });
 }

@@ -535,6 +535,22 @@ def test_univariate_row_sampler_mixed_within_tolerance(tensor_cores, K, mode):
     assert relerr(s.latents(mode), m.latents(mode)) < MIXED_SAMPLE_TOL
 
 
+def test_macau_mixed_cg_precision_option():
+    # mixed mode runs the block-CG in FP64 unless "cg_fp32" selects FP32 with FP64 residual
+    # replacement; both reach the same link matrix within the CG tolerance's reach
+    w = workloads.macau_side(scale=0.05, seed=6)
+    betas = []
+    for opt in (0, 1):
+        s = gpu_sampler(w, 16, 2.0, 17, compute=_lib.MG_COMPUTE_MIXED, init=False)
+        s.set_option("cg_fp32", opt)
+        s.init()
+        for it in range(2):
+            s.sweep(it, eval=False)
+        betas.append(s.beta(0))
+        assert s.stats()["cg_iters"][0] > 0
+    assert relerr(betas[1], betas[0]) < 2e-2
+
+
 def test_cholesky_failure_is_reported_and_context_survives():
     w = small_uniform(seed=4)
     K = 6

@@ -483,6 +483,7 @@ class Context {
         p.beta.alloc_zero((size_t)p.nfeat * CP_, s_);
         p.uhat.alloc_zero((size_t)dims_[m] * KP_, s_);
         p.tmp.alloc_zero((size_t)dims_[m] * CP_, s_);
+        p.B.alloc_zero((size_t)p.nfeat * CP_, s_);  // the link sampler's draws
         std::vector<double> lb(K_, p.lambda_beta0);
         p.lb_one.upload(lb.data(), lb.size(), s_);
       }
@@ -593,11 +594,11 @@ class Context {
                             nullptr, nw_, ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
       launch_beta_one(p.Ft, p.colsq.p, p.lvl_ptr.p, p.lvl_feat.p, p.nlevels, latents(mode),
                       mixed_, KP_, p.mu.p, p.uhat.p, KP_, p.Lambda.p, p.lb_one.p, K_, N, p.beta.p,
-                      CP_, p.tmp.p, CP_, ctl_.p, cfg_.seed, mode, s_);
+                      CP_, p.tmp.p, CP_, p.B.p, ctl_.p, cfg_.seed, mode, s_);
       launch_spmm(p.F, p.beta.p, CP_, p.uhat.p, KP_, K_, false, s_);
       launch_lambda_beta_one(p.beta.p, CP_, p.nfeat, K_, p.lb_a0, p.lb_b0, ctl_.p, cfg_.seed,
                              mode, p.lb_one.p, s_);
-      launches_ += 3;  // beta, spmm, lambda_beta (after the 3 of stats / reduce / NW)
+      launches_ += 4;  // draws, beta, spmm, lambda_beta (after the 3 of stats / reduce / NW)
       return;
     }
     if (!p.macau) {  // BPMFPrior::update_prior (latentprior.cpp:79-81)

@@ -3,6 +3,8 @@
 // (sample_mu_lambda) and compute_uhat reuse the BPMF statistics kernels and the SpMM.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "rng.cuh"
@@ -17,11 +19,11 @@ constexpr int kBetaWarps = kBetaThreads / 32;
 // (macauoneprior.cpp:243-252):
 //   A = lambda_beta_d + lambda_d colsq_f,   B = lambda_d (zx_d + beta_df colsq_f),
 //   beta_df <- B / A + z / sqrt(A),   delta_d = beta_df old - beta_df new.
-// zx, lam, lb are this lane's components; returns delta (0 for lanes >= dc).
+// zx, lam, lb are this lane's components; the N(0,1) draw of (f, d0 + lane) comes from draws
+// (filled by k_beta_draws before the sequential sweep); returns delta (0 for lanes >= dc).
 __device__ __forceinline__ double beta_coef(int lane, int dc, int d0, int f, double zx,
                                             double lam, double lb, double cs, double* beta,
-                                            int bstride, unsigned long long seed, uint32_t sweep,
-                                            uint32_t st) {
+                                            int bstride, const double* __restrict__ draws) {
   if (lane >= dc) return 0.0;
   const int dx = d0 + lane;
   double* bp = beta + (size_t)f * bstride + dx;
@@ -29,7 +31,7 @@ __device__ __forceinline__ double beta_coef(int lane, int dc, int d0, int f, dou
   const double A = lb + lam * cs;
   const double B = lam * (zx + b * cs);
   const double Ainv = 1.0 / A;
-  const double bn = B * Ainv + sqrt(Ainv) * normal_draw(seed, sweep, st, (uint32_t)f, (uint32_t)dx);
+  const double bn = B * Ainv + sqrt(Ainv) * draws[(size_t)f * bstride + dx];
   *bp = bn;
   return b - bn;
 }
@@ -50,13 +52,11 @@ __global__ void __launch_bounds__(kBetaThreads)
                const double* __restrict__ uhat, int hstride, const double* __restrict__ Lambda,
                const double* __restrict__ lambda_beta, int K, long long N,
                double* __restrict__ beta, int bstride, double* __restrict__ Z, int zstride,
-               const Ctl* ctl, unsigned long long seed, int mode) {
+               const double* __restrict__ draws) {
   __shared__ double red[kBetaWarps][4];
   __shared__ double dl[4];
   const int d0 = blockIdx.x * 4, dc = min(4, K - d0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t sweep = ctl->sweep;
-  const uint32_t st = stream_id(kBetaOne, (uint32_t)mode);
   // this lane's dimension d0 + lane (lanes 0 .. dc - 1 update the coefficients)
   const double lam = lane < dc ? Lambda[(size_t)(d0 + lane) * (K + 1)] : 0.0;
   const double lb = lane < dc ? lambda_beta[d0 + lane] : 1.0;
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kBetaThreads)
         for (int d = 0; d < 4; d++)
           if (lane == d) mine = zx[d];
         const double my =
-            beta_coef(lane, dc, d0, f, mine, lam, lb, colsq[f], beta, bstride, seed, sweep, st);
+            beta_coef(lane, dc, d0, f, mine, lam, lb, colsq[f], beta, bstride, draws);
         double delta[4];
 #pragma unroll
         for (int d = 0; d < 4; d++) delta[d] = __shfl_sync(0xffffffffu, my, d);
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kBetaThreads)
           if (lane < dc)
             for (int w = 0; w < kBetaWarps; w++) s += red[w][lane];
           const double my =
-              beta_coef(lane, dc, d0, f, s, lam, lb, colsq[f], beta, bstride, seed, sweep, st);
+              beta_coef(lane, dc, d0, f, s, lam, lb, colsq[f], beta, bstride, draws);
           if (lane < 4) dl[lane] = my;
         }
         __syncthreads();
@@ -137,6 +137,25 @@ __global__ void __launch_bounds__(kBetaThreads)
       }
     }
     __syncthreads();
+  }
+}
+
+// The link sampler's N(0,1) draws, keyed (kBetaOne, feature f, dimension d) like
+// bmrandn_single per feature (macauoneprior.cpp:241): draws[f * stride + d], one Philox block
+// per pair of dimensions.
+__global__ void k_beta_draws(long long nfeat, int K, int stride, const Ctl* ctl,
+                             unsigned long long seed, int mode, double* __restrict__ draws) {
+  const int pairs = (K + 1) / 2;
+  const uint32_t st = stream_id(kBetaOne, (uint32_t)mode);
+  const uint32_t sweep = ctl->sweep;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nfeat * pairs;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long f = e / pairs;
+    const int q = (int)(e % pairs);
+    double z0, z1;
+    normal_pair(seed, sweep, st, (uint32_t)f, (uint32_t)q, &z0, &z1);
+    draws[f * stride + 2 * q] = z0;
+    if (2 * q + 1 < K) draws[f * stride + 2 * q + 1] = z1;
   }
 }
 
@@ -169,17 +188,21 @@ void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
                      const int* lvl_feat, int nlevels, const void* U, bool f32, int ustride,
                      const double* mu, const double* uhat, int hstride, const double* Lambda,
                      const double* lambda_beta, int K, long long N, double* beta, int bstride,
-                     double* Z, int zstride, const Ctl* ctl, unsigned long long seed, int mode,
-                     cudaStream_t s) {
+                     double* Z, int zstride, double* draws, const Ctl* ctl,
+                     unsigned long long seed, int mode, cudaStream_t s) {
+  const long long work = Ft.nrow * ((K + 1) / 2);
+  k_beta_draws<<<(int)std::min<long long>(4736, (work + 255) / 256), 256, 0, s>>>(
+      Ft.nrow, K, bstride, ctl, seed, mode, draws);
+  MG_CUDA(cudaGetLastError());
   const int blocks = (K + 3) / 4;
   if (f32)
     k_beta_one<float><<<blocks, kBetaThreads, 0, s>>>(
         Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const float*)U, ustride, mu,
-        uhat, hstride, Lambda, lambda_beta, K, N, beta, bstride, Z, zstride, ctl, seed, mode);
+        uhat, hstride, Lambda, lambda_beta, K, N, beta, bstride, Z, zstride, draws);
   else
     k_beta_one<double><<<blocks, kBetaThreads, 0, s>>>(
         Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const double*)U, ustride, mu,
-        uhat, hstride, Lambda, lambda_beta, K, N, beta, bstride, Z, zstride, ctl, seed, mode);
+        uhat, hstride, Lambda, lambda_beta, K, N, beta, bstride, Z, zstride, draws);
   MG_CUDA(cudaGetLastError());
 }
 

@@ -140,6 +140,71 @@ __global__ void __launch_bounds__(kBetaThreads)
   }
 }
 
+// The same link sampler with one block per dimension d and this dimension's column of Z held in
+// shared memory (N doubles, N <= kZsMax), so the feature-by-feature chain reads and writes no
+// global memory but beta.  The sums are formed in the order of k_beta_one (lane-strided then an
+// xor tree in a warp; thread-strided, per-warp trees, then the warps in order in a block), so
+// both kernels give the same coefficients.
+constexpr int kZsMax = 26 * 1024;
+template <typename T>
+__global__ void __launch_bounds__(kBetaThreads)
+    k_beta_one_smem(const long long* __restrict__ tptr, const int* __restrict__ tidx,
+                    const double* __restrict__ tval, const double* __restrict__ colsq,
+                    const int* __restrict__ lvl_ptr, const int* __restrict__ lvl_feat, int nlevels,
+                    const T* __restrict__ U, int ustride, const double* __restrict__ mu,
+                    const double* __restrict__ uhat, int hstride,
+                    const double* __restrict__ Lambda, const double* __restrict__ lambda_beta,
+                    int K, int N, double* __restrict__ beta, int bstride,
+                    const double* __restrict__ draws) {
+  extern __shared__ double Zs[];
+  __shared__ double red[kBetaWarps];
+  __shared__ double dl;
+  const int d = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double lam = Lambda[(size_t)d * (K + 1)], lb = lambda_beta[d];
+  for (int i = threadIdx.x; i < N; i += kBetaThreads)
+    Zs[i] = (double)U[(size_t)i * ustride + d] - mu[d] - uhat[(size_t)i * hstride + d];
+  __syncthreads();
+  for (int L = 0; L < nlevels; L++) {
+    const int f0 = lvl_ptr[L], f1 = lvl_ptr[L + 1];
+    if (2 * (f1 - f0) >= kBetaWarps) {
+      for (int q = f0 + warp; q < f1; q += kBetaWarps) {
+        const int f = lvl_feat[q];
+        double zx = 0.0;
+        for (long long e = tptr[f] + lane; e < tptr[f + 1]; e += 32)
+          zx = fma(tval ? tval[e] : 1.0, Zs[tidx[e]], zx);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) zx += __shfl_xor_sync(0xffffffffu, zx, o);
+        const double my = beta_coef(0, 1, d, f, zx, lam, lb, colsq[f], beta, bstride, draws);
+        for (long long e = tptr[f] + lane; e < tptr[f + 1]; e += 32)
+          Zs[tidx[e]] = fma(tval ? tval[e] : 1.0, my, Zs[tidx[e]]);
+        __syncwarp();
+      }
+    } else {
+      for (int q = f0; q < f1; q++) {
+        const int f = lvl_feat[q];
+        double zx = 0.0;
+        for (long long e = tptr[f] + threadIdx.x; e < tptr[f + 1]; e += kBetaThreads)
+          zx = fma(tval ? tval[e] : 1.0, Zs[tidx[e]], zx);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) zx += __shfl_xor_sync(0xffffffffu, zx, o);
+        if (lane == 0) red[warp] = zx;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          double sum = 0.0;
+          for (int w = 0; w < kBetaWarps; w++) sum += red[w];
+          dl = beta_coef(0, 1, d, f, sum, lam, lb, colsq[f], beta, bstride, draws);
+        }
+        __syncthreads();
+        const double delta = dl;
+        for (long long e = tptr[f] + threadIdx.x; e < tptr[f + 1]; e += kBetaThreads)
+          Zs[tidx[e]] = fma(tval ? tval[e] : 1.0, delta, Zs[tidx[e]]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // The link sampler's N(0,1) draws, keyed (kBetaOne, feature f, dimension d) like
 // bmrandn_single per feature (macauoneprior.cpp:241): draws[f * stride + d], one Philox block
 // per pair of dimensions.
@@ -194,6 +259,31 @@ void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
   k_beta_draws<<<(int)std::min<long long>(4736, (work + 255) / 256), 256, 0, s>>>(
       Ft.nrow, K, bstride, ctl, seed, mode, draws);
   MG_CUDA(cudaGetLastError());
+  if (N <= kZsMax) {  // one block per dimension, Z's column in shared memory
+    const size_t smem = sizeof(double) * (size_t)N;
+    static bool configured[64] = {false};
+    int dev = 0;
+    MG_CUDA(cudaGetDevice(&dev));
+    if (!configured[dev & 63]) {
+      MG_CUDA(cudaFuncSetAttribute(k_beta_one_smem<float>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(double) * kZsMax)));
+      MG_CUDA(cudaFuncSetAttribute(k_beta_one_smem<double>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(double) * kZsMax)));
+      configured[dev & 63] = true;
+    }
+    if (f32)
+      k_beta_one_smem<float><<<K, kBetaThreads, smem, s>>>(
+          Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const float*)U, ustride,
+          mu, uhat, hstride, Lambda, lambda_beta, K, (int)N, beta, bstride, draws);
+    else
+      k_beta_one_smem<double><<<K, kBetaThreads, smem, s>>>(
+          Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const double*)U, ustride,
+          mu, uhat, hstride, Lambda, lambda_beta, K, (int)N, beta, bstride, draws);
+    MG_CUDA(cudaGetLastError());
+    return;
+  }
   const int blocks = (K + 3) / 4;
   if (f32)
     k_beta_one<float><<<blocks, kBetaThreads, 0, s>>>(

@@ -226,7 +226,7 @@ struct Prior {
   // level, lvl_ptr[l] .. lvl_ptr[l + 1] the features of level l)
   bool one = false;
   DBuf<double> colsq, lb_one;
-  DBuf<int> lvl_ptr, lvl_feat;
+  DBuf<int> lvl_ptr, lvl_feat, lvl_warp;
   int nlevels = 0;
   double lb_a0 = 0.1, lb_b0 = 0.1;
   bool side() const { return macau || one; }
@@ -427,7 +427,16 @@ class Context {
       for (int l = 0; l < nl; l++) lptr[l + 1] += lptr[l];
       std::vector<int> fill(lptr.begin(), lptr.end() - 1);
       for (int f = 0; f < nfeat; f++) order[fill[level[f]]++] = f;
+      // a level runs one warp per feature when it has many features or only short ones
+      std::vector<int> lwarp(nl, 1);
+      for (int l = 0; l < nl; l++) {
+        long long longest = 0;
+        for (int q = lptr[l]; q < lptr[l + 1]; q++)
+          longest = std::max(longest, t.ptr[order[q] + 1] - t.ptr[order[q]]);
+        lwarp[l] = (lptr[l + 1] - lptr[l] >= 8 || longest <= 1024) ? 1 : 0;
+      }
       p.colsq.upload(cs.data(), cs.size(), s_);
+      p.lvl_warp.upload(lwarp.data(), lwarp.size(), s_);
       p.lvl_ptr.upload(lptr.data(), lptr.size(), s_);
       p.lvl_feat.upload(order.data(), order.size(), s_);
       p.nlevels = nl;
@@ -592,7 +601,8 @@ class Context {
       // compute_uhat, sample_lambda_beta
       launch_normal_wishart(stat_final_.p, 1, N, K_, p.mu0.p, p.b0, p.WI.p, p.df, nullptr, 0,
                             nullptr, nw_, ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
-      launch_beta_one(p.Ft, p.colsq.p, p.lvl_ptr.p, p.lvl_feat.p, p.nlevels, latents(mode),
+      launch_beta_one(p.Ft, p.colsq.p, p.lvl_ptr.p, p.lvl_feat.p, p.lvl_warp.p, p.nlevels,
+                      latents(mode),
                       mixed_, KP_, p.mu.p, p.uhat.p, KP_, p.Lambda.p, p.lb_one.p, K_, N, p.beta.p,
                       CP_, p.tmp.p, CP_, p.B.p, ctl_.p, cfg_.seed, mode, s_);
       launch_spmm(p.F, p.beta.p, CP_, p.uhat.p, KP_, K_, false, s_);

@@ -41,14 +41,15 @@ __device__ __forceinline__ double beta_coef(int lane, int dc, int d0, int f, dou
 // are visited level by level.  lvl_feat lists the features sorted by (level, index), where a
 // feature's level is one more than the highest level of an earlier feature sharing a row with
 // it, so the features of one level touch disjoint rows of Z and their updates commute: the
-// result equals the reference's feature-by-feature order.  A level with many features gives
-// one feature to each warp; a level with few gives each feature to the whole block.
+// result equals the reference's feature-by-feature order.  A level marked in lvl_warp (many
+// features, or none longer than 1024 entries) gives one feature to each warp; the others give
+// each feature in turn to the whole block.
 template <typename T>
 __global__ void __launch_bounds__(kBetaThreads)
     k_beta_one(const long long* __restrict__ tptr, const int* __restrict__ tidx,
                const double* __restrict__ tval, const double* __restrict__ colsq,
-               const int* __restrict__ lvl_ptr, const int* __restrict__ lvl_feat, int nlevels,
-               const T* __restrict__ U, int ustride, const double* __restrict__ mu,
+               const int* __restrict__ lvl_ptr, const int* __restrict__ lvl_feat,
+               const int* __restrict__ lvl_warp, int nlevels, const T* __restrict__ U, int ustride, const double* __restrict__ mu,
                const double* __restrict__ uhat, int hstride, const double* __restrict__ Lambda,
                const double* __restrict__ lambda_beta, int K, long long N,
                double* __restrict__ beta, int bstride, double* __restrict__ Z, int zstride,
@@ -67,7 +68,7 @@ __global__ void __launch_bounds__(kBetaThreads)
   __syncthreads();
   for (int L = 0; L < nlevels; L++) {
     const int f0 = lvl_ptr[L], f1 = lvl_ptr[L + 1];
-    if (2 * (f1 - f0) >= kBetaWarps) {
+    if (lvl_warp[L]) {
       for (int q = f0 + warp; q < f1; q += kBetaWarps) {
         const int f = lvl_feat[q];
         double zx[4] = {0.0, 0.0, 0.0, 0.0};
@@ -150,8 +151,9 @@ template <typename T>
 __global__ void __launch_bounds__(kBetaThreads)
     k_beta_one_smem(const long long* __restrict__ tptr, const int* __restrict__ tidx,
                     const double* __restrict__ tval, const double* __restrict__ colsq,
-                    const int* __restrict__ lvl_ptr, const int* __restrict__ lvl_feat, int nlevels,
-                    const T* __restrict__ U, int ustride, const double* __restrict__ mu,
+                    const int* __restrict__ lvl_ptr, const int* __restrict__ lvl_feat,
+                    const int* __restrict__ lvl_warp, int nlevels, const T* __restrict__ U,
+                    int ustride, const double* __restrict__ mu,
                     const double* __restrict__ uhat, int hstride,
                     const double* __restrict__ Lambda, const double* __restrict__ lambda_beta,
                     int K, int N, double* __restrict__ beta, int bstride,
@@ -167,7 +169,7 @@ __global__ void __launch_bounds__(kBetaThreads)
   __syncthreads();
   for (int L = 0; L < nlevels; L++) {
     const int f0 = lvl_ptr[L], f1 = lvl_ptr[L + 1];
-    if (2 * (f1 - f0) >= kBetaWarps) {
+    if (lvl_warp[L]) {
       for (int q = f0 + warp; q < f1; q += kBetaWarps) {
         const int f = lvl_feat[q];
         double zx = 0.0;
@@ -250,7 +252,7 @@ __global__ void k_lambda_beta_one(const double* __restrict__ beta, int bstride, 
 }  // namespace
 
 void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
-                     const int* lvl_feat, int nlevels, const void* U, bool f32, int ustride,
+                     const int* lvl_feat, const int* lvl_warp, int nlevels, const void* U, bool f32, int ustride,
                      const double* mu, const double* uhat, int hstride, const double* Lambda,
                      const double* lambda_beta, int K, long long N, double* beta, int bstride,
                      double* Z, int zstride, double* draws, const Ctl* ctl,
@@ -275,11 +277,11 @@ void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
     }
     if (f32)
       k_beta_one_smem<float><<<K, kBetaThreads, smem, s>>>(
-          Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const float*)U, ustride,
+          Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, lvl_warp, nlevels, (const float*)U, ustride,
           mu, uhat, hstride, Lambda, lambda_beta, K, (int)N, beta, bstride, draws);
     else
       k_beta_one_smem<double><<<K, kBetaThreads, smem, s>>>(
-          Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const double*)U, ustride,
+          Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, lvl_warp, nlevels, (const double*)U, ustride,
           mu, uhat, hstride, Lambda, lambda_beta, K, (int)N, beta, bstride, draws);
     MG_CUDA(cudaGetLastError());
     return;
@@ -287,11 +289,11 @@ void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
   const int blocks = (K + 3) / 4;
   if (f32)
     k_beta_one<float><<<blocks, kBetaThreads, 0, s>>>(
-        Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const float*)U, ustride, mu,
+        Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, lvl_warp, nlevels, (const float*)U, ustride, mu,
         uhat, hstride, Lambda, lambda_beta, K, N, beta, bstride, Z, zstride, draws);
   else
     k_beta_one<double><<<blocks, kBetaThreads, 0, s>>>(
-        Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, nlevels, (const double*)U, ustride, mu,
+        Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, lvl_warp, nlevels, (const double*)U, ustride, mu,
         uhat, hstride, Lambda, lambda_beta, K, N, beta, bstride, Z, zstride, draws);
   MG_CUDA(cudaGetLastError());
 }

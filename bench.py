@@ -48,6 +48,8 @@ def parse_args():
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="sweeps of the e2e run (0: = steps)")
+    ap.add_argument("--no-side", action="store_true",
+                    help="skip the side-information legs (Macau block-CG and univariate priors)")
     ap.add_argument("--only", choices=["all", "mixed", "fp64"], default="all",
                     help="profiling runs: time one sampler and print its phase times only")
     return ap.parse_args()
@@ -160,6 +162,54 @@ def read_traffic():
     except OSError:
         pass
     return None
+
+
+def side_info_legs(device, sweeps=20, cpu_sweeps=2):
+    """Sweep rates with side information on the 20,000 x 500 matrix with a binary 20,000 x
+    32,768 Zipf feature matrix (K = 32): the Macau prior (block-CG link solve) and the univariate
+    prior, FP64 and mixed, each beside the CPU oracle's FP64 sweep of the same model."""
+    from macau_b200 import _lib, workloads
+    from oracle import oracle as orc
+    from tests.gpu_helpers import oracle_model
+    import scipy.sparse as sp
+    w = workloads.macau_side()
+    fr, fc, _, shp = w["side"]
+    cores = orc.set_threads(os.cpu_count() or 1)
+    out = {"workload": w["name"], "K": K_LATENT, "alpha": ALPHA, "cg_tol": 1e-6,
+           "lambda_beta": 5.0}
+    for prior in ("macau", "univariate"):
+        leg = {}
+        for comp, name in ((_lib.MG_COMPUTE_FP64, "fp64"), (_lib.MG_COMPUTE_MIXED, "mixed")):
+            s = _lib.Sampler(K_LATENT, ALPHA, seed=5, compute=comp, device=device)
+            s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
+            if prior == "macau":
+                s.set_side(0, fr, fc, None, shp, 5.0, 1e-6)
+            else:
+                s.set_side_univariate(0, fr, fc, None, shp, 5.0)
+            s.set_samples(10 ** 6, 1)
+            s.init()
+            s.time_sweeps(0, 3, eval=False)
+            t, _ = s.time_sweeps(3, sweeps, eval=False)
+            st = s.stats()
+            leg[name] = {"sweeps_per_s": sweeps / t, "ms_per_sweep": t / sweeps * 1e3}
+            if prior == "macau":
+                leg[name]["cg_iters_last"] = st["cg_iters"][0]
+            s.close()
+        m = oracle_model(w, K_LATENT, ALPHA, 5)
+        if prior == "univariate":
+            F = sp.coo_matrix((np.ones(len(fr)), (fr, fc)), shape=shp)
+            m.set_side_one(0, orc.Csr.from_scipy(F, True), orc.Csr.from_scipy(F.T, True), 5.0)
+        n_cpu = cpu_sweeps if prior == "macau" else 5 * cpu_sweeps
+        m.sweep(0, 10 ** 6)
+        t0 = time.perf_counter()
+        for it in range(1, 1 + n_cpu):
+            m.sweep(it, 10 ** 6)
+        tc = time.perf_counter() - t0
+        leg["cpu_oracle"] = {"sweeps_per_s": n_cpu / tc, "sample": f"{n_cpu} FP64 sweeps",
+                             "cores": cores}
+        leg["mixed_over_cpu"] = leg["mixed"]["sweeps_per_s"] / leg["cpu_oracle"]["sweeps_per_s"]
+        out[prior] = leg
+    return out
 
 
 def peaks():
@@ -394,6 +444,8 @@ def run_ours(args):
                     "timed": "C-ABI run: data upload + CSR build, init, sweeps with eval and "
                              "RMSE read-back, final predictions read-back",
                     "split_s": e2e_split}}
+    if rank == 0 and world == 1 and not args.no_side:
+        line["side_info"] = side_info_legs(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds, 50)
         line["mixed_over_cpu"] = v_mx / line["cpu_baseline"]["value"]

@@ -50,7 +50,7 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=0, help="sweeps of the e2e run (0: = steps)")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the side-information legs (Macau block-CG and univariate priors)")
-    ap.add_argument("--only", choices=["all", "mixed", "fp64"], default="all",
+    ap.add_argument("--only", choices=["all", "mixed", "fp64", "macau", "univariate"], default="all",
                     help="profiling runs: time one sampler and print its phase times only")
     return ap.parse_args()
 
@@ -331,9 +331,30 @@ def run_ours(args):
     except Exception:
         pass
 
-    w = workload(args.scale, 2)
     seed = ranks.chain_seed()
     K, W = args.steps, args.warmup
+    if args.only in ("macau", "univariate"):
+        # one side-information sampler (FP64) on the Macau workload, for profiling
+        from macau_b200 import workloads
+        ws = workloads.macau_side(scale=args.scale)
+        fr, fc, _, shp = ws["side"]
+        s = _lib.Sampler(K_LATENT, ALPHA, seed=seed, compute=_lib.MG_COMPUTE_FP64, device=local)
+        s.set_relation_data(ws["rows"], ws["cols"], ws["vals"], ws["shape"])
+        if args.only == "macau":
+            s.set_side(0, fr, fc, None, shp, 5.0, 1e-6)
+        else:
+            s.set_side_univariate(0, fr, fc, None, shp, 5.0)
+        s.set_samples(10 ** 6, 1)
+        s.init()
+        s.time_sweeps(0, max(W, 1), eval=False)
+        t, _ = s.time_sweeps(W, K, eval=False)
+        _, ph = s.time_sweeps(W + K, K, eval=False, phase_events=True)
+        print(json.dumps({"only": args.only, "workload": ws["name"], "ms_per_step": t / K * 1e3,
+                          "phase_ms": [x / K * 1e3 for x in ph], "stats": s.stats()}), flush=True)
+        s.close()
+        ranks.close()
+        return 0
+    w = workload(args.scale, 2)
     if args.only != "all":
         comp = _lib.MG_COMPUTE_MIXED if args.only == "mixed" else _lib.MG_COMPUTE_FP64
         s = make_sampler(w, comp, seed, local)

@@ -716,8 +716,8 @@ int grid_for(long long rows, int rows_per_block) {
   return (int)(b < 1 ? 1 : b);
 }
 
-int outer_blocks(long long nrow) {
-  long long b = (nrow + 255) / 256;
+int outer_blocks(long long nrow) {  // about two blocks per SM at the benchmark's 32,768 features
+  long long b = (nrow + 63) / 64;
   if (b > 296) b = 296;
   return (int)(b < 1 ? 1 : b);
 }

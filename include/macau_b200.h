@@ -195,7 +195,11 @@ int mg_get_stats(mg_ctx* ctx, mg_stats* out);
  *                      cores
  *   "cg_fp32"          (default 0) mixed mode: run the Macau block-CG in FP32 with an FP64
  *                      residual replacement every 20 iterations instead of FP64; set before
- *                      mg_init */
+ *                      mg_init
+ *   "gram_precision"   (default 0) mixed mode: inputs of the row Grams, 0 = BF16, 1 = FP16,
+ *                      2 = TF32 (the FP32 latents rounded to TF32 as they are gathered); FP32
+ *                      accumulation, factor and solves in every case.  1 and 2 use the CUDA-core
+ *                      sampler at every K.  Set before mg_init (it undoes a previous mg_init). */
 int mg_set_option(mg_ctx* ctx, const char* name, int value);
 
 /* macau.blockcg(X, B, reg, tol) (macau.pyx:67-91 -> solve_blockcg, linop.h:229-343) on the GPU:

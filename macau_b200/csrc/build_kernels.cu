@@ -178,6 +178,21 @@ long long build_csr_pair(const int* d_r, const int* d_c, const double* d_v, long
   return nu;
 }
 
+__global__ void k_copy16(const float* __restrict__ src, void* __restrict__ dst, long long n,
+                         bool half) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (half) reinterpret_cast<__half*>(dst)[i] = __float2half_rn(src[i]);
+    else reinterpret_cast<__nv_bfloat16*>(dst)[i] = __float2bfloat16_rn(src[i]);
+  }
+}
+
+void launch_copy16(const float* src, void* dst, long long n, bool half, cudaStream_t s) {
+  if (n <= 0) return;
+  k_copy16<<<grid_for(n, 256), 256, 0, s>>>(src, dst, n, half);
+  MG_CUDA(cudaGetLastError());
+}
+
 void launch_pack(const int* idx, const double* val, long long n, double mean, double alpha,
                  uint2* out, cudaStream_t s) {
   if (n <= 0) return;

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <cstdint>
 #include <cstdio>
@@ -80,12 +81,21 @@ struct SampleParams {
   const double* znoise;        // optional injected N(0,1) draws (nrows x K), tests only
   int one;                     // univariate prior (MacauOnePrior): coordinate-wise draws from
                                // the row's Gram with the precisions on Lambda's diagonal
+  int half_copy;               // mixed: the 16-bit gather copy (out_bf16) holds FP16, not BF16
 };
 
 #ifdef __CUDACC__
 // Noise precision of a sampler launch: the device value under adaptive noise, else the fixed one.
 __device__ __forceinline__ double noise_alpha(const SampleParams& p) {
   return p.alpha_dev ? *p.alpha_dev : p.alpha;
+}
+// Store of one value into the 16-bit gather copy of the latents (BF16, or FP16 when the Gram
+// precision is FP16), rounded to nearest even.
+__device__ __forceinline__ void store_copy(const SampleParams& p, size_t i, float x) {
+  if (p.half_copy)
+    reinterpret_cast<__half*>(p.out_bf16)[i] = __float2half_rn(x);
+  else
+    p.out_bf16[i] = __float2bfloat16_rn(x);
 }
 // Factor applied to a packed weight when it is read: packed weights carry the fixed alpha
 // already, and are (y - mean) alone under adaptive noise.

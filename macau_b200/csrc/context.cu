@@ -553,7 +553,10 @@ class Context {
     sp.mean = mean_;
     sp.alpha = cfg_.precision;
     sp.alpha_dev = adaptive_ ? &ctl_.p->alpha : nullptr;
-    sp.other = mixed_ ? (const void*)lat16_[other].p : (const void*)lat64_[other].p;
+    sp.other = !mixed_ ? (const void*)lat64_[other].p
+               : gram_ == 2 ? (const void*)lat32_[other].p   // TF32: rounded from the master
+                            : (const void*)lat16_[other].p;
+    sp.half_copy = mixed_ && gram_ == 1 ? 1 : 0;
     sp.Lambda = p.Lambda.p;
     sp.mu = p.mu.p;
     sp.uhat = p.side() ? p.uhat.p : nullptr;
@@ -568,7 +571,7 @@ class Context {
     sp.mode = mode;
     sp.seed = cfg_.seed;
     sp.znoise = znoise_dev;
-    if (mixed_ && use_tc_ && KP_ == 32) {
+    if (mixed_ && use_tc_ && gram_ == 0 && KP_ == 32) {
       SampleParams tp = sp;
       tp.tasks = md.tasks_tc.p;
       tp.ntasks = md.ntasks_tc;
@@ -579,7 +582,7 @@ class Context {
         return;
       }
     }
-    launch_sample(sp, KP_, mixed_, s_, num_sms_);
+    launch_sample(sp, KP_, mixed_, gram_, s_, num_sms_);
   }
 
   const void* latents(int mode) const {
@@ -910,18 +913,11 @@ class Context {
     const long long N = dims_[mode];
     if (mixed_) {
       std::vector<float> h((size_t)N * KP_, 0.f);
-      std::vector<uint16_t> hb((size_t)N * KP_, 0);
       for (long long n = 0; n < N; n++)
-        for (int k = 0; k < K_; k++) {
-          const float f = (float)in[n * K_ + k];
-          h[n * KP_ + k] = f;
-          uint32_t bits;
-          std::memcpy(&bits, &f, 4);
-          const uint32_t lsb = (bits >> 16) & 1u;  // round to nearest even
-          hb[n * KP_ + k] = (uint16_t)((bits + 0x7FFFu + lsb) >> 16);
-        }
+        for (int k = 0; k < K_; k++) h[n * KP_ + k] = (float)in[n * K_ + k];
       MG_CUDA(cudaMemcpyAsync(lat32_[mode].p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, s_));
-      MG_CUDA(cudaMemcpyAsync(lat16_[mode].p, hb.data(), hb.size() * 2, cudaMemcpyHostToDevice, s_));
+      // the 16-bit gather copy (BF16, or FP16 under that Gram precision), rounded on the device
+      launch_copy16(lat32_[mode].p, lat16_[mode].p, (long long)N * KP_, gram_ == 1, s_);
     } else {
       MG_CUDA(cudaMemcpy2DAsync(lat64_[mode].p, KP_ * 8, in, K_ * 8, K_ * 8, N,
                                 cudaMemcpyHostToDevice, s_));
@@ -1058,6 +1054,13 @@ class Context {
   void set_use_graph(bool b) { use_graph_ = b; drop_graphs(); }
   void set_use_tc(bool b) { use_tc_ = b; drop_graphs(); }
   void set_cg_f32(bool b) { cg_f32_ = b && mixed_; }
+  void set_gram(int g) {
+    if (g < 0 || g > 2) throw MgError(MG_ERR_ARG, "gram_precision must be 0 (BF16), 1 (FP16) or 2 (TF32)");
+    if (!mixed_ && g != 0) throw MgError(MG_ERR_ARG, "gram_precision applies to mixed mode");
+    gram_ = g;
+    drop_graphs();
+    initialised_ = false;
+  }
 
   std::string err;
 
@@ -1156,6 +1159,10 @@ class Context {
   // default: at tol 1e-6 the FP32 iteration needs about 1.5x the iterations of FP64, which
   // costs more than its halved gather traffic saves.
   bool cg_f32_ = false;
+  // Gram precision of the mixed samplers (option "gram_precision"): 0 BF16 gathers (the
+  // tensor-core sampler at K = 32), 1 FP16 gathers, 2 FP32 master rounded to TF32 as gathered;
+  // 1 and 2 run the CUDA-core sampler at every K
+  int gram_ = 0;
   int burnin_ = 50, nsamples_ = 400;
   ModeData md_[2];
   Prior prior_[2];
@@ -1418,6 +1425,7 @@ int mg_set_option(mg_ctx* ctx, const char* name, int value) {
     if (n == "graph") c.set_use_graph(value != 0);
     else if (n == "tensor_core_gram") c.set_use_tc(value != 0);
     else if (n == "cg_fp32") c.set_cg_f32(value != 0);
+    else if (n == "gram_precision") c.set_gram(value);
     else throw mg::MgError(MG_ERR_ARG, "unknown option " + n);
   });
 }

@@ -21,7 +21,12 @@ void launch_pad(const long long* ptr, const long long* pptr, long long nrows, co
                 unsigned sentinel, uint2* out, cudaStream_t s);
 
 // ---- latent sampler (sample_kernels.cu, gram_tc.cu) ----
-void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, int num_sms);
+// gram (mixed only): the Gram precision, 0 = BF16 gathers, 1 = FP16 gathers (p.other is the FP16
+// copy, p.half_copy set), 2 = TF32 (p.other is the FP32 master copy, rounded as it is read).
+void launch_sample(const SampleParams& p, int KP, bool mixed, int gram, cudaStream_t s,
+                   int num_sms);
+// dst[i] = src[i] rounded to BF16 (half = false) or FP16 (half = true), n values.
+void launch_copy16(const float* src, void* dst, long long n, bool half, cudaStream_t s);
 // Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only):
 // k_gram_tc, then (if nsplit > 0) k_sum_parts, then k_finish_tc (k_finish_one_tc when p.one).  It reads the 16-entry padded
 // packed CSR and its task list (p.packed / p.tasks, built by the context) and gathers the other

@@ -39,10 +39,22 @@ __device__ __forceinline__ void gsync(int g) {
   }
 }
 
-template <int KP, int WPR, bool MIXED>
+// Gather element of the mixed path (the Gram precision): BF16 (default), FP16, or FP32 rounded
+// to TF32 as it is read (the FP32 master copy, cvt.rna.tf32.f32).
+enum GatherElem : int { kGeBf16 = 0, kGeFp16 = 1, kGeTf32 = 2 };
+
+__device__ __forceinline__ float tf32_round(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+template <int KP, int WPR, bool MIXED, int GE = kGeBf16>
 struct Cfg {
   using Acc = typename std::conditional<MIXED, float, double>::type;
-  using Elem = typename std::conditional<MIXED, __nv_bfloat16, double>::type;
+  using Elem16 = typename std::conditional<GE == kGeFp16, __half, __nv_bfloat16>::type;
+  using ElemM = typename std::conditional<GE == kGeTf32, float, Elem16>::type;
+  using Elem = typename std::conditional<MIXED, ElemM, double>::type;
   static constexpr int T = 32 * WPR;
   static constexpr int S = WPR == 1 ? 1 : (WPR == 4 ? 2 : 4);
   static constexpr int GR = 8 * S, GC = 4 * S;
@@ -134,9 +146,9 @@ __device__ void add_noise(const SampleParams& p, F* rr, int row, int K, int t, i
 template <int WPR, bool MIXED>
 constexpr int min_ctas() { return WPR == 1 ? (MIXED ? 4 : 3) : 1; }
 
-template <int KP, int WPR, int G, bool MIXED>
+template <int KP, int WPR, int G, bool MIXED, int GE = kGeBf16>
 __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_sample(const SampleParams p) {
-  using C = Cfg<KP, WPR, MIXED>;
+  using C = Cfg<KP, WPR, MIXED, GE>;
   using Acc = typename C::Acc;
   using Elem = typename C::Elem;
   constexpr int T = C::T, GR = C::GR, GC = C::GC, TR = C::TR, TC = C::TC, LD = C::LD;
@@ -215,7 +227,21 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
         if (r < cnt) {
           const uint4 raw = __ldg(reinterpret_cast<const uint4*>(other + (size_t)cidx[r] * KP) + v);
           Acc* dst = gath + r * KP + v * C::EV;
-          if constexpr (MIXED) {
+          if constexpr (MIXED && GE == kGeTf32) {
+            const float4 f = *reinterpret_cast<const float4*>(&raw);
+            dst[0] = tf32_round(f.x);
+            dst[1] = tf32_round(f.y);
+            dst[2] = tf32_round(f.z);
+            dst[3] = tf32_round(f.w);
+          } else if constexpr (MIXED && GE == kGeFp16) {
+            const __half2* h = reinterpret_cast<const __half2*>(&raw);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+              const float2 f = __half22float2(h[q]);
+              dst[2 * q] = f.x;
+              dst[2 * q + 1] = f.y;
+            }
+          } else if constexpr (MIXED) {
             const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&raw);
 #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -309,7 +335,7 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
         if (lane < K) {
           if constexpr (MIXED) {
             p.out_f32[(size_t)row * KP + lane] = (float)un;
-            p.out_bf16[(size_t)row * KP + lane] = __float2bfloat16_rn((float)un);
+            store_copy(p, (size_t)row * KP + lane, (float)un);
           } else {
             p.out_f64[(size_t)row * KP + lane] = un;
           }
@@ -342,7 +368,7 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
                                                 KP + 4, z);
           if (lane < K) {
             p.out_f32[(size_t)row * KP + lane] = x;
-            p.out_bf16[(size_t)row * KP + lane] = __float2bfloat16_rn(x);
+            store_copy(p, (size_t)row * KP + lane, x);
           }
         } else if (lane == 0) {
           atomicAdd(&p.ctl->retries[p.mode], 1u);
@@ -402,7 +428,7 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
       if (t < K) {
         if constexpr (MIXED) {
           p.out_f32[(size_t)row * KP + t] = (float)u;
-          p.out_bf16[(size_t)row * KP + t] = __float2bfloat16_rn((float)u);
+          store_copy(p, (size_t)row * KP + t, (float)u);
         } else {
           p.out_f64[(size_t)row * KP + t] = u;
         }
@@ -441,7 +467,7 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
         back_solve<float, T>(M, LD, rr, K, t, g);
         if (t < K) {
           p.out_f32[(size_t)row * KP + t] = rr[t];
-          p.out_bf16[(size_t)row * KP + t] = __float2bfloat16_rn(rr[t]);
+          store_copy(p, (size_t)row * KP + t, rr[t]);
         }
       } else if (t == 0) {
         atomicAdd(&p.ctl->retries[p.mode], 1u);
@@ -471,7 +497,7 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
         if (t < K) {
           if constexpr (MIXED) {
             p.out_f32[(size_t)row * KP + t] = (float)rr[t];
-            p.out_bf16[(size_t)row * KP + t] = __float2bfloat16_rn((float)rr[t]);
+            store_copy(p, (size_t)row * KP + t, (float)rr[t]);
           } else {
             p.out_f64[(size_t)row * KP + t] = rr[t];
           }
@@ -485,10 +511,10 @@ __global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_samp
   }
 }
 
-template <int KP, int WPR, int G, bool MIXED>
+template <int KP, int WPR, int G, bool MIXED, int GE = kGeBf16>
 void launch_t(const SampleParams& p, cudaStream_t s, int num_sms) {
-  using C = Cfg<KP, WPR, MIXED>;
-  auto kern = k_sample<KP, WPR, G, MIXED>;
+  using C = Cfg<KP, WPR, MIXED, GE>;
+  auto kern = k_sample<KP, WPR, G, MIXED, GE>;
   const size_t smem = C::kCtaBytes + C::kGroupBytes * G;
   static int per_sm_cache[64] = {0};  // per template instance and device
   int dev = 0;
@@ -507,17 +533,26 @@ void launch_t(const SampleParams& p, cudaStream_t s, int num_sms) {
   MG_CUDA(cudaGetLastError());
 }
 
+template <int GE>
+void launch_mixed(const SampleParams& p, int KP, cudaStream_t s, int num_sms) {
+  switch (KP) {
+    case 8: return launch_t<8, 1, 4, true, GE>(p, s, num_sms);
+    case 16: return launch_t<16, 1, 4, true, GE>(p, s, num_sms);
+    case 32: return launch_t<32, 1, 4, true, GE>(p, s, num_sms);
+    case 64: return launch_t<64, 4, 2, true, GE>(p, s, num_sms);
+    case 128: return launch_t<128, 16, 1, true, GE>(p, s, num_sms);
+  }
+  throw MgError(MG_ERR_ARG, "unsupported latent dimension");
+}
+
 }  // namespace
 
-void launch_sample(const SampleParams& p, int KP, bool mixed, cudaStream_t s, int num_sms) {
+void launch_sample(const SampleParams& p, int KP, bool mixed, int gram, cudaStream_t s,
+                   int num_sms) {
   if (mixed) {
-    switch (KP) {
-      case 8: return launch_t<8, 1, 4, true>(p, s, num_sms);
-      case 16: return launch_t<16, 1, 4, true>(p, s, num_sms);
-      case 32: return launch_t<32, 1, 4, true>(p, s, num_sms);
-      case 64: return launch_t<64, 4, 2, true>(p, s, num_sms);
-      case 128: return launch_t<128, 16, 1, true>(p, s, num_sms);
-    }
+    if (gram == kGeFp16) return launch_mixed<kGeFp16>(p, KP, s, num_sms);
+    if (gram == kGeTf32) return launch_mixed<kGeTf32>(p, KP, s, num_sms);
+    return launch_mixed<kGeBf16>(p, KP, s, num_sms);
   } else {
     switch (KP) {
       case 8: return launch_t<8, 1, 4, false>(p, s, num_sms);

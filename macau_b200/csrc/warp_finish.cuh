@@ -305,7 +305,7 @@ __device__ __forceinline__ bool warp_finish_f64_body(const GT* Gs, int ld, const
       p.out_f64[(size_t)row * KP + lane] = x;
     } else {
       p.out_f32[(size_t)row * KP + lane] = (float)x;
-      p.out_bf16[(size_t)row * KP + lane] = __float2bfloat16_rn((float)x);
+      store_copy(p, (size_t)row * KP + lane, (float)x);
     }
   }
   return true;

@@ -50,7 +50,10 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=0, help="sweeps of the e2e run (0: = steps)")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the side-information legs (Macau block-CG and univariate priors)")
-    ap.add_argument("--only", choices=["all", "mixed", "fp64", "macau", "univariate"], default="all",
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the Gram precision sweep on the 2,000 x 1,500 matrix")
+    ap.add_argument("--only", choices=["all", "mixed", "fp64", "macau", "univariate", "precision"],
+                    default="all",
                     help="profiling runs: time one sampler and print its phase times only")
     return ap.parse_args()
 
@@ -212,6 +215,61 @@ def side_info_legs(device, sweeps=20, cpu_sweeps=2):
     return out
 
 
+def precision_sweep(device, Ks=(16, 64, 128), burnin=100, nsamples=100):
+    """The Gram precision sweep on the 2,000 x 1,500 uniform matrix (60,000 entries, 10% holdout,
+    alpha = 4): for each K and Gram input precision (FP64 path; mixed with BF16, FP16 or TF32
+    inputs, FP32 accumulation and factor, FP64 retry), the per-row sample error against the
+    FP64 sampler under identical keyed draws from one common state, the retry rate of that
+    half-sweep, and the test RMSE after burnin + nsamples sweeps from the initial state."""
+    from macau_b200 import _lib, workloads
+    w = workloads.bpmf_uniform()
+    alpha = 4.0
+    variants = (("fp64", _lib.MG_COMPUTE_FP64, 0), ("bf16", _lib.MG_COMPUTE_MIXED, 0),
+                ("fp16", _lib.MG_COMPUTE_MIXED, 1), ("tf32", _lib.MG_COMPUTE_MIXED, 2))
+    out = {"workload": w["name"], "alpha": alpha, "burnin": burnin, "nsamples": nsamples,
+           "error": "max |u - u_fp64| / max |u_fp64| over the rows of one mode-0 half-sweep",
+           "results": {}}
+
+    def sampler(K, comp, g):
+        s = _lib.Sampler(K, alpha, seed=11, compute=comp, device=device)
+        s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
+        s.set_relation_data_test(w["trows"], w["tcols"], w["tvals"], w["shape"])
+        if comp == _lib.MG_COMPUTE_MIXED:
+            s.set_option("gram_precision", g)
+        s.set_samples(burnin, nsamples)
+        s.init()
+        return s
+
+    for K in Ks:
+        rng = np.random.default_rng(K)
+        V = rng.normal(scale=0.3, size=(w["shape"][1], K))
+        mu = rng.normal(scale=0.1, size=K)
+        A = rng.normal(size=(K, K))
+        Lam = 2.0 * (A @ A.T / K + np.eye(K))
+        res, ref = {}, None
+        for name, comp, g in variants:
+            s = sampler(K, comp, g)
+            s.set_latents(1, V)
+            s.set_hyper(0, mu, Lam, None)
+            s.sample_latents(0, 0)
+            U = s.latents(0)
+            st = s.stats()
+            s.close()
+            if ref is None:
+                ref = U
+            s = sampler(K, comp, g)
+            s.sweeps(0, burnin + nsamples, eval=True)
+            rmse = s.rmse()[0]
+            s.close()
+            res[name] = {"sample_error": float(np.abs(U - ref).max() / np.abs(ref).max()),
+                         "retry_rate": st["retries"][0] / max(1, w["shape"][0]),
+                         "test_rmse": rmse}
+        for name in res:
+            res[name]["rmse_minus_fp64"] = res[name]["test_rmse"] - res["fp64"]["test_rmse"]
+        out["results"][f"K={K}"] = res
+    return out
+
+
 def peaks():
     try:
         d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -333,6 +391,11 @@ def run_ours(args):
 
     seed = ranks.chain_seed()
     K, W = args.steps, args.warmup
+    if args.only == "precision":
+        print(json.dumps({"only": "precision", "precision_sweep": precision_sweep(local)}),
+              flush=True)
+        ranks.close()
+        return 0
     if args.only in ("macau", "univariate"):
         # one side-information sampler (FP64) on the Macau workload, for profiling
         from macau_b200 import workloads
@@ -467,6 +530,8 @@ def run_ours(args):
                     "split_s": e2e_split}}
     if rank == 0 and world == 1 and not args.no_side:
         line["side_info"] = side_info_legs(local)
+    if rank == 0 and world == 1 and not args.no_precision:
+        line["precision_sweep"] = precision_sweep(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds, 50)
         line["mixed_over_cpu"] = v_mx / line["cpu_baseline"]["value"]

@@ -552,6 +552,31 @@ def test_macau_mixed_cg_precision_option():
     assert relerr(betas[1], betas[0]) < 2e-2
 
 
+@pytest.mark.parametrize("K", [16, 32, 64])
+@pytest.mark.parametrize("gram", [1, 2])
+def test_mixed_row_sampler_fp16_tf32_grams(K, gram):
+    # Gram inputs in FP16 (1) or TF32 (2) instead of BF16: the CUDA-core sampler at every K
+    # (K = 32 included), against the FP64 oracle under the same keyed draws; TF32 and FP16 keep
+    # 10-11 mantissa bits against BF16's 8, so their error stays below the BF16 run's
+    rng = np.random.default_rng(K + 50 * gram)
+    w = small_uniform(seed=5, nrow=400, ncol=250, nobs=15000)
+    Vo = rng.normal(scale=0.3, size=(w["shape"][1], K))
+    Y = train_matrix(w)
+    errs = []
+    for g in (0, gram):
+        s = gpu_sampler(w, K, 2.0, seed=4242, compute=_lib.MG_COMPUTE_MIXED, init=False)
+        s.set_option("gram_precision", g)
+        s.init()
+        s.set_latents(1, Vo)
+        mu, Lam, _ = s.hyper(0)
+        s.sample_latents(0, 9)
+        want, _ = orc.sample_latents(K, orc.Csr.from_scipy(Y), Vo, s.mean_value(), 2.0, mu, Lam,
+                                     seed=4242, sweep=9, mode=0)
+        errs.append(relerr(s.latents(0), want))
+    assert errs[1] < MIXED_SAMPLE_TOL
+    assert errs[1] < errs[0], errs
+
+
 def test_cholesky_failure_is_reported_and_context_survives():
     w = small_uniform(seed=4)
     K = 6

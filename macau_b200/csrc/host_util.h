@@ -1,0 +1,78 @@
+// Host-side helpers shared by the library's contexts: a device buffer owning one cudaMalloc,
+// and the work split of CSR rows into sampler tasks.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mg {
+
+// Host<->device byte counters of the current process (defined in context.cu).
+extern long long g_h2d_bytes;
+extern long long g_d2h_bytes;
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    reset();
+    if (count == 0) count = 1;
+    MG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void alloc_zero(size_t count, cudaStream_t s) {
+    alloc(count);
+    MG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) MG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    g_h2d_bytes += (long long)(count * sizeof(T));
+  }
+};
+
+// Task list over rows with lengths len(r) = ptr[r+1] - ptr[r] (positions ptr[r]): rows longer
+// than `thr` are cut into near-equal parts whose boundaries are multiples of `align` entries
+// (relative to the row start); tasks sorted by descending length (stable).
+inline std::vector<RowTask> make_tasks(const std::vector<long long>& ptr, long long thr,
+                                       int align, int& nsplit, int& nslots) {
+  const long long n = (long long)ptr.size() - 1;
+  std::vector<RowTask> tasks;
+  tasks.reserve(n + 16);
+  nsplit = 0;
+  nslots = 0;
+  for (long long r = 0; r < n; r++) {
+    const long long len = ptr[r + 1] - ptr[r];
+    if (len <= thr) {
+      tasks.push_back(RowTask{ptr[r], (int)r, (int)len, 0, 1, 0, 0});
+      continue;
+    }
+    const long long units = (len + align - 1) / align;
+    const int parts = (int)((len + thr - 1) / thr);
+    for (int q = 0; q < parts; q++) {
+      const long long b = std::min(len, align * (units * q / parts));
+      const long long e = std::min(len, align * (units * (q + 1) / parts));
+      tasks.push_back(RowTask{ptr[r] + b, (int)r, (int)(e - b), q, parts, nslots, nsplit});
+    }
+    nslots += parts;
+    nsplit++;
+  }
+  std::stable_sort(tasks.begin(), tasks.end(),
+                   [](const RowTask& a, const RowTask& b) { return a.len > b.len; });
+  return tasks;
+}
+
+}  // namespace mg

@@ -485,18 +485,19 @@ __device__ __forceinline__ void stats_load(const T* U, const double* Uhat, long 
   }
 }
 
+// One block's statistics over rows r0 .. r1 - 1 into out[0 .. K + K*K) (shared by k_stats32 and
+// the batched k_stats32_batch).
 template <typename T>
-__global__ void __launch_bounds__(kStatThreads)
-    k_stats32(const T* __restrict__ U, const double* __restrict__ Uhat, long long N, int K,
-              int stride, int uhat_stride, long long rows_per_block, double* __restrict__ partials) {
+__device__ __forceinline__ void stats32_rows(const T* __restrict__ U,
+                                             const double* __restrict__ Uhat, long long r0,
+                                             long long r1, int K, int stride, int uhat_stride,
+                                             double* __restrict__ out) {
   static_assert(kStatRows * 32 == 4 * kStatThreads, "four staged values per thread");
   __shared__ __align__(16) double xs[2][kStatRows][36];
   __shared__ double red[3][64][17];
   const int KK = K * K;
   const int t = threadIdx.x, tile = t & 63, rg = t >> 6;
   const int ti = tile >> 3, tj = tile & 7;
-  const long long r0 = (long long)blockIdx.x * rows_per_block;
-  const long long r1 = min(N, r0 + rows_per_block);
   double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; a++)
@@ -542,7 +543,6 @@ __global__ void __launch_bounds__(kStatThreads)
 #pragma unroll
       for (int b = 0; b < 4; b++) red[rg - 1][tile][a * 4 + b] = acc[a][b];
   __syncthreads();
-  double* out = partials + (size_t)blockIdx.x * (K + KK);
   if (t < K) out[t] = su;
   if (rg == 0) {
 #pragma unroll
@@ -555,6 +555,15 @@ __global__ void __launch_bounds__(kStatThreads)
         if (i < K && j < K) out[K + i + j * K] = v;
       }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kStatThreads)
+    k_stats32(const T* __restrict__ U, const double* __restrict__ Uhat, long long N, int K,
+              int stride, int uhat_stride, long long rows_per_block, double* __restrict__ partials) {
+  const long long r0 = (long long)blockIdx.x * rows_per_block;
+  stats32_rows(U, Uhat, r0, min(N, r0 + rows_per_block), K, stride, uhat_stride,
+               partials + (size_t)blockIdx.x * (K + K * K));
 }
 
 // Sums `nparts` partial records of `len` doubles in a fixed order: CTA c owns elements
@@ -593,12 +602,15 @@ __global__ void __launch_bounds__(256)
 constexpr int kNwLd = 33;
 constexpr int kNwLc = 36;
 
-__global__ void __launch_bounds__(256)
-    k_nw32(const double* __restrict__ partials, int nparts, long long N, int K,
-           const double* __restrict__ mu0, double kappa, const double* __restrict__ T0, int nu,
-           const double* __restrict__ bb_partials, int bb_nparts,
-           const double* __restrict__ lambda_beta, Ctl* ctl, unsigned long long seed, int mode,
-           double* __restrict__ mu_out, double* __restrict__ Lambda_out) {
+// T0 == null stands for the identity.
+__device__ __forceinline__ void nw32_run(const double* __restrict__ partials, int nparts,
+                                         long long N, int K, const double* __restrict__ mu0,
+                                         double kappa, const double* __restrict__ T0, int nu,
+                                         const double* __restrict__ bb_partials, int bb_nparts,
+                                         const double* __restrict__ lambda_beta, Ctl* ctl,
+                                         unsigned long long seed, int mode,
+                                         double* __restrict__ mu_out,
+                                         double* __restrict__ Lambda_out) {
   __shared__ double A[32 * kNwLd], Bm[32 * kNwLd], C[32 * kNwLd], D[32 * kNwLd];
   __shared__ __align__(16) double Lc[32 * kNwLc];
   __shared__ double NU[32], muc[32], m0[32], rl[32], zs[32];
@@ -637,12 +649,13 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int e = t + 256 * q;
-      if (e < KK) Bm[(e % K) * kNwLd + e / K] = T0[e] + lb * sv[q];
+      if (e < KK) Bm[(e % K) * kNwLd + e / K] = (T0 ? T0[e] : (e % K == e / K ? 1.0 : 0.0)) + lb * sv[q];
     }
   } else {
-    for (int e = t; e < KK; e += blockDim.x) Bm[(e % K) * kNwLd + e / K] = T0[e];
+    for (int e = t; e < KK; e += blockDim.x)
+      Bm[(e % K) * kNwLd + e / K] = T0 ? T0[e] : (e % K == e / K ? 1.0 : 0.0);
   }
-  if (t < K) m0[t] = mu0[t];
+  if (t < K) m0[t] = mu0 ? mu0[t] : 0.0;
   __syncthreads();
   const double kappa_c = kappa + (double)N;
   const int nu_c = nu + (int)N;
@@ -733,6 +746,16 @@ __global__ void __launch_bounds__(256)
     }
     if (lane < K) mu_out[lane] = x + muc[lane];
   }
+}
+
+__global__ void __launch_bounds__(256)
+    k_nw32(const double* __restrict__ partials, int nparts, long long N, int K,
+           const double* __restrict__ mu0, double kappa, const double* __restrict__ T0, int nu,
+           const double* __restrict__ bb_partials, int bb_nparts,
+           const double* __restrict__ lambda_beta, Ctl* ctl, unsigned long long seed, int mode,
+           double* __restrict__ mu_out, double* __restrict__ Lambda_out) {
+  nw32_run(partials, nparts, N, K, mu0, kappa, T0, nu, bb_partials, bb_nparts, lambda_beta, ctl,
+           seed, mode, mu_out, Lambda_out);
 }
 
 }  // namespace

@@ -188,6 +188,39 @@ int mg_get_stds(mg_ctx* ctx, double* out);
 int mg_get_test_data(mg_ctx* ctx, double* out);
 int mg_get_stats(mg_ctx* ctx, mg_stats* out);
 
+/* ---- Many independent BPMF chains in one set of launches ----
+ * P problems, each what `macau.bpmf(Y_p, Ytest_p, num_latent=K_p, precision=precision)` runs
+ * (MacauX with two BPMF priors, macau.cpp:110-147, latentprior.cpp:69-99), sampled together in
+ * mixed precision (BF16 tensor-core Grams, FP32 Cholesky with FP64 retry, FP64 hyperpriors):
+ * each sweep is one captured CUDA graph with one Gram launch and one finish launch per mode for
+ * all problems.  Problem p uses seed seeds[p] and its local row / column indices for its keyed
+ * draws, so its chain draws what a single context with that seed draws.  K_p <= 32.  The
+ * reference has no batched form; it runs one Macau object per problem. */
+typedef struct mg_batch mg_batch;
+int mg_batch_create(mg_batch** out, int nprob, const int32_t* nrows, const int32_t* ncols,
+                    const int32_t* num_latent, const uint64_t* seeds, double precision,
+                    int device);
+void mg_batch_destroy(mg_batch* b);
+const char* mg_batch_last_error(const mg_batch* b);
+/* Problem p's train entries are rows / cols / vals[train_off[p] .. train_off[p + 1]) in its own
+ * indices (duplicates summed), its test entries trows / tcols / tvals[test_off[p] ..
+ * test_off[p + 1]). */
+int mg_batch_set_data(mg_batch* b, const int64_t* train_off, const int32_t* rows,
+                      const int32_t* cols, const double* vals, const int64_t* test_off,
+                      const int32_t* trows, const int32_t* tcols, const double* tvals);
+/* MacauX::init for every problem (latents zero, mu = 0, Lambda = 10 I); evaluation averages the
+ * sweeps from `burnin` on. */
+int mg_batch_init(mg_batch* b, int burnin);
+int mg_batch_sweeps(mg_batch* b, int first_iter, int count, int eval);
+/* Device time of `count` sweeps without evaluation (CUDA events on the batch's stream). */
+int mg_batch_time_sweeps(mg_batch* b, int first_iter, int count, double* seconds);
+/* Problem `prob`'s latents of `mode` (nrows_p x K_p row-major, i.e. K_p x N column-major). */
+int mg_batch_get_latents(mg_batch* b, int prob, int mode, double* out);
+/* out[2 p] = posterior-mean test RMSE of problem p, out[2 p + 1] = single-sample RMSE. */
+int mg_batch_get_rmse(mg_batch* b, double* out);
+/* out[0..4] = total rows, total columns, total train entries, FP64 retries in mode 0 and 1. */
+int mg_batch_get_info(mg_batch* b, int64_t* out);
+
 /* Switches of the implementation (no reference counterpart):
  *   "graph"            (default 1) replay captured CUDA graphs for sweeps without host-side
  *                      decisions

@@ -84,6 +84,16 @@ _SIGS = {
     "mg_set_option": (_i, [_p, C.c_char_p, _i]),
     "mg_blockcg": (_i, [_p, _p, _p, _i64, _i, _i, _p, _i, _d, _d, _i, _p, C.POINTER(_i),
                         C.POINTER(_d)]),
+    "mg_batch_create": (_i, [C.POINTER(_p), _i, _p, _p, _p, _p, _d, _i]),
+    "mg_batch_destroy": (None, [_p]),
+    "mg_batch_last_error": (C.c_char_p, [_p]),
+    "mg_batch_set_data": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "mg_batch_init": (_i, [_p, _i]),
+    "mg_batch_sweeps": (_i, [_p, _i, _i, _i]),
+    "mg_batch_time_sweeps": (_i, [_p, _i, _i, C.POINTER(_d)]),
+    "mg_batch_get_latents": (_i, [_p, _i, _i, _p]),
+    "mg_batch_get_rmse": (_i, [_p, _p]),
+    "mg_batch_get_info": (_i, [_p, _p]),
     "mg_normal_wishart_noalloc": (_i, [_p, _i64, _i, _i, _p, _d, _p, _i, C.c_uint64, C.c_uint32,
                                        _i, _p, _p, _p, C.c_char_p, _i]),
 }
@@ -305,6 +315,80 @@ class Sampler:
                 "graph_captured": bool(st.graph_captured),
                 "kernel_launches": int(st.kernel_launches), "h2d_bytes": int(st.h2d_bytes),
                 "d2h_bytes": int(st.d2h_bytes), "ntasks": list(st.ntasks), "nnz": list(st.nnz)}
+
+
+class Batch:
+    """Many independent BPMF chains sampled together (mg_batch): problem p is the matrix
+    problems[p] = dict(rows, cols, vals, trows, tcols, tvals, shape) with latent dimension
+    num_latent[p] <= 32 and seed seeds[p]; mixed precision."""
+
+    def __init__(self, problems, num_latent, seeds, precision, device=0):
+        P = len(problems)
+        self.P = P
+        self.K = [int(k) for k in num_latent]
+        self.shapes = [tuple(int(x) for x in pr["shape"]) for pr in problems]
+        nr = np.array([s[0] for s in self.shapes], np.int32)
+        nc = np.array([s[1] for s in self.shapes], np.int32)
+        kk = np.array(self.K, np.int32)
+        sd = np.array([int(x) & (2**64 - 1) for x in seeds], np.uint64)
+        h = _p()
+        code = lib().mg_batch_create(C.byref(h), P, ptr(nr), ptr(nc), ptr(kk), ptr(sd),
+                                     float(precision), int(device))
+        if code != 0:
+            raise MacauError(code, lib().mg_batch_last_error(None).decode())
+        self.h = h
+
+        def cat(key, dtype):
+            return np.ascontiguousarray(np.concatenate([np.asarray(pr[key], dtype) for pr in problems]))
+
+        def offs(key):
+            return np.concatenate([[0], np.cumsum([len(pr[key]) for pr in problems])]).astype(np.int64)
+
+        a = [cat("rows", np.int32), cat("cols", np.int32), cat("vals", np.float64),
+             cat("trows", np.int32), cat("tcols", np.int32), cat("tvals", np.float64)]
+        to, eo = offs("vals"), offs("tvals")
+        self._chk(lib().mg_batch_set_data(self.h, ptr(to), ptr(a[0]), ptr(a[1]), ptr(a[2]),
+                                          ptr(eo), ptr(a[3]), ptr(a[4]), ptr(a[5])))
+
+    def _chk(self, code):
+        if code != 0:
+            cls = CholeskyError if code == -2 else MacauError
+            raise cls(code, lib().mg_batch_last_error(self.h).decode())
+
+    def init(self, burnin=0):
+        self._chk(lib().mg_batch_init(self.h, int(burnin)))
+
+    def sweeps(self, first, count, eval=True):
+        self._chk(lib().mg_batch_sweeps(self.h, int(first), int(count), int(bool(eval))))
+
+    def time_sweeps(self, first, count):
+        sec = C.c_double(0.0)
+        self._chk(lib().mg_batch_time_sweeps(self.h, int(first), int(count), C.byref(sec)))
+        return sec.value
+
+    def latents(self, p, mode):
+        out = np.zeros((self.shapes[p][mode], self.K[p]))
+        self._chk(lib().mg_batch_get_latents(self.h, int(p), int(mode), ptr(out)))
+        return out
+
+    def rmse(self):
+        out = np.zeros(2 * self.P)
+        self._chk(lib().mg_batch_get_rmse(self.h, ptr(out)))
+        return out.reshape(self.P, 2)
+
+    def info(self):
+        out = np.zeros(5, np.int64)
+        self._chk(lib().mg_batch_get_info(self.h, ptr(out)))
+        return dict(rows=int(out[0]), cols=int(out[1]), nnz=int(out[2]),
+                    retries=[int(out[3]), int(out[4])])
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def blockcg_raw(rows, cols, vals, shape, B, reg, tol, compute=MG_COMPUTE_FP64):

@@ -780,19 +780,15 @@ __global__ void __launch_bounds__(256)
 
 size_t tc_smem_bytes() { return (size_t)kStages * kStageBytes + sizeof(TcShared); }
 
-bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
-                      int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
+bool launch_gram_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
+                    int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
   if (KP != 32 || p.packed == nullptr) return false;
   static bool configured[64] = {false};
   int dev = 0;
   MG_CUDA(cudaGetDevice(&dev));
   const size_t smem = tc_smem_bytes();
-  const size_t fsmem = sizeof(double) * (32 * 33 + 32) + sizeof(float) * 32 * kLc +
-                       (size_t)kFinWarps * kFinWork;
   if (!configured[dev & 63]) {
     MG_CUDA(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    MG_CUDA(cudaFuncSetAttribute(k_finish_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)fsmem));
     configured[dev & 63] = true;
   }
   k_gram_tc<<<num_sms, kTcThreads, smem, s>>>(p, gram);
@@ -802,6 +798,23 @@ bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows
     k_sum_parts<<<(nsplit + 7) / 8, 256, 0, s>>>(p.scratch, split_rows, nsplit, gram);
     MG_CUDA(cudaGetLastError());
   }
+  return true;
+}
+
+bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
+                      int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
+  if (KP != 32 || p.packed == nullptr) return false;
+  static bool configured[64] = {false};
+  int dev = 0;
+  MG_CUDA(cudaGetDevice(&dev));
+  const size_t fsmem = sizeof(double) * (32 * 33 + 32) + sizeof(float) * 32 * kLc +
+                       (size_t)kFinWarps * kFinWork;
+  if (!configured[dev & 63]) {
+    MG_CUDA(cudaFuncSetAttribute(k_finish_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)fsmem));
+    configured[dev & 63] = true;
+  }
+  launch_gram_tc(p, gram, split_rows, nsplit, KP, s, num_sms, mid);
   if (p.one)
     k_finish_one_tc<<<num_sms * 8, 256, 0, s>>>(p, gram);
   else

@@ -799,6 +799,37 @@ void launch_stats(const void* U, bool f32, const double* Uhat, long long N, int 
 #undef MG_STATS
 }
 
+// ---- batched problems (batch.cu): one statistics block and one Normal-Wishart block per
+// problem; problem p owns rows row0[p] .. row0[p + 1] - 1 of U (stride 32), K = Kp[p] ----
+__global__ void __launch_bounds__(kStatThreads)
+    k_stats_batch(const float* __restrict__ U, const int* __restrict__ row0,
+                  const int* __restrict__ Kp, double* __restrict__ partials) {
+  const int p = blockIdx.x;
+  stats32_rows<float>(U, nullptr, row0[p], row0[p + 1], Kp[p], 32, 0,
+                      partials + (size_t)p * (32 + 32 * 32));
+}
+
+// BPMFPrior::update_prior per problem with mu0 = 0, b0 = 2, W0 = I, df = K_p
+// (latentprior.cpp:79-99), keyed with the problem's seed.
+__global__ void __launch_bounds__(256)
+    k_nw_batch(const double* __restrict__ partials, const int* __restrict__ row0,
+               const int* __restrict__ Kp, const unsigned long long* __restrict__ seed, Ctl* ctl,
+               int mode, double* __restrict__ mu, double* __restrict__ Lambda) {
+  const int p = blockIdx.x;
+  nw32_run(partials + (size_t)p * (32 + 32 * 32), 1, row0[p + 1] - row0[p], Kp[p], nullptr, 2.0,
+           nullptr, Kp[p], nullptr, 0, nullptr, ctl, seed[p], mode, mu + (size_t)p * 32,
+           Lambda + (size_t)p * 1024);
+}
+
+void launch_prior_batch(const float* U, const int* row0, const int* Kp,
+                        const unsigned long long* seed, int P, double* partials, Ctl* ctl, int mode,
+                        double* mu, double* Lambda, cudaStream_t s) {
+  k_stats_batch<<<P, kStatThreads, 0, s>>>(U, row0, Kp, partials);
+  MG_CUDA(cudaGetLastError());
+  k_nw_batch<<<P, 256, 0, s>>>(partials, row0, Kp, seed, ctl, mode, mu, Lambda);
+  MG_CUDA(cudaGetLastError());
+}
+
 void launch_reduce_parts(const double* parts, int nparts, int len, double* out, cudaStream_t s) {
   k_reduce_parts<<<(len + 31) / 32, 256, 0, s>>>(parts, nparts, len, out);
   MG_CUDA(cudaGetLastError());

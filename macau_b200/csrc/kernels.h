@@ -38,6 +38,10 @@ void launch_copy16(const float* src, void* dst, long long n, bool half, cudaStre
 // (per-kernel timing).
 bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
                       int KP, cudaStream_t s, int num_sms, cudaEvent_t mid = nullptr);
+// The Gram half of launch_sample_tc: k_gram_tc (+ k_sum_parts), no finish.  Returns false when
+// the configuration is not covered.
+bool launch_gram_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
+                    int KP, cudaStream_t s, int num_sms, cudaEvent_t mid = nullptr);
 
 // ---- hyperprior / eval (hyper_kernels.cu) ----
 struct NwWork {
@@ -75,6 +79,12 @@ void launch_noise_update(const int* erow, const int* col, const double* val, lon
                          const void* U, const void* V, bool f32, int K, int stride, double mean,
                          double var_total, double alpha_max, double* partials, int nblocks,
                          Ctl* ctl, unsigned long long seed, cudaStream_t s);
+// Batched problems: per problem p (rows row0[p] .. row0[p + 1] - 1 of U, stride 32, K = Kp[p]),
+// the statistics into partials + 1056 p, then the Normal-Wishart draw into mu + 32 p and
+// Lambda + 1024 p (K x K), keyed with seed[p].
+void launch_prior_batch(const float* U, const int* row0, const int* Kp,
+                        const unsigned long long* seed, int P, double* partials, Ctl* ctl, int mode,
+                        double* mu, double* Lambda, cudaStream_t s);
 void launch_set_sweep(Ctl* ctl, uint32_t sweep, int burnin, cudaStream_t s);
 void launch_advance(Ctl* ctl, cudaStream_t s);
 

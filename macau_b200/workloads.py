@@ -132,3 +132,33 @@ def macau_side(nrow=20000, ncol=500, nobs=1_000_000, nfeat=32768, rank=32, ones=
     return dict(rows=tr[0], cols=tr[1], vals=tr[2], trows=tr[3], tcols=tr[4], tvals=tr[5],
                 shape=(nrow, ncol), side=(fr, fc, None, (nrow, nfeat)),
                 name=f"macau_side {nrow}x{ncol} nnz={nobs} F={nrow}x{nfeat} nnzF={len(fr)}")
+
+
+def batched_uneven(nprob=512, seed0=5000, holdout=0.1, rows=(200, 4000), cols=(100, 1000),
+                   density=(0.01, 0.05), ks=(8, 16, 32), noise=0.5):
+    """Many independent BPMF problems of uneven size: problem i (numpy seed seed0 + i) has
+    U[rows] x U[cols] entries at density U[density] (unique random positions), latent dimension
+    drawn from ks, values rank-K U V^T + N(0, noise^2) with U, V ~ N(0, 1/sqrt(K)), and a random
+    holdout.  Returns (problems, num_latent, seeds)."""
+    problems, Ks, seeds = [], [], []
+    for i in range(nprob):
+        rng = np.random.default_rng(seed0 + i)
+        nr = int(rng.integers(rows[0], rows[1] + 1))
+        nc = int(rng.integers(cols[0], cols[1] + 1))
+        dens = float(rng.uniform(density[0], density[1]))
+        K = int(rng.choice(ks))
+        want = max(16, int(nr * nc * dens))
+        pos = np.unique(rng.integers(0, nr * nc, size=int(want * 1.1) + 16))
+        pos = rng.permutation(pos)[:want]
+        r = (pos // nc).astype(np.int32)
+        c = (pos % nc).astype(np.int32)
+        sd = 1.0 / np.sqrt(K)
+        U = rng.normal(0.0, sd, size=(nr, K))
+        V = rng.normal(0.0, sd, size=(nc, K))
+        v = np.sum(U[r] * V[c], axis=1) + rng.normal(0.0, noise, size=len(r))
+        tr = _holdout(rng, r, c, v, holdout)
+        problems.append(dict(rows=tr[0], cols=tr[1], vals=tr[2], trows=tr[3], tcols=tr[4],
+                             tvals=tr[5], shape=(nr, nc)))
+        Ks.append(K)
+        seeds.append(seed0 + i)
+    return problems, Ks, seeds

@@ -577,6 +577,44 @@ def test_mixed_row_sampler_fp16_tf32_grams(K, gram):
     assert errs[1] < errs[0], errs
 
 
+# ---- many independent chains in one set of launches (mg_batch) ----
+
+def test_batch_matches_single_problem_contexts():
+    # each problem of the batch follows the chain of a single mixed context with its seed
+    # (same keyed draws; the Gram sums differ only in order), and its RMSE matches
+    problems, Ks, seeds = workloads.batched_uneven(nprob=7, rows=(40, 300), cols=(30, 200),
+                                                   density=(0.05, 0.2))
+    alpha, sweeps, burnin = 4.0, 4, 2
+    b = _lib.Batch(problems, Ks, seeds, alpha)
+    b.init(burnin)
+    b.sweeps(0, sweeps, eval=True)
+    rb = b.rmse()
+    assert b.info()["nnz"] == sum(len(pr["vals"]) for pr in problems)
+    for p, (pr, K, sd) in enumerate(zip(problems, Ks, seeds)):
+        s = gpu_sampler(pr, K, alpha, sd, compute=_lib.MG_COMPUTE_MIXED, burnin=burnin,
+                        nsamples=sweeps - burnin)
+        for it in range(sweeps):
+            s.sweep(it, eval=True)
+        for mode in (0, 1):
+            assert relerr(b.latents(p, mode), s.latents(mode)) < 1e-3, (p, mode)
+        r, r1 = s.rmse()
+        assert abs(rb[p, 0] - r) < 1e-4 and abs(rb[p, 1] - r1) < 1e-4, (p, rb[p], r, r1)
+    b.close()
+
+
+def test_batch_learns_every_problem():
+    problems, Ks, seeds = workloads.batched_uneven(nprob=24, rows=(200, 600), cols=(100, 300),
+                                                   density=(0.05, 0.1))
+    b = _lib.Batch(problems, Ks, seeds, 4.0)
+    b.init(30)
+    b.sweeps(0, 60, eval=True)
+    rm = b.rmse()
+    # the data noise is 0.5: every problem's posterior-mean RMSE lands near it
+    assert np.all(rm[:, 0] < 0.75), rm[:, 0]
+    assert rm[:, 0].mean() < rm[:, 1].mean()  # averaging over samples helps on the whole
+    b.close()
+
+
 def test_cholesky_failure_is_reported_and_context_survives():
     w = small_uniform(seed=4)
     K = 6

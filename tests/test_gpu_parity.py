@@ -581,13 +581,14 @@ def test_mixed_row_sampler_fp16_tf32_grams(K, gram):
 
 def test_batch_matches_single_problem_contexts():
     # each problem of the batch follows the chain of a single mixed context with its seed: the
-    # same keyed draws and arithmetic except the order of the Gram sums (tensor cores at a padded
-    # K = 32 in the batch, the CUDA-core sampler for K < 32 alone), so one sweep agrees closely
-    # and the chains stay close over a few sweeps
+    # same keyed draws and arithmetic except the order of the FP32 Gram sums (tensor cores at a
+    # padded K = 32 in the batch, the CUDA-core sampler for K < 32 alone); a last-bit difference
+    # can move a BF16 rounding of a gathered latent, so the chains agree to the mixed tolerance
+    # (a row of the wrong problem, or a wrong draw, would differ at O(1))
     problems, Ks, seeds = workloads.batched_uneven(nprob=7, rows=(40, 300), cols=(30, 200),
                                                    density=(0.05, 0.2))
     alpha = 4.0
-    for sweeps, tol in ((1, 1e-4), (6, 2e-2)):
+    for sweeps, tol in ((1, 5e-3), (6, 5e-2)):
         b = _lib.Batch(problems, Ks, seeds, alpha)
         b.init(2)
         b.sweeps(0, sweeps, eval=True)
@@ -601,7 +602,7 @@ def test_batch_matches_single_problem_contexts():
             for mode in (0, 1):
                 assert relerr(b.latents(p, mode), s.latents(mode)) < tol, (sweeps, p, mode)
             r, r1 = s.rmse()
-            assert abs(rb[p, 0] - r) < 50 * tol * r and abs(rb[p, 1] - r1) < 50 * tol * r1
+            assert abs(rb[p, 0] - r) < tol * r and abs(rb[p, 1] - r1) < tol * r1
         b.close()
 
 

@@ -50,9 +50,12 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=0, help="sweeps of the e2e run (0: = steps)")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the side-information legs (Macau block-CG and univariate priors)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the 512-problem batched leg")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the Gram precision sweep on the 2,000 x 1,500 matrix")
-    ap.add_argument("--only", choices=["all", "mixed", "fp64", "macau", "univariate", "precision"],
+    ap.add_argument("--only", choices=["all", "mixed", "fp64", "macau", "univariate", "precision",
+                                       "batched"],
                     default="all",
                     help="profiling runs: time one sampler and print its phase times only")
     return ap.parse_args()
@@ -270,6 +273,47 @@ def precision_sweep(device, Ks=(16, 64, 128), burnin=100, nsamples=100):
     return out
 
 
+def batched_legs(device, sweeps=20, single_sweeps=3):
+    """512 independent BPMF problems of uneven size (rows U[200, 4000], columns U[100, 1000],
+    density U[1%, 5%], K in {8, 16, 32}, noise 0.5, alpha = 4): all chains in one graph per sweep
+    (mg_batch, mixed) against one problem at a time with the FP64 single-problem sampler."""
+    from macau_b200 import _lib, workloads
+    problems, Ks, seeds = workloads.batched_uneven()
+    alpha = 4.0
+    b = _lib.Batch(problems, Ks, seeds, alpha, device=device)
+    b.init(10 ** 6)
+    b.time_sweeps(0, 3)
+    t = b.time_sweeps(3, sweeps)
+    info = b.info()
+    b.init(sweeps // 2)
+    b.sweeps(0, sweeps, eval=True)
+    rm = b.rmse()
+    b.close()
+    out = {"problems": len(problems), "ntrain": info["nnz"],
+           "rows": info["rows"], "cols": info["cols"],
+           "K_counts": {str(k): Ks.count(k) for k in sorted(set(Ks))},
+           "batched_mixed": {"sweeps_per_s": sweeps / t, "ms_per_sweep": t / sweeps * 1e3,
+                             "retries": info["retries"],
+                             "mean_test_rmse": float(np.mean(rm[:, 0])),
+                             "note": "one sweep = every problem sampled once; rmse after "
+                                     f"{sweeps // 2} + {sweeps - sweeps // 2} sweeps"}}
+    tot = 0.0
+    for pr, K, sd in zip(problems, Ks, seeds):
+        s = _lib.Sampler(K, alpha, seed=sd, compute=_lib.MG_COMPUTE_FP64, device=device)
+        s.set_relation_data(pr["rows"], pr["cols"], pr["vals"], pr["shape"])
+        s.set_samples(10 ** 6, 1)
+        s.init()
+        s.time_sweeps(0, 1, eval=False)
+        tp, _ = s.time_sweeps(1, single_sweeps, eval=False)
+        tot += tp / single_sweeps
+        s.close()
+    out["single_fp64"] = {"sweeps_per_s": 1.0 / tot, "ms_per_sweep": tot * 1e3,
+                          "note": "sum over problems of each problem's own FP64 sweep time "
+                                  "(captured graph, CUDA events)"}
+    out["batched_over_single_fp64"] = out["batched_mixed"]["sweeps_per_s"] * tot
+    return out
+
+
 def peaks():
     try:
         d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -394,6 +438,10 @@ def run_ours(args):
     if args.only == "precision":
         print(json.dumps({"only": "precision", "precision_sweep": precision_sweep(local)}),
               flush=True)
+        ranks.close()
+        return 0
+    if args.only == "batched":
+        print(json.dumps({"only": "batched", "batched": batched_legs(local)}), flush=True)
         ranks.close()
         return 0
     if args.only in ("macau", "univariate"):
@@ -532,6 +580,8 @@ def run_ours(args):
         line["side_info"] = side_info_legs(local)
     if rank == 0 and world == 1 and not args.no_precision:
         line["precision_sweep"] = precision_sweep(local)
+    if rank == 0 and world == 1 and not args.no_batched:
+        line["batched"] = batched_legs(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds, 50)
         line["mixed_over_cpu"] = v_mx / line["cpu_baseline"]["value"]

@@ -41,8 +41,9 @@ struct BatchRows {
   const int* row0;     // first row of each problem (P + 1 entries)
   const int* K;        // latent dimension of each problem
   const unsigned long long* seed;
-  const double* Lambda;  // 1024 doubles per problem (K_p x K_p used)
-  const double* mu;      // 32 per problem
+  const double* Lambda;  // 1024 doubles per problem (K_p x K_p used; the FP64 retry)
+  const float* LamF;     // 1024 floats per problem: Lambda in FP32, 32 x 32, zero beyond K_p
+  const double* lmu;     // 32 per problem: Lambda mu
   float alpha;
   float* out_f32;
   __nv_bfloat16* out_bf16;
@@ -92,20 +93,23 @@ __global__ void __launch_bounds__(kFinBatchWarps * 32)
   for (int row = blockIdx.x * kFinBatchWarps + warp; row < b.nrows; row += nw) {
     const int p = b.prob[row], K = b.K[p], lr = row - b.row0[p];
     const double* Lam = b.Lambda + (size_t)p * 1024;
-    const double* mu = b.mu + (size_t)p * 32;
+    const float4* lf = reinterpret_cast<const float4*>(b.LamF + (size_t)p * 1024 + lane * 32);
+    const float4* g4 = reinterpret_cast<const float4*>(gram + (size_t)row * kRec + lane * 32);
     const float* gp = gram + (size_t)row * kRec;
     float a[32], d0 = 1.f, rinv = 1.f;
 #pragma unroll
-    for (int j = 0; j < 32; j++) {
-      const float v = (lane < K && j < K)
-                          ? (float)Lam[lane + j * K] + b.alpha * __ldcg(gp + lane * 32 + j)
-                          : (lane == j ? 1.f : 0.f);
-      a[j] = v;
-      if (j == lane) d0 = v;
+    for (int q = 0; q < 8; q++) {
+      const float4 m4 = __ldg(lf + q), v4 = __ldcg(g4 + q);
+      const float mm[4] = {m4.x, m4.y, m4.z, m4.w}, gg[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int j = 4 * q + u;
+        const float v = (lane < K && j < K) ? mm[u] + b.alpha * gg[u] : (lane == j ? 1.f : 0.f);
+        a[j] = v;
+        if (j == lane) d0 = v;
+      }
     }
-    double rhs = (double)__ldcg(gp + 32 * 32 + lane);
-    if (lane < K)
-      for (int j = 0; j < K; j++) rhs += Lam[lane + j * K] * mu[j];
+    const double rhs = (double)__ldcg(gp + 32 * 32 + lane) + b.lmu[(size_t)p * 32 + lane];
     double z0, z1;
     normal_pair(b.seed[p], sweep, stream_id(kRowNoise, (uint32_t)b.mode), (uint32_t)lr,
                 (uint32_t)(lane >> 1), &z0, &z1);
@@ -348,6 +352,11 @@ class Batch {
         for (int i = 0; i < K_[p]; i++) lam[(size_t)p * 1024 + i + (size_t)i * K_[p]] = 10.0;
       mu_[m].upload(mu.data(), mu.size(), s_);
       Lambda_[m].upload(lam.data(), lam.size(), s_);
+      std::vector<float> lf((size_t)P_ * 1024, 0.f);
+      for (int p = 0; p < P_; p++)
+        for (int i = 0; i < K_[p]; i++) lf[(size_t)p * 1024 + i * 32 + i] = 10.f;
+      LamF_[m].upload(lf.data(), lf.size(), s_);
+      lmu_[m].alloc_zero((size_t)P_ * 32, s_);
     }
     partials_.alloc((size_t)P_ * kRec);
     if (ntest_ > 0) {
@@ -518,14 +527,14 @@ class Batch {
     sp.mode = m;
     launch_gram_tc(sp, md.gram.p, md.split.p, md.nsplit, 32, s_, num_sms_);
     BatchRows b{(int)N_[m], prob_d_[m].p, row0_d_[m].p, K_d_.p, seed_d_.p, Lambda_[m].p,
-                mu_[m].p, (float)alpha_, lat32_[m].p, lat16_[m].p, ctl_.p, m};
+                LamF_[m].p, lmu_[m].p, (float)alpha_, lat32_[m].p, lat16_[m].p, ctl_.p, m};
     k_finish_batch<<<num_sms_ * 8, kFinBatchWarps * 32, 0, s_>>>(b, md.gram.p);
     MG_CUDA(cudaGetLastError());
   }
 
   void update_prior(int m) {  // per problem: statistics, then the Normal-Wishart draw
     launch_prior_batch(lat32_[m].p, row0_d_[m].p, K_d_.p, seed_d_.p, P_, partials_.p, ctl_.p,
-                       m, mu_[m].p, Lambda_[m].p, s_);
+                       m, mu_[m].p, Lambda_[m].p, LamF_[m].p, lmu_[m].p, s_);
   }
 
   void eval() {
@@ -566,7 +575,8 @@ class Batch {
   DBuf<unsigned long long> seed_d_;
   DBuf<int> K_d_, row0_d_[2], prob_d_[2];
   DBuf<double> mean_d_, mu_[2], Lambda_[2], partials_, scratch_;
-  DBuf<float> lat32_[2];
+  DBuf<float> lat32_[2], LamF_[2];
+  DBuf<double> lmu_[2];
   DBuf<__nv_bfloat16> lat16_[2];
   DBuf<int> trow_, tcol_, tprob_;
   DBuf<long long> toff_;

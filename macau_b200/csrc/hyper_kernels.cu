@@ -810,23 +810,37 @@ __global__ void __launch_bounds__(kStatThreads)
 }
 
 // BPMFPrior::update_prior per problem with mu0 = 0, b0 = 2, W0 = I, df = K_p
-// (latentprior.cpp:79-99), keyed with the problem's seed.
+// (latentprior.cpp:79-99), keyed with the problem's seed; then the finish's operands: the FP32
+// Lambda (32 x 32, zero beyond K) and Lambda mu (FP64, summed in column order).
 __global__ void __launch_bounds__(256)
     k_nw_batch(const double* __restrict__ partials, const int* __restrict__ row0,
                const int* __restrict__ Kp, const unsigned long long* __restrict__ seed, Ctl* ctl,
-               int mode, double* __restrict__ mu, double* __restrict__ Lambda) {
-  const int p = blockIdx.x;
-  nw32_run(partials + (size_t)p * (32 + 32 * 32), 1, row0[p + 1] - row0[p], Kp[p], nullptr, 2.0,
-           nullptr, Kp[p], nullptr, 0, nullptr, ctl, seed[p], mode, mu + (size_t)p * 32,
-           Lambda + (size_t)p * 1024);
+               int mode, double* __restrict__ mu, double* __restrict__ Lambda,
+               float* __restrict__ LamF, double* __restrict__ lmu) {
+  const int p = blockIdx.x, K = Kp[p];
+  double* L = Lambda + (size_t)p * 1024;
+  double* m = mu + (size_t)p * 32;
+  nw32_run(partials + (size_t)p * (32 + 32 * 32), 1, row0[p + 1] - row0[p], K, nullptr, 2.0,
+           nullptr, K, nullptr, 0, nullptr, ctl, seed[p], mode, m, L);
+  __syncthreads();
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+    const int i = e >> 5, j = e & 31;
+    LamF[(size_t)p * 1024 + e] = (i < K && j < K) ? (float)L[i + j * K] : 0.f;
+  }
+  if (threadIdx.x < 32) {
+    double acc = 0.0;
+    if ((int)threadIdx.x < K)
+      for (int j = 0; j < K; j++) acc += L[threadIdx.x + j * K] * m[j];
+    lmu[(size_t)p * 32 + threadIdx.x] = acc;
+  }
 }
 
 void launch_prior_batch(const float* U, const int* row0, const int* Kp,
                         const unsigned long long* seed, int P, double* partials, Ctl* ctl, int mode,
-                        double* mu, double* Lambda, cudaStream_t s) {
+                        double* mu, double* Lambda, float* LamF, double* lmu, cudaStream_t s) {
   k_stats_batch<<<P, kStatThreads, 0, s>>>(U, row0, Kp, partials);
   MG_CUDA(cudaGetLastError());
-  k_nw_batch<<<P, 256, 0, s>>>(partials, row0, Kp, seed, ctl, mode, mu, Lambda);
+  k_nw_batch<<<P, 256, 0, s>>>(partials, row0, Kp, seed, ctl, mode, mu, Lambda, LamF, lmu);
   MG_CUDA(cudaGetLastError());
 }
 

@@ -81,10 +81,11 @@ void launch_noise_update(const int* erow, const int* col, const double* val, lon
                          Ctl* ctl, unsigned long long seed, cudaStream_t s);
 // Batched problems: per problem p (rows row0[p] .. row0[p + 1] - 1 of U, stride 32, K = Kp[p]),
 // the statistics into partials + 1056 p, then the Normal-Wishart draw into mu + 32 p and
-// Lambda + 1024 p (K x K), keyed with seed[p].
+// Lambda + 1024 p (K x K), keyed with seed[p]; LamF + 1024 p receives Lambda in FP32 (32 x 32,
+// zero beyond K) and lmu + 32 p Lambda mu.
 void launch_prior_batch(const float* U, const int* row0, const int* Kp,
                         const unsigned long long* seed, int P, double* partials, Ctl* ctl, int mode,
-                        double* mu, double* Lambda, cudaStream_t s);
+                        double* mu, double* Lambda, float* LamF, double* lmu, cudaStream_t s);
 void launch_set_sweep(Ctl* ctl, uint32_t sweep, int burnin, cudaStream_t s);
 void launch_advance(Ctl* ctl, cudaStream_t s);
 

@@ -81,10 +81,39 @@ __device__ __noinline__ bool batch_row_f64(const float* gp, const double* Lam, i
   return true;
 }
 
-// One warp per row: MM = Lambda_p + alpha G in FP32 (lane i: row i), rhs = record rhs (alpha
-// baked into the weights) + Lambda_p mu_p, Cholesky and solves with the row's keyed draws, FP64
-// retry on a failed pivot (sample_latent_blas, latentprior.cpp:361-385).
-__global__ void __launch_bounds__(kFinBatchWarps * 32)
+// FP32 finish of one row at width KP >= K (lane i: row i of MM = Lambda_p + alpha G, identity
+// beyond K).  Returns false when the FP32 pivot fails.
+template <int KP>
+__device__ __forceinline__ bool batch_row_f32(const float* __restrict__ lf,
+                                              const float* __restrict__ gp, int K, float alpha,
+                                              double rhs, double z, int lane, float* Lc,
+                                              double* x) {
+  float a[KP], d0 = 1.f, rinv = 1.f;
+#pragma unroll
+  for (int q = 0; q < KP / 4; q++) {
+    const float4 m4 = lane < KP ? __ldg(reinterpret_cast<const float4*>(lf) + q)
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 v4 = lane < KP ? __ldcg(reinterpret_cast<const float4*>(gp) + q)
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float mm[4] = {m4.x, m4.y, m4.z, m4.w}, gg[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int j = 4 * q + u;
+      const float v = (lane < K && j < K) ? mm[u] + alpha * gg[u] : (lane == j ? 1.f : 0.f);
+      a[j] = v;
+      if (j == lane) d0 = v;
+    }
+  }
+  if (!warp_factor<float, KP>(a, rinv, lane, 0x1p-20, d0, Lc, kBLc)) return false;
+  *x = (double)warp_solve<float, KP>(a, rinv, (float)rhs, lane, Lc, kBLc, z);
+  return true;
+}
+
+// One warp per row: MM = Lambda_p + alpha G in FP32 at the smallest width 8, 16 or 32 that holds
+// K_p, rhs = record rhs (alpha baked into the weights) + Lambda_p mu_p, Cholesky and solves
+// with the row's keyed draws, FP64 retry on a failed pivot (sample_latent_blas,
+// latentprior.cpp:361-385).
+__global__ void __launch_bounds__(kFinBatchWarps * 32, 4)
     k_finish_batch(const BatchRows b, const float* __restrict__ gram) {
   __shared__ __align__(16) double Lc_s[kFinBatchWarps][32 * kBLc];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -92,36 +121,23 @@ __global__ void __launch_bounds__(kFinBatchWarps * 32)
   const int nw = gridDim.x * kFinBatchWarps;
   for (int row = blockIdx.x * kFinBatchWarps + warp; row < b.nrows; row += nw) {
     const int p = b.prob[row], K = b.K[p], lr = row - b.row0[p];
-    const double* Lam = b.Lambda + (size_t)p * 1024;
-    const float4* lf = reinterpret_cast<const float4*>(b.LamF + (size_t)p * 1024 + lane * 32);
-    const float4* g4 = reinterpret_cast<const float4*>(gram + (size_t)row * kRec + lane * 32);
+    const float* lf = b.LamF + (size_t)p * 1024 + lane * 32;
     const float* gp = gram + (size_t)row * kRec;
-    float a[32], d0 = 1.f, rinv = 1.f;
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const float4 m4 = __ldg(lf + q), v4 = __ldcg(g4 + q);
-      const float mm[4] = {m4.x, m4.y, m4.z, m4.w}, gg[4] = {v4.x, v4.y, v4.z, v4.w};
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int j = 4 * q + u;
-        const float v = (lane < K && j < K) ? mm[u] + b.alpha * gg[u] : (lane == j ? 1.f : 0.f);
-        a[j] = v;
-        if (j == lane) d0 = v;
-      }
-    }
     const double rhs = (double)__ldcg(gp + 32 * 32 + lane) + b.lmu[(size_t)p * 32 + lane];
     double z0, z1;
     normal_pair(b.seed[p], sweep, stream_id(kRowNoise, (uint32_t)b.mode), (uint32_t)lr,
                 (uint32_t)(lane >> 1), &z0, &z1);
     const double z = lane < K ? ((lane & 1) ? z1 : z0) : 0.0;
     float* Lcf = reinterpret_cast<float*>(Lc_s[warp]);
-    const bool ok = warp_factor<float, 32>(a, rinv, lane, 0x1p-20, d0, Lcf, kBLc);
     double x = 0.0;
-    if (ok) {
-      x = (double)warp_solve<float, 32>(a, rinv, (float)rhs, lane, Lcf, kBLc, z);
-    } else {
+    bool ok;
+    if (K <= 8) ok = batch_row_f32<8>(lf, gp + lane * 32, K, b.alpha, rhs, z, lane, Lcf, &x);
+    else if (K <= 16) ok = batch_row_f32<16>(lf, gp + lane * 32, K, b.alpha, rhs, z, lane, Lcf, &x);
+    else ok = batch_row_f32<32>(lf, gp + lane * 32, K, b.alpha, rhs, z, lane, Lcf, &x);
+    if (!ok) {
       if (lane == 0) atomicAdd(&b.ctl->retries[b.mode], 1u);
       __syncwarp();
+      const double* Lam = b.Lambda + (size_t)p * 1024;
       if (!batch_row_f64(gp, Lam, K, (double)b.alpha, rhs, z, lane, Lc_s[warp], &x)) {
         if (lane == 0) {
           atomicOr(&b.ctl->status, kStatCholFail);

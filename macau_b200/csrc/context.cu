@@ -168,6 +168,7 @@ struct Prior {
   bool one = false;
   DBuf<double> colsq, lb_one;
   DBuf<int> lvl_ptr, lvl_feat, lvl_warp;
+  DBuf<longlong2> lvl_range;
   int nlevels = 0;
   double lb_a0 = 0.1, lb_b0 = 0.1;
   bool side() const { return macau || one; }
@@ -380,6 +381,10 @@ class Context {
       p.lvl_warp.upload(lwarp.data(), lwarp.size(), s_);
       p.lvl_ptr.upload(lptr.data(), lptr.size(), s_);
       p.lvl_feat.upload(order.data(), order.size(), s_);
+      std::vector<longlong2> range(nfeat);
+      for (int q = 0; q < nfeat; q++)
+        range[q] = make_longlong2(t.ptr[order[q]], t.ptr[order[q] + 1]);
+      p.lvl_range.upload(range.data(), range.size(), s_);
       p.nlevels = nl;
     }
     MG_CUDA(cudaStreamSynchronize(s_));
@@ -545,7 +550,8 @@ class Context {
       // compute_uhat, sample_lambda_beta
       launch_normal_wishart(stat_final_.p, 1, N, K_, p.mu0.p, p.b0, p.WI.p, p.df, nullptr, 0,
                             nullptr, nw_, ctl_.p, cfg_.seed, mode, p.mu.p, p.Lambda.p, s_);
-      launch_beta_one(p.Ft, p.colsq.p, p.lvl_ptr.p, p.lvl_feat.p, p.lvl_warp.p, p.nlevels,
+      launch_beta_one(p.Ft, p.colsq.p, p.lvl_ptr.p, p.lvl_feat.p, p.lvl_range.p, p.lvl_warp.p,
+                      p.nlevels,
                       latents(mode),
                       mixed_, KP_, p.mu.p, p.uhat.p, KP_, p.Lambda.p, p.lb_one.p, K_, N, p.beta.p,
                       CP_, p.tmp.p, CP_, p.B.p, ctl_.p, cfg_.seed, mode, s_);

@@ -112,11 +112,12 @@ void launch_spmm(const DevCsr& A, const void* src, int src_stride, void* dst, in
                  int ncomp, bool f32, cudaStream_t s);
 
 // Univariate prior (univariate_kernels.cu): MacauOnePrior::sample_beta over Ft (the columns of
-// F as CSR rows) with the feature levels lvl_ptr / lvl_feat (lvl_warp: one warp per feature in
-// that level), Z (N x zstride doubles) and draws
+// F as CSR rows) with the feature levels lvl_ptr / lvl_feat (lvl_range: each listed feature's
+// entry range in Ft; lvl_warp: one warp per feature in that level), Z (N x zstride doubles) and draws
 // (nfeat x bstride doubles) as workspace; and sample_lambda_beta into lambda_beta[0 .. K).
 void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
-                     const int* lvl_feat, const int* lvl_warp, int nlevels, const void* U, bool f32, int ustride,
+                     const int* lvl_feat, const longlong2* lvl_range, const int* lvl_warp,
+                     int nlevels, const void* U, bool f32, int ustride,
                      const double* mu, const double* uhat, int hstride, const double* Lambda,
                      const double* lambda_beta, int K, long long N, double* beta, int bstride,
                      double* Z, int zstride, double* draws, const Ctl* ctl,

@@ -143,15 +143,17 @@ __global__ void __launch_bounds__(kBetaThreads)
 
 // The same link sampler with one block per dimension d and this dimension's column of Z held in
 // shared memory (N doubles, N <= kZsMax), so the feature-by-feature chain reads and writes no
-// global memory but beta.  The sums are formed in the order of k_beta_one (lane-strided then an
-// xor tree in a warp; thread-strided, per-warp trees, then the warps in order in a block), so
-// both kernels give the same coefficients.
+// global memory but beta, with 32 warps per block and each feature's entry range (lvl_range)
+// read in one load.  The sums are formed as in k_beta_one (lane-strided then an xor tree in a
+// warp; thread-strided, per-warp trees, then the warps in order in a block).
 constexpr int kZsMax = 26 * 1024;
+constexpr int kSmemThreads = 1024;
+constexpr int kSmemWarps = kSmemThreads / 32;
 template <typename T>
-__global__ void __launch_bounds__(kBetaThreads)
-    k_beta_one_smem(const long long* __restrict__ tptr, const int* __restrict__ tidx,
-                    const double* __restrict__ tval, const double* __restrict__ colsq,
-                    const int* __restrict__ lvl_ptr, const int* __restrict__ lvl_feat,
+__global__ void __launch_bounds__(kSmemThreads)
+    k_beta_one_smem(const int* __restrict__ tidx, const double* __restrict__ tval,
+                    const double* __restrict__ colsq, const int* __restrict__ lvl_ptr,
+                    const int* __restrict__ lvl_feat, const longlong2* __restrict__ lvl_range,
                     const int* __restrict__ lvl_warp, int nlevels, const T* __restrict__ U,
                     int ustride, const double* __restrict__ mu,
                     const double* __restrict__ uhat, int hstride,
@@ -159,34 +161,53 @@ __global__ void __launch_bounds__(kBetaThreads)
                     int K, int N, double* __restrict__ beta, int bstride,
                     const double* __restrict__ draws) {
   extern __shared__ double Zs[];
-  __shared__ double red[kBetaWarps];
+  __shared__ double red[kSmemWarps];
   __shared__ double dl;
   const int d = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double lam = Lambda[(size_t)d * (K + 1)], lb = lambda_beta[d];
-  for (int i = threadIdx.x; i < N; i += kBetaThreads)
+  for (int i = threadIdx.x; i < N; i += kSmemThreads)
     Zs[i] = (double)U[(size_t)i * ustride + d] - mu[d] - uhat[(size_t)i * hstride + d];
   __syncthreads();
   for (int L = 0; L < nlevels; L++) {
     const int f0 = lvl_ptr[L], f1 = lvl_ptr[L + 1];
     if (lvl_warp[L]) {
-      for (int q = f0 + warp; q < f1; q += kBetaWarps) {
-        const int f = lvl_feat[q];
+      // one feature per warp; the next feature's id and entry range are loaded while the
+      // current one is processed
+      int q = f0 + warp, f = 0;
+      longlong2 rg = make_longlong2(0, 0);
+      if (q < f1) {
+        f = lvl_feat[q];
+        rg = lvl_range[q];
+      }
+      while (q < f1) {
+        const int qn = q + kSmemWarps;
+        int fn = 0;
+        longlong2 rn = make_longlong2(0, 0);
+        if (qn < f1) {
+          fn = lvl_feat[qn];
+          rn = lvl_range[qn];
+        }
+        const double cs = colsq[f];
         double zx = 0.0;
-        for (long long e = tptr[f] + lane; e < tptr[f + 1]; e += 32)
+        for (long long e = rg.x + lane; e < rg.y; e += 32)
           zx = fma(tval ? tval[e] : 1.0, Zs[tidx[e]], zx);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) zx += __shfl_xor_sync(0xffffffffu, zx, o);
-        const double my = beta_coef(0, 1, d, f, zx, lam, lb, colsq[f], beta, bstride, draws);
-        for (long long e = tptr[f] + lane; e < tptr[f + 1]; e += 32)
+        const double my = beta_coef(0, 1, d, f, zx, lam, lb, cs, beta, bstride, draws);
+        for (long long e = rg.x + lane; e < rg.y; e += 32)
           Zs[tidx[e]] = fma(tval ? tval[e] : 1.0, my, Zs[tidx[e]]);
         __syncwarp();
+        q = qn;
+        f = fn;
+        rg = rn;
       }
     } else {
       for (int q = f0; q < f1; q++) {
         const int f = lvl_feat[q];
+        const longlong2 rg = lvl_range[q];
         double zx = 0.0;
-        for (long long e = tptr[f] + threadIdx.x; e < tptr[f + 1]; e += kBetaThreads)
+        for (long long e = rg.x + threadIdx.x; e < rg.y; e += kSmemThreads)
           zx = fma(tval ? tval[e] : 1.0, Zs[tidx[e]], zx);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) zx += __shfl_xor_sync(0xffffffffu, zx, o);
@@ -194,12 +215,12 @@ __global__ void __launch_bounds__(kBetaThreads)
         __syncthreads();
         if (threadIdx.x == 0) {
           double sum = 0.0;
-          for (int w = 0; w < kBetaWarps; w++) sum += red[w];
+          for (int w = 0; w < kSmemWarps; w++) sum += red[w];
           dl = beta_coef(0, 1, d, f, sum, lam, lb, colsq[f], beta, bstride, draws);
         }
         __syncthreads();
         const double delta = dl;
-        for (long long e = tptr[f] + threadIdx.x; e < tptr[f + 1]; e += kBetaThreads)
+        for (long long e = rg.x + threadIdx.x; e < rg.y; e += kSmemThreads)
           Zs[tidx[e]] = fma(tval ? tval[e] : 1.0, delta, Zs[tidx[e]]);
       }
     }
@@ -252,7 +273,8 @@ __global__ void k_lambda_beta_one(const double* __restrict__ beta, int bstride, 
 }  // namespace
 
 void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
-                     const int* lvl_feat, const int* lvl_warp, int nlevels, const void* U, bool f32, int ustride,
+                     const int* lvl_feat, const longlong2* lvl_range, const int* lvl_warp,
+                     int nlevels, const void* U, bool f32, int ustride,
                      const double* mu, const double* uhat, int hstride, const double* Lambda,
                      const double* lambda_beta, int K, long long N, double* beta, int bstride,
                      double* Z, int zstride, double* draws, const Ctl* ctl,
@@ -276,13 +298,15 @@ void launch_beta_one(const DevCsr& Ft, const double* colsq, const int* lvl_ptr,
       configured[dev & 63] = true;
     }
     if (f32)
-      k_beta_one_smem<float><<<K, kBetaThreads, smem, s>>>(
-          Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, lvl_warp, nlevels, (const float*)U, ustride,
-          mu, uhat, hstride, Lambda, lambda_beta, K, (int)N, beta, bstride, draws);
+      k_beta_one_smem<float><<<K, kSmemThreads, smem, s>>>(
+          Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, lvl_range, lvl_warp, nlevels,
+          (const float*)U, ustride, mu, uhat, hstride, Lambda, lambda_beta, K, (int)N, beta,
+          bstride, draws);
     else
-      k_beta_one_smem<double><<<K, kBetaThreads, smem, s>>>(
-          Ft.ptr, Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, lvl_warp, nlevels, (const double*)U, ustride,
-          mu, uhat, hstride, Lambda, lambda_beta, K, (int)N, beta, bstride, draws);
+      k_beta_one_smem<double><<<K, kSmemThreads, smem, s>>>(
+          Ft.idx, Ft.val, colsq, lvl_ptr, lvl_feat, lvl_range, lvl_warp, nlevels,
+          (const double*)U, ustride, mu, uhat, hstride, Lambda, lambda_beta, K, (int)N, beta,
+          bstride, draws);
     MG_CUDA(cudaGetLastError());
     return;
   }

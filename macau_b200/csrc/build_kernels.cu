@@ -6,6 +6,8 @@
 //   launch_pad      the 16-entry padded copy of the packed entries (tensor-core sampler).
 // The sorts are CUB radix sorts over 64-bit (major << 32 | minor) keys; de-duplication, the row
 // pointers and the packing are kernels of this file.
+#include <algorithm>
+
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -176,6 +178,51 @@ long long build_csr_pair(const int* d_r, const int* d_c, const double* d_v, long
   MG_CUDA(cudaFreeAsync(flags, s));
   MG_CUDA(cudaFreeAsync(pos, s));
   return nu;
+}
+
+// Sum of (v[i] - center) (sq = false) or of its square (sq = true) over n values: a fixed grid
+// of blocks, each adding a grid-strided set in order and reducing in a fixed tree, then one
+// warp over the block sums (deterministic for a given n).
+__global__ void k_moment(const double* __restrict__ v, long long n, double center, bool sq,
+                         double* __restrict__ partials) {
+  __shared__ double ws[8];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double x = v[i] - center;
+    acc += sq ? x * x : x;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
+    partials[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_moment_final(const double* __restrict__ partials, int nb, double* out) {
+  const int lane = threadIdx.x & 31;
+  double t = 0.0;
+  for (int b = lane; b < nb; b += 32) t += partials[b];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (lane == 0) out[0] = t;
+}
+
+double value_moment(const double* v, long long n, double center, bool sq, cudaStream_t s) {
+  const int nb = (int)std::max(1LL, std::min(1184LL, (n + 255) / 256));
+  double* d = nullptr;
+  MG_CUDA(cudaMallocAsync(&d, sizeof(double) * (nb + 1), s));
+  k_moment<<<nb, 256, 0, s>>>(v, n, center, sq, d + 1);
+  k_moment_final<<<1, 32, 0, s>>>(d + 1, nb, d);
+  double h = 0.0;
+  MG_CUDA(cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, s));
+  MG_CUDA(cudaFreeAsync(d, s));
+  MG_CUDA(cudaStreamSynchronize(s));
+  return h;
 }
 
 __global__ void k_copy16(const float* __restrict__ src, void* __restrict__ dst, long long n,

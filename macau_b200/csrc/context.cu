@@ -236,26 +236,17 @@ class Context {
       nu = build_csr_pair(dr.p, dc.p, dv.p, nnz, dims_[0], dims_[1], md_[0].ptr.p, md_[0].idx.p,
                           md_[0].val.p, md_[1].ptr.p, md_[1].idx.p, md_[1].val.p, s_);
     }
-    // mean_value = Y.sum() / Y.nonZeros() over the column-major storage (sparsetensor.cpp:82):
-    // summed on the host in that order
-    std::vector<double> cval((size_t)nu);
+    // mean_value = Y.sum() / Y.nonZeros() over the column-major storage (sparsetensor.cpp:82),
+    // and AdaptiveGaussianNoise::init's var_total (noisemodels.cpp:14-33), summed on the device
     std::vector<long long> p0((size_t)dims_[0] + 1), p1((size_t)dims_[1] + 1);
-    MG_CUDA(cudaMemcpyAsync(cval.data(), md_[1].val.p, sizeof(double) * nu,
-                            cudaMemcpyDeviceToHost, s_));
     MG_CUDA(cudaMemcpyAsync(p0.data(), md_[0].ptr.p, sizeof(long long) * p0.size(),
                             cudaMemcpyDeviceToHost, s_));
     MG_CUDA(cudaMemcpyAsync(p1.data(), md_[1].ptr.p, sizeof(long long) * p1.size(),
                             cudaMemcpyDeviceToHost, s_));
-    MG_CUDA(cudaStreamSynchronize(s_));
-    g_d2h_bytes += (long long)(sizeof(double) * nu + sizeof(long long) * (p0.size() + p1.size()));
-    double sum = 0.0;
-    for (double v : cval) sum += v;
+    g_d2h_bytes += (long long)(sizeof(long long) * (p0.size() + p1.size()) + 16);
     ntrain_ = nu;
-    mean_ = sum / (double)ntrain_;
-    // AdaptiveGaussianNoise::init (noisemodels.cpp:14-33): var_total over the same order
-    double se = 0.0;
-    for (double v : cval) se += (v - mean_) * (v - mean_);
-    var_total_ = se / (double)ntrain_;
+    mean_ = value_moment(md_[1].val.p, nu, 0.0, false, s_) / (double)ntrain_;
+    var_total_ = value_moment(md_[1].val.p, nu, mean_, true, s_) / (double)ntrain_;
     if (var_total_ <= 0.0 || std::isnan(var_total_)) var_total_ = 1.0;
     upload_mode(0, p0, nu);
     upload_mode(1, p1, nu);

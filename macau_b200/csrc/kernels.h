@@ -25,6 +25,9 @@ void launch_pad(const long long* ptr, const long long* pptr, long long nrows, co
 // copy, p.half_copy set), 2 = TF32 (p.other is the FP32 master copy, rounded as it is read).
 void launch_sample(const SampleParams& p, int KP, bool mixed, int gram, cudaStream_t s,
                    int num_sms);
+// Sum over the n values of (v[i] - center), or of its square when sq, on the device in a fixed
+// order; returns it to the host (synchronises the stream).
+double value_moment(const double* v, long long n, double center, bool sq, cudaStream_t s);
 // dst[i] = src[i] rounded to BF16 (half = false) or FP16 (half = true), n values.
 void launch_copy16(const float* src, void* dst, long long n, bool half, cudaStream_t s);
 // Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only):

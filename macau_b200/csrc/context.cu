@@ -196,9 +196,6 @@ class Context {
       throw MgError(MG_ERR_NOGPU, std::string("sm_100a device required, found ") + prop.name);
     num_sms_ = prop.multiProcessorCount;
     MG_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
-    MG_CUDA(cudaStreamCreateWithFlags(&s2_, cudaStreamNonBlocking));
-    MG_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
-    MG_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
     ctl_.alloc_zero(1, s_);
     for (int m = 0; m < 2; m++) prior_[m].df = K_;
     MG_CUDA(cudaEventCreate(&ev0_));
@@ -209,9 +206,6 @@ class Context {
     drop_graphs();
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
-    if (fork_) cudaEventDestroy(fork_);
-    if (join_) cudaEventDestroy(join_);
-    if (s2_) cudaStreamDestroy(s2_);
     if (s_) cudaStreamDestroy(s_);
   }
 
@@ -646,35 +640,14 @@ class Context {
   // One sweep; ev (optional, 8 events) brackets: sample 0 | sample 1 | prior 0 | prior 1 |
   // noise update + eval + advance; ev[6], ev[7] end the tensor-core Gram kernel of mode 0, 1 (recorded only
   // when that sampler runs).
-  //
-  // Without events, the prior of mode 0 (which needs only U) runs on a second stream beside the
-  // sampling of mode 1 (which needs U and the mode-1 prior of the previous sweep) and joins
-  // before the mode-1 prior; the draws are keyed, so the order changes no result.
   void sweep_body(bool do_eval, cudaEvent_t* ev = nullptr) {
     MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[0], 0, 8 * sizeof(uint32_t), s_));
     if (ev) MG_CUDA(cudaEventRecord(ev[0], s_));
     sample(0, nullptr, false, ev ? ev[6] : nullptr);
     if (ev) MG_CUDA(cudaEventRecord(ev[1], s_));
-    const bool overlap = ev == nullptr && !prior_[0].macau;
-    if (overlap) {
-      MG_CUDA(cudaEventRecord(fork_, s_));
-      MG_CUDA(cudaStreamWaitEvent(s2_, fork_, 0));
-      struct Swap {  // update_prior enqueues on s_: point it at the second stream meanwhile
-        cudaStream_t& a;
-        cudaStream_t& b;
-        Swap(cudaStream_t& x, cudaStream_t& y) : a(x), b(y) { std::swap(a, b); }
-        ~Swap() { std::swap(a, b); }
-      };
-      {
-        Swap sw(s_, s2_);
-        update_prior(0);
-      }
-      MG_CUDA(cudaEventRecord(join_, s2_));
-    }
     sample(1, nullptr, false, ev ? ev[7] : nullptr);
     if (ev) MG_CUDA(cudaEventRecord(ev[2], s_));
-    if (overlap) MG_CUDA(cudaStreamWaitEvent(s_, join_, 0));
-    else update_prior(0);
+    update_prior(0);
     if (ev) MG_CUDA(cudaEventRecord(ev[3], s_));
     update_prior(1);
     if (ev) MG_CUDA(cudaEventRecord(ev[4], s_));
@@ -1107,8 +1080,8 @@ class Context {
   int K_ = 0, KP_ = 0, CP_ = 32;
   bool mixed_ = false;
   int dev_ = 0, num_sms_ = 148;
-  cudaStream_t s_ = nullptr, s2_ = nullptr;  // s2_: the mode-0 prior beside the mode-1 sampler
-  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, fork_ = nullptr, join_ = nullptr;
+  cudaStream_t s_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   long long dims_[2] = {0, 0};
   long long ntrain_ = 0, ntest_ = 0;
   double mean_ = 0.0;

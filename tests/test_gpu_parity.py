@@ -498,6 +498,24 @@ def test_univariate_update_prior_fp64_matches_oracle(kind):
         assert abs(lb_mean - lb.mean()) <= 1e-12 * lb.mean()
 
 
+def test_univariate_update_prior_large_mode_fp64():
+    # a mode with more rows than the shared-memory link sampler holds (26K) takes the
+    # global-memory variant (k_beta_one, four dimensions per block)
+    rng = np.random.default_rng(12)
+    K, mode = 10, 0
+    w = workloads.bpmf_uniform(nrow=27000, ncol=120, nobs=60000, seed=3)
+    F = side_matrix(rng, w["shape"][mode], "sparse")
+    s, m = univariate_pair(w, K, 66, mode, F)
+    U = rng.normal(scale=0.5, size=(w["shape"][mode], K))
+    s.set_latents(mode, U)
+    m.set("latents", mode, U)
+    s.update_prior(mode, 4)
+    assert m.update_prior(mode, 4) == 0
+    assert relerr(s.beta(mode), m.beta(mode)) < FP64_TOL
+    assert relerr(s.uhat(mode), m.uhat(mode)) < FP64_TOL
+    assert relerr(s.lambda_beta_univariate(mode), m.lambda_beta_one(mode)) < FP64_TOL
+
+
 def test_univariate_sweeps_fp64_match_oracle():
     # whole sweeps: univariate prior on the rows (dense side), BPMF on the columns, evaluation
     rng = np.random.default_rng(77)

@@ -147,6 +147,36 @@ __global__ void __launch_bounds__(kBetaThreads)
 // read in one load.  The sums are formed as in k_beta_one (lane-strided then an xor tree in a
 // warp; thread-strided, per-warp trees, then the warps in order in a block).
 constexpr int kZsMax = 26 * 1024;
+
+// What a warp loads ahead about a feature: id, entry range, squared column norm, coefficient,
+// draw, and this lane's first entry (row, value).
+struct FeaturePre {
+  int f;
+  longlong2 rg;
+  double cs, b, z;
+  int i0;
+  double v0;
+};
+
+__device__ __forceinline__ FeaturePre fetch_feature(int q, int lane, int d,
+                                                   const int* __restrict__ lvl_feat,
+                                                   const longlong2* __restrict__ lvl_range,
+                                                   const double* __restrict__ colsq,
+                                                   const double* beta, int bstride,
+                                                   const double* __restrict__ draws,
+                                                   const int* __restrict__ tidx,
+                                                   const double* __restrict__ tval) {
+  FeaturePre r;
+  r.f = lvl_feat[q];
+  r.rg = lvl_range[q];
+  r.cs = colsq[r.f];
+  r.b = beta[(size_t)r.f * bstride + d];
+  r.z = draws[(size_t)r.f * bstride + d];
+  const long long e = r.rg.x + lane;
+  r.i0 = e < r.rg.y ? tidx[e] : 0;
+  r.v0 = e < r.rg.y ? (tval ? tval[e] : 1.0) : 0.0;
+  return r;
+}
 constexpr int kSmemThreads = 1024;
 constexpr int kSmemWarps = kSmemThreads / 32;
 template <typename T>
@@ -169,38 +199,50 @@ __global__ void __launch_bounds__(kSmemThreads)
   for (int i = threadIdx.x; i < N; i += kSmemThreads)
     Zs[i] = (double)U[(size_t)i * ustride + d] - mu[d] - uhat[(size_t)i * hstride + d];
   __syncthreads();
+  FeaturePre cur{};
+  int cur_q = -1;
+  bool have = false;
   for (int L = 0; L < nlevels; L++) {
     const int f0 = lvl_ptr[L], f1 = lvl_ptr[L + 1];
     if (lvl_warp[L]) {
-      // one feature per warp; the next feature's id and entry range are loaded while the
-      // current one is processed
-      int q = f0 + warp, f = 0;
-      longlong2 rg = make_longlong2(0, 0);
-      if (q < f1) {
-        f = lvl_feat[q];
-        rg = lvl_range[q];
+      // one feature per warp; while a feature is processed, the warp loads everything about its
+      // next one that no other feature changes (id, entry range, colsq, its coefficient and
+      // draw, the first 32 entries), including the first feature it takes in the next level
+      int q = f0 + warp;
+      if (!(have && cur_q == q) && q < f1) {
+        cur = fetch_feature(q, lane, d, lvl_feat, lvl_range, colsq, beta, bstride, draws, tidx,
+                            tval);
+        cur_q = q;
+        have = true;
       }
-      while (q < f1) {
-        const int qn = q + kSmemWarps;
-        int fn = 0;
-        longlong2 rn = make_longlong2(0, 0);
-        if (qn < f1) {
-          fn = lvl_feat[qn];
-          rn = lvl_range[qn];
+      for (; q < f1; q += kSmemWarps) {
+        int qn = q + kSmemWarps;
+        if (qn >= f1) {
+          qn = (L + 1 < nlevels && lvl_warp[L + 1] && f1 + warp < lvl_ptr[L + 2]) ? f1 + warp : -1;
         }
-        const double cs = colsq[f];
+        FeaturePre nxt{};
+        if (qn >= 0)
+          nxt = fetch_feature(qn, lane, d, lvl_feat, lvl_range, colsq, beta, bstride, draws, tidx,
+                              tval);
         double zx = 0.0;
-        for (long long e = rg.x + lane; e < rg.y; e += 32)
+        if (cur.rg.x + lane < cur.rg.y) zx = fma(cur.v0, Zs[cur.i0], zx);
+        for (long long e = cur.rg.x + 32 + lane; e < cur.rg.y; e += 32)
           zx = fma(tval ? tval[e] : 1.0, Zs[tidx[e]], zx);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) zx += __shfl_xor_sync(0xffffffffu, zx, o);
-        const double my = beta_coef(0, 1, d, f, zx, lam, lb, cs, beta, bstride, draws);
-        for (long long e = rg.x + lane; e < rg.y; e += 32)
+        const double A = lb + lam * cur.cs;
+        const double B = lam * (zx + cur.b * cur.cs);
+        const double Ainv = 1.0 / A;
+        const double bn = B * Ainv + sqrt(Ainv) * cur.z;
+        const double my = cur.b - bn;
+        if (lane == 0) beta[(size_t)cur.f * bstride + d] = bn;
+        if (cur.rg.x + lane < cur.rg.y) Zs[cur.i0] = fma(cur.v0, my, Zs[cur.i0]);
+        for (long long e = cur.rg.x + 32 + lane; e < cur.rg.y; e += 32)
           Zs[tidx[e]] = fma(tval ? tval[e] : 1.0, my, Zs[tidx[e]]);
         __syncwarp();
-        q = qn;
-        f = fn;
-        rg = rn;
+        cur = nxt;
+        cur_q = qn;
+        have = qn >= 0;
       }
     } else {
       for (int q = f0; q < f1; q++) {

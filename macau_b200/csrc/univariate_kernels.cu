@@ -248,6 +248,12 @@ __global__ void __launch_bounds__(kSmemThreads)
       for (int q = f0; q < f1; q++) {
         const int f = lvl_feat[q];
         const longlong2 rg = lvl_range[q];
+        double cs = 0.0, bv = 0.0, zz = 0.0;  // thread 0 loads them before the reduction
+        if (threadIdx.x == 0) {
+          cs = colsq[f];
+          bv = beta[(size_t)f * bstride + d];
+          zz = draws[(size_t)f * bstride + d];
+        }
         double zx = 0.0;
         for (long long e = rg.x + threadIdx.x; e < rg.y; e += kSmemThreads)
           zx = fma(tval ? tval[e] : 1.0, Zs[tidx[e]], zx);
@@ -258,7 +264,12 @@ __global__ void __launch_bounds__(kSmemThreads)
         if (threadIdx.x == 0) {
           double sum = 0.0;
           for (int w = 0; w < kSmemWarps; w++) sum += red[w];
-          dl = beta_coef(0, 1, d, f, sum, lam, lb, colsq[f], beta, bstride, draws);
+          const double A = lb + lam * cs;
+          const double B = lam * (sum + bv * cs);
+          const double Ainv = 1.0 / A;
+          const double bn = B * Ainv + sqrt(Ainv) * zz;
+          beta[(size_t)f * bstride + d] = bn;
+          dl = bv - bn;
         }
         __syncthreads();
         const double delta = dl;

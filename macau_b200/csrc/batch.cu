@@ -123,7 +123,9 @@ __global__ void __launch_bounds__(kFinBatchWarps * 32, 4)
     const int p = b.prob[row], K = b.K[p], lr = row - b.row0[p];
     const float* lf = b.LamF + (size_t)p * 1024 + lane * 32;
     const float* gp = gram + (size_t)row * kRec;
-    const double rhs = (double)__ldcg(gp + 32 * 32 + lane) + b.lmu[(size_t)p * 32 + lane];
+    // the record holds the first 8, 16 or 32 rows and columns (k_gram_tc's row_width)
+    const double rhs = lane < K ? (double)__ldcg(gp + 32 * 32 + lane) + b.lmu[(size_t)p * 32 + lane]
+                                : 0.0;
     double z0, z1;
     normal_pair(b.seed[p], sweep, stream_id(kRowNoise, (uint32_t)b.mode), (uint32_t)lr,
                 (uint32_t)(lane >> 1), &z0, &z1);
@@ -267,6 +269,12 @@ class Batch {
       for (int p = 0; p < P; p++)
         for (long long r = off_[m][p]; r < off_[m][p + 1]; r++) pr[r] = p;
       prob_d_[m].upload(pr.data(), pr.size(), s_);
+      std::vector<int> wd(N_[m]);  // Gram record width of each row: 8, 16 or 32 >= K_p
+      for (long long r = 0; r < N_[m]; r++) {
+        const int k = K_[pr[r]];
+        wd[r] = k <= 8 ? 8 : (k <= 16 ? 16 : 32);
+      }
+      width_d_[m].upload(wd.data(), wd.size(), s_);
     }
     MG_CUDA(cudaStreamSynchronize(s_));
   }
@@ -541,6 +549,7 @@ class Batch {
     sp.ctl = ctl_.p;
     sp.qslot = m;
     sp.mode = m;
+    sp.row_width = width_d_[m].p;
     launch_gram_tc(sp, md.gram.p, md.split.p, md.nsplit, 32, s_, num_sms_);
     BatchRows b{(int)N_[m], prob_d_[m].p, row0_d_[m].p, K_d_.p, seed_d_.p, Lambda_[m].p,
                 LamF_[m].p, lmu_[m].p, (float)alpha_, lat32_[m].p, lat16_[m].p, ctl_.p, m};
@@ -589,7 +598,7 @@ class Batch {
   Mode md_[2];
   DBuf<Ctl> ctl_;
   DBuf<unsigned long long> seed_d_;
-  DBuf<int> K_d_, row0_d_[2], prob_d_[2];
+  DBuf<int> K_d_, row0_d_[2], prob_d_[2], width_d_[2];
   DBuf<double> mean_d_, mu_[2], Lambda_[2], partials_, scratch_;
   DBuf<float> lat32_[2], LamF_[2];
   DBuf<double> lmu_[2];

@@ -82,6 +82,8 @@ struct SampleParams {
   int one;                     // univariate prior (MacauOnePrior): coordinate-wise draws from
                                // the row's Gram with the precisions on Lambda's diagonal
   int half_copy;               // mixed: the 16-bit gather copy (out_bf16) holds FP16, not BF16
+  const int* row_width;        // tensor-core Gram records: per row, the width 8, 16 or 32 of the
+                               // Gram block and rhs entries the finish reads (null: 32)
 };
 
 #ifdef __CUDACC__

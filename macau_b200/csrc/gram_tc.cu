@@ -585,10 +585,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         sp[32 * 32 + lane] = (double)rhs;
       } else {
         float* gp = gram + (size_t)row * kGramRec;
+        const int w = p.row_width ? p.row_width[row] : 32;  // rows and columns the finish reads
+        if (lane < w) {
 #pragma unroll
-        for (int j = 0; j < 32; j += 4)
-          *reinterpret_cast<float4*>(gp + lane * 32 + j) = make_float4(gr[j], gr[j + 1], gr[j + 2], gr[j + 3]);
-        gp[32 * 32 + lane] = rhs;
+          for (int j = 0; j < 32; j += 4)
+            if (j < w)
+              *reinterpret_cast<float4*>(gp + lane * 32 + j) =
+                  make_float4(gr[j], gr[j + 1], gr[j + 2], gr[j + 3]);
+          gp[32 * 32 + lane] = rhs;
+        }
       }
     }
   }

@@ -760,9 +760,9 @@ __global__ void __launch_bounds__(256)
 
 }  // namespace
 
-int stats_blocks(long long N) {
+int stats_blocks(long long N) {  // at most two blocks per SM: fewer partials to reduce
   long long b = (N + 127) / 128;
-  if (b > 1184) b = 1184;
+  if (b > 296) b = 296;
   return (int)(b < 1 ? 1 : b);
 }
 

@@ -226,6 +226,7 @@ __global__ void __launch_bounds__(kSmemThreads)
                               tval);
         double zx = 0.0;
         if (cur.rg.x + lane < cur.rg.y) zx = fma(cur.v0, Zs[cur.i0], zx);
+#pragma unroll 4
         for (long long e = cur.rg.x + 32 + lane; e < cur.rg.y; e += 32)
           zx = fma(tval ? tval[e] : 1.0, Zs[tidx[e]], zx);
 #pragma unroll
@@ -237,6 +238,7 @@ __global__ void __launch_bounds__(kSmemThreads)
         const double my = cur.b - bn;
         if (lane == 0) beta[(size_t)cur.f * bstride + d] = bn;
         if (cur.rg.x + lane < cur.rg.y) Zs[cur.i0] = fma(cur.v0, my, Zs[cur.i0]);
+#pragma unroll 4
         for (long long e = cur.rg.x + 32 + lane; e < cur.rg.y; e += 32)
           Zs[tidx[e]] = fma(tval ? tval[e] : 1.0, my, Zs[tidx[e]]);
         __syncwarp();
@@ -255,6 +257,7 @@ __global__ void __launch_bounds__(kSmemThreads)
           zz = draws[(size_t)f * bstride + d];
         }
         double zx = 0.0;
+#pragma unroll 4
         for (long long e = rg.x + threadIdx.x; e < rg.y; e += kSmemThreads)
           zx = fma(tval ? tval[e] : 1.0, Zs[tidx[e]], zx);
 #pragma unroll
@@ -273,6 +276,7 @@ __global__ void __launch_bounds__(kSmemThreads)
         }
         __syncthreads();
         const double delta = dl;
+#pragma unroll 4
         for (long long e = rg.x + threadIdx.x; e < rg.y; e += kSmemThreads)
           Zs[tidx[e]] = fma(tval ? tval[e] : 1.0, delta, Zs[tidx[e]]);
       }

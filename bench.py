@@ -513,8 +513,11 @@ def run_ours(args):
     h2d0, d2h0 = st_fp["h2d_bytes"], st_fp["d2h_bytes"]
     t0 = time.perf_counter()
     s = _lib.Sampler(K_LATENT, ALPHA, seed=seed, compute=_lib.MG_COMPUTE_MIXED, device=local)
+    ta = time.perf_counter()
     s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
+    tb = time.perf_counter()
     s.set_relation_data_test(w["trows"], w["tcols"], w["tvals"], w["shape"])
+    tc = time.perf_counter()
     s.set_samples(0, E)
     s.init()
     t1 = time.perf_counter()
@@ -524,7 +527,9 @@ def run_ours(args):
     t2 = time.perf_counter()
     preds = s.predictions()
     t_e2e = time.perf_counter() - t0
-    e2e_split = {"setup_s": t1 - t0, "sweeps_s": t2 - t1, "readback_s": t0 + t_e2e - t2}
+    e2e_split = {"setup_s": t1 - t0, "sweeps_s": t2 - t1, "readback_s": t0 + t_e2e - t2,
+                 "setup_parts_s": {"create": ta - t0, "train": tb - ta, "test": tc - tb,
+                                   "init": t1 - tc}}
     st_e = s.stats()
     s.close()
     t_e2e = max_over_ranks(t_e2e)

@@ -2,6 +2,9 @@
 //   build_csr_pair  COO triplets -> CSR of the rows and CSR of the columns (the CSC of Y), both
 //                   with indices ascending and duplicate (i, j) entries summed in their input
 //                   order, like Eigen's setFromTriplets (sparseFromIJV, bpmfutils.h:57-82).
+//   build_coo_sorted  the same sort and duplicate sums, returned as COO triplets in (major,
+//                   minor) order (the test set in column-major order).
+// Both check every index against the dimensions on the device.
 //   launch_pack     per entry {index, float bits of (y - mean) * alpha} (mixed mode).
 //   launch_pad      the 16-entry padded copy of the packed entries (tensor-core sampler).
 // The sorts are CUB radix sorts over 64-bit (major << 32 | minor) keys; de-duplication, the row
@@ -17,11 +20,27 @@
 namespace mg {
 namespace {
 
+// Keys (major << 32 | minor).  An index outside [0, nmajor) x [0, nminor) sets *bad and gets
+// key 0, so that the sort and the de-duplication stay in bounds until the host reads *bad.
 __global__ void k_make_keys(const int* __restrict__ major, const int* __restrict__ minor,
-                            long long n, unsigned long long* __restrict__ keys) {
+                            long long n, long long nmajor, long long nminor,
+                            unsigned long long* __restrict__ keys, int* __restrict__ bad) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x)
-    keys[e] = ((unsigned long long)(unsigned)major[e] << 32) | (unsigned)minor[e];
+       e += (long long)gridDim.x * blockDim.x) {
+    const int a = major[e], b = minor[e];
+    const bool ok = a >= 0 && a < nmajor && b >= 0 && b < nminor;
+    if (!ok) *bad = 1;
+    keys[e] = ok ? ((unsigned long long)(unsigned)a << 32) | (unsigned)b : 0ull;
+  }
+}
+
+__global__ void k_split_keys(const unsigned long long* __restrict__ keys, long long n,
+                             int* __restrict__ major, int* __restrict__ minor) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    major[e] = (int)(keys[e] >> 32);
+    minor[e] = (int)(keys[e] & 0xffffffffull);
+  }
 }
 
 __global__ void k_heads(const unsigned long long* __restrict__ keys, long long n,
@@ -113,6 +132,67 @@ void sort_pairs(unsigned long long* keys_in, unsigned long long* keys_out, doubl
   MG_CUDA(e);
 }
 
+// Scratch of one build: two key and two value arrays, run-head flags with one extra int for the
+// index check, and their output positions.
+struct BuildScratch {
+  unsigned long long *k0 = nullptr, *k1 = nullptr;
+  double *v0 = nullptr, *v1 = nullptr;
+  int *flags = nullptr, *pos = nullptr;
+  cudaStream_t s;
+  BuildScratch(long long n, cudaStream_t st) : s(st) {
+    MG_CUDA(cudaMallocAsync(&k0, sizeof(unsigned long long) * n, s));
+    MG_CUDA(cudaMallocAsync(&k1, sizeof(unsigned long long) * n, s));
+    MG_CUDA(cudaMallocAsync(&v0, sizeof(double) * n, s));
+    MG_CUDA(cudaMallocAsync(&v1, sizeof(double) * n, s));
+    MG_CUDA(cudaMallocAsync(&flags, sizeof(int) * (n + 1), s));
+    MG_CUDA(cudaMallocAsync(&pos, sizeof(int) * n, s));
+  }
+  ~BuildScratch() {
+    cudaFreeAsync(k0, s);
+    cudaFreeAsync(k1, s);
+    cudaFreeAsync(v0, s);
+    cudaFreeAsync(v1, s);
+    cudaFreeAsync(flags, s);
+    cudaFreeAsync(pos, s);
+  }
+};
+
+// COO entries sorted by (major, minor) with their values; the LSD radix sort is stable, so
+// duplicates keep their input order, and each run of equal keys is summed in that order into
+// (b.k0, uvals).  Returns the number of distinct keys.  Throws MG_ERR_ARG with `what` when an
+// index is out of range, before any kernel indexes by the keys.
+long long sort_unique(const int* d_major, const int* d_minor, const double* d_v, long long nnz,
+                      long long nmajor, long long nminor, const char* what, BuildScratch& b,
+                      double* uvals) {
+  cudaStream_t s = b.s;
+  const int T = 256;
+  MG_CUDA(cudaMemsetAsync(b.flags + nnz, 0, sizeof(int), s));
+  k_make_keys<<<grid_for(nnz, T), T, 0, s>>>(d_major, d_minor, nnz, nmajor, nminor, b.k0,
+                                             b.flags + nnz);
+  MG_CUDA(cudaGetLastError());
+  MG_CUDA(cudaMemcpyAsync(b.v0, d_v, sizeof(double) * nnz, cudaMemcpyDeviceToDevice, s));
+  sort_pairs(b.k0, b.k1, b.v0, b.v1, nnz, 32 + bits_for(nmajor), s);
+  // run heads, their output positions, sums in input order
+  k_heads<<<grid_for(nnz, T), T, 0, s>>>(b.k1, nnz, b.flags);
+  MG_CUDA(cudaGetLastError());
+  size_t tb = 0;
+  MG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, b.flags, b.pos, (int)nnz, s));
+  void* tmp = nullptr;
+  MG_CUDA(cudaMallocAsync(&tmp, tb, s));
+  const cudaError_t se = cub::DeviceScan::ExclusiveSum(tmp, tb, b.flags, b.pos, (int)nnz, s);
+  MG_CUDA(cudaFreeAsync(tmp, s));
+  MG_CUDA(se);
+  k_dedupe<<<grid_for(nnz, T), T, 0, s>>>(b.k1, b.v1, b.flags, b.pos, nnz, b.k0, uvals);
+  MG_CUDA(cudaGetLastError());
+  int last[3] = {0, 0, 0};
+  MG_CUDA(cudaMemcpyAsync(&last[0], b.pos + nnz - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MG_CUDA(cudaMemcpyAsync(&last[1], b.flags + nnz - 1, sizeof(int) * 2, cudaMemcpyDeviceToHost,
+                          s));
+  MG_CUDA(cudaStreamSynchronize(s));
+  if (last[2]) throw MgError(MG_ERR_ARG, what);
+  return (long long)last[0] + last[1];
+}
+
 }  // namespace
 
 long long build_csr_pair(const int* d_r, const int* d_c, const double* d_v, long long nnz,
@@ -120,63 +200,31 @@ long long build_csr_pair(const int* d_r, const int* d_c, const double* d_v, long
                          double* row_val, long long* col_ptr, int* col_idx, double* col_val,
                          cudaStream_t s) {
   if (nnz > 0x7fffffffLL) throw MgError(MG_ERR_ARG, "more than 2^31 - 1 training entries");
-  unsigned long long *k0 = nullptr, *k1 = nullptr;
-  double *v0 = nullptr, *v1 = nullptr;
-  int *flags = nullptr, *pos = nullptr;
-  MG_CUDA(cudaMallocAsync(&k0, sizeof(unsigned long long) * nnz, s));
-  MG_CUDA(cudaMallocAsync(&k1, sizeof(unsigned long long) * nnz, s));
-  MG_CUDA(cudaMallocAsync(&v0, sizeof(double) * nnz, s));
-  MG_CUDA(cudaMallocAsync(&v1, sizeof(double) * nnz, s));
-  MG_CUDA(cudaMallocAsync(&flags, sizeof(int) * nnz, s));
-  MG_CUDA(cudaMallocAsync(&pos, sizeof(int) * nnz, s));
-  long long nu = 0;
-  try {
-    const int T = 256;
-    // 1. sort by (row, col); LSD radix sort is stable, so duplicates keep their input order
-    k_make_keys<<<grid_for(nnz, T), T, 0, s>>>(d_r, d_c, nnz, k0);
-    MG_CUDA(cudaGetLastError());
-    MG_CUDA(cudaMemcpyAsync(v0, d_v, sizeof(double) * nnz, cudaMemcpyDeviceToDevice, s));
-    sort_pairs(k0, k1, v0, v1, nnz, 32 + bits_for(nrow), s);
-    // 2. de-duplicate: run heads, their output positions, sums in input order
-    k_heads<<<grid_for(nnz, T), T, 0, s>>>(k1, nnz, flags);
-    MG_CUDA(cudaGetLastError());
-    size_t tb = 0;
-    MG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flags, pos, (int)nnz, s));
-    void* tmp = nullptr;
-    MG_CUDA(cudaMallocAsync(&tmp, tb, s));
-    const cudaError_t se = cub::DeviceScan::ExclusiveSum(tmp, tb, flags, pos, (int)nnz, s);
-    MG_CUDA(cudaFreeAsync(tmp, s));
-    MG_CUDA(se);
-    k_dedupe<<<grid_for(nnz, T), T, 0, s>>>(k1, v1, flags, pos, nnz, k0, row_val);
-    MG_CUDA(cudaGetLastError());
-    int last[2] = {0, 0};
-    MG_CUDA(cudaMemcpyAsync(&last[0], pos + nnz - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-    MG_CUDA(cudaMemcpyAsync(&last[1], flags + nnz - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-    MG_CUDA(cudaStreamSynchronize(s));
-    nu = (long long)last[0] + last[1];
-    // 3. CSR of the rows; swapped keys (col, row) for the columns
-    k_csr_from_sorted<<<grid_for(nu + 1, T), T, 0, s>>>(k0, nu, nrow, row_ptr, row_idx, k1);
-    MG_CUDA(cudaGetLastError());
-    // 4. CSR of the columns: sort (col, row) keys with the values
-    sort_pairs(k1, k0, row_val, col_val, nu, 32 + bits_for(ncol), s);
-    k_csr_from_sorted<<<grid_for(nu + 1, T), T, 0, s>>>(k0, nu, ncol, col_ptr, col_idx, nullptr);
-    MG_CUDA(cudaGetLastError());
-    MG_CUDA(cudaStreamSynchronize(s));
-  } catch (...) {
-    cudaFreeAsync(k0, s);
-    cudaFreeAsync(k1, s);
-    cudaFreeAsync(v0, s);
-    cudaFreeAsync(v1, s);
-    cudaFreeAsync(flags, s);
-    cudaFreeAsync(pos, s);
-    throw;
-  }
-  MG_CUDA(cudaFreeAsync(k0, s));
-  MG_CUDA(cudaFreeAsync(k1, s));
-  MG_CUDA(cudaFreeAsync(v0, s));
-  MG_CUDA(cudaFreeAsync(v1, s));
-  MG_CUDA(cudaFreeAsync(flags, s));
-  MG_CUDA(cudaFreeAsync(pos, s));
+  BuildScratch b(nnz, s);
+  const int T = 256;
+  // 1. sort by (row, col), duplicates summed in input order
+  const long long nu =
+      sort_unique(d_r, d_c, d_v, nnz, nrow, ncol, "training index out of range", b, row_val);
+  // 2. CSR of the rows; swapped keys (col, row) for the columns
+  k_csr_from_sorted<<<grid_for(nu + 1, T), T, 0, s>>>(b.k0, nu, nrow, row_ptr, row_idx, b.k1);
+  MG_CUDA(cudaGetLastError());
+  // 3. CSR of the columns: sort (col, row) keys with the values
+  sort_pairs(b.k1, b.k0, row_val, col_val, nu, 32 + bits_for(ncol), s);
+  k_csr_from_sorted<<<grid_for(nu + 1, T), T, 0, s>>>(b.k0, nu, ncol, col_ptr, col_idx, nullptr);
+  MG_CUDA(cudaGetLastError());
+  MG_CUDA(cudaStreamSynchronize(s));
+  return nu;
+}
+
+long long build_coo_sorted(const int* d_major, const int* d_minor, const double* d_v,
+                           long long nnz, long long nmajor, long long nminor, const char* what,
+                           int* out_major, int* out_minor, double* out_val, cudaStream_t s) {
+  if (nnz > 0x7fffffffLL) throw MgError(MG_ERR_ARG, "more than 2^31 - 1 entries");
+  BuildScratch b(nnz, s);
+  const long long nu = sort_unique(d_major, d_minor, d_v, nnz, nmajor, nminor, what, b, out_val);
+  k_split_keys<<<grid_for(nu, 256), 256, 0, s>>>(b.k0, nu, out_major, out_minor);
+  MG_CUDA(cudaGetLastError());
+  MG_CUDA(cudaStreamSynchronize(s));
   return nu;
 }
 

@@ -190,11 +190,14 @@ class Context {
       throw MgError(MG_ERR_NOGPU, "no CUDA device");
     dev_ = c.device;
     MG_CUDA(cudaSetDevice(dev_));
-    cudaDeviceProp prop;
-    MG_CUDA(cudaGetDeviceProperties(&prop, dev_));
-    if (prop.major < 10)
+    int major = 0;
+    MG_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev_));
+    if (major < 10) {
+      cudaDeviceProp prop;
+      MG_CUDA(cudaGetDeviceProperties(&prop, dev_));
       throw MgError(MG_ERR_NOGPU, std::string("sm_100a device required, found ") + prop.name);
-    num_sms_ = prop.multiProcessorCount;
+    }
+    MG_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev_));
     MG_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
     ctl_.alloc_zero(1, s_);
     for (int m = 0; m < 2; m++) prior_[m].df = K_;
@@ -217,10 +220,11 @@ class Context {
     dims_[1] = dims[1];
     const int* r = idx;
     const int* c = idx + nnz;
-    for (long long e = 0; e < nnz; e++)
-      if (r[e] < 0 || r[e] >= dims_[0] || c[e] < 0 || c[e] >= dims_[1])
-        throw MgError(MG_ERR_ARG, "training index out of range");
-    // CSR of the rows and of the columns, built on the device (build_kernels.cu)
+    // CSR of the rows and of the columns, built on the device (build_kernels.cu), which also
+    // checks the indices; a rejected set leaves the context without training data.
+    have_data_ = false;
+    initialised_ = false;
+    drop_graphs();
     long long nu = 0;
     {
       DBuf<int> dr, dc;
@@ -258,25 +262,22 @@ class Context {
   void set_test(const int32_t* idx, int nmodes, const double* vals, long long nnz,
                 const int32_t* dims) {
     if (nmodes != 2) throw MgError(MG_ERR_ARG, "MatrixData: tensor test input not supported.");
-    const int* r = idx;
-    const int* c = idx + nnz;
-    for (long long e = 0; e < nnz; e++)
-      if (r[e] < 0 || r[e] >= dims[0] || c[e] < 0 || c[e] >= dims[1])
-        throw MgError(MG_ERR_ARG, "test index out of range");
-    // Ytest in CSC order (sparseFromIJV -> column-major storage): CSR of the transpose.
-    HostCsr cs = coo_to_csr(c, r, vals, nnz, dims[1], dims[0]);
-    ntest_ = (long long)cs.idx.size();
-    test_row_.resize(ntest_);
-    test_col_.resize(ntest_);
-    test_val_ = cs.val;
-    for (long long col = 0; col < dims[1]; col++)
-      for (long long e = cs.ptr[col]; e < cs.ptr[col + 1]; e++) {
-        test_row_[e] = cs.idx[e];
-        test_col_[e] = (int)col;
-      }
-    trow_.upload(test_row_.data(), ntest_, s_);
-    tcol_.upload(test_col_.data(), ntest_, s_);
-    tval_.upload(test_val_.data(), ntest_, s_);
+    // Ytest in CSC order (sparseFromIJV -> column-major storage): entries sorted by (column,
+    // row), duplicates summed in input order, built and index-checked on the device.
+    ntest_ = 0;
+    drop_graphs();
+    if (nnz > 0) {
+      DBuf<int> dr, dc;
+      DBuf<double> dv;
+      dr.upload(idx, (size_t)nnz, s_);
+      dc.upload(idx + nnz, (size_t)nnz, s_);
+      dv.upload(vals, (size_t)nnz, s_);
+      trow_.alloc((size_t)nnz);
+      tcol_.alloc((size_t)nnz);
+      tval_.alloc((size_t)nnz);
+      ntest_ = build_coo_sorted(dc.p, dr.p, dv.p, nnz, dims[1], dims[0], "test index out of range",
+                                tcol_.p, trow_.p, tval_.p, s_);
+    }
     pred_.alloc_zero(ntest_, s_);
     pvar_.alloc_zero(ntest_, s_);
     eval_partials_.alloc(2 * (size_t)eval_blocks(ntest_));
@@ -284,7 +285,6 @@ class Context {
     const double nan2[2] = {NAN, NAN};
     MG_CUDA(cudaMemcpyAsync(rmse_.p, nan2, sizeof(nan2), cudaMemcpyHostToDevice, s_));
     MG_CUDA(cudaStreamSynchronize(s_));
-    drop_graphs();
   }
 
   // univariate = false: MacauPrior<SparseDoubleFeat> (block-CG link solve); true: MacauOnePrior
@@ -944,10 +944,16 @@ class Context {
     for (long long i = 0; i < ntest_; i++) out[i] = std::sqrt(out[i] * inorm);
   }
   void get_test_data(double* out) {
+    if (ntest_ == 0) return;
+    std::vector<int> r((size_t)ntest_), c((size_t)ntest_);
+    MG_CUDA(cudaMemcpyAsync(r.data(), trow_.p, ntest_ * 4, cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaMemcpyAsync(c.data(), tcol_.p, ntest_ * 4, cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaMemcpyAsync(out + 2 * ntest_, tval_.p, ntest_ * 8, cudaMemcpyDeviceToHost, s_));
+    g_d2h_bytes += ntest_ * 16;
+    MG_CUDA(cudaStreamSynchronize(s_));
     for (long long i = 0; i < ntest_; i++) {
-      out[i] = test_row_[i];
-      out[i + ntest_] = test_col_[i];
-      out[i + 2 * ntest_] = test_val_[i];
+      out[i] = r[i];
+      out[i + ntest_] = c[i];
     }
   }
   void get_stats(mg_stats* st) {
@@ -1112,8 +1118,6 @@ class Context {
   DBuf<Ctl> ctl_;
   DBuf<int> trow_, tcol_;
   DBuf<double> tval_, pred_, pvar_, eval_partials_, rmse_;
-  std::vector<int> test_row_, test_col_;
-  std::vector<double> test_val_;
   cudaGraphExec_t graph_[2] = {nullptr, nullptr};
   long long retries_[2] = {0, 0}, rows_[2] = {0, 0};
   long long sweeps_done_ = 0;

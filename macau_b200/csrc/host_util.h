@@ -70,9 +70,15 @@ inline std::vector<RowTask> make_tasks(const std::vector<long long>& ptr, long l
     nslots += parts;
     nsplit++;
   }
-  std::stable_sort(tasks.begin(), tasks.end(),
-                   [](const RowTask& a, const RowTask& b) { return a.len > b.len; });
-  return tasks;
+  // stable sort by descending length: a counting sort over the lengths (each at most thr + align)
+  int maxlen = 0;
+  for (const RowTask& t : tasks) maxlen = std::max(maxlen, t.len);
+  std::vector<size_t> start((size_t)maxlen + 2, 0);
+  for (const RowTask& t : tasks) start[(size_t)(maxlen - t.len) + 1]++;
+  for (size_t b = 1; b < start.size(); b++) start[b] += start[b - 1];
+  std::vector<RowTask> out(tasks.size());
+  for (const RowTask& t : tasks) out[start[(size_t)(maxlen - t.len)]++] = t;
+  return out;
 }
 
 }  // namespace mg

@@ -13,6 +13,12 @@ long long build_csr_pair(const int* d_r, const int* d_c, const double* d_v, long
                          long long nrow, long long ncol, long long* row_ptr, int* row_idx,
                          double* row_val, long long* col_ptr, int* col_idx, double* col_val,
                          cudaStream_t s);
+// COO (device) -> triplets sorted by (major, minor) with duplicates summed in input order into
+// out_major / out_minor / out_val (capacity nnz); returns the unique count.  Both builders throw
+// MG_ERR_ARG (`what` for this one) when an index is outside the dimensions.
+long long build_coo_sorted(const int* d_major, const int* d_minor, const double* d_v,
+                           long long nnz, long long nmajor, long long nminor, const char* what,
+                           int* out_major, int* out_minor, double* out_val, cudaStream_t s);
 // out[e] = {idx[e], float bits of (val[e] - mean) * alpha}
 void launch_pack(const int* idx, const double* val, long long n, double mean, double alpha,
                  uint2* out, cudaStream_t s);

@@ -666,3 +666,45 @@ def test_eval_rmse_golden_on_gpu():  # tests.cpp:552-591 through mg_eval
         assert s.predictions()[0] == pytest.approx(pred)
     s.set_samples(0, 3)
     assert s.stds()[0] == pytest.approx(np.sqrt(14.0 / 2))
+
+
+def test_device_index_checks_and_test_set_order():
+    """Training and test indices are checked on the device during the CSR builds; the test set
+    comes back in column-major order with duplicates summed (sparseFromIJV, bpmfutils.h:57-82),
+    and a rejected training set leaves a context that accepts a valid one."""
+    w = small_uniform(seed=6)
+    nr, nc = w["shape"]
+    s = _lib.Sampler(4, 1.0, seed=1)
+    bad_rows = np.array(w["rows"], np.int32)
+    bad_rows[len(bad_rows) // 2] = nr
+    with pytest.raises(_lib.MacauError, match="training index out of range"):
+        s.set_relation_data(bad_rows, w["cols"], w["vals"], w["shape"])
+    bad_cols = np.array(w["cols"], np.int32)
+    bad_cols[-1] = -1
+    with pytest.raises(_lib.MacauError, match="training index out of range"):
+        s.set_relation_data(w["rows"], bad_cols, w["vals"], w["shape"])
+    with pytest.raises(_lib.MacauError):
+        s.init()
+    s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
+    with pytest.raises(_lib.MacauError, match="test index out of range"):
+        s.set_relation_data_test(np.array([0, nr]), np.array([0, 0]), np.array([1.0, 2.0]),
+                                 w["shape"])
+    rng = np.random.default_rng(3)
+    tr = rng.integers(0, nr, 400).astype(np.int32)
+    tc = rng.integers(0, nc, 400).astype(np.int32)
+    tr[200:260], tc[200:260] = tr[:60], tc[:60]  # duplicates, summed in input order
+    tv = rng.integers(-4, 5, 400).astype(np.float64)
+    s.set_relation_data_test(tr, tc, tv, w["shape"])
+    got = s.test_data()
+    key = tc.astype(np.int64) * nr + tr
+    order = np.argsort(key, kind="stable")
+    uk, first = np.unique(key[order], return_index=True)
+    want_v = np.add.reduceat(tv[order], first)
+    assert got.shape == (len(uk), 3)
+    np.testing.assert_array_equal(got[:, 0], uk % nr)
+    np.testing.assert_array_equal(got[:, 1], uk // nr)
+    np.testing.assert_array_equal(got[:, 2], want_v)
+    s.set_samples(0, 2)
+    s.init()
+    s.sweep(0, eval=True)
+    assert np.isfinite(s.rmse()[0])

@@ -47,6 +47,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default work split and CTA shape (no autotuner) in the headline arms")
     ap.add_argument("--e2e-steps", type=int, default=0, help="sweeps of the e2e run (0: = steps)")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the side-information legs (Macau block-CG and univariate priors)")
@@ -135,12 +137,16 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------ helpers
-def make_sampler(w, compute, seed, device, burnin=10 ** 6, nsamples=1):
+def make_sampler(w, compute, seed, device, burnin=10 ** 6, nsamples=1, autotune=0):
+    """autotune: 0 default work split and CTA shape, 1 the autotuner with its choice cache,
+    2 the autotuner timing every candidate (mg_set_option "autotune", run by mg_init)."""
     from macau_b200 import _lib
     s = _lib.Sampler(K_LATENT, ALPHA, seed=seed, compute=compute, device=device)
     s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
     s.set_relation_data_test(w["trows"], w["tcols"], w["tvals"], w["shape"])
     s.set_samples(burnin, nsamples)
+    if autotune:
+        s.set_option("autotune", autotune)
     s.init()
     return s
 
@@ -273,7 +279,7 @@ def precision_sweep(device, Ks=(16, 64, 128), burnin=100, nsamples=100):
     return out
 
 
-def batched_legs(device, sweeps=20, single_sweeps=3):
+def batched_legs(device, sweeps=20, single_sweeps=3, autotune=True):
     """512 independent BPMF problems of uneven size (rows U[200, 4000], columns U[100, 1000],
     density U[1%, 5%], K in {8, 16, 32}, noise 0.5, alpha = 4): all chains in one graph per sweep
     (mg_batch, mixed) against one problem at a time with the FP64 single-problem sampler."""
@@ -282,6 +288,7 @@ def batched_legs(device, sweeps=20, single_sweeps=3):
     alpha = 4.0
     b = _lib.Batch(problems, Ks, seeds, alpha, device=device)
     b.init(10 ** 6)
+    tuning = b.autotune(use_cache=False) if autotune else b.tuning()
     b.time_sweeps(0, 3)
     t = b.time_sweeps(3, sweeps)
     info = b.info()
@@ -296,12 +303,15 @@ def batched_legs(device, sweeps=20, single_sweeps=3):
                              "retries": info["retries"],
                              "mean_test_rmse": float(np.mean(rm[:, 0])),
                              "note": "one sweep = every problem sampled once; rmse after "
-                                     f"{sweeps // 2} + {sweeps - sweeps // 2} sweeps"}}
+                                     f"{sweeps // 2} + {sweeps - sweeps // 2} sweeps",
+                             "autotune": tuning}}
     tot = 0.0
     for pr, K, sd in zip(problems, Ks, seeds):
         s = _lib.Sampler(K, alpha, seed=sd, compute=_lib.MG_COMPUTE_FP64, device=device)
         s.set_relation_data(pr["rows"], pr["cols"], pr["vals"], pr["shape"])
         s.set_samples(10 ** 6, 1)
+        if autotune:
+            s.set_option("autotune", 2)
         s.init()
         s.time_sweeps(0, 1, eval=False)
         tp, _ = s.time_sweeps(1, single_sweeps, eval=False)
@@ -441,7 +451,9 @@ def run_ours(args):
         ranks.close()
         return 0
     if args.only == "batched":
-        print(json.dumps({"only": "batched", "batched": batched_legs(local)}), flush=True)
+        print(json.dumps({"only": "batched",
+                          "batched": batched_legs(local, autotune=not args.no_autotune)}),
+              flush=True)
         ranks.close()
         return 0
     if args.only in ("macau", "univariate"):
@@ -468,7 +480,7 @@ def run_ours(args):
     w = workload(args.scale, 2)
     if args.only != "all":
         comp = _lib.MG_COMPUTE_MIXED if args.only == "mixed" else _lib.MG_COMPUTE_FP64
-        s = make_sampler(w, comp, seed, local)
+        s = make_sampler(w, comp, seed, local, autotune=0 if args.no_autotune else 2)
         s.time_sweeps(0, max(W, 1), eval=False)
         t, _ = s.time_sweeps(W, K, eval=False)
         _, ph = s.time_sweeps(W + K, K, eval=False, phase_events=True)
@@ -478,7 +490,9 @@ def run_ours(args):
         ranks.close()
         return 0
     # ---- mixed-precision batched sampler: headline value ----
-    mx = make_sampler(w, _lib.MG_COMPUTE_MIXED, seed, local)
+    tune = 0 if args.no_autotune else 2
+    mx = make_sampler(w, _lib.MG_COMPUTE_MIXED, seed, local, autotune=tune)
+    tuning = {"mixed": mx.tuning()}
     mx.time_sweeps(0, max(W, 1), eval=False)
     barrier()
     with ClockSampler(bus) as clk:
@@ -496,7 +510,8 @@ def run_ours(args):
     retries = st_mx["retries"]
     mx.close()
     # ---- FP64 plain sampler ----
-    fp = make_sampler(w, _lib.MG_COMPUTE_FP64, seed, local)
+    fp = make_sampler(w, _lib.MG_COMPUTE_FP64, seed, local, autotune=tune)
+    tuning["fp64"] = fp.tuning()
     fp.time_sweeps(0, max(W, 1), eval=False)
     barrier()
     t_fp, _ = fp.time_sweeps(W, K, eval=False)
@@ -513,6 +528,8 @@ def run_ours(args):
     h2d0, d2h0 = st_fp["h2d_bytes"], st_fp["d2h_bytes"]
     t0 = time.perf_counter()
     s = _lib.Sampler(K_LATENT, ALPHA, seed=seed, compute=_lib.MG_COMPUTE_MIXED, device=local)
+    if tune:
+        s.set_option("autotune", 1)  # the choice of the mixed arm, from the autotuner's cache
     ta = time.perf_counter()
     s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
     tb = time.perf_counter()
@@ -521,6 +538,7 @@ def run_ours(args):
     s.set_samples(0, E)
     s.init()
     t1 = time.perf_counter()
+    tuning["e2e"] = [t["state"] for t in s.tuning()]
     for i in range(E):
         s.sweep(i, eval=True)
         s.rmse()
@@ -578,15 +596,17 @@ def run_ours(args):
             "clocks": clk.summary(), "roofline": roofline,
             "e2e": {"value": ranks.rate(E, t_e2e), "unit": UNIT, "h2d_bytes_per_step": h2d / E,
                     "d2h_bytes_per_step": d2h / E,
-                    "timed": "C-ABI run: data upload + CSR build, init, sweeps with eval and "
-                             "RMSE read-back, final predictions read-back",
-                    "split_s": e2e_split}}
+                    "timed": "C-ABI run: data upload + CSR build, init (autotuner choice "
+                             "from its cache), sweeps with eval and RMSE read-back, final "
+                             "predictions read-back",
+                    "split_s": e2e_split},
+            "autotune": tuning}
     if rank == 0 and world == 1 and not args.no_side:
         line["side_info"] = side_info_legs(local)
     if rank == 0 and world == 1 and not args.no_precision:
         line["precision_sweep"] = precision_sweep(local)
     if rank == 0 and world == 1 and not args.no_batched:
-        line["batched"] = batched_legs(local)
+        line["batched"] = batched_legs(local, autotune=not args.no_autotune)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds, 50)
         line["mixed_over_cpu"] = v_mx / line["cpu_baseline"]["value"]

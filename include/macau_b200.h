@@ -232,8 +232,46 @@ int mg_batch_get_info(mg_batch* b, int64_t* out);
  *   "gram_precision"   (default 0) mixed mode: inputs of the row Grams, 0 = BF16, 1 = FP16,
  *                      2 = TF32 (the FP32 latents rounded to TF32 as they are gathered); FP32
  *                      accumulation, factor and solves in every case.  1 and 2 use the CUDA-core
- *                      sampler at every K.  Set before mg_init (it undoes a previous mg_init). */
+ *                      sampler at every K.  Set before mg_init (it undoes a previous mg_init).
+ *   "autotune"         (default 0) run mg_autotune at the end of mg_init: 1 with the choice
+ *                      cache (set before mg_set_relation_data, a cached choice also shapes
+ *                      the task lists built there), 2 always timing the candidates
+ *   "split_threshold"  the row samplers' work split for both modes, in [256, 16384] entries
+ *                      (default nnz / (32 * SMs) clamped to that range); after the training data
+ *   "cta_groups"       row groups per CTA of the CUDA-core sampler (0 = default; 4 or 2 at
+ *                      K <= 32, 2 or 1 at K = 64, FP64 or BF16 Grams) */
 int mg_set_option(mg_ctx* ctx, const char* name, int value);
+
+/* ---- Autotuner of the row samplers (no reference counterpart; the reference's OpenMP
+ * `schedule(dynamic, 2)` row loop, latentprior.cpp:73, has no shape to tune) ----
+ * For each mode, times every candidate work split of the row sampler (rows longer than the
+ * split threshold are cut into parts; thresholds nnz / (d * 16 * SMs), d = 1, 2, 4, 8, 16,
+ * clamped to [256, 16384] entries) and, for the CUDA-core sampler, its CTA shapes, as half-sweeps
+ * on the current state, and keeps the fastest.  Latents, hyperparameters and counters are
+ * restored, so the chain continues as if untuned (only split rows' summation order can change).
+ * Choices are cached per process, and in the file named by MACAU_B200_TUNE_CACHE if set, by
+ * (sampler, K, SM count, the rows' log2 length histogram); use_cache = 0 always re-times.
+ * Call after mg_init. */
+int mg_autotune(mg_ctx* ctx, int use_cache);
+
+typedef struct mg_tuning {
+  int64_t split_threshold; /* entries: longer rows are split into parts */
+  int cta_groups;          /* row groups per CTA of the CUDA-core sampler (0: tensor-core) */
+  int tensor_core;         /* 1 when the mode's Grams run on the tcgen05 sampler */
+  int state;               /* 0 default shape, 1 timed by mg_autotune, 2 taken from the cache */
+  int candidates;          /* candidates timed */
+  double ms_best;          /* half-sweep time of the choice (ms) */
+  double ms_default;       /* half-sweep time of the default shape (ms) */
+  int finish_ctas_per_sm;  /* batch: CTAs per SM of the row finish (0 for a context) */
+} mg_tuning;
+int mg_get_tuning(mg_ctx* ctx, int mode, mg_tuning* out);
+
+/* The same autotuner for the batched sampler (mg_batch): per mode, the split threshold of the
+ * Gram task list over every problem's rows and the row finish's CTAs per SM (8, 4 or 16;
+ * reported in finish_ctas_per_sm).  Call after mg_batch_init; the chains continue as if
+ * untuned. */
+int mg_batch_autotune(mg_batch* b, int use_cache);
+int mg_batch_get_tuning(mg_batch* b, int mode, mg_tuning* out);
 
 /* macau.blockcg(X, B, reg, tol) (macau.pyx:67-91 -> solve_blockcg, linop.h:229-343) on the GPU:
  * solves (F'F + reg I) X' = B' for nrhs right-hand sides with the reference's 32+8 RHS blocking

@@ -43,6 +43,12 @@ class MgStats(C.Structure):
                 ("d2h_bytes", C.c_int64), ("ntasks", C.c_int64 * 2), ("nnz", C.c_int64 * 2)]
 
 
+class MgTuning(C.Structure):
+    _fields_ = [("split_threshold", C.c_int64), ("cta_groups", C.c_int), ("tensor_core", C.c_int),
+                ("state", C.c_int), ("candidates", C.c_int), ("ms_best", C.c_double),
+                ("ms_default", C.c_double), ("finish_ctas_per_sm", C.c_int)]
+
+
 _p = C.c_void_p
 _i = C.c_int
 _d = C.c_double
@@ -82,6 +88,8 @@ _SIGS = {
     "mg_get_test_data": (_i, [_p, _p]),
     "mg_get_stats": (_i, [_p, C.POINTER(MgStats)]),
     "mg_set_option": (_i, [_p, C.c_char_p, _i]),
+    "mg_autotune": (_i, [_p, _i]),
+    "mg_get_tuning": (_i, [_p, _i, C.POINTER(MgTuning)]),
     "mg_blockcg": (_i, [_p, _p, _p, _i64, _i, _i, _p, _i, _d, _d, _i, _p, C.POINTER(_i),
                         C.POINTER(_d)]),
     "mg_batch_create": (_i, [C.POINTER(_p), _i, _p, _p, _p, _p, _d, _i]),
@@ -94,6 +102,8 @@ _SIGS = {
     "mg_batch_get_latents": (_i, [_p, _i, _i, _p]),
     "mg_batch_get_rmse": (_i, [_p, _p]),
     "mg_batch_get_info": (_i, [_p, _p]),
+    "mg_batch_autotune": (_i, [_p, _i]),
+    "mg_batch_get_tuning": (_i, [_p, _i, C.POINTER(MgTuning)]),
     "mg_normal_wishart_noalloc": (_i, [_p, _i64, _i, _i, _p, _d, _p, _i, C.c_uint64, C.c_uint32,
                                        _i, _p, _p, _p, C.c_char_p, _i]),
 }
@@ -317,6 +327,27 @@ class Sampler:
                 "d2h_bytes": int(st.d2h_bytes), "ntasks": list(st.ntasks), "nnz": list(st.nnz)}
 
 
+    def autotune(self, use_cache=True):
+        """Times the row samplers' candidate work splits and CTA shapes and keeps the fastest
+        (mg_autotune); returns tuning()."""
+        self._chk(lib().mg_autotune(self.h, 1 if use_cache else 0))
+        return self.tuning()
+
+    _TUNE_STATES = ("default", "timed", "cached")
+
+    def tuning(self):
+        """Per mode: the sampler's split threshold, CTA shape and the autotuner's record."""
+        out = []
+        for m in (0, 1):
+            t = MgTuning()
+            self._chk(lib().mg_get_tuning(self.h, m, C.byref(t)))
+            out.append({"split_threshold": int(t.split_threshold), "cta_groups": t.cta_groups,
+                        "tensor_core": bool(t.tensor_core), "state": self._TUNE_STATES[t.state],
+                        "candidates": t.candidates, "ms_best": t.ms_best,
+                        "ms_default": t.ms_default})
+        return out
+
+
 class Batch:
     """Many independent BPMF chains sampled together (mg_batch): problem p is the matrix
     problems[p] = dict(rows, cols, vals, trows, tcols, tvals, shape) with latent dimension
@@ -375,6 +406,23 @@ class Batch:
         out = np.zeros(2 * self.P)
         self._chk(lib().mg_batch_get_rmse(self.h, ptr(out)))
         return out.reshape(self.P, 2)
+
+    def autotune(self, use_cache=True):
+        """Times the batched sampler's candidate work splits and finish grids and keeps the
+        fastest (mg_batch_autotune); returns tuning()."""
+        self._chk(lib().mg_batch_autotune(self.h, 1 if use_cache else 0))
+        return self.tuning()
+
+    def tuning(self):
+        out = []
+        for m in (0, 1):
+            t = MgTuning()
+            self._chk(lib().mg_batch_get_tuning(self.h, m, C.byref(t)))
+            out.append({"split_threshold": int(t.split_threshold),
+                        "finish_ctas_per_sm": t.finish_ctas_per_sm,
+                        "state": Sampler._TUNE_STATES[t.state], "candidates": t.candidates,
+                        "ms_best": t.ms_best, "ms_default": t.ms_default})
+        return out
 
     def info(self):
         out = np.zeros(5, np.int64)

@@ -26,6 +26,7 @@
 #include "host_util.h"
 #include "kernels.h"
 #include "rng.cuh"
+#include "tune.h"
 #include "warp_finish.cuh"
 
 namespace mg {
@@ -488,7 +489,42 @@ class Batch {
     DBuf<int4> split;
     DBuf<float> gram;
     int ntasks = 0, nsplit = 0, nslots = 0;
+    // host copy of the padded row pointers, the split threshold of the task list, the row
+    // finish's CTAs per SM, and the autotuner's record
+    std::vector<long long> hpptr;
+    long long thr = 0;
+    int fin_per_sm = 8;
+    TuneChoice tune;
+    int tune_state = 0;
   };
+
+  // Split threshold nnz / (div * 16 * SMs), clamped to [256, 16384] and rounded up to 16
+  // entries; div = 2 is the default, the autotuner tries 1 to 16.
+  long long split_divisor_thr(int m, int div) const {
+    long long thr = md_[m].nnz / ((long long)div * num_sms_ * 16);
+    thr = std::max(256LL, std::min(16384LL, thr));
+    return (thr + 15) / 16 * 16;
+  }
+
+  // Task list of mode m over the padded rows at split threshold thr (16-entry aligned parts),
+  // its split-row table and the split-part scratch.
+  void build_tasks(int m, long long thr) {
+    Mode& md = md_[m];
+    md.thr = thr;
+    int ns = 0, nsl = 0;
+    std::vector<RowTask> tt = make_tasks(md.hpptr, thr, 16, ns, nsl);
+    md.ntasks = (int)tt.size();
+    md.nsplit = ns;
+    md.nslots = nsl;
+    md.tasks.upload(tt.data(), tt.size(), s_);
+    std::vector<int4> sr;
+    for (const RowTask& t : tt)
+      if (t.nparts > 1 && t.part == 0) sr.push_back(make_int4(t.row, t.nparts, t.slot, 0));
+    std::sort(sr.begin(), sr.end(), [](const int4& a, const int4& b) { return a.x < b.x; });
+    md.split.upload(sr.data(), sr.size(), s_);
+    const size_t need = (size_t)std::max(md_[0].nslots, md_[1].nslots) * kRec;
+    if (need > scratch_.n) scratch_.alloc(need);
+  }
 
   void build_mode(int m, const std::vector<long long>& hptr, long long nnz) {
     Mode& md = md_[m];
@@ -504,23 +540,11 @@ class Batch {
     md.pptr.upload(pptr.data(), pptr.size(), s_);
     md.packed_tc.alloc((size_t)std::max(1LL, pptr[N]));
     launch_pad(md.ptr.p, md.pptr.p, N, md.packed.p, (unsigned)N_[1 - m], md.packed_tc.p, s_);
-    long long thr = nnz / (2LL * num_sms_ * 16);
-    thr = std::max(256LL, std::min(16384LL, thr));
-    thr = (thr + 15) / 16 * 16;
-    int ns = 0, nsl = 0;
-    std::vector<RowTask> tt = make_tasks(pptr, thr, 16, ns, nsl);
-    md.ntasks = (int)tt.size();
-    md.nsplit = ns;
-    md.nslots = nsl;
-    md.tasks.upload(tt.data(), tt.size(), s_);
-    std::vector<int4> sr;
-    for (const RowTask& t : tt)
-      if (t.nparts > 1 && t.part == 0) sr.push_back(make_int4(t.row, t.nparts, t.slot, 0));
-    std::sort(sr.begin(), sr.end(), [](const int4& a, const int4& b) { return a.x < b.x; });
-    md.split.upload(sr.data(), sr.size(), s_);
+    md.hpptr = pptr;
+    md.fin_per_sm = 8;
+    md.tune_state = 0;
+    build_tasks(m, split_divisor_thr(m, 2));
     md.gram.alloc((size_t)std::max(1LL, N) * kRec);
-    const size_t need = (size_t)std::max(md_[0].nslots, md_[1].nslots) * kRec;
-    if (need > scratch_.n) scratch_.alloc(need);
     MG_CUDA(cudaStreamSynchronize(s_));
   }
 
@@ -553,9 +577,115 @@ class Batch {
     launch_gram_tc(sp, md.gram.p, md.split.p, md.nsplit, 32, s_, num_sms_);
     BatchRows b{(int)N_[m], prob_d_[m].p, row0_d_[m].p, K_d_.p, seed_d_.p, Lambda_[m].p,
                 LamF_[m].p, lmu_[m].p, (float)alpha_, lat32_[m].p, lat16_[m].p, ctl_.p, m};
-    k_finish_batch<<<num_sms_ * 8, kFinBatchWarps * 32, 0, s_>>>(b, md.gram.p);
+    k_finish_batch<<<num_sms_ * md.fin_per_sm, kFinBatchWarps * 32, 0, s_>>>(b, md.gram.p);
     MG_CUDA(cudaGetLastError());
   }
+
+ public:
+  // Autotuner of the batched sampler (tune.h): per mode, the split threshold of the task list
+  // (divisors 1, 2, 4, 8, 16) and the row finish's CTAs per SM (8, 4, 16), each timed as one
+  // warm-up and three timed Gram + finish launches on the current state; the fastest is kept.
+  // Latents and the control block are restored afterwards.
+  void autotune(bool use_cache) {
+    if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_batch_init before autotuning");
+    drop_graphs();
+    Ctl saved{};
+    MG_CUDA(cudaMemcpyAsync(&saved, ctl_.p, sizeof(Ctl), cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    MG_CUDA(cudaEventCreate(&e0));
+    MG_CUDA(cudaEventCreate(&e1));
+    try {
+      for (int m = 0; m < 2; m++) {
+        Mode& md = md_[m];
+        std::string key = tune_key("batch", 32, num_sms_, md.hpptr);
+        for (int p = 0; p < P_; p++) key += (p ? "," : ":k") + std::to_string(K_[p]);
+        TuneChoice c;
+        if (use_cache && TuneCache::get().find(key, &c)) {
+          md.fin_per_sm = c.groups;
+          build_tasks(m, c.thr);
+          md.tune = c;
+          md.tune_state = 2;
+          continue;
+        }
+        DBuf<float> k32;
+        DBuf<__nv_bfloat16> k16;
+        k32.alloc(lat32_[m].n);
+        k16.alloc(lat16_[m].n);
+        MG_CUDA(cudaMemcpyAsync(k32.p, lat32_[m].p, lat32_[m].n * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s_));
+        MG_CUDA(cudaMemcpyAsync(k16.p, lat16_[m].p, lat16_[m].n * sizeof(__nv_bfloat16),
+                                cudaMemcpyDeviceToDevice, s_));
+        std::vector<long long> thrs;
+        for (int div : {2, 1, 4, 8, 16}) {
+          const long long t = split_divisor_thr(m, div);
+          if (std::find(thrs.begin(), thrs.end(), t) == thrs.end()) thrs.push_back(t);
+        }
+        TuneChoice best;
+        best.ms = 1e30;
+        int tried = 0;
+        for (int fin : {8, 4, 16})
+          for (long long t : thrs) {
+            md.fin_per_sm = fin;
+            build_tasks(m, t);
+            float best_ms = 1e30f;
+            for (int rep = 0; rep < 4; rep++) {
+              MG_CUDA(cudaMemsetAsync(&ctl_.p->queue[0], 0, 8 * sizeof(uint32_t), s_));
+              MG_CUDA(cudaEventRecord(e0, s_));
+              sample(m);
+              MG_CUDA(cudaEventRecord(e1, s_));
+              MG_CUDA(cudaEventSynchronize(e1));
+              float ms = 0.f;
+              MG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+              if (rep > 0) best_ms = std::min(best_ms, ms);
+            }
+            check_status();
+            tried++;
+            if (tried == 1) best.ms_default = best_ms;
+            if (best_ms < best.ms) {
+              best.ms = best_ms;
+              best.thr = t;
+              best.groups = fin;
+            }
+          }
+        best.candidates = tried;
+        md.fin_per_sm = best.groups;
+        build_tasks(m, best.thr);
+        md.tune = best;
+        md.tune_state = 1;
+        TuneCache::get().put(key, best);
+        MG_CUDA(cudaMemcpyAsync(lat32_[m].p, k32.p, lat32_[m].n * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s_));
+        MG_CUDA(cudaMemcpyAsync(lat16_[m].p, k16.p, lat16_[m].n * sizeof(__nv_bfloat16),
+                                cudaMemcpyDeviceToDevice, s_));
+        MG_CUDA(cudaStreamSynchronize(s_));
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MG_CUDA(cudaMemcpyAsync(ctl_.p, &saved, sizeof(Ctl), cudaMemcpyHostToDevice, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    drop_graphs();
+  }
+
+  void get_tuning(int m, mg_tuning* out) const {
+    if (m < 0 || m > 1) throw MgError(MG_ERR_ARG, "mode must be 0 or 1");
+    const Mode& md = md_[m];
+    out->split_threshold = md.thr;
+    out->cta_groups = 0;
+    out->tensor_core = 1;
+    out->state = md.tune_state;
+    out->candidates = md.tune_state ? md.tune.candidates : 0;
+    out->ms_best = md.tune_state ? md.tune.ms : 0.0;
+    out->ms_default = md.tune_state ? md.tune.ms_default : 0.0;
+    out->finish_ctas_per_sm = md.fin_per_sm;
+  }
+
+ private:
 
   void update_prior(int m) {  // per problem: statistics, then the Normal-Wishart draw
     launch_prior_batch(lat32_[m].p, row0_d_[m].p, K_d_.p, seed_d_.p, P_, partials_.p, ctl_.p,
@@ -702,6 +832,15 @@ int mg_batch_get_latents(mg_batch* h, int prob, int mode, double* out) {
 int mg_batch_get_rmse(mg_batch* h, double* out) {
   if (!out) return MG_ERR_ARG;
   return bguarded(h, [&](mg::Batch& b) { b.get_rmse(out); });
+}
+
+int mg_batch_autotune(mg_batch* h, int use_cache) {
+  return bguarded(h, [&](mg::Batch& b) { b.autotune(use_cache != 0); });
+}
+
+int mg_batch_get_tuning(mg_batch* h, int mode, mg_tuning* out) {
+  if (!out) return MG_ERR_ARG;
+  return bguarded(h, [&](mg::Batch& b) { b.get_tuning(mode, out); });
 }
 
 int mg_batch_get_info(mg_batch* h, int64_t* out) {

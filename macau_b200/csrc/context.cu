@@ -29,6 +29,7 @@
 
 #include "common.cuh"
 #include "host_util.h"
+#include "tune.h"
 #include "kernels.h"
 
 namespace mg {
@@ -120,6 +121,14 @@ struct ModeData {
   DBuf<float> gram_tc;     // N Gram records (32 x 32 + 32 floats) written by k_gram_tc
   DBuf<int4> split_tc;     // split rows {row, parts, scratch slot of part 0, 0}
   int ntasks_tc = 0, nsplit_tc = 0, nslots_tc = 0;
+  // host copy of the row pointers (task lists are rebuilt from it by the autotuner), the split
+  // threshold of the current task lists, the CUDA-core sampler's CTA shape (0: default) and the
+  // autotuner's record for this mode
+  std::vector<long long> hptr;
+  long long thr = 0;
+  int groups = 0;
+  TuneChoice tune;
+  int tune_state = 0;  // 0 not tuned, 1 timed here, 2 taken from the cache
 };
 
 // Work split of a CSR for the side-information SpMMs (k_spmm_split): rows longer than
@@ -466,6 +475,7 @@ class Context {
     t_sample_ = t_prior_ = t_eval_ = 0.0;
     drop_graphs();
     initialised_ = true;
+    if (autotune_) autotune(autotune_ == 1);
   }
 
 
@@ -519,7 +529,146 @@ class Context {
         return;
       }
     }
-    launch_sample(sp, KP_, mixed_, gram_, s_, num_sms_);
+    launch_sample(sp, KP_, mixed_, gram_, s_, num_sms_, md.groups);
+  }
+
+  // Sampler kind of mode m in the autotuner's keys.
+  const char* tune_kind(int m) const {
+    if (uses_tc(m)) return "tc";
+    if (!mixed_) return "fp64";
+    return gram_ == 0 ? "bf16" : gram_ == 1 ? "fp16" : "tf32";
+  }
+
+  // True when mode m's latents are drawn by the tensor-core sampler.
+  bool uses_tc(int m) const {
+    return mixed_ && use_tc_ && gram_ == 0 && KP_ == 32 && md_[m].packed_tc.p != nullptr;
+  }
+
+  // Autotuner (tune.h): for each mode, the split threshold of the task lists (divisors 1, 2, 4,
+  // 8, 16 of nnz per row group) and, for the CUDA-core sampler, its CTA shape, each timed as
+  // one warm-up and three timed half-sweeps (CUDA events, the fastest kept) on the current
+  // state.  The latents, the control block and the counters are restored afterwards, so the
+  // chain continues as if untuned; only the summation order of split rows can differ.
+  void autotune(bool use_cache) {
+    if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_init before autotuning");
+    drop_graphs();
+    Ctl saved_ctl{};
+    MG_CUDA(cudaMemcpyAsync(&saved_ctl, ctl_.p, sizeof(Ctl), cudaMemcpyDeviceToHost, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    const long long saved_launches = launches_;
+    const double saved_ts = t_sample_;
+    const long long saved_retries[2] = {retries_[0], retries_[1]};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    MG_CUDA(cudaEventCreate(&e0));
+    MG_CUDA(cudaEventCreate(&e1));
+    try {
+      for (int m = 0; m < 2; m++) {
+        ModeData& md = md_[m];
+        const bool tc = uses_tc(m);
+        const std::string key = tune_key(tune_kind(m), K_, num_sms_, md.hptr);
+        TuneChoice c;
+        if (use_cache && TuneCache::get().find(key, &c)) {
+          if (md.thr != c.thr || md.groups != c.groups) {
+            md.groups = c.groups;
+            build_tasks(m, c.thr);
+          }
+          md.tune = c;
+          md.tune_state = 2;
+          continue;
+        }
+        // the latents this mode's timing runs overwrite
+        const size_t n = (size_t)dims_[m] * KP_;
+        DBuf<double> keep64;
+        DBuf<float> keep32;
+        DBuf<__nv_bfloat16> keep16;
+        if (lat64_[m].p) {
+          keep64.alloc(n);
+          MG_CUDA(cudaMemcpyAsync(keep64.p, lat64_[m].p, n * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+        }
+        if (lat32_[m].p) {
+          keep32.alloc(n);
+          MG_CUDA(cudaMemcpyAsync(keep32.p, lat32_[m].p, n * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+        }
+        if (lat16_[m].p) {
+          keep16.alloc(lat16_[m].n);
+          MG_CUDA(cudaMemcpyAsync(keep16.p, lat16_[m].p, lat16_[m].n * sizeof(__nv_bfloat16),
+                                  cudaMemcpyDeviceToDevice, s_));
+        }
+        std::vector<long long> thrs;
+        for (int div : {2, 1, 4, 8, 16}) {
+          const long long t = split_divisor_thr(m, div);
+          if (std::find(thrs.begin(), thrs.end(), t) == thrs.end()) thrs.push_back(t);
+        }
+        const std::vector<int> shapes =
+            tc ? std::vector<int>{0} : sample_group_options(KP_, mixed_, gram_);
+        TuneChoice best;
+        best.ms = 1e30;
+        int tried = 0;
+        for (int g : shapes)
+          for (long long t : thrs) {
+            md.groups = g;
+            build_tasks(m, t);
+            float best_ms = 1e30f;
+            for (int rep = 0; rep < 4; rep++) {
+              MG_CUDA(cudaEventRecord(e0, s_));
+              sample(m, nullptr);
+              MG_CUDA(cudaEventRecord(e1, s_));
+              MG_CUDA(cudaEventSynchronize(e1));
+              float ms = 0.f;
+              MG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+              if (rep > 0) best_ms = std::min(best_ms, ms);
+            }
+            check_status();
+            tried++;
+            if (tried == 1) best.ms_default = best_ms;
+            if (best_ms < best.ms) {
+              best.ms = best_ms;
+              best.thr = t;
+              best.groups = g;
+            }
+          }
+        best.candidates = tried;
+        md.groups = best.groups;
+        build_tasks(m, best.thr);
+        md.tune = best;
+        md.tune_state = 1;
+        TuneCache::get().put(key, best);
+        if (keep64.p)
+          MG_CUDA(cudaMemcpyAsync(lat64_[m].p, keep64.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+        if (keep32.p)
+          MG_CUDA(cudaMemcpyAsync(lat32_[m].p, keep32.p, n * sizeof(float), cudaMemcpyDeviceToDevice, s_));
+        if (keep16.p)
+          MG_CUDA(cudaMemcpyAsync(lat16_[m].p, keep16.p, lat16_[m].n * sizeof(__nv_bfloat16),
+                                  cudaMemcpyDeviceToDevice, s_));
+        MG_CUDA(cudaStreamSynchronize(s_));
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MG_CUDA(cudaMemcpyAsync(ctl_.p, &saved_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, s_));
+    MG_CUDA(cudaStreamSynchronize(s_));
+    launches_ = saved_launches;
+    t_sample_ = saved_ts;
+    retries_[0] = saved_retries[0];
+    retries_[1] = saved_retries[1];
+    drop_graphs();
+  }
+
+  void get_tuning(int mode, mg_tuning* out) const {
+    if (mode < 0 || mode > 1) throw MgError(MG_ERR_ARG, "mode must be 0 or 1");
+    const ModeData& md = md_[mode];
+    out->split_threshold = md.thr;
+    out->cta_groups = uses_tc(mode) ? 0 : (md.groups ? md.groups : sample_default_groups(KP_));
+    out->tensor_core = uses_tc(mode) ? 1 : 0;
+    out->state = md.tune_state;
+    out->candidates = md.tune_state ? md.tune.candidates : 0;
+    out->ms_best = md.tune_state ? md.tune.ms : 0.0;
+    out->ms_default = md.tune_state ? md.tune.ms_default : 0.0;
+    out->finish_ctas_per_sm = 0;
   }
 
   const void* latents(int mode) const {
@@ -998,6 +1147,31 @@ class Context {
   void set_use_graph(bool b) { use_graph_ = b; drop_graphs(); }
   void set_use_tc(bool b) { use_tc_ = b; drop_graphs(); }
   void set_cg_f32(bool b) { cg_f32_ = b && mixed_; }
+  // A fixed work split / CTA shape for both modes' row samplers (the autotuner's knobs).
+  void set_split_threshold(int t) {
+    if (!have_data_) throw MgError(MG_ERR_STATE, "set the training data before split_threshold");
+    if (t < 256 || t > 16384) throw MgError(MG_ERR_ARG, "split_threshold must be in [256, 16384]");
+    drop_graphs();
+    for (int m = 0; m < 2; m++) {
+      build_tasks(m, t);
+      md_[m].tune_state = 0;
+    }
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+  void set_cta_groups(int g) {
+    const std::vector<int> opts = sample_group_options(KP_, mixed_, gram_);
+    if (g != 0 && std::find(opts.begin(), opts.end(), g) == opts.end())
+      throw MgError(MG_ERR_ARG, "cta_groups not offered for this K and precision");
+    drop_graphs();
+    for (int m = 0; m < 2; m++) {
+      md_[m].groups = g;
+      md_[m].tune_state = 0;
+    }
+  }
+  void set_autotune(int v) {
+    if (v < 0 || v > 2) throw MgError(MG_ERR_ARG, "autotune must be 0, 1 or 2");
+    autotune_ = v;
+  }
   void set_gram(int g) {
     if (g < 0 || g > 2) throw MgError(MG_ERR_ARG, "gram_precision must be 0 (BF16), 1 (FP16) or 2 (TF32)");
     if (!mixed_ && g != 0) throw MgError(MG_ERR_ARG, "gram_precision applies to mixed mode");
@@ -1023,14 +1197,52 @@ class Context {
     ModeData& md = md_[m];
     md.N = dims_[m];
     md.nnz = nnz;
+    md.hptr = hptr;
     if (mixed_) md.packed.alloc((size_t)std::max(1LL, nnz));
-    // Task list: rows sorted by descending length; rows above the split threshold are cut into
-    // near-equal parts so that no task is much longer than the average work per row group.
-    const long long groups = (long long)num_sms_ * 16;
-    long long thr = md.nnz / (2 * groups);
-    thr = std::max(256LL, std::min(16384LL, thr));
     md.max_len = 0;
     for (long long r = 0; r < md.N; r++) md.max_len = std::max(md.max_len, hptr[r + 1] - hptr[r]);
+    if (mixed_ && KP_ == 32) {
+      // padded copy for the tensor-core sampler: rows at 16-entry boundaries, sentinel padding
+      std::vector<long long> pptr(md.N + 1, 0);
+      for (long long r = 0; r < md.N; r++)
+        pptr[r + 1] = pptr[r] + (hptr[r + 1] - hptr[r] + 15) / 16 * 16;
+      md.pptr_tc.upload(pptr.data(), pptr.size(), s_);
+      md.packed_tc.alloc((size_t)std::max(1LL, pptr[md.N]));
+      md.gram_tc.alloc((size_t)std::max(1LL, md.N) * (32 * 32 + 32));
+    }
+    md.groups = 0;
+    md.tune_state = 0;
+    long long thr = split_divisor_thr(m, 2);
+    if (autotune_ == 1) {  // a cached choice for this data: build its task lists right away
+      TuneChoice c;
+      if (TuneCache::get().find(tune_key(tune_kind(m), K_, num_sms_, md.hptr), &c)) {
+        thr = c.thr;
+        md.groups = c.groups;
+        md.tune = c;
+        md.tune_state = 2;
+      }
+    }
+    build_tasks(m, thr);
+    pack_mode(m);
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+
+  // Split threshold nnz / (div * row groups), row groups = 16 per SM, clamped to [256, 16384]:
+  // div = 2 is the default; the autotuner tries 1 to 16.
+  long long split_divisor_thr(int m, int div) const {
+    const long long groups = (long long)num_sms_ * 16;
+    return std::max(256LL, std::min(16384LL, md_[m].nnz / (div * groups)));
+  }
+
+  // Task lists of mode m at split threshold thr: rows sorted by descending length, rows above
+  // the threshold cut into near-equal parts so that no task is much longer than the average
+  // work per row group (the CUDA-core list; for the tensor-core sampler the 16-entry aligned
+  // list over the padded copy, with its split-row table); split counters and the shared
+  // split-part scratch sized to match.
+  void build_tasks(int m, long long thr) {
+    ModeData& md = md_[m];
+    const std::vector<long long>& hptr = md.hptr;
+    md.thr = thr;
     int nsplit = 0, nslots = 0;
     std::vector<RowTask> tasks = make_tasks(hptr, thr, 1, nsplit, nslots);
     md.ntasks = (int)tasks.size();
@@ -1038,13 +1250,9 @@ class Context {
     md.nslots = nslots;
     md.tasks.upload(tasks.data(), tasks.size(), s_);
     if (mixed_ && KP_ == 32) {
-      // padded copy for the tensor-core sampler: rows at 16-entry boundaries, sentinel padding
-      const int other_n = (int)dims_[1 - m];
       std::vector<long long> pptr(md.N + 1, 0);
       for (long long r = 0; r < md.N; r++)
         pptr[r + 1] = pptr[r] + (hptr[r + 1] - hptr[r] + 15) / 16 * 16;
-      md.pptr_tc.upload(pptr.data(), pptr.size(), s_);
-      md.packed_tc.alloc((size_t)std::max(1LL, pptr[md.N]));
       const long long thr16 = (thr + 15) / 16 * 16;
       int ns = 0, nsl = 0;
       std::vector<RowTask> tt = make_tasks(pptr, thr16, 16, ns, nsl);
@@ -1057,7 +1265,6 @@ class Context {
         if (t.nparts > 1 && t.part == 0) sr.push_back(make_int4(t.row, t.nparts, t.slot, 0));
       std::sort(sr.begin(), sr.end(), [](const int4& a, const int4& b) { return a.x < b.x; });
       md.split_tc.upload(sr.data(), sr.size(), s_);
-      md.gram_tc.alloc((size_t)std::max(1LL, md.N) * (32 * 32 + 32));
     }
     md.split_cnt.alloc_zero(std::max(1, nsplit), s_);
     const size_t need =
@@ -1065,8 +1272,6 @@ class Context {
                          std::max(md_[0].nslots_tc, md_[1].nslots_tc)) *
         (KP_ * KP_ + KP_);
     if (need > scratch_.n) scratch_.alloc(need);
-    pack_mode(m);
-    MG_CUDA(cudaStreamSynchronize(s_));
   }
 
   // Mixed mode: the packed (index, weight) entries of mode m and their padded copy.  The weights
@@ -1103,6 +1308,9 @@ class Context {
   // default: at tol 1e-6 the FP32 iteration needs about 1.5x the iterations of FP64, which
   // costs more than its halved gather traffic saves.
   bool cg_f32_ = false;
+  // Autotuning at mg_init (option "autotune"): 0 off, 1 on with the choice cache, 2 on and
+  // always timed
+  int autotune_ = 0;
   // Gram precision of the mixed samplers (option "gram_precision"): 0 BF16 gathers (the
   // tensor-core sampler at K = 32), 1 FP16 gathers, 2 FP32 master rounded to TF32 as gathered;
   // 1 and 2 run the CUDA-core sampler at every K
@@ -1368,8 +1576,20 @@ int mg_set_option(mg_ctx* ctx, const char* name, int value) {
     else if (n == "tensor_core_gram") c.set_use_tc(value != 0);
     else if (n == "cg_fp32") c.set_cg_f32(value != 0);
     else if (n == "gram_precision") c.set_gram(value);
+    else if (n == "autotune") c.set_autotune(value);
+    else if (n == "split_threshold") c.set_split_threshold(value);
+    else if (n == "cta_groups") c.set_cta_groups(value);
     else throw mg::MgError(MG_ERR_ARG, "unknown option " + n);
   });
+}
+
+int mg_autotune(mg_ctx* ctx, int use_cache) {
+  return guarded(ctx, [&](mg::Context& c) { c.autotune(use_cache != 0); });
+}
+
+int mg_get_tuning(mg_ctx* ctx, int mode, mg_tuning* out) {
+  if (!out) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.get_tuning(mode, out); });
 }
 
 int mg_blockcg(const int32_t* rows, const int32_t* cols, const double* vals, int64_t nnz,

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace mg {
@@ -29,8 +31,14 @@ void launch_pad(const long long* ptr, const long long* pptr, long long nrows, co
 // ---- latent sampler (sample_kernels.cu, gram_tc.cu) ----
 // gram (mixed only): the Gram precision, 0 = BF16 gathers, 1 = FP16 gathers (p.other is the FP16
 // copy, p.half_copy set), 2 = TF32 (p.other is the FP32 master copy, rounded as it is read).
+// groups: row groups per CTA (0 or any value not offered by sample_group_options: the
+// default shape).
 void launch_sample(const SampleParams& p, int KP, bool mixed, int gram, cudaStream_t s,
-                   int num_sms);
+                   int num_sms, int groups = 0);
+// The default CTA shape of the CUDA-core sampler at KP, and the shapes the autotuner may pick
+// from (the default first).
+int sample_default_groups(int KP);
+std::vector<int> sample_group_options(int KP, bool mixed, int gram);
 // Sum over the n values of (v[i] - center), or of its square when sq, on the device in a fixed
 // order; returns it to the host (synchronises the stream).
 double value_moment(const double* v, long long n, double center, bool sq, cudaStream_t s);

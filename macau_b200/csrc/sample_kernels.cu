@@ -141,13 +141,17 @@ __device__ void add_noise(const SampleParams& p, F* rr, int row, int K, int t, i
   gsync<T>(g);
 }
 
-// Minimum resident CTAs requested from the register allocator (warp-per-row instances: 16
-// warps per SM for FP32 Grams, 12 for FP64).
-template <int WPR, bool MIXED>
-constexpr int min_ctas() { return WPR == 1 ? (MIXED ? 4 : 3) : 1; }
+// Minimum resident CTAs requested from the register allocator: the resident threads per SM
+// (warp-per-row instances: 16 warps for FP32 Grams, 12 for FP64; 8 warps at WPR = 4, 16 at
+// WPR = 16) divided by the CTA size, so every CTA shape gets the same register budget.
+template <int WPR, int G, bool MIXED>
+constexpr int min_ctas() {
+  constexpr int thr = WPR == 1 ? (MIXED ? 512 : 384) : (WPR == 4 ? 256 : 512);
+  return thr / (32 * WPR * G) > 0 ? thr / (32 * WPR * G) : 1;
+}
 
 template <int KP, int WPR, int G, bool MIXED, int GE = kGeBf16>
-__global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, MIXED>())) k_sample(const SampleParams p) {
+__global__ void __launch_bounds__(32 * WPR * G, (min_ctas<WPR, G, MIXED>())) k_sample(const SampleParams p) {
   using C = Cfg<KP, WPR, MIXED, GE>;
   using Acc = typename C::Acc;
   using Elem = typename C::Elem;
@@ -533,13 +537,28 @@ void launch_t(const SampleParams& p, cudaStream_t s, int num_sms) {
   MG_CUDA(cudaGetLastError());
 }
 
+// Row groups per CTA: the default shape, or the autotuner's alternative (groups = 2 at
+// WPR = 1, 1 at WPR = 4) for BF16 gathers and FP64.
 template <int GE>
-void launch_mixed(const SampleParams& p, int KP, cudaStream_t s, int num_sms) {
+void launch_mixed(const SampleParams& p, int KP, int groups, cudaStream_t s, int num_sms) {
+  constexpr bool alt_ok = GE == kGeBf16;
   switch (KP) {
-    case 8: return launch_t<8, 1, 4, true, GE>(p, s, num_sms);
-    case 16: return launch_t<16, 1, 4, true, GE>(p, s, num_sms);
-    case 32: return launch_t<32, 1, 4, true, GE>(p, s, num_sms);
-    case 64: return launch_t<64, 4, 2, true, GE>(p, s, num_sms);
+    case 8:
+      if constexpr (alt_ok)
+        if (groups == 2) return launch_t<8, 1, 2, true, GE>(p, s, num_sms);
+      return launch_t<8, 1, 4, true, GE>(p, s, num_sms);
+    case 16:
+      if constexpr (alt_ok)
+        if (groups == 2) return launch_t<16, 1, 2, true, GE>(p, s, num_sms);
+      return launch_t<16, 1, 4, true, GE>(p, s, num_sms);
+    case 32:
+      if constexpr (alt_ok)
+        if (groups == 2) return launch_t<32, 1, 2, true, GE>(p, s, num_sms);
+      return launch_t<32, 1, 4, true, GE>(p, s, num_sms);
+    case 64:
+      if constexpr (alt_ok)
+        if (groups == 1) return launch_t<64, 4, 1, true, GE>(p, s, num_sms);
+      return launch_t<64, 4, 2, true, GE>(p, s, num_sms);
     case 128: return launch_t<128, 16, 1, true, GE>(p, s, num_sms);
   }
   throw MgError(MG_ERR_ARG, "unsupported latent dimension");
@@ -547,18 +566,35 @@ void launch_mixed(const SampleParams& p, int KP, cudaStream_t s, int num_sms) {
 
 }  // namespace
 
+int sample_default_groups(int KP) { return KP <= 32 ? 4 : (KP == 64 ? 2 : 1); }
+
+std::vector<int> sample_group_options(int KP, bool mixed, int gram) {
+  if (mixed && gram != kGeBf16) return {sample_default_groups(KP)};
+  if (KP <= 32) return {4, 2};
+  if (KP == 64) return {2, 1};
+  return {1};
+}
+
 void launch_sample(const SampleParams& p, int KP, bool mixed, int gram, cudaStream_t s,
-                   int num_sms) {
+                   int num_sms, int groups) {
   if (mixed) {
-    if (gram == kGeFp16) return launch_mixed<kGeFp16>(p, KP, s, num_sms);
-    if (gram == kGeTf32) return launch_mixed<kGeTf32>(p, KP, s, num_sms);
-    return launch_mixed<kGeBf16>(p, KP, s, num_sms);
+    if (gram == kGeFp16) return launch_mixed<kGeFp16>(p, KP, groups, s, num_sms);
+    if (gram == kGeTf32) return launch_mixed<kGeTf32>(p, KP, groups, s, num_sms);
+    return launch_mixed<kGeBf16>(p, KP, groups, s, num_sms);
   } else {
     switch (KP) {
-      case 8: return launch_t<8, 1, 4, false>(p, s, num_sms);
-      case 16: return launch_t<16, 1, 4, false>(p, s, num_sms);
-      case 32: return launch_t<32, 1, 4, false>(p, s, num_sms);
-      case 64: return launch_t<64, 4, 2, false>(p, s, num_sms);
+      case 8:
+        if (groups == 2) return launch_t<8, 1, 2, false>(p, s, num_sms);
+        return launch_t<8, 1, 4, false>(p, s, num_sms);
+      case 16:
+        if (groups == 2) return launch_t<16, 1, 2, false>(p, s, num_sms);
+        return launch_t<16, 1, 4, false>(p, s, num_sms);
+      case 32:
+        if (groups == 2) return launch_t<32, 1, 2, false>(p, s, num_sms);
+        return launch_t<32, 1, 4, false>(p, s, num_sms);
+      case 64:
+        if (groups == 1) return launch_t<64, 4, 1, false>(p, s, num_sms);
+        return launch_t<64, 4, 2, false>(p, s, num_sms);
       case 128: return launch_t<128, 16, 1, false>(p, s, num_sms);
     }
   }

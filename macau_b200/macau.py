@@ -211,7 +211,8 @@ def macau(Y,
           save_prefix=None,
           verbose=True,
           seed=None,
-          compute=None):
+          compute=None,
+          autotune=False):
     """
     Matrix factorization with side information, sampled on a B200 GPU.
       Y          training data to factorize (sparse matrix or DataFrame)
@@ -235,6 +236,9 @@ def macau(Y,
       seed         key of all random draws (None: drawn from the OS)
       compute      "fp64" or "mixed" (BF16/FP32 tensor-core sampler), default from
                    MACAU_GPU_PRECISION or "fp64"
+      autotune     time the row samplers' work splits and CTA shapes on this data before
+                   sampling and keep the fastest (choices cached per process, and in the file
+                   named by MACAU_B200_TUNE_CACHE if set); the draws are unchanged
     """
     data = Data(Y, Ytest)
 
@@ -272,6 +276,8 @@ def macau(Y,
     try:
         if adaptive:
             s.set_noise_adaptive(1.0, float(sn_max))
+        if autotune:
+            s.set_option("autotune", 1)
         s.set_relation_data(data.idxTrain[0], data.idxTrain[1], data.valTrain, data.shape)
         if len(data.valTest) > 0:
             s.set_relation_data_test(data.idxTest[0], data.idxTest[1], data.valTest, data.shape)

@@ -100,3 +100,16 @@ def test_low_rank_matrix_is_learned(variant, compute):
     else:
         r = macau_b200.bpmf(Ytr, Yte, precision=1 / 0.09, **kw)
     assert r.rmse_test < 0.45, r.rmse_test
+
+
+def test_autotuned_run_draws_the_same_chain():
+    # the autotuner only reshapes the work of the row samplers; with no row long enough to be
+    # split, the FP64 chain is the same draw for draw
+    Y, F = low_rank(4)
+    Ytr, Yte = macau_b200.make_train_test(Y, 0.1, seed=5)
+    kw = dict(num_latent=8, burnin=20, nsamples=20, verbose=False, seed=11, compute="fp64",
+              precision=1 / 0.09)
+    a = macau_b200.bpmf(Ytr, Yte, **kw)
+    b = macau_b200.bpmf(Ytr, Yte, autotune=True, **kw)
+    assert abs(a.rmse_test - b.rmse_test) < 1e-9
+    np.testing.assert_allclose(a.prediction["y_pred"], b.prediction["y_pred"], rtol=1e-9)

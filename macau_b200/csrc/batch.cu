@@ -589,33 +589,28 @@ class Batch {
   void autotune(bool use_cache) {
     if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_batch_init before autotuning");
     drop_graphs();
-    Ctl saved{};
-    MG_CUDA(cudaMemcpyAsync(&saved, ctl_.p, sizeof(Ctl), cudaMemcpyDeviceToHost, s_));
-    MG_CUDA(cudaStreamSynchronize(s_));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    MG_CUDA(cudaEventCreate(&e0));
-    MG_CUDA(cudaEventCreate(&e1));
     try {
+      DeviceBackup ctl_backup(s_);
+      ctl_backup.save(ctl_.p, sizeof(Ctl));
+      MG_CUDA(cudaEventCreate(&e0));
+      MG_CUDA(cudaEventCreate(&e1));
       for (int m = 0; m < 2; m++) {
         Mode& md = md_[m];
-        std::string key = tune_key("batch", 32, num_sms_, md.hpptr);
-        for (int p = 0; p < P_; p++) key += (p ? "," : ":k") + std::to_string(K_[p]);
+        const std::string key = tune_key("batch", 32, num_sms_, md.hpptr) + ":k" + ks_digest();
         TuneChoice c;
         if (use_cache && TuneCache::get().find(key, &c)) {
-          md.fin_per_sm = c.groups;
-          build_tasks(m, c.thr);
+          if (md.thr != c.thr || md.fin_per_sm != c.groups) {
+            md.fin_per_sm = c.groups;
+            build_tasks(m, c.thr);
+          }
           md.tune = c;
           md.tune_state = 2;
           continue;
         }
-        DBuf<float> k32;
-        DBuf<__nv_bfloat16> k16;
-        k32.alloc(lat32_[m].n);
-        k16.alloc(lat16_[m].n);
-        MG_CUDA(cudaMemcpyAsync(k32.p, lat32_[m].p, lat32_[m].n * sizeof(float),
-                                cudaMemcpyDeviceToDevice, s_));
-        MG_CUDA(cudaMemcpyAsync(k16.p, lat16_[m].p, lat16_[m].n * sizeof(__nv_bfloat16),
-                                cudaMemcpyDeviceToDevice, s_));
+        DeviceBackup lat_backup(s_);  // put back before the next mode, or when a run throws
+        lat_backup.save(lat32_[m].p, lat32_[m].n * sizeof(float));
+        lat_backup.save(lat16_[m].p, lat16_[m].n * sizeof(__nv_bfloat16));
         std::vector<long long> thrs;
         for (int div : {2, 1, 4, 8, 16}) {
           const long long t = split_divisor_thr(m, div);
@@ -654,22 +649,28 @@ class Batch {
         md.tune = best;
         md.tune_state = 1;
         TuneCache::get().put(key, best);
-        MG_CUDA(cudaMemcpyAsync(lat32_[m].p, k32.p, lat32_[m].n * sizeof(float),
-                                cudaMemcpyDeviceToDevice, s_));
-        MG_CUDA(cudaMemcpyAsync(lat16_[m].p, k16.p, lat16_[m].n * sizeof(__nv_bfloat16),
-                                cudaMemcpyDeviceToDevice, s_));
-        MG_CUDA(cudaStreamSynchronize(s_));
       }
     } catch (...) {
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
       throw;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    MG_CUDA(cudaMemcpyAsync(ctl_.p, &saved, sizeof(Ctl), cudaMemcpyHostToDevice, s_));
     MG_CUDA(cudaStreamSynchronize(s_));
     drop_graphs();
+  }
+
+  // Problem count and an FNV-1a digest of the problems' K values (part of the tuning key).
+  std::string ks_digest() const {
+    unsigned long long h = 1469598103934665603ull;
+    for (int k : K_) {
+      h ^= (unsigned long long)k;
+      h *= 1099511628211ull;
+    }
+    char buf[48];
+    std::snprintf(buf, sizeof(buf), "%d:%016llx", P_, h);
+    return buf;
   }
 
   void get_tuning(int m, mg_tuning* out) const {

@@ -552,16 +552,15 @@ class Context {
   void autotune(bool use_cache) {
     if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_init before autotuning");
     drop_graphs();
-    Ctl saved_ctl{};
-    MG_CUDA(cudaMemcpyAsync(&saved_ctl, ctl_.p, sizeof(Ctl), cudaMemcpyDeviceToHost, s_));
-    MG_CUDA(cudaStreamSynchronize(s_));
     const long long saved_launches = launches_;
     const double saved_ts = t_sample_;
     const long long saved_retries[2] = {retries_[0], retries_[1]};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    MG_CUDA(cudaEventCreate(&e0));
-    MG_CUDA(cudaEventCreate(&e1));
     try {
+      DeviceBackup ctl_backup(s_);  // the control block (sweep, queues, retry counts, alpha)
+      ctl_backup.save(ctl_.p, sizeof(Ctl));
+      MG_CUDA(cudaEventCreate(&e0));
+      MG_CUDA(cudaEventCreate(&e1));
       for (int m = 0; m < 2; m++) {
         ModeData& md = md_[m];
         const bool tc = uses_tc(m);
@@ -576,24 +575,13 @@ class Context {
           md.tune_state = 2;
           continue;
         }
-        // the latents this mode's timing runs overwrite
+        // the latents this mode's timing runs overwrite, put back before the next mode (whose
+        // sampler reads them) or when a run throws
+        DeviceBackup lat_backup(s_);
         const size_t n = (size_t)dims_[m] * KP_;
-        DBuf<double> keep64;
-        DBuf<float> keep32;
-        DBuf<__nv_bfloat16> keep16;
-        if (lat64_[m].p) {
-          keep64.alloc(n);
-          MG_CUDA(cudaMemcpyAsync(keep64.p, lat64_[m].p, n * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-        }
-        if (lat32_[m].p) {
-          keep32.alloc(n);
-          MG_CUDA(cudaMemcpyAsync(keep32.p, lat32_[m].p, n * sizeof(float), cudaMemcpyDeviceToDevice, s_));
-        }
-        if (lat16_[m].p) {
-          keep16.alloc(lat16_[m].n);
-          MG_CUDA(cudaMemcpyAsync(keep16.p, lat16_[m].p, lat16_[m].n * sizeof(__nv_bfloat16),
-                                  cudaMemcpyDeviceToDevice, s_));
-        }
+        if (lat64_[m].p) lat_backup.save(lat64_[m].p, n * sizeof(double));
+        if (lat32_[m].p) lat_backup.save(lat32_[m].p, n * sizeof(float));
+        if (lat16_[m].p) lat_backup.save(lat16_[m].p, lat16_[m].n * sizeof(__nv_bfloat16));
         std::vector<long long> thrs;
         for (int div : {2, 1, 4, 8, 16}) {
           const long long t = split_divisor_thr(m, div);
@@ -633,23 +621,18 @@ class Context {
         md.tune = best;
         md.tune_state = 1;
         TuneCache::get().put(key, best);
-        if (keep64.p)
-          MG_CUDA(cudaMemcpyAsync(lat64_[m].p, keep64.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-        if (keep32.p)
-          MG_CUDA(cudaMemcpyAsync(lat32_[m].p, keep32.p, n * sizeof(float), cudaMemcpyDeviceToDevice, s_));
-        if (keep16.p)
-          MG_CUDA(cudaMemcpyAsync(lat16_[m].p, keep16.p, lat16_[m].n * sizeof(__nv_bfloat16),
-                                  cudaMemcpyDeviceToDevice, s_));
-        MG_CUDA(cudaStreamSynchronize(s_));
       }
     } catch (...) {
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+      launches_ = saved_launches;
+      t_sample_ = saved_ts;
+      retries_[0] = saved_retries[0];
+      retries_[1] = saved_retries[1];
       throw;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    MG_CUDA(cudaMemcpyAsync(ctl_.p, &saved_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, s_));
     MG_CUDA(cudaStreamSynchronize(s_));
     launches_ = saved_launches;
     t_sample_ = saved_ts;

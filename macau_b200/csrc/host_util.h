@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <list>
 #include <vector>
 
 #include "common.cuh"
@@ -42,6 +43,41 @@ struct DBuf {
     if (count) MG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
     g_h2d_bytes += (long long)(count * sizeof(T));
   }
+};
+
+// Device copies of buffers, taken on a stream and written back when the object goes out of
+// scope, also while an exception unwinds (a failed write-back there is ignored; it surfaces at
+// the next checked call).  The autotuner keeps the state its timing runs overwrite in one.
+class DeviceBackup {
+ public:
+  explicit DeviceBackup(cudaStream_t s) : s_(s) {}
+  DeviceBackup(const DeviceBackup&) = delete;
+  DeviceBackup& operator=(const DeviceBackup&) = delete;
+  void save(void* p, size_t bytes) {
+    if (!p || bytes == 0) return;
+    items_.emplace_back();
+    Item& it = items_.back();
+    it.dst = p;
+    it.bytes = bytes;
+    it.copy.alloc(bytes);
+    MG_CUDA(cudaMemcpyAsync(it.copy.p, p, bytes, cudaMemcpyDeviceToDevice, s_));
+    it.ok = true;
+  }
+  ~DeviceBackup() {
+    for (Item& it : items_)
+      if (it.ok) cudaMemcpyAsync(it.dst, it.copy.p, it.bytes, cudaMemcpyDeviceToDevice, s_);
+    cudaStreamSynchronize(s_);
+  }
+
+ private:
+  struct Item {
+    void* dst = nullptr;
+    size_t bytes = 0;
+    bool ok = false;
+    DBuf<unsigned char> copy;
+  };
+  cudaStream_t s_;
+  std::list<Item> items_;  // DBuf does not move: list nodes stay in place
 };
 
 // Task list over rows with lengths len(r) = ptr[r+1] - ptr[r] (positions ptr[r]): rows longer

@@ -19,7 +19,9 @@ variable, else "fp64").
 """
 import numbers
 import os
+import signal
 import sys
+import threading
 
 import numpy as np
 import pandas as pd
@@ -174,6 +176,35 @@ def _side_coo(s, nrows):
     raise TypeError("Unsupported side information type: '%s'" % type(s).__name__)
 
 
+class _StopOnInterrupt(object):
+    """Ctrl-C during the sweeps: the reference's SIGINT handler (macau.cpp:30-35) prints a note
+    and the run stops after the current iteration (macau.cpp:111-114), returning the results so
+    far.  Installed only from the main thread; the previous handler is put back on exit (the
+    reference's caller restores Python's default one, macau.pyx:421)."""
+
+    MESSAGE = "[Received Ctrl-C. Stopping after finishing the current iteration.]"
+
+    def __init__(self):
+        self.requested = False
+        self._previous = None
+
+    def _handler(self, signum, frame):
+        self.requested = True
+        print(self.MESSAGE)
+        sys.stdout.flush()
+
+    def __enter__(self):
+        if threading.current_thread() is threading.main_thread():
+            self._previous = signal.signal(signal.SIGINT, self._handler)
+        return self
+
+    def __exit__(self, *exc):
+        if self._previous is not None:
+            signal.signal(signal.SIGINT, self._previous)
+            self._previous = None
+        return False
+
+
 def _compute_mode(compute):
     if compute is None:
         compute = os.environ.get("MACAU_GPU_PRECISION", "fp64")
@@ -305,21 +336,25 @@ def macau(Y,
         if save_prefix is not None:
             _write_csv(save_prefix + "-meanvalue.csv", [[s.mean_value()]])
         import time
-        for i in range(burnin + nsamples):
-            if verbose and i == burnin:
-                print(" ====== Burn-in complete, averaging samples ====== ")
-            t0 = time.time()
-            s.sweep(i, eval=True)
-            if save_prefix is not None and i >= burnin:
-                _save_sample(s, save_prefix, i - burnin + 1)
-            if verbose:
-                r, r1 = s.rmse()
-                norms = [np.linalg.norm(s.latents(m)) for m in range(2)]
-                links = ["%1.2e" % np.linalg.norm(s.beta(m)) if s.nfeat[m] else "nan" for m in range(2)]
-                prec = "Prec:%.2g" % s.noise()[0] if adaptive else ""  # noisemodels.h:77-79
-                print("Iter %3d: RMSE: %.5f (1samp: %.5f)  U:[%1.2e, %1.2e]\tSide:[%s]%s [took %0.1fs]" %
-                      (i, r, r1, norms[0], norms[1], ", ".join(links), prec, time.time() - t0))
-                sys.stdout.flush()
+        with _StopOnInterrupt() as stop:
+            for i in range(burnin + nsamples):
+                if stop.requested:
+                    break
+                if verbose and i == burnin:
+                    print(" ====== Burn-in complete, averaging samples ====== ")
+                t0 = time.time()
+                s.sweep(i, eval=True)
+                if save_prefix is not None and i >= burnin:
+                    _save_sample(s, save_prefix, i - burnin + 1)
+                if verbose:
+                    r, r1 = s.rmse()
+                    norms = [np.linalg.norm(s.latents(m)) for m in range(2)]
+                    links = ["%1.2e" % np.linalg.norm(s.beta(m)) if s.nfeat[m] else "nan"
+                             for m in range(2)]
+                    prec = "Prec:%.2g" % s.noise()[0] if adaptive else ""  # noisemodels.h:77-79
+                    print("Iter %3d: RMSE: %.5f (1samp: %.5f)  U:[%1.2e, %1.2e]\tSide:[%s]%s [took %0.1fs]" %
+                          (i, r, r1, norms[0], norms[1], ", ".join(links), prec, time.time() - t0))
+                    sys.stdout.flush()
         rmse_test, _ = s.rmse()
         yhat = s.predictions()
         yhat_sd = s.stds()

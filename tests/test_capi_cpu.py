@@ -101,3 +101,25 @@ def test_workload_generators_shapes():
     w = workloads.macau_side(scale=0.01)
     fr, fc, fv, shp = w["side"]
     assert fv is None and fc.max() < shp[1]
+
+
+def test_ctrl_c_stops_after_the_current_iteration(capsys):
+    # macau()'s sweep loop runs inside _StopOnInterrupt: SIGINT sets a flag and prints the
+    # reference's note (macau.cpp:30-35) instead of raising, and the previous handler comes back
+    import os
+    import signal
+    import time
+
+    from macau_b200.macau import _StopOnInterrupt
+
+    before = signal.getsignal(signal.SIGINT)
+    with _StopOnInterrupt() as stop:
+        assert not stop.requested
+        os.kill(os.getpid(), signal.SIGINT)
+        for _ in range(100):
+            if stop.requested:
+                break
+            time.sleep(0.01)
+        assert stop.requested
+    assert signal.getsignal(signal.SIGINT) is before
+    assert _StopOnInterrupt.MESSAGE in capsys.readouterr().out

@@ -53,3 +53,29 @@ def test_single_process_needs_no_process_group():
     assert r.world == 1 and r.dist is None and r.chain_seed() == 1000
     assert r.max(3.5) == 3.5 and r.rate(10, 2.0) == 5.0
     r.close()
+
+
+def test_reference_arm_under_torchrun_prints_one_line():
+    # bench.py --impl reference launched like the N > 1 runs: rank 0 times the CPU oracle and
+    # prints the one JSON line, the other rank exits 0 without work
+    import json
+    import socket
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parent.parent
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(root / "bench.py"),
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1",
+           "--scale", "0.01"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=240, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0

@@ -123,3 +123,24 @@ def test_ctrl_c_stops_after_the_current_iteration(capsys):
         assert stop.requested
     assert signal.getsignal(signal.SIGINT) is before
     assert _StopOnInterrupt.MESSAGE in capsys.readouterr().out
+
+
+def test_cpp_host_class_builds_and_reports_errors(tmp_path):
+    # include/macau_b200.hpp compiles against the header, links the library, and turns the
+    # library's error into std::runtime_error (here: no GPU in this process's view)
+    import shutil
+
+    from macau_b200 import workloads
+    from tests import cpp_host
+
+    if shutil.which("g++") is None:
+        pytest.skip("needs g++")
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present (the GPU run is compared with the ctypes path elsewhere)")
+    exe = cpp_host.build(tmp_path)
+    w = workloads.bpmf_uniform(nrow=50, ncol=40, nobs=600, seed=1)
+    cpp_host.write_data(tmp_path / "d.bin", w, 4, 2, 2)
+    code, out, err = cpp_host.run(exe, tmp_path / "d.bin", 5)
+    assert code == 2 and out.get("ERROR"), (code, out, err)
+    assert "CUDA" in out["ERROR"] or "GPU" in out["ERROR"] or "device" in out["ERROR"], out

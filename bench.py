@@ -13,6 +13,8 @@ events on the library's stream; `e2e` is the same metric through the C ABI with 
 (data upload and CSR build, per-sweep RMSE read-back and the final prediction read-back inside
 the timed region).  `--impl reference` times the CPU oracle (FP64 restatement of the reference,
 OpenMP on all host cores).  Under torchrun each rank runs an independent chain on its own GPU.
+Both GPU arms pick their row samplers' work split and CTA shape with the library's autotuner at
+initialisation (outside the timed region; `--no-autotune` keeps the default shapes).
 """
 import argparse
 import json

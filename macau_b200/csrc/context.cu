@@ -936,7 +936,9 @@ class Context {
           get_noise(nz);
           snprintf(prec, sizeof prec, "Prec:%.2g", nz[0]);
         }
-        printf("Iter %3d: RMSE: %.5f (1samp: %.5f)  U:[%1.2e, %1.2e]\tSide:[%s, %s]%s [took %0.1fs]\n",
+        // NoiseModel::getEvalString (noisemodels.h:46): to_string_with_precision(rmse, 5), an
+        // ostream at precision 5 in its default float format, which is printf's %.5g
+        printf("Iter %3d: RMSE: %.5g (1samp: %.5g)  U:[%1.2e, %1.2e]\tSide:[%s, %s]%s [took %0.1fs]\n",
                i, r[0], r[1], latent_norm(0), latent_norm(1), link_norm_str(0).c_str(),
                link_norm_str(1).c_str(), prec, took);
         fflush(stdout);

@@ -352,7 +352,9 @@ def macau(Y,
                     links = ["%1.2e" % np.linalg.norm(s.beta(m)) if s.nfeat[m] else "nan"
                              for m in range(2)]
                     prec = "Prec:%.2g" % s.noise()[0] if adaptive else ""  # noisemodels.h:77-79
-                    print("Iter %3d: RMSE: %.5f (1samp: %.5f)  U:[%1.2e, %1.2e]\tSide:[%s]%s [took %0.1fs]" %
+                    # getEvalString (noisemodels.h:46): 5 significant digits, C++ ostream
+                    # default format = %.5g
+                    print("Iter %3d: RMSE: %.5g (1samp: %.5g)  U:[%1.2e, %1.2e]\tSide:[%s]%s [took %0.1fs]" %
                           (i, r, r1, norms[0], norms[1], ", ".join(links), prec, time.time() - t0))
                     sys.stdout.flush()
         rmse_test, _ = s.rmse()

@@ -186,6 +186,7 @@ class _StopOnInterrupt(object):
 
     def __init__(self):
         self.requested = False
+        self._installed = False
         self._previous = None
 
     def _handler(self, signum, frame):
@@ -196,11 +197,15 @@ class _StopOnInterrupt(object):
     def __enter__(self):
         if threading.current_thread() is threading.main_thread():
             self._previous = signal.signal(signal.SIGINT, self._handler)
+            self._installed = True
         return self
 
     def __exit__(self, *exc):
-        if self._previous is not None:
-            signal.signal(signal.SIGINT, self._previous)
+        if self._installed:
+            # None: the previous handler was not set from Python; fall back to Python's default
+            prev = self._previous if self._previous is not None else signal.default_int_handler
+            signal.signal(signal.SIGINT, prev)
+            self._installed = False
             self._previous = None
         return False
 

@@ -7,11 +7,13 @@
 // row, the producers gather the four rows' BF16 other-factor vectors (64 B each, by CSR column
 // index) with 16-byte cp.async copies into one shared-memory stage of five SW64 MN-major column
 // blocks (32 elements wide, two K-atoms of 8 k-rows x 64 B): block p holds row p's 32 latent
-// values, block 4 holds the rows' (y - mean) * alpha in elements 0..3.  One tcgen05.mma
-// (M = 128, N = 160, K = 16, BF16 in, FP32 accumulate in TMEM) per stage adds
+// values, block 4 holds the rows' weights w = (y - mean) * alpha split into two BF16 parts, the
+// rounded weight in elements 0..3 and the remainder w - bf16(w) in elements 4..7.  One
+// tcgen05.mma (M = 128, N = 160, K = 16, BF16 in, FP32 accumulate in TMEM) per stage adds
 //     D[32p + i][32q + j] += sum_k X_p[k][i] X_q[k][j],   D[32p + i][128 + q] += sum_k X_p[k][i] w_q[k]
-// whose diagonal blocks p == q are the four rows' Grams and whose column 128 + p is row p's
-// right-hand side sum v (y - mean) alpha (the off-diagonal blocks are not used).  D row r lives
+// whose diagonal blocks p == q are the four rows' Grams and whose columns 128 + p and 132 + p
+// sum to row p's right-hand side sum v (y - mean) alpha (the off-diagonal blocks are not used);
+// the weights thus enter with 16 significant bits, not BF16's 8.  D row r lives
 // in TMEM lane r, so the epilogue warp of quadrant p reads row p's Gram with one 32x32b load.
 // (A TMA tile::gather4 variant of the producers was measured slower: a gather4 of 64-byte rows
 // into a 64B-swizzled stage must start on the 512-byte swizzle period, which leaves half of each
@@ -349,7 +351,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 
   // ---- set-up ----
-  // zero the stages once: k-rows 4..7 of every K-atom and weight elements 4..31 stay zero
+  // zero the stages once: weight elements 8..31 stay zero
   for (int e = threadIdx.x; e < kStages * kStageBytes / 16; e += blockDim.x)
     reinterpret_cast<uint4*>(stages)[e] = make_uint4(0u, 0u, 0u, 0u);
   if (threadIdx.x == 0) {
@@ -395,7 +397,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     constexpr int kLag = 1;
     const int r = warp % kRowSlots, h = warp / kRowSlots;
     const int ch = lane & 3, e0 = lane >> 2;
-    const uint32_t woff = stage_off(128 + r, lane & 15);  // this lane's weight in a stage
+    // this lane's weight element in a stage: lanes 0-15 hold the BF16 weight of entry lane % 16
+    // in B column 128 + r, lanes 16-31 the BF16 remainder w - bf16(w) in column 132 + r, so the
+    // two accumulated right-hand-side columns add up to sum v w with w kept to 16 mantissa bits
+    const uint32_t woff = stage_off(128 + r + 4 * (lane >> 4), lane & 15);
     const uint32_t o0 = stage_off(32 * r + 8 * ch, e0), o1 = stage_off(32 * r + 8 * ch, e0 + 8);
     const __nv_bfloat16* V = reinterpret_cast<const __nv_bfloat16*>(p.other);
     const unsigned sentinel = (unsigned)p.nother;  // the zero row of the BF16 factor
@@ -411,6 +416,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const unsigned col0 = v ? sh->csr[h][slot][r][e0].x : sentinel;
       const unsigned col1 = v ? sh->csr[h][slot][r][e0 + 8].x : sentinel;
       const float w = v ? __uint_as_float(sh->csr[h][slot][r][lane & 15].y) * wscale : 0.f;
+      const __nv_bfloat16 w_hi = __float2bfloat16_rn(w);
+      const __nv_bfloat16 w_st =
+          lane < 16 ? w_hi : __float2bfloat16_rn(w - __bfloat162float(w_hi));
       const int stage = m.x % kStages;
       const uint32_t phase = (uint32_t)((m.x / kStages) & 1);
       __syncwarp();
@@ -420,7 +428,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       cp16(sbase + o0, V + (size_t)col0 * 32 + 8 * ch);
       cp16(sbase + o1, V + (size_t)col1 * 32 + 8 * ch);
       cp_commit();
-      if (lane < 16) *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = __float2bfloat16_rn(w);
+      *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = w_st;
 #pragma unroll
       for (int q = 0; q <= kLag; q++)
         if (q == i % (kLag + 1)) pend[q] = stage;
@@ -570,8 +578,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       if (!stop) {
         const uint32_t lanes = (uint32_t)(32 * qd) << 16;
         tmem_ld32(tmem + lanes + (uint32_t)(slot * kSlotCols + 32 * qd), gr);
-        rhs = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 128 + qd));
+        const float rhs_hi = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 128 + qd));
+        const float rhs_lo = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 132 + qd));
         tmem_wait_ld();
+        rhs = rhs_hi + rhs_lo;
       }
       tc_fence_before();
       __syncwarp();

@@ -17,7 +17,7 @@ from tests.gpu_helpers import gpu_sampler, oracle_model, random_spd, relerr, tra
 pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-9
-MIXED_SAMPLE_TOL = 2e-2   # BF16 Gram + FP32 factor vs FP64, norm-wise relative per sweep
+MIXED_SAMPLE_TOL = 6e-3   # BF16 Gram + FP32 factor vs FP64, norm-wise relative per sweep
 
 
 def small_uniform(seed=0, nrow=300, ncol=200, nobs=6000):
@@ -622,6 +622,32 @@ def test_batch_matches_single_problem_contexts():
             r, r1 = s.rmse()
             assert abs(rb[p, 0] - r) < tol * r and abs(rb[p, 1] - r1) < tol * r1
         b.close()
+
+
+def test_batch_matches_oracle_per_problem():
+    # the reference runs one Macau object per problem (macau.pyx:221-234); here every problem of
+    # one batch is compared after each of its first sweeps with an FP64 oracle chain of that
+    # problem and seed (same keyed draws): latents of both modes, hyperparameters and the
+    # running RMSE.  K = 8, 16 and 32 all occur.
+    problems, Ks, seeds = workloads.batched_uneven(nprob=10, rows=(60, 400), cols=(40, 260),
+                                                   density=(0.04, 0.2))
+    assert {8, 16, 32} <= set(Ks), Ks
+    alpha, burnin = 4.0, 1
+    b = _lib.Batch(problems, Ks, seeds, alpha)
+    b.init(burnin)
+    models = [oracle_model(pr, K, alpha, sd) for pr, K, sd in zip(problems, Ks, seeds)]
+    for it, tol in enumerate((MIXED_SAMPLE_TOL, 2 * MIXED_SAMPLE_TOL, 4 * MIXED_SAMPLE_TOL)):
+        b.sweeps(it, 1, eval=True)
+        rb = b.rmse()
+        for p, m in enumerate(models):
+            assert m.sweep(it, burnin) == 0
+            for mode in (0, 1):
+                err = relerr(b.latents(p, mode), m.latents(mode))
+                assert err < tol, (it, p, Ks[p], mode, err)
+            ro = m.rmse()
+            assert abs(rb[p, 0] - ro[0]) < tol * ro[0], (it, p, rb[p], ro)
+            assert abs(rb[p, 1] - ro[1]) < tol * ro[1], (it, p, rb[p], ro)
+    b.close()
 
 
 def test_batch_learns_every_problem():

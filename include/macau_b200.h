@@ -285,20 +285,21 @@ int mg_blockcg(const int32_t* rows, const int32_t* cols, const double* vals, int
 
 /* Hyperprior update without device allocation.  No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc when they resample the Normal-Wishart hyperparameters --
- * a process whose memory pool already owns the device memory, code recording a CUDA graph
- * (cudaMalloc is not allowed during stream capture), or a loop that cannot take cudaMalloc's
- * implicit synchronisation.  It computes what mg_update_prior does for a BPMF prior
- * (CondNormalWishart, mvnormal.cpp:314-336) from device inputs into device outputs:
+ * a process whose memory pool already owns the device memory, or a loop that cannot take
+ * cudaMalloc's implicit synchronisation.  It draws the same (mu, Lambda) as mg_update_prior does
+ * for a BPMF prior (the posterior of the latent vectors' mean and precision under the
+ * Normal-Wishart prior, then one draw of each), from device inputs into device outputs:
  *   U           N latent vectors of K doubles, vector n at U + n * stride (device)
  *   mu0, T      prior mean (K) and scale matrix (K x K, column-major), device
- *   kappa, nu   prior strength and degrees of freedom (BPMFPrior: 2 and K)
+ *   kappa, nu   prior strength (> 0) and degrees of freedom (>= K); a BPMF prior uses 2 and K
  *   seed, sweep, mode  key of the Wishart / mean draws (same keys as mg_update_prior)
  *   mu_out, Lambda_out device outputs (K and K x K); stream: cudaStream_t (NULL = default)
  *   err / errlen optional caller buffer for a message (NULL allowed)
  * Its scratch is one fixed 2.3 MB array in the library (every GPU that loads the library holds
- * it until exit), so K is limited to 64; larger K returns MG_ERR_ARG.  All calls share that
- * array: calls whose kernels overlap on the GPU race.  The first call on a device looks the
- * array up; make it before any stream capture.  Synchronous (waits for `stream`). */
+ * it until exit), so K is limited to 64; larger K, nu < K or kappa <= 0 return MG_ERR_ARG.  All
+ * calls share that array and it keeps the last call's contents: calls whose kernels overlap on
+ * the GPU race.  The first call in a device's CUDA context looks the array's address up.
+ * Synchronous: it reads the status word back and waits for `stream`. */
 int mg_normal_wishart_noalloc(const double* U, int64_t N, int K, int stride, const double* mu0,
                               double kappa, const double* T, int nu, uint64_t seed,
                               uint32_t sweep, int mode, double* mu_out, double* Lambda_out,

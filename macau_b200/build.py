@@ -71,7 +71,7 @@ def build(verbose=False, ptxas=False):
             sys.stdout.write(log)
     if not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         cmd = [nvcc(), "-shared", "-o", str(LIB)] + [str(o) for o in objs] + ARCH + [
-            "-ccbin", host_compiler(), "-lcudart", "-lcuda"]
+            "-ccbin", host_compiler(), "-lcudart"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -3,12 +3,11 @@
 // The context API (mg_update_prior) keeps its reduction partials and Normal-Wishart workspace in
 // buffers it cudaMalloc's at mg_init.  Some hosts cannot allocate at the point where they want
 // to resample the hyperparameters: a serving process whose memory pool already owns all of the
-// device memory, a caller that is recording work into a CUDA graph (plain cudaMalloc is not
-// allowed while a stream is being captured), or a latency-sensitive loop that cannot afford
-// cudaMalloc's implicit device synchronisation.  For them this entry point runs the same kernels
-// (k_stats + k_normal_wishart) with all of their scratch in one file-scope __device__ array of
-// fixed size, so the only device memory it touches besides that array is the caller's inputs
-// and outputs.
+// device memory (a further cudaMalloc would fail, or would have to evict the pool's blocks), or
+// a latency-sensitive loop that cannot afford cudaMalloc's implicit device synchronisation.  For
+// them this entry point runs the same kernels (k_stats + k_normal_wishart) with all of their
+// scratch in one file-scope __device__ array of fixed size, so the only device memory it touches
+// besides that array is the caller's inputs and outputs.
 //
 // Limits and sharing rules:
 //   * K <= kNoAllocMaxK (64); the row reduction uses at most kNoAllocMaxParts (64) partial sums.
@@ -17,8 +16,12 @@
 //     The control block (status word, sweep index) is cleared by each call; the partials and
 //     workspace are fully overwritten before they are read.  Calls whose kernels overlap on the
 //     GPU (different streams, or different host threads without ordering) race on the array.
-//   * The first call on a device looks up the array's device address (cudaGetSymbolAddress)
-//     with that device current and caches it; make that first call before any stream capture.
+//   * The call is synchronous: it copies the status word back and waits for `stream`, so it
+//     cannot be recorded into a CUDA graph.
+//   * The first call in a CUDA context of a device looks up the array's device address
+//     (cudaGetSymbolAddress) with that device current and caches it under the context's unique
+//     id; a context created later on the same device (after cudaDeviceReset) is looked up anew.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -43,24 +46,56 @@ __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 std::mutex g_setup_mutex;
 void* g_scratch_addr[64] = {nullptr};
+unsigned long long g_scratch_ctx[64] = {0};  // unique id of the context the address belongs to
 
 // Copies a message into the caller's buffer (no allocation).
 void set_error(char* buf, int len, const char* msg) {
   if (buf && len > 0) snprintf(buf, (size_t)len, "%s", msg);
 }
 
-// Device address of the scratch array on the current device (looked up once per device).
+// Unique id of the CUDA context current on this thread, 0 when none is bound yet.  The two
+// driver functions are fetched through the runtime (cudaGetDriverEntryPoint), so the library
+// needs no link-time dependency on the driver library.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f0 = nullptr;
+    void* f1 = nullptr;
+    cudaDriverEntryPointQueryResult q0 = cudaDriverEntryPointSymbolNotFound, q1 = q0;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+      return 0;
+    get_current = reinterpret_cast<GetCurrent>(f0);
+    get_id = reinterpret_cast<GetId>(f1);
+  }
+  CUcontext cu = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&cu) != CUDA_SUCCESS || cu == nullptr) return 0;
+  if (get_id(cu, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of the scratch array on the current device, looked up once per device and
+// CUDA context (the lookup itself binds the device's primary context when none is current).
 cudaError_t scratch_address(double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
+  unsigned long long ctx_id = current_context_id();
+  if (ctx_id == 0 || !g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx_id) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
+    if (ctx_id == 0) ctx_id = current_context_id();
+    if (ctx_id == 0) return cudaErrorDeviceUninitialized;
     g_scratch_addr[dev] = p;
+    g_scratch_ctx[dev] = ctx_id;
   }
   *out = static_cast<double*>(g_scratch_addr[dev]);
   return cudaSuccess;
@@ -83,6 +118,12 @@ extern "C" int mg_normal_wishart_noalloc(const double* U, int64_t N, int K, int 
   }
   if (N < 1 || stride < K || !U || !mu0 || !T || !mu_out || !Lambda_out) {
     set_error(err, errlen, "mg_normal_wishart_noalloc: invalid argument");
+    return MG_ERR_ARG;
+  }
+  // the Bartlett factor draws chi-square variates with nu + N - i degrees of freedom (i < K)
+  // and the posterior mean is scaled by 1 / (kappa + N): both need nu >= K and kappa > 0
+  if (nu < K || !(kappa > 0.0)) {
+    set_error(err, errlen, "mg_normal_wishart_noalloc: needs nu >= K and kappa > 0");
     return MG_ERR_ARG;
   }
   try {

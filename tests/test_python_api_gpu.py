@@ -113,3 +113,59 @@ def test_autotuned_run_draws_the_same_chain():
     b = macau_b200.bpmf(Ytr, Yte, autotune=True, **kw)
     assert abs(a.rmse_test - b.rmse_test) < 1e-9
     np.testing.assert_allclose(a.prediction["y_pred"], b.prediction["y_pred"], rtol=1e-9)
+
+
+def _read_csv_checked(path):
+    """A model file of writeToCSVfile (bpmfutils.h:169-173): lines of ','-joined values, six
+    significant digits (the %.6g form of C++'s default stream format), no trailing newline."""
+    text = path.read_text()
+    assert not text.endswith("\n")
+    rows = [line.split(",") for line in text.split("\n")]
+    for row in rows:
+        for tok in row:
+            assert format(float(tok), ".6g") == tok, tok
+    return np.array([[float(t) for t in row] for row in rows])
+
+
+def test_save_prefix_writes_the_reference_model_files(tmp_path):
+    # MacauX::saveGlobalParams / saveModel (macau.cpp:191-205), BPMFPrior / MacauPrior::saveModel
+    # (latentprior.cpp:307-315): file names, K x N shapes, six significant digits, and the last
+    # sample's values against the same chain run through the C ABI
+    from macau_b200 import _lib
+    rng = np.random.default_rng(5)
+    nrow, ncol, nfeat, K, burnin, nsamples, seed = 120, 80, 30, 6, 2, 3, 9
+    Y, Ytest = macau_b200.make_train_test(rand(nrow, ncol, 0.25, 6), 0.2, seed=3)
+    F = sp.random(nrow, nfeat, density=0.1, format="coo", random_state=7)
+    F.data[:] = 1.0
+    prefix = tmp_path / "model"
+    macau_b200.macau(Y, Ytest=Ytest, side=[F, None], num_latent=K, precision=2.0, burnin=burnin,
+                     nsamples=nsamples, save_prefix=str(prefix), verbose=False, seed=seed)
+    want = {"model-meanvalue.csv"}
+    for n in range(1, nsamples + 1):
+        for m in (1, 2):
+            want |= {f"model-sample{n}-U{m}-latents.csv", f"model-sample{n}-U{m}-latentmean.csv"}
+        want.add(f"model-sample{n}-U1-link.csv")
+    assert {p.name for p in tmp_path.iterdir()} == want
+    last = f"model-sample{nsamples}-"
+    U = _read_csv_checked(tmp_path / (last + "U1-latents.csv"))
+    V = _read_csv_checked(tmp_path / (last + "U2-latents.csv"))
+    mu = _read_csv_checked(tmp_path / (last + "U1-latentmean.csv"))
+    link = _read_csv_checked(tmp_path / (last + "U1-link.csv"))
+    mean = _read_csv_checked(tmp_path / "model-meanvalue.csv")
+    assert U.shape == (K, nrow) and V.shape == (K, ncol)
+    assert mu.shape == (K, 1) and link.shape == (K, nfeat) and mean.shape == (1, 1)
+    Yc = Y.tocoo()
+    Tc = Ytest.tocoo()
+    s = _lib.Sampler(K, 2.0, seed=seed)
+    s.set_relation_data(Yc.row, Yc.col, Yc.data, Y.shape)
+    s.set_relation_data_test(Tc.row, Tc.col, Tc.data, Y.shape)
+    s.set_side(0, F.row, F.col, None, F.shape, 5.0, 1e-6)
+    s.set_samples(burnin, nsamples)
+    s.init()
+    s.sweeps(0, burnin + nsamples, eval=True)
+    for got, ref in ((U, s.latents(0).T), (V, s.latents(1).T), (mu[:, 0], s.hyper(0)[0]),
+                     (link, s.beta(0).T),
+                     (mean[0, 0], s.mean_value())):
+        ref = np.asarray(ref)
+        assert np.all(np.abs(got - ref) <= 5.01e-6 * np.abs(ref))
+    s.close()

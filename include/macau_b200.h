@@ -226,6 +226,15 @@ int mg_batch_get_info(mg_batch* b, int64_t* out);
  *                      decisions
  *   "tensor_core_gram" (default 1) mixed mode: run the K = 32 row Grams on the tcgen05 tensor
  *                      cores
+ *   "fused_finish"     (default 1) the tensor-core sampler finishes each row (factor, solves,
+ *                      draw) in its Gram kernel's epilogue; 0 = Gram records in HBM and a
+ *                      separate finish kernel (the same arithmetic; an FP32 factor that fails
+ *                      is redone in FP64 from the CSR when fused, from the record otherwise)
+ *   "tc_wait_us"       (default 0 = about 2 s) budget of each barrier wait of the tensor-core
+ *                      sampler in microseconds; a wait that runs out ends the launch with
+ *                      MG_ERR_TIMEOUT and leaves the context usable after mg_init
+ *   "tc_wait_test"     (default 0; tests only) 1 = the tensor-core sampler's MMA warp first
+ *                      waits on a barrier that nothing arrives on, so that wait runs out
  *   "cg_fp32"          (default 0) mixed mode: run the Macau block-CG in FP32 with an FP64
  *                      residual replacement every 20 iterations instead of FP64; set before
  *                      mg_init

@@ -13,6 +13,9 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libmacau_b200.so"
 MG_COMPUTE_FP64 = 0
 MG_COMPUTE_MIXED = 1
 
+MG_ERR_ARG, MG_ERR_CHOL, MG_ERR_CG, MG_ERR_CUDA = -1, -2, -3, -4
+MG_ERR_STATE, MG_ERR_TIMEOUT, MG_ERR_NOGPU = -5, -6, -7
+
 ERRORS = {-1: "invalid argument", -2: "Cholesky Decomposition failed!", -3: "block-CG failure",
           -4: "CUDA error", -5: "call out of order", -6: "device wait timed out",
           -7: "no sm_100 GPU"}

@@ -466,10 +466,10 @@ class Batch {
     MG_CUDA(cudaStreamSynchronize(s_));
     retries_[0] = h.retries[0];
     retries_[1] = h.retries[1];
+    if (h.status & kStatTimeout) throw MgError(MG_ERR_TIMEOUT, "device wait timed out");
     if (h.status & kStatCholFail) throw MgError(MG_ERR_CHOL, "Cholesky Decomposition failed!");
     if (h.status & kStatHyperFail)
       throw MgError(MG_ERR_CHOL, "Cholesky Decomposition failed! (hyperprior)");
-    if (h.status & kStatTimeout) throw MgError(MG_ERR_TIMEOUT, "device wait timed out");
   }
 
   long long retries(int m) const { return retries_[m]; }

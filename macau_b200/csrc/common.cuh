@@ -84,6 +84,10 @@ struct SampleParams {
   int half_copy;               // mixed: the 16-bit gather copy (out_bf16) holds FP16, not BF16
   const int* row_width;        // tensor-core Gram records: per row, the width 8, 16 or 32 of the
                                // Gram block and rhs entries the finish reads (null: 32)
+  long long wait_cycles;       // tensor-core sampler: clock budget of each barrier wait before
+                               // the kernel gives up with kStatTimeout (0: about 2 s)
+  int wait_test;               // tensor-core sampler, tests only: the MMA warp first waits on a
+                               // barrier that nothing arrives on, so that wait runs out
 };
 
 #ifdef __CUDACC__

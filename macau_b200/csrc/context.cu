@@ -401,6 +401,7 @@ class Context {
   void init() {
     if (!have_data_) throw MgError(MG_ERR_STATE, "no training data");
     for (int m = 0; m < 2; m++) {
+      size_gram_records(m);  // the prior kind decides whether the mode keeps per-row records
       const size_t n = (size_t)dims_[m] * KP_;
       if (mixed_) {
         lat32_[m].alloc_zero(n, s_);
@@ -518,14 +519,20 @@ class Context {
     sp.mode = mode;
     sp.seed = cfg_.seed;
     sp.znoise = znoise_dev;
+    sp.wait_cycles = tc_wait_cycles_;
+    sp.wait_test = tc_wait_test_ ? 1 : 0;
     if (mixed_ && use_tc_ && gram_ == 0 && KP_ == 32) {
       SampleParams tp = sp;
       tp.tasks = md.tasks_tc.p;
       tp.ntasks = md.ntasks_tc;
       tp.packed = md.packed_tc.p;
       if (launch_sample_tc(tp, md.gram_tc.p, md.split_tc.p, md.nsplit_tc, KP_, s_, num_sms_,
-                           mid)) {
-        launches_ += 1 + (md.nsplit_tc > 0 ? 1 : 0);  // k_gram_tc (+ k_sum_parts) + k_finish_tc
+                           mid, fused_)) {
+        // k_gram_tc (+ k_sum_parts) + k_finish_tc; fused: k_gram_tc (+ k_sum_parts + k_finish_tc)
+        if (fused_ && !p.one)
+          launches_ += md.nsplit_tc > 0 ? 2 : 0;
+        else
+          launches_ += 1 + (md.nsplit_tc > 0 ? 1 : 0);
         return;
       }
     }
@@ -864,12 +871,13 @@ class Context {
     MG_CUDA(cudaStreamSynchronize(s_));
     retries_[0] = h.retries[0];
     retries_[1] = h.retries[1];
+    // a timed-out launch left its work unfinished, so its status comes before what followed
+    if (h.status & kStatTimeout) throw MgError(MG_ERR_TIMEOUT, "device wait timed out");
     if (h.status & kStatCholFail)
       throw MgError(MG_ERR_CHOL, "Cholesky Decomposition failed!");
     if (h.status & kStatHyperFail)
       throw MgError(MG_ERR_CHOL, "Cholesky Decomposition failed! (hyperprior)");
     if (h.status & kStatCgFail) throw MgError(MG_ERR_CG, "block-CG breakdown");
-    if (h.status & kStatTimeout) throw MgError(MG_ERR_TIMEOUT, "device wait timed out");
   }
 
   void sweeps(int first_iter, int count, bool do_eval, bool sync = true) {
@@ -1131,6 +1139,21 @@ class Context {
   bool initialised() const { return initialised_; }
   void set_use_graph(bool b) { use_graph_ = b; drop_graphs(); }
   void set_use_tc(bool b) { use_tc_ = b; drop_graphs(); }
+  void set_tc_wait(int us) {
+    if (us < 0) throw MgError(MG_ERR_ARG, "tc_wait_us must be >= 0");
+    tc_wait_cycles_ = 2000LL * us;
+    drop_graphs();
+  }
+  void set_tc_wait_test(bool b) {
+    tc_wait_test_ = b;
+    drop_graphs();
+  }
+  void set_fused(bool b) {
+    fused_ = b;
+    drop_graphs();
+    if (have_data_)
+      for (int m = 0; m < 2; m++) size_gram_records(m);
+  }
   void set_cg_f32(bool b) { cg_f32_ = b && mixed_; }
   // A fixed work split / CTA shape for both modes' row samplers (the autotuner's knobs).
   void set_split_threshold(int t) {
@@ -1193,7 +1216,6 @@ class Context {
         pptr[r + 1] = pptr[r] + (hptr[r + 1] - hptr[r] + 15) / 16 * 16;
       md.pptr_tc.upload(pptr.data(), pptr.size(), s_);
       md.packed_tc.alloc((size_t)std::max(1LL, pptr[md.N]));
-      md.gram_tc.alloc((size_t)std::max(1LL, md.N) * (32 * 32 + 32));
     }
     md.groups = 0;
     md.tune_state = 0;
@@ -1250,6 +1272,7 @@ class Context {
         if (t.nparts > 1 && t.part == 0) sr.push_back(make_int4(t.row, t.nparts, t.slot, 0));
       std::sort(sr.begin(), sr.end(), [](const int4& a, const int4& b) { return a.x < b.x; });
       md.split_tc.upload(sr.data(), sr.size(), s_);
+      size_gram_records(m);
     }
     md.split_cnt.alloc_zero(std::max(1, nsplit), s_);
     const size_t need =
@@ -1257,6 +1280,18 @@ class Context {
                          std::max(md_[0].nslots_tc, md_[1].nslots_tc)) *
         (KP_ * KP_ + KP_);
     if (need > scratch_.n) scratch_.alloc(need);
+  }
+
+  // Gram records of the tensor-core sampler of mode m: one per split row when the fused kernel
+  // finishes the mode's rows, one per row when a separate finish kernel reads them (option
+  // "fused_finish" = 0, or the univariate prior).  Kept when large enough.
+  void size_gram_records(int m) {
+    ModeData& md = md_[m];
+    if (!(mixed_ && KP_ == 32) || md.N == 0) return;
+    const bool per_row = !fused_ || prior_[m].one;
+    const size_t need = (size_t)std::max(1LL, per_row ? md.N : (long long)md.nsplit_tc) *
+                        (32 * 32 + 32);
+    if (md.gram_tc.n < need) md.gram_tc.alloc(need);
   }
 
   // Mixed mode: the packed (index, weight) entries of mode m and their padded copy.  The weights
@@ -1289,6 +1324,16 @@ class Context {
   DBuf<double> noise_partials_;
   bool have_data_ = false, initialised_ = false;
   bool use_graph_ = true, use_tc_ = true;
+  // The tensor-core sampler finishes rows in its Gram kernel's epilogue (option "fused_finish",
+  // default on); off: Gram records in HBM and a separate finish kernel.
+  bool fused_ = true;
+  // Clock budget of each barrier wait of the tensor-core sampler (option "tc_wait_us", in
+  // microseconds at 2 GHz; 0 = the kernel's default of about 2 s).  Tests shorten it to make a
+  // wait run out.
+  long long tc_wait_cycles_ = 0;
+  // Option "tc_wait_test" (tests only): the tensor-core sampler's MMA warp first waits on a
+  // barrier that nothing arrives on, so that the wait runs out and the launch aborts.
+  bool tc_wait_test_ = false;
   // Block-CG in FP32 with FP64 residual replacement (mixed mode, option "cg_fp32").  Off by
   // default: at tol 1e-6 the FP32 iteration needs about 1.5x the iterations of FP64, which
   // costs more than its halved gather traffic saves.
@@ -1559,6 +1604,9 @@ int mg_set_option(mg_ctx* ctx, const char* name, int value) {
     const std::string n(name);
     if (n == "graph") c.set_use_graph(value != 0);
     else if (n == "tensor_core_gram") c.set_use_tc(value != 0);
+    else if (n == "fused_finish") c.set_fused(value != 0);
+    else if (n == "tc_wait_us") c.set_tc_wait(value);
+    else if (n == "tc_wait_test") c.set_tc_wait_test(value != 0);
     else if (n == "cg_fp32") c.set_cg_f32(value != 0);
     else if (n == "gram_precision") c.set_gram(value);
     else if (n == "autotune") c.set_autotune(value);

@@ -1,7 +1,9 @@
-// Mixed-precision latent sampler whose row Grams run on the tcgen05 tensor cores (KP = 32), in
-// two kernels: k_gram_tc accumulates every sampled row's Gram V^T V and right-hand side on the
-// tensor cores and stores them to HBM; k_finish_tc then finishes each row (Lambda + alpha G,
-// Cholesky, solves, noise) with one warp per row at full occupancy.
+// Mixed-precision latent sampler whose row Grams run on the tcgen05 tensor cores (KP = 32).
+// k_gram_tc<true> (the sampler of a BPMF / Macau mode) accumulates every sampled row's Gram
+// V^T V and right-hand side on the tensor cores and finishes the row in its epilogue (Lambda +
+// alpha G, FP32 Cholesky, solves, noise), so a row's Gram never leaves the SM.  k_gram_tc<false>
+// stores the Grams to HBM as records instead, for finishes that run as a separate kernel: the
+// univariate prior (k_finish_one_tc), the batched problems (batch.cu), and k_finish_tc.
 //
 // k_gram_tc.  Four sampler rows ("a group") share each MMA.  For a k-block of 16 entries per
 // row, the producers gather the four rows' BF16 other-factor vectors (64 B each, by CSR column
@@ -35,9 +37,14 @@
 //               issues the MMAs, releases stages (tcgen05.commit -> "empty") and publishes
 //               finished accumulators (tcgen05.commit -> "acc full").
 //   warps 9-12  epilogue (warp w reads TMEM quadrant w % 4 = row slot): TMEM -> registers,
-//               release the accumulator, store the row's FP32 Gram and rhs to its Gram record
-//               (or, for a part of a split row, the FP64 partial to the part's scratch slot),
-//               and release the group's descriptor slot ("desc free").
+//               release the accumulator and the group's descriptor slot ("desc free"); a part
+//               of a split row goes to the part's scratch slot as an FP64 partial.  Records
+//               kernel: the row's FP32 Gram and rhs go to its Gram record.  Fused kernel: the
+//               warp takes groups two at a time and finishes its quadrant's two rows as a pair
+//               (half-warp h = the row of group 2i + h; the pair routines of warp_finish.cuh,
+//               the arithmetic of k_finish_tc), so the FP32 factor of one pair overlaps the MMAs
+//               of the next groups.  A half whose FP32 factor fails is redone by the whole warp
+//               in FP64 from the row's CSR entries and BF16 latents (retry_row_from_csr).
 //   warp 13     scheduler: takes 4 tasks per group from the work queue (four claims in flight)
 //               and publishes the group descriptors into a ring of kDesc slots as far ahead as
 //               the ring allows, so that the queue atomics and task loads stay off the MMA warp.
@@ -45,12 +52,15 @@
 //               k-blocks of their parity ahead, copy each k-block's four 128-byte row segments
 //               with one 16-byte cp.async per lane into the ring, with a meta record (stage
 //               index, valid rows, stop / end) for the producers.
-// Every barrier wait is bounded by a clock budget; on expiry the CTA raises an abort flag, all
-// roles leave their loops, the MMA lane drains its MMAs, TMEM is freed and the status word
-// reports a timeout.
+// Every barrier wait is bounded by a clock budget (SampleParams::wait_cycles, about 2 s by
+// default); on expiry the CTA raises an abort flag, all roles leave their loops, the MMA lane
+// drains its MMAs (a wait of the full default budget), TMEM is freed and the status word reports
+// a timeout.
 //
-// k_finish_tc.  One warp per row: the Gram record (or the FP64 sum of the row's split parts, in
-// part order), then the FP32 warp Cholesky and solves of warp_finish.cuh with the FP64 retry.
+// k_finish_tc.  One warp per two rows: the Gram records (or the FP64 sums of split rows' parts,
+// in part order, written by k_sum_parts), then the FP32 pair Cholesky and solves of
+// warp_finish.cuh with an FP64 retry of the same Gram.  After the fused kernel it finishes the
+// split rows only, from a compact list of their records.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -69,7 +79,7 @@ constexpr int kEpiWarp0 = kProducers + 1;           // warps 9-12
 constexpr int kSchedWarp = kProducers + 5;           // warp 13
 constexpr int kCsrWarp0 = kProducers + 6;            // warps 14-15
 constexpr int kTcThreads = (kProducers + 8) * 32;
-constexpr int kStages = 32;               // gather stages in flight (even: stage s has parity s % 2)
+constexpr int kStages = 24;               // gather stages in flight (even: stage s has parity s % 2)
 constexpr int kBlockBytes = 2 * 512;      // one column block: 2 K-atoms x 512 B
 constexpr int kStageBytes = 5 * kBlockBytes;
 constexpr int kSlots = 3;                 // TMEM accumulators
@@ -107,6 +117,7 @@ struct TcShared {
   uint64_t acc_full[kSlots];
   uint64_t acc_empty[kSlots];  // 4 epilogue warps
   uint64_t drain;
+  uint64_t never;              // nothing arrives here (SampleParams::wait_test)
   uint64_t desc_full[kDesc];   // scheduler -> producers, MMA, epilogue
   uint64_t desc_free[kDesc];   // epilogue (4 warps) -> scheduler
   uint64_t csr_full[kParity][kCsr];   // 32 cp.async completions + the loader's meta arrive
@@ -115,6 +126,7 @@ struct TcShared {
   alignas(16) uint2 csr[kParity][kCsr][4][16];  // CSR entries of one k-block: [row slot][16]
   uint32_t tmem_base;
   int abort;
+  long long wait_cycles;  // budget of one barrier wait (SampleParams::wait_cycles, or kWaitCycles)
   GroupDesc desc[kDesc];
 };
 
@@ -161,10 +173,11 @@ __device__ __forceinline__ bool mbar_test_suspend(uint64_t* b, uint32_t parity, 
 // checked between them.
 __device__ __noinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, TcShared* sh, Ctl* ctl) {
   const long long t0 = clock64();
+  const long long budget = sh->wait_cycles;
   for (;;) {
     if (mbar_test_suspend(b, parity, 20000u)) return true;
     if (*(volatile int*)&sh->abort) return false;
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > budget) {
       atomicOr(&ctl->status, kStatTimeout);
       *(volatile int*)&sh->abort = 1;
       return false;
@@ -337,12 +350,304 @@ __device__ __forceinline__ bool cursor_advance(Cursor& c, int step, TcShared* sh
   return true;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Row finish shared by the fused epilogue and k_finish_tc.
+constexpr int kFinWarps = 8;
+constexpr int kLc = 36;                 // L^T leading dimension
+constexpr int kFinWork = 32 * 36 * 8;   // per warp: the FP64 retry's L^T (leading dimension kLc)
+
+// Entry (c, j) of MM = Lambda + alpha G in FP32 from (float) Lambda(c, j) and G(c, j); the
+// identity beyond K.
+__device__ __forceinline__ float mm_entry(float lam, float g, float alpha_f, int c, int j, int K) {
+  return (c < K && j < K) ? lam + alpha_f * g : (c == j ? 1.f : 0.f);
+}
+
+// Per-launch constants of the row finish in shared memory: Lambda in FP64 (row stride 33) and
+// FP32 (row stride kLc), and Lambda mu in FP64.
+struct FinConst {
+  double Lam[32 * 33];
+  double lmu[32];
+  alignas(16) float LamF[32 * kLc];
+};
+
+// Fills FinConst with `nthreads` threads (thread index t), `bar` ordering the two steps.
+template <typename Bar>
+__device__ __forceinline__ void fin_const_fill(FinConst* fc, const SampleParams& p, int t,
+                                               int nthreads, Bar bar) {
+  const int K = p.K;
+  for (int e = t; e < 32 * 32; e += nthreads) {
+    const int i = e / 32, j = e % 32;
+    const double v = (i < K && j < K) ? p.Lambda[i + j * K] : 0.0;
+    fc->Lam[i * 33 + j] = v;
+    fc->LamF[i * kLc + j] = (float)v;
+  }
+  bar();
+  if (t < 32) {
+    double s = 0.0;
+    if (t < K)
+      for (int j = 0; j < K; j++) s += fc->Lam[t * 33 + j] * p.mu[j];
+    fc->lmu[t] = s;
+  }
+  bar();
+}
+
+// Rows i, i + 8, i + 16, i + 24 of the quarter's MM = Lambda + alpha G (FP32, the quad layout of
+// warp_finish.cuh) from its Gram rows at gp (row-major, 32 floats a row; staged: each row's
+// 16-byte chunk c stored at chunk c ^ (row % 8), which keeps the quarter's reads and the
+// epilogue's writes free of bank conflicts), d0[k] = the diagonal entry of row i + 8k.
+template <bool kStaged>
+__device__ __forceinline__ void quad_load_mm(const FinConst* fc, const float* gp, int i, int K,
+                                             float alpha_f, float (&a)[80], float (&d0)[4]) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int r = i + 8 * k;
+    d0[k] = 1.f;
+#pragma unroll
+    for (int c4 = 0; c4 < 2 * (k + 1); c4++) {
+      const float* src = gp + r * 32 + 4 * (kStaged ? (c4 ^ i) : c4);
+      const float4 g = kStaged ? *reinterpret_cast<const float4*>(src)
+                               : __ldcg(reinterpret_cast<const float4*>(src));
+      const float4 m = *reinterpret_cast<const float4*>(fc->LamF + r * kLc + 4 * c4);
+      const float gv[4] = {g.x, g.y, g.z, g.w}, mv[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int c = 4 * c4 + u;
+        const float v = mm_entry(mv[u], gv[u], alpha_f, r, c, K);
+        a[qoff(k) + c] = v;
+        if (c == r) d0[k] = v;
+      }
+    }
+  }
+}
+
+// Right-hand sides of components i + 8k of `row` in FP32: the Gram rhs (rhs[c]) + Lambda mu
+// (Macau: Lambda (mu + Uhat[row])), summed in FP64.
+template <bool kStaged>
+__device__ __forceinline__ void quad_rhs(const SampleParams& p, const FinConst* fc,
+                                         const float* rhs, int row, int i, float (&b)[4]) {
+  const int K = p.K;
+  double m[4] = {0.0, 0.0, 0.0, 0.0};
+  if (p.uhat) {
+    for (int j = 0; j < K; j++) {
+      const double mj = p.mu[j] + p.uhat[(size_t)row * 32 + j];
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if (i + 8 * k < K) m[k] += fc->Lam[(i + 8 * k) * 33 + j] * mj;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; k++) m[k] = fc->lmu[i + 8 * k];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const float rv = kStaged ? rhs[i + 8 * k] : __ldcg(rhs + i + 8 * k);
+    double rl = (double)rv;
+    rl += m[k];
+    b[k] = (float)rl;
+  }
+}
+
+// Finishes four rows, one per quarter (the quarter's row `row`, < 0: takes no part, computing on
+// row rw's draws): MM from its Gram at gp, FP32 factor, solves and the draw, the latents stored
+// when the factor held.  Returns the ballot of lanes whose quarter has a row and a failed factor
+// (bit 8q for quarter q).
+template <bool kStaged>
+__device__ __forceinline__ unsigned quad_finish(const SampleParams& p, const FinConst* fc,
+                                                const float* gp, int row, int rw, float alpha_f,
+                                                uint32_t sweep, int lane) {
+  const int i = lane & 7;
+  const int K = p.K;
+  float a[80], d0[4], rinv[4] = {1.f, 1.f, 1.f, 1.f}, b[4], z[4];
+  quad_load_mm<kStaged>(fc, gp, i, K, alpha_f, a, d0);
+  quad_rhs<kStaged>(p, fc, gp + 32 * 32, rw, i, b);
+  quad_noise(p, rw, K, i, sweep, z);
+  const bool ok = quad_factor(a, rinv, i, d0);
+  quad_solve(a, rinv, b, z, i);
+  if (ok && row >= 0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int c = i + 8 * k;
+      if (c < K) {
+        p.out_f32[(size_t)row * 32 + c] = b[k];
+        p.out_bf16[(size_t)row * 32 + c] = __float2bfloat16_rn(b[k]);
+      }
+    }
+  }
+  return __ballot_sync(0xffffffffu, !ok && row >= 0);
+}
+
+// FP64 redo of one row whose FP32 factor failed, by the whole warp (lane = component), from the
+// same FP32 Gram record (the two-kernel path): rhs + Lambda mu recomputed in FP64, then
+// warp_finish_f64.
+__device__ __noinline__ void retry_row_from_record(const SampleParams& p, const FinConst* fc,
+                                                   const float* rec, int row, uint32_t sweep,
+                                                   unsigned char* work) {
+  const int lane = threadIdx.x & 31;
+  const int K = p.K;
+  double rl = 0.0;
+  if (lane < K) {
+    rl = (double)__ldcg(rec + 32 * 32 + lane);
+    double m = 0.0;
+    if (p.uhat) {
+      for (int j = 0; j < K; j++) m += fc->Lam[lane * 33 + j] * (p.mu[j] + p.uhat[(size_t)row * 32 + j]);
+    } else {
+      m = fc->lmu[lane];
+    }
+    rl += m;
+  }
+  if (lane == 0) atomicAdd(&p.ctl->retries[p.mode], 1u);
+  const bool ok = warp_finish_f64<32, float>(rec, 32, fc->Lam, rl, p, row, sweep, work);
+  if (!ok && lane == 0) {
+    atomicOr(&p.ctl->status, kStatCholFail);
+    atomicCAS(&p.ctl->bad_row, -1, row);
+  }
+  __syncwarp();
+}
+
+// FP64 redo of one row whose FP32 factor failed, by the whole warp (lane = component): the
+// Gram sum v v^T and rhs sum v w re-accumulated in FP64 from the row's padded CSR entries
+// [begin, begin + len) and the BF16 latents they gather (the inputs of the tensor-core Gram,
+// without its FP32 rounding), then MM = Lambda + alpha G, the FP64 warp Cholesky and solves with
+// the row's keyed draws.  Counts a retry; a failed FP64 factor raises kStatCholFail.
+__device__ __noinline__ void retry_row_from_csr(const SampleParams& p, const FinConst* fc,
+                                                int row, long long begin, int len,
+                                                uint32_t sweep, unsigned char* work) {
+  const int lane = threadIdx.x & 31;
+  const int K = p.K;
+  const __nv_bfloat16* V = reinterpret_cast<const __nv_bfloat16*>(p.other);
+  const float wscale = (float)packed_scale(p);
+  double g[32];
+#pragma unroll
+  for (int j = 0; j < 32; j++) g[j] = 0.0;
+  double b = 0.0;
+  for (int e = 0; e < len; e++) {
+    const uint2 ent = p.packed[begin + e];
+    const float vi = __bfloat162float(V[(size_t)ent.x * 32 + lane]);
+    const double w = (double)(__uint_as_float(ent.y) * wscale);
+    b = fma((double)vi, w, b);
+#pragma unroll
+    for (int j = 0; j < 32; j++) g[j] = fma((double)vi, (double)__shfl_sync(0xffffffffu, vi, j), g[j]);
+  }
+  const double alpha = noise_alpha(p);
+  double a[32], d0 = 1.0, rinv = 1.0;
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    a[j] = (lane < K && j < K) ? fc->Lam[lane * 33 + j] + alpha * g[j] : (lane == j ? 1.0 : 0.0);
+    if (j == lane) d0 = a[j];
+  }
+  double rr = 0.0;
+  if (lane < K) {
+    rr = b;
+    if (p.uhat) {
+      for (int j = 0; j < K; j++)
+        rr += fc->Lam[lane * 33 + j] * (p.mu[j] + p.uhat[(size_t)row * 32 + j]);
+    } else {
+      rr += fc->lmu[lane];
+    }
+  }
+  const double z = row_noise(p, row, K, lane, sweep);
+  if (lane == 0) atomicAdd(&p.ctl->retries[p.mode], 1u);
+  double* Lc = reinterpret_cast<double*>(work);
+  __syncwarp();
+  if (!warp_factor<double, 32>(a, rinv, lane, 0.0, d0, Lc, kLc)) {
+    if (lane == 0) {
+      atomicOr(&p.ctl->status, kStatCholFail);
+      atomicCAS(&p.ctl->bad_row, -1, row);
+    }
+    return;
+  }
+  const double x = warp_solve<double, 32>(a, rinv, rr, lane, Lc, kLc, z);
+  if (lane < K) {
+    p.out_f32[(size_t)row * 32 + lane] = (float)x;
+    p.out_bf16[(size_t)row * 32 + lane] = __float2bfloat16_rn((float)x);
+  }
+  __syncwarp();
+}
+
+// What the fused epilogue needs of its quadrant's task in a group.
+struct EpiTask {
+  long long begin;
+  int row, len, part, nparts, pslot, stop;
+};
+
+// Fused epilogue: waits for group g's accumulator, reads this warp's quadrant qd (lane l: Gram
+// row l of the group's row slot qd and the rhs component l) and the slot's task, then releases
+// the accumulator and the descriptor.  False on timeout / abort.
+__device__ __forceinline__ bool epi_take(TcShared* sh, Ctl* ctl, uint32_t tmem, int g, int qd,
+                                         int lane, EpiTask& t, float (&gr)[32], float& rhs) {
+  const int slot = g % kSlots;
+  if (!mbar_wait(&sh->acc_full[slot], (uint32_t)((g / kSlots) & 1), sh, ctl)) return false;
+  if (!mbar_wait(&sh->desc_full[g % kDesc], (uint32_t)((g / kDesc) & 1), sh, ctl)) return false;
+  tc_fence_after();
+  const GroupDesc& d = sh->desc[g % kDesc];
+  t.stop = d.stop;
+  t.row = d.row[qd];
+  t.len = d.len[qd];
+  t.begin = d.begin[qd];
+  t.part = d.part[qd];
+  t.nparts = d.nparts[qd];
+  t.pslot = d.slot[qd];
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&sh->desc_free[g % kDesc]);
+  rhs = 0.f;
+  if (!t.stop) {
+    const uint32_t lanes = (uint32_t)(32 * qd) << 16;
+    tmem_ld32(tmem + lanes + (uint32_t)(slot * kSlotCols + 32 * qd), gr);
+    const float rhs_hi = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 128 + qd));
+    const float rhs_lo = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 132 + qd));
+    tmem_wait_ld();
+    rhs = rhs_hi + rhs_lo;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 32; j++) gr[j] = 0.f;
+  }
+  tc_fence_before();
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&sh->acc_empty[slot]);
+  return true;
+}
+
+// A split row's part: its FP32 partial Gram (lane = Gram row) and rhs to the part's FP64 scratch
+// slot, summed in part order by k_sum_parts.
+__device__ __forceinline__ void store_part(const SampleParams& p, const EpiTask& t,
+                                           const float (&gr)[32], float rhs, int lane) {
+  double* sp = p.scratch + (size_t)(t.pslot + t.part) * kGramRec;
+#pragma unroll
+  for (int j = 0; j < 32; j++) sp[lane * 32 + j] = (double)gr[j];
+  sp[32 * 32 + lane] = (double)rhs;
+}
+
+// Staging of one group's quadrant for the quad finish: the 32 Gram rows (row r's 16-byte chunk c
+// at chunk c ^ (r % 8)), then the 32 rhs values.
+constexpr int kStageRec = 32 * 32 + 32;
+
+__device__ __forceinline__ void stage_rows(float* st, const float (&gr)[32], float rhs, int lane) {
+#pragma unroll
+  for (int c4 = 0; c4 < 8; c4++)
+    *reinterpret_cast<float4*>(st + lane * 32 + 4 * (c4 ^ (lane & 7))) =
+        make_float4(gr[4 * c4], gr[4 * c4 + 1], gr[4 * c4 + 2], gr[4 * c4 + 3]);
+  st[32 * 32 + lane] = rhs;
+}
+
+// Shared memory of the fused kernel beyond TcShared: the finish constants and, per epilogue warp,
+// the staged Grams of its four groups (also the FP64 retry's L^T) and their quarters' tasks.
+struct FusedShared {
+  FinConst fc;
+  alignas(16) float stage[4][4 * kStageRec];
+  long long begin[4][4];
+  int row[4][4], len[4][4];
+};
+static_assert(sizeof(float) * 4 * kStageRec >= (size_t)kFinWork, "retry work area");
+
+template <bool kFused>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_gram_tc(const SampleParams p, float* gram) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // layout: stages (1024-aligned) | TcShared
+  // layout: stages (1024-aligned) | TcShared | FusedShared (fused kernel)
   unsigned char* stages = smem_raw;
   TcShared* sh = reinterpret_cast<TcShared*>(stages + (size_t)kStages * kStageBytes);
+  FusedShared* fs = reinterpret_cast<FusedShared*>(reinterpret_cast<unsigned char*>(sh) +
+                                                   (sizeof(TcShared) + 15) / 16 * 16);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // The stage descriptors' 64-byte swizzle pattern assumes 1024-byte aligned stages.
   if ((su32(stages) & 1023u) != 0) {
@@ -364,6 +669,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(&sh->acc_empty[s], 4);
     }
     mbar_init(&sh->drain, 1);
+    mbar_init(&sh->never, 1);
     for (int d = 0; d < kDesc; d++) {
       mbar_init(&sh->desc_full[d], 1);
       mbar_init(&sh->desc_free[d], 4);
@@ -374,6 +680,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         mbar_init(&sh->csr_empty[h][c], kRowSlots);
       }
     sh->abort = 0;
+    sh->wait_cycles = p.wait_cycles > 0 ? p.wait_cycles : kWaitCycles;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == kMmaWarp) {
@@ -462,7 +769,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ================= MMA issuer =================
     int stage = 0;
     uint32_t phase = 0;
-    for (int g = 0;; g++) {
+    // test hook: a wait that runs out (the abort path then ends every role)
+    const bool go = !p.wait_test || mbar_wait(&sh->never, 0, sh, p.ctl);
+    for (int g = 0; go; g++) {
       const int slot = g % kSlots;
       if (g >= kSlots &&
           !mbar_wait(&sh->acc_empty[slot], (uint32_t)(((g / kSlots) & 1) ^ 1), sh, p.ctl))
@@ -560,49 +869,104 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     cp_wait_all();
   } else {
-    // ================= epilogue: accumulators -> Gram records =================
     const int qd = warp & 3;  // TMEM quadrant = row slot of the group
-    for (int g = 0;; g++) {
-      const int slot = g % kSlots;
-      if (!mbar_wait(&sh->acc_full[slot], (uint32_t)((g / kSlots) & 1), sh, p.ctl)) break;
-      if (!mbar_wait(&sh->desc_full[g % kDesc], (uint32_t)((g / kDesc) & 1), sh, p.ctl)) break;
-      tc_fence_after();
-      const GroupDesc& d = sh->desc[g % kDesc];
-      const int stop = d.stop;
-      const int row = d.row[qd];
-      const int part = d.part[qd], nparts = d.nparts[qd], pslot = d.slot[qd];
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&sh->desc_free[g % kDesc]);
-      float gr[32];
-      float rhs = 0.f;
-      if (!stop) {
-        const uint32_t lanes = (uint32_t)(32 * qd) << 16;
-        tmem_ld32(tmem + lanes + (uint32_t)(slot * kSlotCols + 32 * qd), gr);
-        const float rhs_hi = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 128 + qd));
-        const float rhs_lo = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 132 + qd));
-        tmem_wait_ld();
-        rhs = rhs_hi + rhs_lo;
+    if constexpr (kFused) {
+      // ================= epilogue: accumulators -> finished rows =================
+      // four groups at a time: each group's quadrant is staged in shared memory as it arrives
+      // (its accumulator released at once), then the warp finishes the four rows, quarter q the
+      // row of group g + q
+      const int et = threadIdx.x - kEpiWarp0 * 32;
+      const int ew = warp - kEpiWarp0;
+      fin_const_fill(&fs->fc, p, et, 128,
+                     [] { asm volatile("bar.sync 1, 128;" ::: "memory"); });
+      const float alpha_f = (float)noise_alpha(p);
+      const uint32_t sweep = p.ctl->sweep;
+      float* stage = fs->stage[ew];
+      for (int e = lane; e < 4 * kStageRec; e += 32) stage[e] = 0.f;
+      bool done = false;
+      for (int g = 0; !done; g += 4) {
+        int nq = 0;
+        for (int q = 0; q < 4; q++) {
+          EpiTask t;
+          float gr[32], rhs;
+          if (!epi_take(sh, p.ctl, tmem, g + q, qd, lane, t, gr, rhs)) {
+            done = true;
+            nq = 0;  // aborted: nothing is finished
+            break;
+          }
+          if (t.stop) {
+            done = true;
+            break;
+          }
+          stage_rows(stage + q * kStageRec, gr, rhs, lane);
+          if (t.row >= 0 && t.nparts > 1) store_part(p, t, gr, rhs, lane);
+          if (lane == 0) {
+            fs->row[ew][q] = (t.row >= 0 && t.nparts == 1) ? t.row : -1;
+            fs->begin[ew][q] = t.begin;
+            fs->len[ew][q] = t.len;
+          }
+          nq = q + 1;
+        }
+        __syncwarp();
+        int first = -1;
+        for (int q = 0; q < nq; q++)
+          if (first < 0 && fs->row[ew][q] >= 0) first = fs->row[ew][q];
+        if (first < 0) continue;  // nothing to finish (done ends the loop)
+        const int qq = lane >> 3;
+        const int row = qq < nq ? fs->row[ew][qq] : -1;
+        const unsigned fails = quad_finish<true>(p, &fs->fc, stage + qq * kStageRec, row,
+                                                 row >= 0 ? row : first, alpha_f, sweep, lane);
+        __syncwarp();
+        for (int q = 0; q < nq; q++)
+          if ((fails >> (8 * q)) & 1u)
+            retry_row_from_csr(p, &fs->fc, fs->row[ew][q], fs->begin[ew][q], fs->len[ew][q],
+                               sweep, reinterpret_cast<unsigned char*>(stage));
+        __syncwarp();
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&sh->acc_empty[slot]);
-      if (stop) break;
-      if (row < 0) continue;
-      if (nparts > 1) {
-        double* sp = p.scratch + (size_t)(pslot + part) * kGramRec;
+    } else {
+      // ================= epilogue: accumulators -> Gram records =================
+      for (int g = 0;; g++) {
+        const int slot = g % kSlots;
+        if (!mbar_wait(&sh->acc_full[slot], (uint32_t)((g / kSlots) & 1), sh, p.ctl)) break;
+        if (!mbar_wait(&sh->desc_full[g % kDesc], (uint32_t)((g / kDesc) & 1), sh, p.ctl)) break;
+        tc_fence_after();
+        const GroupDesc& d = sh->desc[g % kDesc];
+        const int stop = d.stop;
+        const int row = d.row[qd];
+        const int part = d.part[qd], nparts = d.nparts[qd], pslot = d.slot[qd];
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sh->desc_free[g % kDesc]);
+        float gr[32];
+        float rhs = 0.f;
+        if (!stop) {
+          const uint32_t lanes = (uint32_t)(32 * qd) << 16;
+          tmem_ld32(tmem + lanes + (uint32_t)(slot * kSlotCols + 32 * qd), gr);
+          const float rhs_hi = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 128 + qd));
+          const float rhs_lo = tmem_ld1(tmem + lanes + (uint32_t)(slot * kSlotCols + 132 + qd));
+          tmem_wait_ld();
+          rhs = rhs_hi + rhs_lo;
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sh->acc_empty[slot]);
+        if (stop) break;
+        if (row < 0) continue;
+        if (nparts > 1) {
+          double* sp = p.scratch + (size_t)(pslot + part) * kGramRec;
 #pragma unroll
-        for (int j = 0; j < 32; j++) sp[lane * 32 + j] = (double)gr[j];
-        sp[32 * 32 + lane] = (double)rhs;
-      } else {
-        float* gp = gram + (size_t)row * kGramRec;
-        const int w = p.row_width ? p.row_width[row] : 32;  // rows and columns the finish reads
-        if (lane < w) {
+          for (int j = 0; j < 32; j++) sp[lane * 32 + j] = (double)gr[j];
+          sp[32 * 32 + lane] = (double)rhs;
+        } else {
+          float* gp = gram + (size_t)row * kGramRec;
+          const int w = p.row_width ? p.row_width[row] : 32;  // rows and columns the finish reads
+          if (lane < w) {
 #pragma unroll
-          for (int j = 0; j < 32; j += 4)
-            if (j < w)
-              *reinterpret_cast<float4*>(gp + lane * 32 + j) =
-                  make_float4(gr[j], gr[j + 1], gr[j + 2], gr[j + 3]);
-          gp[32 * 32 + lane] = rhs;
+            for (int j = 0; j < 32; j += 4)
+              if (j < w)
+                *reinterpret_cast<float4*>(gp + lane * 32 + j) =
+                    make_float4(gr[j], gr[j + 1], gr[j + 2], gr[j + 3]);
+            gp[32 * 32 + lane] = rhs;
+          }
         }
       }
     }
@@ -617,23 +981,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 }
 
 // ---------------------------------------------------------------------------------------------
-// k_finish_tc: one warp per row (rows warp, warp + total warps, ...).
-constexpr int kFinWarps = 8;
-constexpr int kLc = 36;                 // L^T leading dimension
-constexpr int kFinWork = 32 * 36 * 8;   // per warp: two FP32 L^T (one per half), or the FP64
-                                        // retry's L^T
-
 // k_sum_parts: one warp per split row: its parts' FP64 partial Grams summed in part order, one
-// entry at a time, and rounded once into the row's FP32 Gram record (lane i: Gram row i).
+// entry at a time, and rounded once into an FP32 Gram record (lane i: Gram row i): the row's own
+// record, or with `compact` record w of a list of the split rows' records.
 __global__ void __launch_bounds__(256)
     k_sum_parts(const double* __restrict__ scratch, const int4* __restrict__ split_rows,
-                int nsplit, float* __restrict__ gram) {
+                int nsplit, float* __restrict__ gram, int compact) {
   const int lane = threadIdx.x & 31;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= nsplit) return;
   const int4 sr = split_rows[w];  // {row, parts, scratch slot of part 0, unused}
   const double* s0 = scratch + (size_t)sr.z * kGramRec;
-  float* gp = gram + (size_t)sr.x * kGramRec;
+  float* gp = gram + (size_t)(compact ? w : sr.x) * kGramRec;
   for (int j = 0; j < 32; j++) {
     double acc = 0.0;
     for (int prt = 0; prt < sr.y; prt++) acc += __ldcg(s0 + (size_t)prt * kGramRec + lane * 32 + j);
@@ -644,120 +1003,38 @@ __global__ void __launch_bounds__(256)
   gp[32 * 32 + lane] = (float)rs;
 }
 
-// k_finish_tc: one warp per two rows (rows 2q, 2q + 1 for q = warp, warp + total warps, ...),
-// half-warp h finishing row 2q + h with the pair routines of warp_finish.cuh from the row's
-// Gram record (split rows: written by k_sum_parts).  A half whose FP32 factorisation fails is
-// redone in FP64 by the whole warp.
+// k_finish_tc: one warp per four rows (rows 4w .. 4w + 3 for w = warp, warp + total warps, ...),
+// quarter q finishing row 4w + q with the quad routines from the row's Gram record.  Rows are
+// 0 .. nrows - 1 with record r, or with a list the rows list[i].x with record i (the split rows
+// after the fused kernel).  A row whose FP32 factorisation fails is redone in FP64 by the whole
+// warp from the same record.
 __global__ void __launch_bounds__(kFinWarps * 32, 2)
-    k_finish_tc(const SampleParams p, const float* __restrict__ gram) {
+    k_finish_tc(const SampleParams p, const float* __restrict__ gram,
+                const int4* __restrict__ list, int nlist) {
   extern __shared__ __align__(16) unsigned char fsm[];
-  double* Lam_s = reinterpret_cast<double*>(fsm);
-  double* lmu_s = Lam_s + 32 * 33;
-  float* LamF = reinterpret_cast<float*>(lmu_s + 32);  // (float) Lambda, ld kLc
-  unsigned char* works = reinterpret_cast<unsigned char*>(LamF + 32 * kLc);
+  FinConst* fc = reinterpret_cast<FinConst*>(fsm);
+  unsigned char* works = fsm + (sizeof(FinConst) + 15) / 16 * 16;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int h = lane >> 4, l = lane & 15;
-  const int K = p.K;
   const uint32_t sweep = p.ctl->sweep;
-  for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
-    const int i = e / 32, j = e % 32;
-    const double v = (i < K && j < K) ? p.Lambda[i + j * K] : 0.0;
-    Lam_s[i * 33 + j] = v;
-    LamF[i * kLc + j] = (float)v;
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    double s = 0.0;
-    if (lane < K)
-      for (int j = 0; j < K; j++) s += Lam_s[lane * 33 + j] * p.mu[j];
-    lmu_s[lane] = s;
-  }
-  __syncthreads();
+  fin_const_fill(fc, p, threadIdx.x, blockDim.x, [] { __syncthreads(); });
   const float alpha_f = (float)noise_alpha(p);
   unsigned char* work = works + (size_t)warp * kFinWork;
-  float* Lc = reinterpret_cast<float*>(work) + h * 32 * kLc;  // this half's L^T
-  const int c_lo = l, c_hi = l + 16;                        // this lane's two components
+  const int n = list ? nlist : p.nrows;
   const int stride = gridDim.x * kFinWarps;
-  for (int q = blockIdx.x * kFinWarps + warp; 2 * q < p.nrows; q += stride) {
-    const int row = 2 * q + h;
-    const bool have = row < p.nrows;  // the second half of a last odd pair only follows along
-    const int rw = have ? row : 2 * q;
-    const float* gp = gram + (size_t)rw * kGramRec;
-    // rows c_lo (columns 0..15) and c_hi (columns 0..31) of Lambda + alpha G: (float) Lambda +
-    // (float) alpha * G, the identity beyond K
-    float lo[16], hi[32], d0_lo = 1.f, d0_hi = 1.f;
-#pragma unroll
-    for (int j = 0; j < 16; j += 4) {
-      const float4 v = __ldcg(reinterpret_cast<const float4*>(gp + c_lo * 32 + j));
-      const float4 m = *reinterpret_cast<const float4*>(LamF + c_lo * kLc + j);
-      const float g4[4] = {v.x, v.y, v.z, v.w}, m4[4] = {m.x, m.y, m.z, m.w};
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int jj = j + u;
-        lo[jj] = (c_lo < K && jj < K) ? m4[u] + alpha_f * g4[u] : (c_lo == jj ? 1.f : 0.f);
-        if (jj == c_lo) d0_lo = lo[jj];
+  for (int w = blockIdx.x * kFinWarps + warp; 4 * w < n; w += stride) {
+    const int idx = 4 * w + (lane >> 3);
+    const bool have = idx < n;  // the last quarters of a short final group only follow along
+    const int iw = have ? idx : 4 * w;
+    const int rw = list ? list[iw].x : iw;
+    const unsigned fails = quad_finish<false>(p, fc, gram + (size_t)iw * kGramRec, have ? rw : -1,
+                                              rw, alpha_f, sweep, lane);
+    __syncwarp();
+    for (int q = 0; q < 4; q++)
+      if ((fails >> (8 * q)) & 1u) {
+        const int fi = 4 * w + q;
+        retry_row_from_record(p, fc, gram + (size_t)fi * kGramRec, list ? list[fi].x : fi, sweep,
+                              work);
       }
-    }
-#pragma unroll
-    for (int j = 0; j < 32; j += 4) {
-      const float4 v = __ldcg(reinterpret_cast<const float4*>(gp + c_hi * 32 + j));
-      const float4 m = *reinterpret_cast<const float4*>(LamF + c_hi * kLc + j);
-      const float g4[4] = {v.x, v.y, v.z, v.w}, m4[4] = {m.x, m.y, m.z, m.w};
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int jj = j + u;
-        hi[jj] = (c_hi < K && jj < K) ? m4[u] + alpha_f * g4[u] : (c_hi == jj ? 1.f : 0.f);
-        if (jj == c_hi) d0_hi = hi[jj];
-      }
-    }
-    // rhs + Lambda mu (Macau: mu + Uhat[row]) of the two components, in FP64
-    double rl_lo = (double)__ldcg(gp + 32 * 32 + c_lo), rl_hi = (double)__ldcg(gp + 32 * 32 + c_hi);
-    if (p.uhat) {
-      double m_lo = 0.0, m_hi = 0.0;
-      for (int j = 0; j < K; j++) {
-        const double mj = p.mu[j] + p.uhat[(size_t)rw * 32 + j];
-        if (c_lo < K) m_lo += Lam_s[c_lo * 33 + j] * mj;
-        if (c_hi < K) m_hi += Lam_s[c_hi * 33 + j] * mj;
-      }
-      rl_lo += m_lo;
-      rl_hi += m_hi;
-    } else {
-      rl_lo += lmu_s[c_lo];
-      rl_hi += lmu_s[c_hi];
-    }
-    const float z_lo = (float)comp_noise(p, rw, K, c_lo, sweep);
-    const float z_hi = (float)comp_noise(p, rw, K, c_hi, sweep);
-    float rinv_lo = 1.f, rinv_hi = 1.f;
-    const bool ok = pair_factor(lo, hi, rinv_lo, rinv_hi, l, d0_lo, d0_hi, Lc, kLc);
-    float x_lo = (float)rl_lo, x_hi = (float)rl_hi;
-    pair_solve(lo, hi, rinv_lo, rinv_hi, x_lo, x_hi, l, Lc, kLc, z_lo, z_hi);
-    if (ok && have) {
-      if (c_lo < K) {
-        p.out_f32[(size_t)row * 32 + c_lo] = x_lo;
-        p.out_bf16[(size_t)row * 32 + c_lo] = __float2bfloat16_rn(x_lo);
-      }
-      if (c_hi < K) {
-        p.out_f32[(size_t)row * 32 + c_hi] = x_hi;
-        p.out_bf16[(size_t)row * 32 + c_hi] = __float2bfloat16_rn(x_hi);
-      }
-    }
-    // FP64 retry of a failed half by the whole warp (lane = component)
-    const unsigned okm = __ballot_sync(0xffffffffu, ok);
-#pragma unroll
-    for (int hf = 0; hf < 2; hf++) {
-      const int rf = 2 * q + hf;
-      if (((okm >> (16 * hf)) & 1u) || rf >= p.nrows) continue;
-      const int src = 16 * hf + (lane & 15);
-      const double v_lo = __shfl_sync(0xffffffffu, rl_lo, src);
-      const double v_hi = __shfl_sync(0xffffffffu, rl_hi, src);
-      if (lane == 0) atomicAdd(&p.ctl->retries[p.mode], 1u);
-      const bool ok2 = warp_finish_f64<32, float>(gram + (size_t)rf * kGramRec, 32, Lam_s,
-                                                  lane < 16 ? v_lo : v_hi, p, rf, sweep, work);
-      if (!ok2 && lane == 0) {
-        atomicOr(&p.ctl->status, kStatCholFail);
-        atomicCAS(&p.ctl->bad_row, -1, rf);
-      }
-    }
     __syncwarp();
   }
 }
@@ -793,47 +1070,71 @@ __global__ void __launch_bounds__(256)
 
 }  // namespace
 
-size_t tc_smem_bytes() { return (size_t)kStages * kStageBytes + sizeof(TcShared); }
+size_t tc_smem_bytes(bool fused) {
+  return (size_t)kStages * kStageBytes + (sizeof(TcShared) + 15) / 16 * 16 +
+         (fused ? sizeof(FusedShared) : 0);
+}
+
+namespace {
+// Opt-in shared memory sizes, set once per device and kernel.
+template <typename Kern>
+void set_smem(Kern k, size_t bytes, bool (&configured)[64]) {
+  int dev = 0;
+  MG_CUDA(cudaGetDevice(&dev));
+  if (!configured[dev & 63]) {
+    MG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    configured[dev & 63] = true;
+  }
+}
+constexpr size_t kFinSmem = (sizeof(FinConst) + 15) / 16 * 16 + (size_t)kFinWarps * kFinWork;
+static_assert((size_t)kStages * kStageBytes + sizeof(TcShared) + 16 + sizeof(FusedShared) <=
+                  227 * 1024,
+              "fused tensor-core sampler exceeds the shared memory of one CTA");
+}  // namespace
 
 bool launch_gram_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
                     int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
   if (KP != 32 || p.packed == nullptr) return false;
   static bool configured[64] = {false};
-  int dev = 0;
-  MG_CUDA(cudaGetDevice(&dev));
-  const size_t smem = tc_smem_bytes();
-  if (!configured[dev & 63]) {
-    MG_CUDA(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured[dev & 63] = true;
-  }
-  k_gram_tc<<<num_sms, kTcThreads, smem, s>>>(p, gram);
+  const size_t smem = tc_smem_bytes(false);
+  set_smem(k_gram_tc<false>, smem, configured);
+  k_gram_tc<false><<<num_sms, kTcThreads, smem, s>>>(p, gram);
   MG_CUDA(cudaGetLastError());
   if (mid) MG_CUDA(cudaEventRecord(mid, s));
   if (nsplit > 0) {
-    k_sum_parts<<<(nsplit + 7) / 8, 256, 0, s>>>(p.scratch, split_rows, nsplit, gram);
+    k_sum_parts<<<(nsplit + 7) / 8, 256, 0, s>>>(p.scratch, split_rows, nsplit, gram, 0);
     MG_CUDA(cudaGetLastError());
   }
   return true;
 }
 
 bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
-                      int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
+                      int KP, cudaStream_t s, int num_sms, cudaEvent_t mid, bool fused) {
   if (KP != 32 || p.packed == nullptr) return false;
-  static bool configured[64] = {false};
-  int dev = 0;
-  MG_CUDA(cudaGetDevice(&dev));
-  const size_t fsmem = sizeof(double) * (32 * 33 + 32) + sizeof(float) * 32 * kLc +
-                       (size_t)kFinWarps * kFinWork;
-  if (!configured[dev & 63]) {
-    MG_CUDA(cudaFuncSetAttribute(k_finish_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)fsmem));
-    configured[dev & 63] = true;
+  static bool configured_fin[64] = {false}, configured_fused[64] = {false};
+  set_smem(k_finish_tc, kFinSmem, configured_fin);
+  if (fused && !p.one) {
+    // the fused kernel finishes every unsplit row; split rows: parts summed into a compact list
+    // of records, then finished from there
+    const size_t smem = tc_smem_bytes(true);
+    set_smem(k_gram_tc<true>, smem, configured_fused);
+    k_gram_tc<true><<<num_sms, kTcThreads, smem, s>>>(p, nullptr);
+    MG_CUDA(cudaGetLastError());
+    if (mid) MG_CUDA(cudaEventRecord(mid, s));
+    if (nsplit > 0) {
+      k_sum_parts<<<(nsplit + 7) / 8, 256, 0, s>>>(p.scratch, split_rows, nsplit, gram, 1);
+      MG_CUDA(cudaGetLastError());
+      const int blocks = std::min(num_sms * 2, (nsplit + 4 * kFinWarps - 1) / (4 * kFinWarps));
+      k_finish_tc<<<blocks, kFinWarps * 32, kFinSmem, s>>>(p, gram, split_rows, nsplit);
+      MG_CUDA(cudaGetLastError());
+    }
+    return true;
   }
   launch_gram_tc(p, gram, split_rows, nsplit, KP, s, num_sms, mid);
   if (p.one)
     k_finish_one_tc<<<num_sms * 8, 256, 0, s>>>(p, gram);
   else
-    k_finish_tc<<<num_sms * 2, kFinWarps * 32, fsmem, s>>>(p, gram);
+    k_finish_tc<<<num_sms * 2, kFinWarps * 32, kFinSmem, s>>>(p, gram, nullptr, 0);
   MG_CUDA(cudaGetLastError());
   return true;
 }

@@ -44,17 +44,23 @@ std::vector<int> sample_group_options(int KP, bool mixed, int gram);
 double value_moment(const double* v, long long n, double center, bool sq, cudaStream_t s);
 // dst[i] = src[i] rounded to BF16 (half = false) or FP16 (half = true), n values.
 void launch_copy16(const float* src, void* dst, long long n, bool half, cudaStream_t s);
-// Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only):
-// k_gram_tc, then (if nsplit > 0) k_sum_parts, then k_finish_tc (k_finish_one_tc when p.one).  It reads the 16-entry padded
-// packed CSR and its task list (p.packed / p.tasks, built by the context) and gathers the other
-// factor's BF16 rows from p.other, whose row nother is all zeros (the padding sentinel).
-// `gram` holds nrows Gram records of 32 * 32 + 32 floats; split_rows lists the nsplit rows
-// whose Grams are split into parts, as {row, parts, scratch slot of part 0, 0} (their partial
-// Grams go to p.scratch, 1056 doubles per slot).  Returns false when the configuration is not
-// covered (caller uses the CUDA-core kernel).  `mid`, if given, is recorded after k_gram_tc
-// (per-kernel timing).
+// Mixed-precision sampler whose Grams run on the tcgen05 tensor cores (KP = 32 only).  It reads
+// the 16-entry padded packed CSR and its task list (p.packed / p.tasks, built by the context) and
+// gathers the other factor's BF16 rows from p.other, whose row nother is all zeros (the padding
+// sentinel).  split_rows lists the nsplit rows whose Grams are split into parts, as {row,
+// parts, scratch slot of part 0, 0} (their partial Grams go to p.scratch, 1056 doubles per
+// slot).
+//   fused (and not p.one): k_gram_tc<true> finishes every unsplit row in its epilogue; if
+//     nsplit > 0, k_sum_parts writes the split rows' Grams to records 0 .. nsplit - 1 of `gram`
+//     and k_finish_tc finishes them.  `gram` needs max(1, nsplit) records.
+//   otherwise: k_gram_tc<false> writes every row's Gram record (`gram` holds nrows records of
+//     32 * 32 + 32 floats), k_sum_parts the split rows', then k_finish_tc (k_finish_one_tc when
+//     p.one) finishes all rows.
+// Returns false when the configuration is not covered (caller uses the CUDA-core kernel).
+// `mid`, if given, is recorded after k_gram_tc (per-kernel timing).
 bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
-                      int KP, cudaStream_t s, int num_sms, cudaEvent_t mid = nullptr);
+                      int KP, cudaStream_t s, int num_sms, cudaEvent_t mid = nullptr,
+                      bool fused = true);
 // The Gram half of launch_sample_tc: k_gram_tc (+ k_sum_parts), no finish.  Returns false when
 // the configuration is not covered.
 bool launch_gram_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,

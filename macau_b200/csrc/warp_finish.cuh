@@ -319,3 +319,134 @@ __device__ __noinline__ bool warp_finish_f64(const GT* Gs, int ld, const double*
 }
 
 }  // namespace mg
+
+namespace mg {
+
+// ---- Four rows per warp (K <= 32, FP32), the "quad" layout: quarter q = lane / 8 finishes
+// matrix q, and lane i = lane % 8 of the quarter holds rows i, i + 8, i + 16, i + 24 (slot
+// k = row / 8), row i + 8k with its columns 0 .. 8k + 7 at a[qoff(k) + c] (its lower triangle and
+// the few entries above it, which receive discarded values).  Every lane holds 80 entries.
+// Column broadcasts go through 8-wide shuffles, so the four matrices of a warp share every step
+// of the dependency chain and no shared memory is needed.  The factor applies the same fma with
+// the same operands in the same order as warp_factor / pair_factor, so it produces the same L.
+
+__host__ __device__ constexpr int qoff(int k) { return 4 * k * (k + 1); }  // 0, 8, 24, 48
+
+__device__ __forceinline__ float shfl8(float v, int src) {
+  return __shfl_sync(0xffffffffu, v, src, 8);
+}
+
+// Factorises the quarter's matrix (d0[k]: the original diagonal entry of row i + 8k); rinv[k]
+// receives 1 / L(i + 8k, i + 8k).  Returns the quarter's verdict: every pivot positive and above
+// 2^-20 of its original diagonal (warp_factor with rel_floor 2^-20).
+__device__ __forceinline__ bool quad_factor(float (&a)[80], float (&rinv)[4], int i,
+                                            const float (&d0)[4]) {
+  float dg[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) dg[k] = d0[k];
+  bool bad = false;
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    const int jk = j >> 3, ji = j & 7;
+    if (i == ji) bad |= !(dg[jk] > 0.f) || !(dg[jk] > 0x1p-20f * d0[jk]);
+    const float r = shfl8(rsqrtf(dg[jk]), ji);
+    if (i == ji) rinv[jk] = r;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (8 * k + 7 >= j) {
+        const bool own = (i + 8 * k == j);
+        a[qoff(k) + j] = (own ? dg[k] : a[qoff(k) + j]) * r;
+      }
+    if (j + 1 < 32) {
+      const float lnext = shfl8(a[qoff((j + 1) >> 3) + j], (j + 1) & 7);  // L(j+1, j)
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (8 * k + 7 > j && i + 8 * k > j)
+          dg[k] = fmaf(-a[qoff(k) + j], a[qoff(k) + j], dg[k]);
+        if (8 * k + 7 >= j + 1)
+          a[qoff(k) + j + 1] = fmaf(-a[qoff(k) + j], lnext, a[qoff(k) + j + 1]);
+      }
+    }
+#pragma unroll
+    for (int c = 2; c < 32; c++) {  // constant bounds so that both loops unroll fully
+      if (c >= j + 2) {
+        const float lc = shfl8(a[qoff(c >> 3) + j], c & 7);  // L(c, j)
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          if (8 * k + 7 >= c) a[qoff(k) + c] = fmaf(-a[qoff(k) + j], lc, a[qoff(k) + c]);
+      }
+    }
+  }
+  const unsigned b = __ballot_sync(0xffffffffu, bad);
+  return ((b >> ((threadIdx.x & 31) & 24)) & 0xFFu) == 0u;
+}
+
+// y = L^{-1} b (the same operations as warp_solve's forward pass), y += z, then x = L^{-T} y by
+// columns from the last: x_j = (y_j - sum_{r > j} L(r, j) x_r) / L(j, j), each sum reduced over
+// the quarter's lanes.  b[k] (component i + 8k) holds the right-hand side in and x out.
+__device__ __forceinline__ void quad_solve(const float (&a)[80], const float (&rinv)[4],
+                                           float (&b)[4], const float (&z)[4], int i) {
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    const int jk = j >> 3, ji = j & 7;
+    if (i == ji) b[jk] = b[jk] * rinv[jk];
+    const float yj = shfl8(b[jk], ji);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (8 * k + 7 > j && i + 8 * k > j) b[k] = fmaf(-a[qoff(k) + j], yj, b[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) b[k] += z[k];
+#pragma unroll
+  for (int j = 31; j >= 0; j--) {
+    const int jk = j >> 3, ji = j & 7;
+    float part = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (8 * k + 7 > j && i + 8 * k > j) part = fmaf(a[qoff(k) + j], b[k], part);
+    part += __shfl_xor_sync(0xffffffffu, part, 4, 8);
+    part += __shfl_xor_sync(0xffffffffu, part, 2, 8);
+    part += __shfl_xor_sync(0xffffffffu, part, 1, 8);
+    if (i == ji) b[jk] = (b[jk] - part) * rinv[jk];
+  }
+}
+
+// The N(0,1) draws of components i + 8k (k = 0..3) of `row`, in FP32 (0 beyond K): injected, or
+// keyed like comp_noise.  Lanes i and i ^ 1 need the two normals of the same four Philox blocks;
+// each computes two blocks and they swap halves.
+__device__ __forceinline__ void quad_noise(const SampleParams& p, int row, int K, int i,
+                                           uint32_t sweep, float (&z)[4]) {
+  if (p.znoise) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int c = i + 8 * k;
+      z[k] = c < K ? (float)p.znoise[(size_t)row * K + c] : 0.f;
+    }
+    return;
+  }
+  const int odd = i & 1;
+  double z0[2], z1[2];
+#pragma unroll
+  for (int t = 0; t < 2; t++)
+    normal_pair(p.seed, sweep, stream_id(kRowNoise, (uint32_t)p.mode), (uint32_t)row,
+                (uint32_t)((i >> 1) + 4 * (2 * odd + t)), &z0[t], &z1[t]);
+  // even lane: its z0 of blocks k = 0, 1, and sends z1 of them; odd lane: its z1 of k = 2, 3
+  const double s0 = __shfl_xor_sync(0xffffffffu, odd ? z0[0] : z1[0], 1);
+  const double s1 = __shfl_xor_sync(0xffffffffu, odd ? z0[1] : z1[1], 1);
+  double zz[4];
+  if (odd) {
+    zz[0] = s0;
+    zz[1] = s1;
+    zz[2] = z1[0];
+    zz[3] = z1[1];
+  } else {
+    zz[0] = z0[0];
+    zz[1] = z0[1];
+    zz[2] = s0;
+    zz[3] = s1;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) z[k] = (i + 8 * k) < K ? (float)zz[k] : 0.f;
+}
+
+}  // namespace mg

@@ -36,29 +36,31 @@
 //   warp 8      MMA: allocates TMEM (512 columns: three accumulators of 160 columns); one lane
 //               issues the MMAs, releases stages (tcgen05.commit -> "empty") and publishes
 //               finished accumulators (tcgen05.commit -> "acc full").
-//   warps 9-12  epilogue (warp w reads TMEM quadrant w % 4 = row slot): TMEM -> registers,
-//               release the accumulator and the group's descriptor slot ("desc free"); a part
-//               of a split row goes to the part's scratch slot as an FP64 partial.  Records
-//               kernel: the row's FP32 Gram and rhs go to its Gram record.  Fused kernel: the
-//               warp takes groups two at a time and finishes its quadrant's two rows as a pair
-//               (half-warp h = the row of group 2i + h; the pair routines of warp_finish.cuh,
-//               the arithmetic of k_finish_tc), so the FP32 factor of one pair overlaps the MMAs
-//               of the next groups.  A half whose FP32 factor fails is redone by the whole warp
-//               in FP64 from the row's CSR entries and BF16 latents (retry_row_from_csr).
-//   warp 13     scheduler: takes 4 tasks per group from the work queue (four claims in flight)
+//   warp 9      scheduler: takes 4 tasks per group from the work queue (four claims in flight)
 //               and publishes the group descriptors into a ring of kDesc slots as far ahead as
 //               the ring allows, so that the queue atomics and task loads stay off the MMA warp.
-//   warps 14-15 CSR loaders, one per k-block parity: walk the group descriptors and, up to kCsr
+//   warps 10-11 CSR loaders, one per k-block parity: walk the group descriptors and, up to kCsr
 //               k-blocks of their parity ahead, copy each k-block's four 128-byte row segments
 //               with one 16-byte cp.async per lane into the ring, with a meta record (stage
 //               index, valid rows, stop / end) for the producers.
+//   warps 12-15 epilogue (warp w reads TMEM quadrant w % 4 = row slot): TMEM -> registers,
+//               release the accumulator and the group's descriptor slot ("desc free"); a part
+//               of a split row goes to the part's scratch slot as an FP64 partial.  Records
+//               kernel: the row's FP32 Gram and rhs go to its Gram record.  Fused kernel: the
+//               warp takes groups four at a time, staging each quadrant in shared memory as it
+//               arrives, and finishes the four rows together (quarter q of the warp: the row of
+//               group 4i + q; the quad routines of warp_finish.cuh), so the factors of one batch
+//               overlap the MMAs of the next groups.  In the fused kernel the epilogue
+//               warpgroup takes registers from the other three (setmaxnreg).  A row whose FP32
+//               factor fails is redone by the whole warp in FP64 from the row's CSR entries and
+//               BF16 latents (retry_row_from_csr).
 // Every barrier wait is bounded by a clock budget (SampleParams::wait_cycles, about 2 s by
 // default); on expiry the CTA raises an abort flag, all roles leave their loops, the MMA lane
 // drains its MMAs (a wait of the full default budget), TMEM is freed and the status word reports
 // a timeout.
 //
-// k_finish_tc.  One warp per two rows: the Gram records (or the FP64 sums of split rows' parts,
-// in part order, written by k_sum_parts), then the FP32 pair Cholesky and solves of
+// k_finish_tc.  One warp per four rows: the Gram records (or the FP64 sums of split rows' parts,
+// in part order, written by k_sum_parts), then the FP32 quad Cholesky and solves of
 // warp_finish.cuh with an FP64 retry of the same Gram.  After the fused kernel it finishes the
 // split rows only, from a compact list of their records.
 #include <cuda_bf16.h>
@@ -73,12 +75,23 @@ namespace {
 
 constexpr int kRowSlots = 4;
 constexpr int kParity = 2;                          // producers per row slot
-constexpr int kProducers = kRowSlots * kParity;     // warps 0-7
-constexpr int kMmaWarp = kProducers;                // warp 8
-constexpr int kEpiWarp0 = kProducers + 1;           // warps 9-12
-constexpr int kSchedWarp = kProducers + 5;           // warp 13
-constexpr int kCsrWarp0 = kProducers + 6;            // warps 14-15
+constexpr int kProducers = kRowSlots * kParity;     // warps 0-7 (warpgroups 0 and 1)
+constexpr int kMmaWarp = kProducers;                // warp 8   (warpgroup 2)
+constexpr int kSchedWarp = kProducers + 1;          // warp 9
+constexpr int kCsrWarp0 = kProducers + 2;           // warps 10-11
+constexpr int kEpiWarp0 = kProducers + 4;           // warps 12-15 (warpgroup 3)
 constexpr int kTcThreads = (kProducers + 8) * 32;
+// Fused kernel: registers per thread after the warpgroups rebalance (setmaxnreg) from the 128 of
+// the launch: warpgroups 0-2 give theirs up to the epilogue, whose four-row finish keeps 80
+// matrix entries per lane plus the dependency chains of four matrices in flight.  The split
+// must fit the launch allocation: 12 warps x 32 x 80 + 4 x 32 x 256 = 63,488 <= 512 x 128.
+constexpr int kLaunchRegs = 128;
+constexpr int kOtherRegs = 80;
+constexpr int kEpiRegs = 256;
+static_assert((kTcThreads - 128) * kOtherRegs + 128 * kEpiRegs <= kTcThreads * kLaunchRegs,
+              "register split exceeds the launch allocation");
+static_assert(kEpiWarp0 % 4 == 0 && kTcThreads - kEpiWarp0 * 32 == 128,
+              "the epilogue must be the last warpgroup");
 constexpr int kStages = 24;               // gather stages in flight (even: stage s has parity s % 2)
 constexpr int kBlockBytes = 2 * 512;      // one column block: 2 K-atoms x 512 B
 constexpr int kStageBytes = 5 * kBlockBytes;
@@ -170,8 +183,9 @@ __device__ __forceinline__ bool mbar_test_suspend(uint64_t* b, uint32_t parity, 
 }
 
 // Slow path of mbar_wait: suspended tries of up to 20 us, the abort flag and the clock budget
-// checked between them.
-__device__ __noinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, TcShared* sh, Ctl* ctl) {
+// checked between them.  Inlined like every device function of the fused kernel: a call from
+// warpgroups that run with different register counts (setmaxnreg) does not allocate.
+__device__ __forceinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, TcShared* sh, Ctl* ctl) {
   const long long t0 = clock64();
   const long long budget = sh->wait_cycles;
   for (;;) {
@@ -509,7 +523,7 @@ __device__ __noinline__ void retry_row_from_record(const SampleParams& p, const 
 // [begin, begin + len) and the BF16 latents they gather (the inputs of the tensor-core Gram,
 // without its FP32 rounding), then MM = Lambda + alpha G, the FP64 warp Cholesky and solves with
 // the row's keyed draws.  Counts a retry; a failed FP64 factor raises kStatCholFail.
-__device__ __noinline__ void retry_row_from_csr(const SampleParams& p, const FinConst* fc,
+__device__ __forceinline__ void retry_row_from_csr(const SampleParams& p, const FinConst* fc,
                                                 int row, long long begin, int len,
                                                 uint32_t sweep, unsigned char* work) {
   const int lane = threadIdx.x & 31;
@@ -695,7 +709,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_fence_after();
   const uint32_t tmem = sh->tmem_base;
 
+  // Fused kernel: each role branch starts with its warpgroup's register rebalance (setmaxnreg
+  // is executed by all warps of a warpgroup at the same instruction, so warpgroup 2's three
+  // roles share one branch).
   if (warp < kProducers) {
+    if constexpr (kFused) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kOtherRegs));
     // ================= producer of row slot r, parity h =================
     // lane l copies 16-byte chunk l % 4 of the rows of entries l / 4 and l / 4 + 8.  A k-block's
     // copies form one cp.async group; kLag k-blocks later the producer waits for that group,
@@ -765,7 +783,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (q == qo) so = pend[q];
       if (lane == 0) mbar_arrive(&sh->full[so]);
     }
-  } else if (warp == kMmaWarp) {
+  } else if (warp < kEpiWarp0) {
+    if constexpr (kFused) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kOtherRegs));
+    if (warp == kMmaWarp) {
     // ================= MMA issuer =================
     int stage = 0;
     uint32_t phase = 0;
@@ -811,7 +831,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       while (!mbar_test(&sh->drain, 0) && clock64() - t0 < kWaitCycles) __nanosleep(128);
     }
     __syncwarp();
-  } else if (warp == kSchedWarp) {
+    } else if (warp == kSchedWarp) {
     // ================= scheduler =================
     // lane 0 keeps four queue claims in flight (q[0] oldest); the next group's tasks are
     // loaded while the current group is published
@@ -839,7 +859,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       t_cur = t_nxt;
       tk_cur = tk_nxt;
     }
-  } else if (warp >= kCsrWarp0) {
+    } else {
     // ================= CSR loader of parity h =================
     // lane l copies entries 2 (l % 8) .. + 1 of row slot l / 8's k-block
     const int h = warp - kCsrWarp0, rs = lane >> 3, c2 = 2 * (lane & 7);
@@ -868,9 +888,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       ok = cursor_advance(c, kParity, sh, p.ctl, rs);
     }
     cp_wait_all();
+    }
   } else {
     const int qd = warp & 3;  // TMEM quadrant = row slot of the group
     if constexpr (kFused) {
+      asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kEpiRegs));
       // ================= epilogue: accumulators -> finished rows =================
       // four groups at a time: each group's quadrant is staged in shared memory as it arrives
       // (its accumulator released at once), then the warp finishes the four rows, quarter q the
@@ -1118,6 +1140,15 @@ bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows
     // of records, then finished from there
     const size_t smem = tc_smem_bytes(true);
     set_smem(k_gram_tc<true>, smem, configured_fused);
+    // the warpgroups' register rebalance needs the launch allocation it was sized for
+    static int launch_regs = 0;
+    if (launch_regs == 0) {
+      cudaFuncAttributes fa{};
+      MG_CUDA(cudaFuncGetAttributes(&fa, k_gram_tc<true>));
+      launch_regs = fa.numRegs;
+    }
+    if (launch_regs < kLaunchRegs)
+      throw MgError(MG_ERR_CUDA, "fused tensor-core sampler built with too few registers");
     k_gram_tc<true><<<num_sms, kTcThreads, smem, s>>>(p, nullptr);
     MG_CUDA(cudaGetLastError());
     if (mid) MG_CUDA(cudaEventRecord(mid, s));

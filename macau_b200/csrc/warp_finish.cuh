@@ -412,8 +412,9 @@ __device__ __forceinline__ void quad_solve(const float (&a)[80], const float (&r
 }
 
 // The N(0,1) draws of components i + 8k (k = 0..3) of `row`, in FP32 (0 beyond K): injected, or
-// keyed like comp_noise.  Lanes i and i ^ 1 need the two normals of the same four Philox blocks;
-// each computes two blocks and they swap halves.
+// keyed like comp_noise and evaluated in FP32 (normal_pair_f32, as the fused kernel's drainers
+// do).  Lanes i and i ^ 1 need the two normals of the same four Philox blocks; each computes two
+// blocks and they swap halves.
 __device__ __forceinline__ void quad_noise(const SampleParams& p, int row, int K, int i,
                                            uint32_t sweep, float (&z)[4]) {
   if (p.znoise) {
@@ -425,15 +426,15 @@ __device__ __forceinline__ void quad_noise(const SampleParams& p, int row, int K
     return;
   }
   const int odd = i & 1;
-  double z0[2], z1[2];
+  float z0[2], z1[2];
 #pragma unroll
   for (int t = 0; t < 2; t++)
-    normal_pair(p.seed, sweep, stream_id(kRowNoise, (uint32_t)p.mode), (uint32_t)row,
-                (uint32_t)((i >> 1) + 4 * (2 * odd + t)), &z0[t], &z1[t]);
+    normal_pair_f32(p.seed, sweep, stream_id(kRowNoise, (uint32_t)p.mode), (uint32_t)row,
+                    (uint32_t)((i >> 1) + 4 * (2 * odd + t)), &z0[t], &z1[t]);
   // even lane: its z0 of blocks k = 0, 1, and sends z1 of them; odd lane: its z1 of k = 2, 3
-  const double s0 = __shfl_xor_sync(0xffffffffu, odd ? z0[0] : z1[0], 1);
-  const double s1 = __shfl_xor_sync(0xffffffffu, odd ? z0[1] : z1[1], 1);
-  double zz[4];
+  const float s0 = __shfl_xor_sync(0xffffffffu, odd ? z0[0] : z1[0], 1);
+  const float s1 = __shfl_xor_sync(0xffffffffu, odd ? z0[1] : z1[1], 1);
+  float zz[4];
   if (odd) {
     zz[0] = s0;
     zz[1] = s1;
@@ -446,7 +447,7 @@ __device__ __forceinline__ void quad_noise(const SampleParams& p, int row, int K
     zz[3] = s1;
   }
 #pragma unroll
-  for (int k = 0; k < 4; k++) z[k] = (i + 8 * k) < K ? (float)zz[k] : 0.f;
+  for (int k = 0; k < 4; k++) z[k] = (i + 8 * k) < K ? zz[k] : 0.f;
 }
 
 }  // namespace mg

@@ -54,110 +54,111 @@ def _is_matrix(Y):
                                            Y.format in ("coo", "csr", "csc"))
 
 
-def make_train_test(Y, ntest, seed=None):
-    """Splits a sparse matrix Y into a train and a test matrix (macau.pyx:109-130).
-       Y      scipy sparse matrix (coo_matrix, csr_matrix or csc_matrix)
-       ntest  either a float below 1.0 or integer.
-              if float, then indicates the ratio of test cells
-              if integer, then indicates the number of test cells
-       returns Ytrain, Ytest (type coo_matrix)
-    """
-    if not _is_matrix(Y):
-        raise TypeError("Unsupported Y type: %s" % type(Y))
+def _holdout_split(n, ntest, seed):
+    """Random train / test positions among n items: ntest < 1 is a fraction of n, otherwise a
+    count (rounded).  Returns (train positions, test positions)."""
     if not isinstance(ntest, numbers.Real) or ntest < 0:
         raise TypeError("ntest has to be a non-negative number (number or ratio of test samples).")
-    Y = Y.tocoo(copy=False)
-    if ntest < 1:
-        ntest = Y.nnz * ntest
-    ntest = int(round(ntest))
-    rng = np.random if seed is None else np.random.default_rng(seed)
-    rperm = rng.permutation(Y.nnz)
-    train = rperm[ntest:]
-    test = rperm[0:ntest]
-    Ytrain = scipy.sparse.coo_matrix((Y.data[train], (Y.row[train], Y.col[train])), shape=Y.shape)
-    Ytest = scipy.sparse.coo_matrix((Y.data[test], (Y.row[test], Y.col[test])), shape=Y.shape)
-    return Ytrain, Ytest
+    count = int(round(n * ntest if ntest < 1 else ntest))
+    order = (np.random if seed is None else np.random.default_rng(seed)).permutation(n)
+    return order[count:], order[:count]
+
+
+def make_train_test(Y, ntest, seed=None):
+    """Random holdout of the observed cells of a sparse matrix.
+
+    Y: a scipy sparse matrix (COO, CSR or CSC).  ntest: a fraction in [0, 1) of the cells, or a
+    number of cells, that go to the test matrix.  seed: None uses numpy's global generator.
+    Returns the train and test matrices as COO matrices of Y's shape.  Same arguments and
+    errors as the reference's make_train_test (macau.pyx:109-130)."""
+    if not _is_matrix(Y):
+        raise TypeError("Unsupported Y type: %s" % type(Y))
+    C = Y.tocoo(copy=False)
+    tr, te = _holdout_split(C.nnz, ntest, seed)
+
+    def pick(idx):
+        return scipy.sparse.coo_matrix((C.data[idx], (C.row[idx], C.col[idx])), shape=C.shape)
+    return pick(tr), pick(te)
 
 
 def make_train_test_df(Y, ntest, seed=None):
-    """Splits rows of dataframe Y into a train and a test dataframe (macau.pyx:132-152)."""
+    """Random holdout of the rows of a DataFrame of (index columns..., value) records; ntest as
+    in make_train_test.  Returns the train and test frames (macau.pyx:132-152)."""
     if type(Y) != pd.core.frame.DataFrame:
         raise TypeError("Y should be DataFrame.")
-    if not isinstance(ntest, numbers.Real) or ntest < 0:
-        raise TypeError("ntest has to be a non-negative number (number or ratio of test samples).")
-    if ntest < 1:
-        ntest = Y.shape[0] * ntest
-    ntest = int(round(ntest))
-    rng = np.random if seed is None else np.random.default_rng(seed)
-    rperm = rng.permutation(Y.shape[0])
-    train = rperm[ntest:]
-    test = rperm[0:ntest]
-    return Y.iloc[train], Y.iloc[test]
+    tr, te = _holdout_split(Y.shape[0], ntest, seed)
+    return Y.iloc[tr], Y.iloc[te]
 
 
 def remove_nan(Y):
-    if not np.any(np.isnan(Y.data)):
+    """Drops the cells of a COO matrix whose value is NaN (returns Y itself when none is)."""
+    keep = ~np.isnan(Y.data)
+    if keep.all():
         return Y
-    idx = np.where(np.isnan(Y.data) == False)[0]  # noqa: E712
-    return scipy.sparse.coo_matrix((Y.data[idx], (Y.row[idx], Y.col[idx])), shape=Y.shape)
+    return scipy.sparse.coo_matrix((Y.data[keep], (Y.row[keep], Y.col[keep])), shape=Y.shape)
 
 
 class Data:
-    """Input validation and COO extraction (macau.pyx:242-306)."""
+    """Training and test data as index arrays and values, from a sparse matrix pair or a
+    DataFrame pair; the checks and their messages are those of the reference's Python entry
+    (macau.pyx:242-306).  A number for Ytest holds out that fraction / count of Y."""
 
     def __init__(self, Y, Ytest):
         if _is_matrix(Y):
-            if Ytest is None:
-                Ytest = scipy.sparse.coo_matrix(Y.shape, dtype=np.float64)
-            if isinstance(Ytest, numbers.Real):
-                Y, Ytest = make_train_test(Y, Ytest)
-            if not _is_matrix(Ytest):
-                raise ValueError("When Y is a sparse matrix Ytest must be too.")
-            if Y.shape != Ytest.shape:
-                raise ValueError("Y (%d x %d) and Ytest (%d x %d) must have the same shape." %
-                                 (Y.shape[0], Y.shape[1], Ytest.shape[0], Ytest.shape[1]))
-            Y = remove_nan(Y.tocoo(copy=False))
-            Ytest = remove_nan(Ytest.tocoo(copy=False))
-            self.shape = np.array(Y.shape, dtype=np.int32)
-            self.idxTrain = [Y.row, Y.col]
-            self.valTrain = Y.data
-            self.idxTest = [Ytest.row, Ytest.col]
-            self.valTest = Ytest.data
-            self.colnames = np.array(["row", "col"], dtype=object)
+            self._from_matrices(Y, Ytest)
         elif type(Y) == pd.core.frame.DataFrame:
-            if Ytest is None:
-                Ytest = Y[0:0]
-            if isinstance(Ytest, numbers.Real):
-                Y, Ytest = make_train_test_df(Y, Ytest)
-            if type(Ytest) != pd.core.frame.DataFrame:
-                raise TypeError("When Y is a DataFrame Ytest must be too.")
-            if (Y.columns != Ytest.columns).any():
-                raise ValueError("Columns of Y and Ytest must be the same.")
-            if (Y.dtypes != Ytest.dtypes).any():
-                raise TypeError("Y.dtypes and Ytest.dtypes must be the same.")
-            int_cols = [c for c in Y.columns if Y[c].dtype in (np.int64, np.int32)]
-            float_cols = [c for c in Y.columns if Y[c].dtype in (np.float32, np.float64)]
-            if len(int_cols) > 10:
-                raise ValueError("Y has too many index(int) columns (%d), maximum is 10." % len(int_cols))
-            if len(int_cols) < 2:
-                raise ValueError("Y must have at least 2 index (int) columns.")
-            if len(float_cols) != 1:
-                raise ValueError("Y has %d float columns but must have exactly 1 value column." % len(float_cols))
-            if Y.shape[0] == 0:
-                raise ValueError("Ytrain must not be empty.")
-            value_col = float_cols[0]
-            self.colnames = int_cols
-            if Ytest.shape[0] > 0:
-                self.shape = np.array(np.maximum([Y[c].max() for c in int_cols],
-                                                 [Ytest[c].max() for c in int_cols]) + 1, dtype=np.int32)
-            else:
-                self.shape = np.array([Y[c].max() for c in int_cols], dtype=np.int32) + 1
-            self.idxTrain = [np.array(Y[c], dtype=np.int32) for c in int_cols]
-            self.idxTest = [np.array(Ytest[c], dtype=np.int32) for c in int_cols]
-            self.valTrain = np.array(Y[value_col], dtype=np.float64)
-            self.valTest = np.array(Ytest[value_col], dtype=np.float64)
+            self._from_frames(Y, Ytest)
         else:
             raise TypeError("Unsupported Y type: %s" % type(Y))
+
+    def _from_matrices(self, Y, Ytest):
+        if Ytest is None:
+            Ytest = scipy.sparse.coo_matrix(Y.shape, dtype=np.float64)
+        if isinstance(Ytest, numbers.Real):
+            Y, Ytest = make_train_test(Y, Ytest)
+        if not _is_matrix(Ytest):
+            raise ValueError("When Y is a sparse matrix Ytest must be too.")
+        if Y.shape != Ytest.shape:
+            raise ValueError("Y (%d x %d) and Ytest (%d x %d) must have the same shape." %
+                             (Y.shape[0], Y.shape[1], Ytest.shape[0], Ytest.shape[1]))
+        tr = remove_nan(Y.tocoo(copy=False))
+        te = remove_nan(Ytest.tocoo(copy=False))
+        self.shape = np.array(tr.shape, dtype=np.int32)
+        self.idxTrain, self.valTrain = [tr.row, tr.col], tr.data
+        self.idxTest, self.valTest = [te.row, te.col], te.data
+        self.colnames = np.array(["row", "col"], dtype=object)
+
+    def _from_frames(self, Y, Ytest):
+        if Ytest is None:
+            Ytest = Y[0:0]
+        if isinstance(Ytest, numbers.Real):
+            Y, Ytest = make_train_test_df(Y, Ytest)
+        if type(Ytest) != pd.core.frame.DataFrame:
+            raise TypeError("When Y is a DataFrame Ytest must be too.")
+        if (Y.columns != Ytest.columns).any():
+            raise ValueError("Columns of Y and Ytest must be the same.")
+        if (Y.dtypes != Ytest.dtypes).any():
+            raise TypeError("Y.dtypes and Ytest.dtypes must be the same.")
+        index_cols = [c for c in Y.columns if Y[c].dtype in (np.int64, np.int32)]
+        value_cols = [c for c in Y.columns if Y[c].dtype in (np.float32, np.float64)]
+        if len(index_cols) > 10:
+            raise ValueError("Y has too many index(int) columns (%d), maximum is 10." % len(index_cols))
+        if len(index_cols) < 2:
+            raise ValueError("Y must have at least 2 index (int) columns.")
+        if len(value_cols) != 1:
+            raise ValueError("Y has %d float columns but must have exactly 1 value column." % len(value_cols))
+        if Y.shape[0] == 0:
+            raise ValueError("Ytrain must not be empty.")
+        # each mode's size is one more than the largest index seen in train or test
+        largest = np.array([Y[c].max() for c in index_cols])
+        if Ytest.shape[0] > 0:
+            largest = np.maximum(largest, [Ytest[c].max() for c in index_cols])
+        self.shape = np.array(largest + 1, dtype=np.int32)
+        self.colnames = index_cols
+        self.idxTrain = [np.array(Y[c], dtype=np.int32) for c in index_cols]
+        self.idxTest = [np.array(Ytest[c], dtype=np.int32) for c in index_cols]
+        self.valTrain = np.array(Y[value_cols[0]], dtype=np.float64)
+        self.valTest = np.array(Ytest[value_cols[0]], dtype=np.float64)
 
 
 def _side_coo(s, nrows):

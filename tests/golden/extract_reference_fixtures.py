@@ -6,7 +6,7 @@ are read as *text* from ``lib/macau-cpp/tests.cpp`` and stored as small fixtures
 read only the JSON this script writes (``reference_tests_cpp.json``); the reference tree is
 needed only to regenerate it:
 
-    python tests/golden/extract_reference_fixtures.py /root/reference
+    python tests/golden/extract_reference_fixtures.py <path of the reference checkout>
 
 Eigen comma initialisers (``M << a, b, ...;``) fill matrices row by row; the JSON keeps that
 row-major order together with the matrix shape declared in the test.
@@ -120,4 +120,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract_reference_fixtures.py <path of the reference checkout>")
+    main(sys.argv[1])

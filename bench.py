@@ -36,7 +36,7 @@ METRIC = "Gibbs sweeps/s at K=32: mixed-prec batched vs FP64 plain, equal test R
 UNIT = "sweeps/s"
 K_LATENT = 32
 ALPHA = 2.0
-PROFILE_SUMMARY = ROOT / "profiles" / "k_gram_tc_bpmf_powerlaw_k32.md"
+PROFILE_SUMMARY = ROOT / "profiles" / "k_gram_tc_fused_bpmf_powerlaw_k32.md"
 
 
 def parse_args():
@@ -58,6 +58,8 @@ def parse_args():
                     help="skip the 512-problem batched leg")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the Gram precision sweep on the 2,000 x 1,500 matrix")
+    ap.add_argument("--no-uniform", action="store_true",
+                    help="skip the K = 10 legs on the 2,000 x 1,500 matrix (GPU and CPU rates)")
     ap.add_argument("--only", choices=["all", "mixed", "fp64", "macau", "univariate", "precision",
                                        "batched"],
                     default="all",
@@ -167,8 +169,8 @@ def sampler_bytes(st, w, compute, mode):
 
 
 def read_traffic():
-    """DRAM bytes per half-sweep of the sampler (k_gram_tc + k_finish_tc, mean of the two modes,
-    full size) from the committed ncu summary, if any."""
+    """DRAM bytes per half-sweep of the sampler (the fused k_gram_tc, mean of the two modes, full
+    size) from the committed ncu summary, if any."""
     try:
         for line in PROFILE_SUMMARY.read_text().splitlines():
             if line.startswith("dram_bytes_per_launch:"):
@@ -223,6 +225,40 @@ def side_info_legs(device, sweeps=20, cpu_sweeps=2):
                              "cores": cores}
         leg["mixed_over_cpu"] = leg["mixed"]["sweeps_per_s"] / leg["cpu_oracle"]["sweeps_per_s"]
         out[prior] = leg
+    return out
+
+
+def uniform_legs(device, burnin=200, nsamples=200):
+    """The CPU-scale BPMF case: the 2,000 x 1,500 uniform matrix (60,000 entries, 10% holdout,
+    K = 10, alpha = 4, seed 0), burnin + nsamples sweeps.  Sweep rates (CUDA events) of the GPU
+    FP64 and mixed samplers, the CPU oracle's FP64 rate on all host cores, and each chain's
+    posterior-mean test RMSE."""
+    from macau_b200 import _lib, workloads
+    from oracle import oracle as orc
+    from tests.gpu_helpers import oracle_model
+    w = workloads.bpmf_uniform(seed=0)
+    K, alpha, n = 10, 4.0, burnin + nsamples
+    out = {"workload": w["name"], "K": K, "alpha": alpha, "burnin": burnin, "nsamples": nsamples}
+    for comp, name in ((_lib.MG_COMPUTE_FP64, "gpu_fp64"), (_lib.MG_COMPUTE_MIXED, "gpu_mixed")):
+        s = _lib.Sampler(K, alpha, seed=0, compute=comp, device=device)
+        s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
+        s.set_relation_data_test(w["trows"], w["tcols"], w["tvals"], w["shape"])
+        s.set_samples(burnin, nsamples)
+        s.init()
+        t, _ = s.time_sweeps(0, n, eval=True)
+        out[name] = {"sweeps_per_s": n / t, "test_rmse": s.rmse()[0],
+                     "note": "sweeps with test evaluation, captured graph"}
+        s.close()
+    cores = orc.set_threads(os.cpu_count() or 1)
+    m = oracle_model(w, K, alpha, 0)
+    t0 = time.perf_counter()
+    for it in range(n):
+        m.sweep(it, burnin)
+    tc = time.perf_counter() - t0
+    out["cpu_oracle"] = {"sweeps_per_s": n / tc, "test_rmse": m.rmse()[0], "cores": cores,
+                         "kind": "port"}
+    out["gpu_fp64_over_cpu"] = out["gpu_fp64"]["sweeps_per_s"] / out["cpu_oracle"]["sweeps_per_s"]
+    out["rmse_mixed_minus_oracle"] = out["gpu_mixed"]["test_rmse"] - out["cpu_oracle"]["test_rmse"]
     return out
 
 
@@ -323,6 +359,42 @@ def batched_legs(device, sweeps=20, single_sweeps=3, autotune=True):
                           "note": "sum over problems of each problem's own FP64 sweep time "
                                   "(captured graph, CUDA events)"}
     out["batched_over_single_fp64"] = out["batched_mixed"]["sweeps_per_s"] * tot
+    # one problem at a time with the mixed sampler (default shapes)
+    tot_mx = 0.0
+    for pr, K, sd in zip(problems, Ks, seeds):
+        s = _lib.Sampler(K, alpha, seed=sd, compute=_lib.MG_COMPUTE_MIXED, device=device)
+        s.set_relation_data(pr["rows"], pr["cols"], pr["vals"], pr["shape"])
+        s.set_samples(10 ** 6, 1)
+        s.init()
+        s.time_sweeps(0, 1, eval=False)
+        tp, _ = s.time_sweeps(1, single_sweeps, eval=False)
+        tot_mx += tp / single_sweeps
+        s.close()
+    out["single_mixed"] = {"sweeps_per_s": 1.0 / tot_mx, "ms_per_sweep": tot_mx * 1e3,
+                           "note": "sum over problems of each problem's own mixed sweep time"}
+    out["batched_over_single_mixed"] = out["batched_mixed"]["sweeps_per_s"] * tot_mx
+    # CPU oracle (FP64, all host cores) on a bounded sample of the problems, scaled to the set
+    # by training entries
+    from oracle import oracle as orc
+    from tests.gpu_helpers import oracle_model
+    cores = orc.set_threads(os.cpu_count() or 1)
+    t_cpu, nnz_cpu, ncpu = 0.0, 0, 0
+    for pr, K, sd in zip(problems, Ks, seeds):
+        m = oracle_model(pr, K, alpha, sd)
+        m.sweep(0, 10 ** 6)
+        t0 = time.perf_counter()
+        for it in range(1, 3):
+            m.sweep(it, 10 ** 6)
+        t_cpu += (time.perf_counter() - t0) / 2
+        nnz_cpu += len(pr["vals"])
+        ncpu += 1
+        if t_cpu > 10.0:
+            break
+    t_set = t_cpu * info["nnz"] / nnz_cpu
+    out["cpu_oracle"] = {"sweeps_per_s": 1.0 / t_set, "cores": cores, "kind": "port",
+                         "sample": f"2 FP64 sweeps of each of the first {ncpu} problems, the "
+                                   "set's time scaled by its training entries"}
+    out["batched_over_cpu"] = out["batched_mixed"]["sweeps_per_s"] * t_set
     return out
 
 
@@ -557,7 +629,7 @@ def run_ours(args):
     d2h = st_e["d2h_bytes"] - d2h0
     del preds
 
-    # ---- roofline of the dominant step: the latent sampler (k_gram_tc + k_finish_tc) ----
+    # ---- roofline of the dominant step: the latent sampler (the fused k_gram_tc) ----
     hbm, tflops, src = peaks()
     b = sampler_bytes(st_mx, w, "mixed", 0) + sampler_bytes(st_mx, w, "mixed", 1)
     t_launch = (ph[0] + ph[1]) / (2 * nph)     # mean seconds per half-sweep of the sampler
@@ -565,15 +637,16 @@ def run_ours(args):
     traffic = read_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
-                "kernel": "latent sampler half-sweep (k_gram_tc + k_finish_tc), mean of the two "
-                          "modes, CUDA events on the library stream",
+                "kernel": "latent sampler half-sweep (fused k_gram_tc: tensor-core Grams and "
+                          "the rows' finish), mean of the two modes, CUDA events on the library "
+                          "stream",
                 "algorithmic_bytes_per_launch": b / 2}
     if ph[5] > 0:
         t_gram = (ph[5] + ph[6]) / (2 * nph)   # mean seconds per k_gram_tc launch
         gflop = sum(st_mx["nnz"][m] * (K_LATENT * (K_LATENT + 1) + 2 * K_LATENT) for m in (0, 1)) / 2
         gathered = sum(st_mx["nnz"][m] for m in (0, 1)) / 2 * K_LATENT * 2
         roofline["gram_kernel"] = {
-            "name": "k_gram_tc", "ms_per_launch": t_gram * 1e3,
+            "name": "k_gram_tc (fused: Gram + finish)", "ms_per_launch": t_gram * 1e3,
             "share_of_sampler": (ph[5] + ph[6]) / (ph[0] + ph[1]),
             "algorithmic_tflops": gflop / t_gram / 1e12, "tensor_peak_bf16": tflops,
             "tensor_frac": gflop / t_gram / 1e12 / tflops,
@@ -607,6 +680,8 @@ def run_ours(args):
         line["side_info"] = side_info_legs(local)
     if rank == 0 and world == 1 and not args.no_precision:
         line["precision_sweep"] = precision_sweep(local)
+    if rank == 0 and world == 1 and not args.no_uniform:
+        line["uniform_k10"] = uniform_legs(local)
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched"] = batched_legs(local, autotune=not args.no_autotune)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

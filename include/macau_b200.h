@@ -30,7 +30,8 @@ extern "C" {
 #define MG_OK 0
 #define MG_ERR_ARG (-1)        /* invalid argument (reference: ValueError / runtime_error) */
 #define MG_ERR_CHOL (-2)       /* "Cholesky Decomposition failed!" (latentprior.cpp:374-376) */
-#define MG_ERR_CG (-3)         /* block-CG breakdown or iteration cap (linop.h:279) */
+#define MG_ERR_CG (-3)         /* block-CG breakdown, or a solve that reached its iteration cap
+                                  without converging (the reference stops silently, linop.h:279) */
 #define MG_ERR_CUDA (-4)       /* CUDA runtime error */
 #define MG_ERR_STATE (-5)      /* call out of order (e.g. sweep before data) */
 #define MG_ERR_TIMEOUT (-6)    /* a bounded device-side wait gave up */
@@ -235,6 +236,10 @@ int mg_batch_get_info(mg_batch* b, int64_t* out);
  *                      MG_ERR_TIMEOUT and leaves the context usable after mg_init
  *   "tc_wait_test"     (default 0; tests only) 1 = the tensor-core sampler's MMA warp first
  *                      waits on a barrier that nothing arrives on, so that wait runs out
+ *   "cg_max_iter"      (default 100000, the reference's cap, linop.h:279) iterations of each
+ *                      block-CG solve; a solve that reaches the cap keeps its last iterate, the
+ *                      update completes, and the call returns MG_ERR_CG ("block-CG did not
+ *                      converge within N iterations")
  *   "cg_fp32"          (default 0) mixed mode: run the Macau block-CG in FP32 with an FP64
  *                      residual replacement every 20 iterations instead of FP64; set before
  *                      mg_init

@@ -22,7 +22,7 @@ namespace {
 
 constexpr int kReplaceEvery = 20;
 constexpr int kCgBatch = 8;         // CG iterations queued between host convergence checks
-constexpr int kMaxCgIter = 100000;  // iteration cap (the breakdown flag ends a run earlier)
+constexpr int kMaxCgIter = 100000;  // default iteration cap, the reference's (linop.h:279)
 constexpr int kOuterThreads = 256;
 constexpr int kOuterRows = 32;
 
@@ -758,7 +758,7 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
             const double* B, int bstride, int n, double tol, double* Xout, int xstride,
             Ctl* ctl, cudaStream_t s, V* R, V* P, V* KPm, V* inner, double* Xd, double* Bn,
             double* KX, double* innerd, double* small, double* partials, int* flag_dev,
-            volatile int* flag_host) {
+            volatile int* flag_host, int max_iter, bool& converged) {
   const long long nfeat = Ft.nrow;
   const int nb = outer_blocks(nfeat);
   double* reduced = partials + (size_t)296 * 64 * 64;
@@ -801,8 +801,9 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
   // at once, so the result is that of stopping at the converged iteration.
   const uint32_t* done = &ctl->cg_done;
   int iter = 0;
-  while (iter < kMaxCgIter) {
-    for (int b = 0; b < kCgBatch && iter < kMaxCgIter; b++, iter++) {
+  converged = false;
+  while (iter < max_iter) {
+    for (int b = 0; b < kCgBatch && iter < max_iter; b++, iter++) {
       spmm_t<V, NRP>(F, P, NRP, inner, NRP, n, nullptr, 0, 0.0, nullptr, s, done);
       spmm_t<V, NRP>(Ft, inner, NRP, KPm, NRP, n, P, NRP, reg, reg_dev, s, done);
       outer<V, NRP>(P, KPm, nfeat, partials, nb, s, done);
@@ -830,6 +831,7 @@ int cg_core(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev
     MG_CUDA(cudaStreamSynchronize(s));
     if (flag_host[0]) {
       iter = flag_host[1];
+      converged = true;
       break;
     }
   }
@@ -938,18 +940,22 @@ int BlockCg::core(const DevCsr& F, const DevCsr& Ft, double reg, const double* r
     if (n <= 32)
       return cg_core<float, 32>(F, Ft, reg, reg_dev, B, bstride, n, tol, X, xstride, ctl, s,
                                 (float*)R_, (float*)P_, (float*)KP_, (float*)inner_, Xd_, Bn_,
-                                KX_, innerd_, small_, partials_, flag_dev, flag_host_);
+                                KX_, innerd_, small_, partials_, flag_dev, flag_host_,
+                                max_iter_, last_converged_);
     return cg_core<float, 64>(F, Ft, reg, reg_dev, B, bstride, n, tol, X, xstride, ctl, s,
                               (float*)R_, (float*)P_, (float*)KP_, (float*)inner_, Xd_, Bn_,
-                              KX_, innerd_, small_, partials_, flag_dev, flag_host_);
+                              KX_, innerd_, small_, partials_, flag_dev, flag_host_,
+                              max_iter_, last_converged_);
   }
   if (n <= 32)
     return cg_core<double, 32>(F, Ft, reg, reg_dev, B, bstride, n, tol, X, xstride, ctl, s,
                                (double*)R_, (double*)P_, (double*)KP_, (double*)inner_, Xd_,
-                               Bn_, KX_, innerd_, small_, partials_, flag_dev, flag_host_);
+                               Bn_, KX_, innerd_, small_, partials_, flag_dev, flag_host_,
+                               max_iter_, last_converged_);
   return cg_core<double, 64>(F, Ft, reg, reg_dev, B, bstride, n, tol, X, xstride, ctl, s,
                              (double*)R_, (double*)P_, (double*)KP_, (double*)inner_, Xd_, Bn_,
-                             KX_, innerd_, small_, partials_, flag_dev, flag_host_);
+                             KX_, innerd_, small_, partials_, flag_dev, flag_host_,
+                             max_iter_, last_converged_);
 }
 
 int BlockCg::solve(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev,
@@ -959,13 +965,18 @@ int BlockCg::solve(const DevCsr& F, const DevCsr& Ft, double reg, const double* 
   // overlapping extra block when a remainder block is followed by one more start index.
   const int blocksize = 32, excess = 8;
   reserve(F.nrow, Ft.nrow, 64, f32);
-  if (nrhs <= excess + blocksize)
-    return core(F, Ft, reg, reg_dev, B, bstride, nrhs, tol, X, xstride, ctl, s, f32);
+  if (nrhs <= excess + blocksize) {
+    const int it = core(F, Ft, reg, reg_dev, B, bstride, nrhs, tol, X, xstride, ctl, s, f32);
+    converged_ = last_converged_;
+    return it;
+  }
   int total = 0;
+  converged_ = true;
   for (int i = 0; i < nrhs; i += blocksize) {
     int nr = blocksize;
     if (i + blocksize + excess >= nrhs) nr = nrhs - i;
     total += core(F, Ft, reg, reg_dev, B + i, bstride, nr, tol, X + i, xstride, ctl, s, f32);
+    converged_ = converged_ && last_converged_;
   }
   return total;
 }

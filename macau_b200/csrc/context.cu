@@ -709,8 +709,12 @@ class Context {
                         mode, p.tmp.p, CP_, s_);
     launch_beta_rhs_b(p.Ft, p.tmp.p, CP_, K_, p.Lchol.p, p.lambda_beta.p, ctl_.p, cfg_.seed,
                       mode, p.B.p, CP_, s_);
+    p.cg.set_max_iter(cg_max_iter_);
     p.cg_iters = p.cg.solve(p.F, p.Ft, 0.0, p.lambda_beta.p, p.B.p, CP_, K_, p.tol, p.beta.p,
                             CP_, ctl_.p, s_, cg_f32_);
+    // a solve that reached its cap keeps its last iterate; the update completes and the
+    // status check after it reports MG_ERR_CG
+    if (!p.cg.converged()) cg_noconv_ = true;
     // stats x3 (+ reductions), NW, chol, tmp, spmm, noise, uhat spmm, lambda_beta + the CG's
     // (set-up, then 10 per iteration)
     launches_ += 12 + 6 + 10LL * p.cg_iters;
@@ -873,6 +877,11 @@ class Context {
     retries_[1] = h.retries[1];
     // a timed-out launch left its work unfinished, so its status comes before what followed
     if (h.status & kStatTimeout) throw MgError(MG_ERR_TIMEOUT, "device wait timed out");
+    if (cg_noconv_) {
+      cg_noconv_ = false;
+      throw MgError(MG_ERR_CG, "block-CG did not converge within " + std::to_string(cg_max_iter_) +
+                                   " iterations");
+    }
     if (h.status & kStatCholFail)
       throw MgError(MG_ERR_CHOL, "Cholesky Decomposition failed!");
     if (h.status & kStatHyperFail)
@@ -1144,6 +1153,10 @@ class Context {
     tc_wait_cycles_ = 2000LL * us;
     drop_graphs();
   }
+  void set_cg_max_iter(int n) {
+    if (n < 1) throw MgError(MG_ERR_ARG, "cg_max_iter must be >= 1");
+    cg_max_iter_ = n;
+  }
   void set_tc_wait_test(bool b) {
     tc_wait_test_ = b;
     drop_graphs();
@@ -1338,6 +1351,10 @@ class Context {
   // default: at tol 1e-6 the FP32 iteration needs about 1.5x the iterations of FP64, which
   // costs more than its halved gather traffic saves.
   bool cg_f32_ = false;
+  // Block-CG iteration cap per solve (option "cg_max_iter"; the reference's 100,000,
+  // linop.h:279) and whether a solve since the last status check reached it.
+  int cg_max_iter_ = 100000;
+  bool cg_noconv_ = false;
   // Autotuning at mg_init (option "autotune"): 0 off, 1 on with the choice cache, 2 on and
   // always timed
   int autotune_ = 0;
@@ -1608,6 +1625,7 @@ int mg_set_option(mg_ctx* ctx, const char* name, int value) {
     else if (n == "tc_wait_us") c.set_tc_wait(value);
     else if (n == "tc_wait_test") c.set_tc_wait_test(value != 0);
     else if (n == "cg_fp32") c.set_cg_f32(value != 0);
+    else if (n == "cg_max_iter") c.set_cg_max_iter(value);
     else if (n == "gram_precision") c.set_gram(value);
     else if (n == "autotune") c.set_autotune(value);
     else if (n == "split_threshold") c.set_split_threshold(value);
@@ -1688,6 +1706,11 @@ int mg_blockcg(const int32_t* rows, const int32_t* cols, const double* vals, int
     if (seconds) *seconds = ms * 1e-3;
     if (h.status & mg::kStatCgFail) {
       g_create_error = "block-CG breakdown";
+      return MG_ERR_CG;
+    }
+    if (!cg.converged()) {  // X holds the last iterate
+      g_create_error = "block-CG did not converge within " + std::to_string(cg.max_iter()) +
+                       " iterations";
       return MG_ERR_CG;
     }
     return MG_OK;

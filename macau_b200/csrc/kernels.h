@@ -174,6 +174,11 @@ class BlockCg {
   int solve(const DevCsr& F, const DevCsr& Ft, double reg, const double* reg_dev,
             const double* B, int bstride, int nrhs, double tol, double* X, int xstride,
             Ctl* ctl, cudaStream_t s, bool f32);
+  // Iteration cap of each block's solve (default 100,000 like the reference, linop.h:279); a
+  // block that reaches it keeps its last iterate and solve() reports converged() == false.
+  void set_max_iter(int n) { max_iter_ = n; }
+  int max_iter() const { return max_iter_; }
+  bool converged() const { return converged_; }
   ~BlockCg() { release(); }
 
  private:
@@ -182,6 +187,8 @@ class BlockCg {
            cudaStream_t s, bool f32);
   long long nrow_ = 0, nfeat_ = 0;
   int maxr_ = 0;
+  int max_iter_ = 100000;
+  bool converged_ = true, last_converged_ = true;
   bool f32_ = false;
   void *R_ = nullptr, *P_ = nullptr, *KP_ = nullptr, *inner_ = nullptr;
   double *Xd_ = nullptr, *Bn_ = nullptr, *KX_ = nullptr, *innerd_ = nullptr;

@@ -9,7 +9,8 @@ Each generator returns a dict with train / test COO arrays in the sampler's inpu
   bpmf_powerlaw 138,000 x 27,000 matrix, 20M observations; row and column degrees from the
                 truncated power law p(k) ~ 1/k on [5, 20000] (inverse CDF), rescaled to the target
                 total and clipped to [5, 20000], paired by a configuration model (duplicate
-                (i, j) pairs dropped); rank-32 U V^T + N(0, 0.8^2) shifted to mean 3.5, rounded to
+                (i, j) pairs dropped, then topped up to 20M unique cells with extra pairs drawn
+                in proportion to the degrees); rank-32 U V^T + N(0, 0.8^2) shifted to mean 3.5, rounded to
                 0.5 steps in [0.5, 5]; 10% holdout (K = 32, alpha = 2).  Same shape as the public
                 MovieLens-20M rating matrix, generated synthetically.
   macau_side    20,000 x 500 matrix, 1M observations, rank-32 signal + N(0, 1) standardised to mean
@@ -86,6 +87,15 @@ def bpmf_powerlaw(nrow=138000, ncol=27000, nobs=20_000_000, rank=32, noise=0.8, 
     cs = np.repeat(np.arange(ncol, dtype=np.int64), dc)
     rng.shuffle(cs)
     key = np.unique(rs * ncol + cs)
+    # the pairing repeats some (i, j); top up to nobs unique cells with extra pairs drawn in
+    # proportion to the row and column degrees
+    pr, pc = dr / dr.sum(), dc / dc.sum()
+    while len(key) < nobs:
+        m = int((nobs - len(key)) * 1.1) + 16
+        extra = rng.choice(nrow, size=m, p=pr) * ncol + rng.choice(ncol, size=m, p=pc)
+        extra = np.setdiff1d(np.unique(extra), key, assume_unique=True)
+        extra = rng.permutation(extra)[:nobs - len(key)]
+        key = np.union1d(key, extra)
     r = (key // ncol).astype(np.int32)
     c = (key % ncol).astype(np.int32)
     sd = rank ** -0.25

@@ -240,6 +240,25 @@ def test_blockcg_matches_oracle_fp64(oracle_parts, tol, bar):
     assert relerr(X.T, Xo) < bar
 
 
+def test_blockcg_iteration_cap_is_reported():
+    # linop.h:279 stops at its iteration cap silently; here a solve that reaches the cap keeps
+    # its last iterate, the prior update completes, and the call reports MG_ERR_CG; the context
+    # carries on, and with the default cap the next sweep's solve converges
+    w = workloads.macau_side(scale=0.02, seed=5)
+    s = gpu_sampler(w, 8, 1.0, 77, tol=1e-10, init=False)
+    s.set_option("cg_max_iter", 2)
+    s.init()
+    with pytest.raises(_lib.MacauError, match="did not converge within 2 iterations") as e:
+        s.sweep(0, eval=False)
+    assert e.value.code == _lib.MG_ERR_CG
+    assert s.stats()["cg_iters"][0] == 2
+    assert np.isfinite(s.beta(0)).all()
+    s.set_option("cg_max_iter", 100000)
+    s.sweep(1, eval=False)
+    assert s.stats()["cg_iters"][0] > 2
+    s.close()
+
+
 def test_blockcg_fp32_with_fp64_residual_replacement():
     w = workloads.macau_side(scale=0.05, seed=6)
     fr, fc, _, shp = w["side"]

@@ -12,7 +12,9 @@ evaluation excluded from the timed region and reported separately).
 events on the library's stream; `e2e` is the same metric through the C ABI with host buffers
 (data upload and CSR build, per-sweep RMSE read-back and the final prediction read-back inside
 the timed region).  `--impl reference` times the CPU oracle (FP64 restatement of the reference,
-OpenMP on all host cores).  Under torchrun each rank runs an independent chain on its own GPU.
+OpenMP on all host cores).  Under torchrun (N > 1) the ranks run one chain whose half-sweeps
+are split by rows (an all-gather of the new rows after each), or with `--sharding replicas`
+one independent chain each.
 Both GPU arms pick their row samplers' work split and CTA shape with the library's autotuner at
 initialisation (outside the timed region; `--no-autotune` keeps the default shapes).
 """
@@ -58,6 +60,10 @@ def parse_args():
                     help="skip the 512-problem batched leg")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the Gram precision sweep on the 2,000 x 1,500 matrix")
+    ap.add_argument("--sharding", choices=["rows", "replicas"], default=None,
+                    help="one chain with each half-sweep's rows split over the ranks (rows, the "
+                         "default for N > 1; given explicitly it also runs at N = 1) or one "
+                         "independent chain per rank (replicas)")
     ap.add_argument("--no-uniform", action="store_true",
                     help="skip the K = 10 legs on the 2,000 x 1,500 matrix (GPU and CPU rates)")
     ap.add_argument("--only", choices=["all", "mixed", "fp64", "macau", "univariate", "precision",
@@ -77,7 +83,8 @@ def config_dict(w, args, n):
             "holdout": "10% random", "rows": w["shape"][0], "cols": w["shape"][1],
             "ntrain": int(len(w["vals"])), "ntest": int(len(w["tvals"])),
             "parallelism": f"independent chains x{n}" if n > 1 else "single GPU",
-            "l2": "inputs larger than L2 (per sweep the two CSR streams are >=290 MB)",
+            "l2": "inputs larger than L2 (per sweep the two packed CSR streams are %.0f MB)"
+                  % (2 * len(w["vals"]) * 8 / 1e6),
             "eval": "excluded from the timed sweeps"}
 
 
@@ -501,6 +508,88 @@ def run_reference(args):
     return 0
 
 
+def run_sharded(args, ranks, w, local, clk_bus):
+    """N > 1, --sharding rows: one mixed-precision chain whose half-sweeps are split over the
+    ranks by rows (macau_b200/sharded.py): each rank samples an entry-balanced row range, the
+    new rows are all-gathered over NCCL into every rank's latent buffer (on the library's
+    stream), and every rank updates the hyperparameters itself from the same latents.  `value`
+    is that one chain's sweeps/s (the whole job's throughput; strong scaling), timed with CUDA
+    events on the library stream and taken as the maximum over ranks."""
+    import torch
+    from macau_b200 import _lib, sharded
+    K, W = args.steps, args.warmup
+    world, rank = ranks.world, ranks.rank
+    lengths = [np.bincount(w["rows"], minlength=w["shape"][0]),
+               np.bincount(w["cols"], minlength=w["shape"][1])]
+    dev = torch.device(f"cuda:{local}")
+    seed = 1000  # one chain: the same seed on every rank
+
+    def chain_for(s):
+        return sharded.ShardedChain(sharded.LibraryBackend(s, dev), ranks.dist, rank, world,
+                                    lengths)
+
+    mx = make_sampler(w, _lib.MG_COMPUTE_MIXED, seed, local)
+    chain = chain_for(mx)
+    for it in range(W):
+        chain.sweep(it)
+    stream = torch.cuda.ExternalStream(mx.stream(), device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ranks.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(clk_bus) as clk:
+        e0.record(stream)
+        for it in range(W, W + K):
+            chain.sweep(it)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize(dev)
+    t = ranks.max(e0.elapsed_time(e1) * 1e-3)
+    st = mx.stats()
+    mx.close()
+    # e2e: set-up from host buffers, the sharded sweeps with evaluation, result read-back
+    ranks.barrier()
+    t0 = time.perf_counter()
+    s = _lib.Sampler(K_LATENT, ALPHA, seed=seed, compute=_lib.MG_COMPUTE_MIXED, device=local)
+    s.set_relation_data(w["rows"], w["cols"], w["vals"], w["shape"])
+    s.set_relation_data_test(w["trows"], w["tcols"], w["tvals"], w["shape"])
+    s.set_samples(0, K)
+    s.init()
+    h2d0, d2h0 = s.stats()["h2d_bytes"], s.stats()["d2h_bytes"]
+    ch = chain_for(s)
+    for it in range(K):
+        ch.sweep(it)
+        s.eval(it)
+        s.rmse()
+    preds = s.predictions()
+    t_e2e = ranks.max(time.perf_counter() - t0)
+    st_e = s.stats()
+    rmse = s.rmse()[0]
+    s.close()
+    del preds
+    line = {"metric": METRIC, "value": K / t, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": t / K * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "bf16-gram/f32-chol/f64-hyper",
+            "data": "synthetic (seeded power-law stand-in, no dataset read)",
+            "config": dict(config_dict(w, args, world),
+                           parallelism=f"rows of each half-sweep split over {world} ranks, "
+                                       "all-gather of the new rows (NCCL)"),
+            "sharding": {"ranges": [ch.ranges[m][rank] for m in (0, 1)],
+                         "collective": "all_gather of each half-sweep's latent rows"},
+            "test_rmse": {"mixed": rmse},
+            "gpu_launches": int(round(st["kernel_launches"] / max(1, st["sweeps"]) * K)),
+            "clocks": clk.summary(),
+            "e2e": {"value": K / t_e2e, "unit": UNIT,
+                    "h2d_bytes_per_step": (st_e["h2d_bytes"] - h2d0) / K,
+                    "d2h_bytes_per_step": (st_e["d2h_bytes"] - d2h0) / K,
+                    "timed": "C-ABI set-up from host buffers, sharded sweeps with evaluation "
+                             "and RMSE read-back, predictions read-back"}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ranks.close()
+    return 0
+
+
 def run_ours(args):
     from macau_b200 import _lib
     ranks = Ranks("nccl")
@@ -552,6 +641,9 @@ def run_ours(args):
         ranks.close()
         return 0
     w = workload(args.scale, 2)
+    sharding = args.sharding or ("rows" if world > 1 else "replicas")
+    if sharding == "rows" and args.only == "all":
+        return run_sharded(args, ranks, w, local, bus)
     if args.only != "all":
         comp = _lib.MG_COMPUTE_MIXED if args.only == "mixed" else _lib.MG_COMPUTE_FP64
         s = make_sampler(w, comp, seed, local, autotune=0 if args.no_autotune else 2)

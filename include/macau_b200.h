@@ -179,6 +179,29 @@ int mg_get_uhat(mg_ctx* ctx, int mode, double* uhat);
 int mg_get_dims(mg_ctx* ctx, int64_t* nrow, int64_t* ncol, int64_t* ntrain, int64_t* ntest,
                 double* mean_value);
 
+/* ---- Row-sharded chains over several GPUs (no reference counterpart; the reference's own
+ * distributed form is the MPI split of block-CG's right-hand sides, macau_mpi.cpp:380-397).
+ * Within a half-sweep the rows of a mode are independent given the other mode's latents and
+ * the hyperparameters, so each rank's context samples a contiguous row range and the ranks
+ * exchange the new rows (an all-gather into every rank's latent buffer) before the next
+ * half-sweep.  Every rank then holds the same latents, and mg_update_prior computes the same
+ * hyperparameters on each rank from them (same data, same kernels, same keyed draws): the
+ * N-rank chain is the 1-rank chain.  Draws are keyed by the global row index.
+ *   mg_set_row_range   rows [lo, hi) of `mode` sampled by this context (after the training
+ *                      data; the split of long rows keeps the whole mode's threshold)
+ *   mg_latents_device  device buffer of the mode's latents as the samplers write them: rows of
+ *                      *row_stride values of *elem_bytes bytes (8: FP64 mode, 4: the FP32 master
+ *                      of mixed mode), for the caller's collective
+ *   mg_latents_changed after rows of that buffer were written from outside: refreshes the
+ *                      samplers' derived copy (mixed mode: the 16-bit gather copy), on the
+ *                      context's stream
+ *   mg_get_stream      the context's CUDA stream (cudaStream_t), to order collectives with the
+ *                      context's kernels */
+int mg_set_row_range(mg_ctx* ctx, int mode, int64_t lo, int64_t hi);
+int mg_latents_device(mg_ctx* ctx, int mode, void** ptr, int* row_stride, int* elem_bytes);
+int mg_latents_changed(mg_ctx* ctx, int mode);
+int mg_get_stream(mg_ctx* ctx, void** stream);
+
 /* Results: Macau::getRmseTest / getPredictions / getStds / getTestData (macau.h:45-51,
  * macau.cpp:174-188).  rmse[0] = posterior-mean RMSE, rmse[1] = last single-sample RMSE.
  * Test data rows are (row, col, value) in the CSC order of the test matrix, ntest x 3

@@ -107,6 +107,10 @@ _SIGS = {
     "mg_batch_get_info": (_i, [_p, _p]),
     "mg_batch_autotune": (_i, [_p, _i]),
     "mg_batch_get_tuning": (_i, [_p, _i, C.POINTER(MgTuning)]),
+    "mg_set_row_range": (_i, [_p, _i, _i64, _i64]),
+    "mg_latents_device": (_i, [_p, _i, C.POINTER(_p), C.POINTER(_i), C.POINTER(_i)]),
+    "mg_latents_changed": (_i, [_p, _i]),
+    "mg_get_stream": (_i, [_p, C.POINTER(_p)]),
     "mg_normal_wishart_noalloc": (_i, [_p, _i64, _i, _i, _p, _d, _p, _i, C.c_uint64, C.c_uint32,
                                        _i, _p, _p, _p, C.c_char_p, _i]),
 }
@@ -329,6 +333,25 @@ class Sampler:
                 "kernel_launches": int(st.kernel_launches), "h2d_bytes": int(st.h2d_bytes),
                 "d2h_bytes": int(st.d2h_bytes), "ntasks": list(st.ntasks), "nnz": list(st.nnz)}
 
+
+    def set_row_range(self, mode, lo, hi):
+        """Rows [lo, hi) of `mode` are the ones this context samples (mg_set_row_range)."""
+        self._chk(lib().mg_set_row_range(self.h, int(mode), int(lo), int(hi)))
+
+    def latents_device(self, mode):
+        """(device pointer, row stride in elements, element bytes) of the mode's latents."""
+        ptr, stride, eb = C.c_void_p(), C.c_int(), C.c_int()
+        self._chk(lib().mg_latents_device(self.h, int(mode), C.byref(ptr), C.byref(stride),
+                                          C.byref(eb)))
+        return ptr.value, stride.value, eb.value
+
+    def latents_changed(self, mode):
+        self._chk(lib().mg_latents_changed(self.h, int(mode)))
+
+    def stream(self):
+        s = C.c_void_p()
+        self._chk(lib().mg_get_stream(self.h, C.byref(s)))
+        return s.value or 0
 
     def autotune(self, use_cache=True):
         """Times the row samplers' candidate work splits and CTA shapes and keeps the fastest

@@ -521,6 +521,9 @@ class Context {
     sp.znoise = znoise_dev;
     sp.wait_cycles = tc_wait_cycles_;
     sp.wait_test = tc_wait_test_ ? 1 : 0;
+    if (range_hi_[mode] >= 0 && uses_tc(mode) && (!fused_ || p.one))
+      throw MgError(MG_ERR_STATE, "a row range needs the fused tensor-core sampler or the "
+                                  "CUDA-core sampler (its record-based finish covers all rows)");
     if (mixed_ && use_tc_ && gram_ == 0 && KP_ == 32) {
       SampleParams tp = sp;
       tp.tasks = md.tasks_tc.p;
@@ -1148,6 +1151,35 @@ class Context {
   bool initialised() const { return initialised_; }
   void set_use_graph(bool b) { use_graph_ = b; drop_graphs(); }
   void set_use_tc(bool b) { use_tc_ = b; drop_graphs(); }
+  void set_row_range(int mode, long long lo, long long hi) {
+    if (mode < 0 || mode > 1) throw MgError(MG_ERR_ARG, "mode must be 0 or 1");
+    if (!have_data_) throw MgError(MG_ERR_STATE, "set the training data before a row range");
+    if (lo < 0 || hi < lo || hi > dims_[mode])
+      throw MgError(MG_ERR_ARG, "row range must satisfy 0 <= lo <= hi <= rows of the mode");
+    if (prior_[mode].one)
+      throw MgError(MG_ERR_ARG, "row ranges are not supported with the univariate prior");
+    range_lo_[mode] = lo;
+    range_hi_[mode] = hi;
+    drop_graphs();
+    build_tasks(mode, md_[mode].thr);
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
+  // Device buffer of a mode's latents as the samplers write them: N rows of KP values, FP64
+  // (FP64 mode) or the FP32 master (mixed mode).
+  void latents_device(int mode, void** ptr, int* row_stride, int* elem_bytes) const {
+    if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_init first");
+    if (ptr) *ptr = mixed_ ? (void*)lat32_[mode].p : (void*)lat64_[mode].p;
+    if (row_stride) *row_stride = KP_;
+    if (elem_bytes) *elem_bytes = mixed_ ? 4 : 8;
+  }
+  // Rows of the buffer above were written from outside (an exchange between ranks): refresh
+  // what the samplers derive from it (mixed mode: the 16-bit gather copy).  Ordered on the
+  // context's stream.
+  void latents_changed(int mode) {
+    if (!initialised_) throw MgError(MG_ERR_STATE, "call mg_init first");
+    if (mixed_)
+      launch_copy16(lat32_[mode].p, lat16_[mode].p, dims_[mode] * (long long)KP_, gram_ == 1, s_);
+  }
   void set_tc_wait(int us) {
     if (us < 0) throw MgError(MG_ERR_ARG, "tc_wait_us must be >= 0");
     tc_wait_cycles_ = 2000LL * us;
@@ -1264,7 +1296,8 @@ class Context {
     const std::vector<long long>& hptr = md.hptr;
     md.thr = thr;
     int nsplit = 0, nslots = 0;
-    std::vector<RowTask> tasks = make_tasks(hptr, thr, 1, nsplit, nslots);
+    std::vector<RowTask> tasks = make_tasks(hptr, thr, 1, nsplit, nslots, range_lo_[m],
+                                            range_hi_[m]);
     md.ntasks = (int)tasks.size();
     md.nsplit = nsplit;
     md.nslots = nslots;
@@ -1275,7 +1308,7 @@ class Context {
         pptr[r + 1] = pptr[r] + (hptr[r + 1] - hptr[r] + 15) / 16 * 16;
       const long long thr16 = (thr + 15) / 16 * 16;
       int ns = 0, nsl = 0;
-      std::vector<RowTask> tt = make_tasks(pptr, thr16, 16, ns, nsl);
+      std::vector<RowTask> tt = make_tasks(pptr, thr16, 16, ns, nsl, range_lo_[m], range_hi_[m]);
       md.ntasks_tc = (int)tt.size();
       md.nsplit_tc = ns;
       md.nslots_tc = nsl;
@@ -1337,6 +1370,10 @@ class Context {
   DBuf<double> noise_partials_;
   bool have_data_ = false, initialised_ = false;
   bool use_graph_ = true, use_tc_ = true;
+  // Rows of each mode this context samples (mg_set_row_range): [lo, hi), hi < 0 = all rows.
+  // The split threshold is the one of the whole mode, so a row's arithmetic does not depend on
+  // the range.
+  long long range_lo_[2] = {0, 0}, range_hi_[2] = {-1, -1};
   // The tensor-core sampler finishes rows in its Gram kernel's epilogue (option "fused_finish",
   // default on); off: Gram records in HBM and a separate finish kernel.
   bool fused_ = true;
@@ -1569,6 +1606,25 @@ int mg_get_latents(mg_ctx* ctx, int mode, double* out) {
   if (mode < 0 || mode > 1 || !out) return MG_ERR_ARG;
   return guarded(ctx, [&](mg::Context& c) { c.get_latents(mode, out); });
 }
+int mg_set_row_range(mg_ctx* ctx, int mode, int64_t lo, int64_t hi) {
+  return guarded(ctx, [&](mg::Context& c) { c.set_row_range(mode, lo, hi); });
+}
+
+int mg_latents_device(mg_ctx* ctx, int mode, void** ptr, int* row_stride, int* elem_bytes) {
+  if (mode < 0 || mode > 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.latents_device(mode, ptr, row_stride, elem_bytes); });
+}
+
+int mg_latents_changed(mg_ctx* ctx, int mode) {
+  if (mode < 0 || mode > 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.latents_changed(mode); });
+}
+
+int mg_get_stream(mg_ctx* ctx, void** stream) {
+  if (!stream) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { *stream = (void*)c.stream(); });
+}
+
 int mg_set_latents(mg_ctx* ctx, int mode, const double* in) {
   if (mode < 0 || mode > 1 || !in) return MG_ERR_ARG;
   return guarded(ctx, [&](mg::Context& c) {

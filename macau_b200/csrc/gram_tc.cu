@@ -1117,6 +1117,7 @@ static_assert((size_t)kStages * kStageBytes + sizeof(TcShared) + 16 + sizeof(Fus
 bool launch_gram_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
                     int KP, cudaStream_t s, int num_sms, cudaEvent_t mid) {
   if (KP != 32 || p.packed == nullptr) return false;
+  if (p.ntasks == 0) throw MgError(MG_ERR_STATE, "tensor-core Gram kernel without tasks");
   static bool configured[64] = {false};
   const size_t smem = tc_smem_bytes(false);
   set_smem(k_gram_tc<false>, smem, configured);
@@ -1133,6 +1134,10 @@ bool launch_gram_tc(const SampleParams& p, float* gram, const int4* split_rows, 
 bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
                       int KP, cudaStream_t s, int num_sms, cudaEvent_t mid, bool fused) {
   if (KP != 32 || p.packed == nullptr) return false;
+  if (p.ntasks == 0) {  // an empty row range: nothing to sample
+    if (mid) MG_CUDA(cudaEventRecord(mid, s));
+    return true;
+  }
   static bool configured_fin[64] = {false}, configured_fused[64] = {false};
   set_smem(k_finish_tc, kFinSmem, configured_fin);
   if (fused && !p.one) {

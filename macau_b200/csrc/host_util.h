@@ -80,17 +80,21 @@ class DeviceBackup {
   std::list<Item> items_;  // DBuf does not move: list nodes stay in place
 };
 
-// Task list over rows with lengths len(r) = ptr[r+1] - ptr[r] (positions ptr[r]): rows longer
-// than `thr` are cut into near-equal parts whose boundaries are multiples of `align` entries
-// (relative to the row start); tasks sorted by descending length (stable).
+// Task list over rows lo .. hi - 1 (all rows when hi < 0) with lengths len(r) = ptr[r+1] - ptr[r]
+// (positions ptr[r]): rows longer than `thr` are cut into near-equal parts whose boundaries are
+// multiples of `align` entries (relative to the row start); tasks sorted by descending length
+// (stable).
 inline std::vector<RowTask> make_tasks(const std::vector<long long>& ptr, long long thr,
-                                       int align, int& nsplit, int& nslots) {
+                                       int align, int& nsplit, int& nslots, long long lo = 0,
+                                       long long hi = -1) {
   const long long n = (long long)ptr.size() - 1;
+  if (hi < 0 || hi > n) hi = n;
+  if (lo < 0) lo = 0;
   std::vector<RowTask> tasks;
-  tasks.reserve(n + 16);
+  tasks.reserve((size_t)std::max(0LL, hi - lo) + 16);
   nsplit = 0;
   nslots = 0;
-  for (long long r = 0; r < n; r++) {
+  for (long long r = lo; r < hi; r++) {
     const long long len = ptr[r + 1] - ptr[r];
     if (len <= thr) {
       tasks.push_back(RowTask{ptr[r], (int)r, (int)len, 0, 1, 0, 0});

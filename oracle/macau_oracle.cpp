@@ -206,15 +206,15 @@ int orc_set_threads(int n) {
 // mu + Uhat[:, n]).  z: optional K x nrow standard normals; when null the keyed draws
 // (purpose kRowNoise, index n) are used.  Returns 0, or -1 when a Cholesky factorisation fails
 // ("Cholesky Decomposition failed!", latentprior.cpp:374-376).
-int orc_sample_latents(int K, int nrow, int ncol, const int64_t* ptr, const int32_t* idx,
-                       const double* val, double mean_rating, const double* other, double alpha,
-                       const double* mu, const double* Lambda, const double* Uhat,
-                       uint64_t seed, uint32_t sweep, uint32_t mode, const double* z,
-                       double* U_out) {
-  (void)ncol;
+// Rows lo .. hi - 1 of the sampler below (the draws keyed by the global row index n).
+static int sample_latent_rows(int K, int lo, int hi, const int64_t* ptr, const int32_t* idx,
+                              const double* val, double mean_rating, const double* other,
+                              double alpha, const double* mu, const double* Lambda,
+                              const double* Uhat, uint64_t seed, uint32_t sweep, uint32_t mode,
+                              const double* z, double* U_out) {
   int failed = 0;
 #pragma omp parallel for schedule(dynamic, 2)
-  for (int n = 0; n < nrow; n++) {
+  for (int n = lo; n < hi; n++) {
     std::vector<double> MM(Lambda, Lambda + (size_t)K * K);
     std::vector<double> rr(K, 0.0), mun(K);
     for (int64_t e = ptr[n]; e < ptr[n + 1]; e++) {
@@ -244,6 +244,16 @@ int orc_sample_latents(int K, int nrow, int ncol, const int64_t* ptr, const int3
     for (int i = 0; i < K; i++) U_out[(int64_t)n * K + i] = rr[i];
   }
   return failed ? -1 : 0;
+}
+
+int orc_sample_latents(int K, int nrow, int ncol, const int64_t* ptr, const int32_t* idx,
+                       const double* val, double mean_rating, const double* other, double alpha,
+                       const double* mu, const double* Lambda, const double* Uhat,
+                       uint64_t seed, uint32_t sweep, uint32_t mode, const double* z,
+                       double* U_out) {
+  (void)ncol;
+  return sample_latent_rows(K, 0, nrow, ptr, idx, val, mean_rating, other, alpha, mu, Lambda,
+                            Uhat, seed, sweep, mode, z, U_out);
 }
 
 // CondNormalWishart(U, mu, kappa, T, nu) (mvnormal.cpp:314-336) followed by NormalWishart /
@@ -836,6 +846,19 @@ void orc_model_set_side_one(void* h, int mode, int nfeat, const int64_t* fptr,
   p.colsq.assign(nfeat, 0.0);
   for (int f = 0; f < nfeat; f++)
     for (int64_t e = tptr[f]; e < tptr[f + 1]; e++) p.colsq[f] += tval ? tval[e] * tval[e] : 1.0;
+}
+
+// sample_mode restricted to rows lo .. hi - 1 (BPMF and Macau priors): one rank's share of a
+// row-sharded half-sweep.
+int orc_model_sample_rows(void* h, int mode, int iter, int lo, int hi) {
+  Model& m = *static_cast<Model*>(h);
+  Prior& p = m.prior[mode];
+  const Csr& R = m.Y[mode];
+  if (p.one || lo < 0 || hi < lo || hi > R.nrow) return -2;
+  return sample_latent_rows(m.K, lo, hi, R.ptr, R.idx, R.val, m.mean, m.lat[1 - mode].data(),
+                            m.alpha, p.mu.data(), p.Lambda.data(),
+                            p.macau ? p.Uhat.data() : nullptr, m.seed, (uint32_t)iter,
+                            (uint32_t)mode, nullptr, m.lat[mode].data());
 }
 
 int orc_model_sample_mode(void* h, int mode, int iter) {

@@ -54,6 +54,7 @@ def _load():
         "orc_model_set_test": (None, [_p, _i, _p, _p, _p]),
         "orc_model_set_side": (None, [_p, _i, _i, _p, _p, _p, _p, _p, _p, _d, _d]),
         "orc_model_sample_mode": (_i, [_p, _i, _i]),
+        "orc_model_sample_rows": (_i, [_p, _i, _i, _i, _i]),
         "orc_model_update_prior": (_i, [_p, _i, _i]),
         "orc_model_eval": (None, [_p, _i]),
         "orc_model_sweep": (_i, [_p, _i, _i]),
@@ -288,6 +289,10 @@ class Model:
 
     def sample_mode(self, mode, it):
         return lib().orc_model_sample_mode(self.h, mode, it)
+
+    def sample_rows(self, mode, it, lo, hi):
+        """sample_mode for rows lo .. hi - 1 only (draws keyed by the global row index)."""
+        return lib().orc_model_sample_rows(self.h, mode, it, int(lo), int(hi))
 
     def update_prior(self, mode, it):
         return lib().orc_model_update_prior(self.h, mode, it)

@@ -27,22 +27,29 @@
 // entries left in a k-block.
 //
 // Warp roles (one CTA of 16 warps per SM, persistent):
-//   warps 0-7   producers: warp w fills column block r = w % 4 of the stages of the k-blocks
-//               with global index t = w / 4 (mod 2): per k-block it takes row r's 16 CSR
+//   warps 0-7   producers: the k-blocks go through the pipeline in blocks of kBlk = 4 (global
+//               k-blocks 4b .. 4b + 3 in the stages of block b % 6), with one barrier handshake
+//               per block, not per k-block: a barrier wait or arrive costs tens to ~150 cycles,
+//               as much as the work of a k-block.  Warp w fills column block r = w % 4 of the
+//               stages of the blocks b = w / 4 (mod 2): per block it takes row r's 4 x 16 CSR
 //               entries from the CSR ring of its parity, issues two 16-byte cp.async per lane
-//               (lane l: chunk l % 4 of entries l / 4 and l / 4 + 8) as one commit group and
-//               stores the 16 weights; one k-block later it waits for that group, fences the
-//               async proxy and arrives on the stage's "full" barrier (4 arrivals per stage).
-//   warp 8      MMA: allocates TMEM (512 columns: three accumulators of 160 columns); one lane
-//               issues the MMAs, releases stages (tcgen05.commit -> "empty") and publishes
-//               finished accumulators (tcgen05.commit -> "acc full").
+//               and k-block (lane l: chunk l % 4 of entries l / 4 and l / 4 + 8) as one commit
+//               group and stores the weights; one block later it waits for that group, fences
+//               the async proxy and arrives on the block's "full" barrier (4 arrivals).
+//   warp 8      MMA: allocates TMEM (512 columns: three accumulators of 160 columns); lane 0
+//               alone waits for each block, issues its MMAs, releases the block's stages
+//               (tcgen05.commit -> "empty") and publishes finished accumulators (tcgen05.commit
+//               -> "acc full").  One wait per block, not per MMA: on B200 an mbarrier wait (or
+//               any shared-memory read) issued right after a tcgen05.mma took ~150 cycles,
+//               about as long as the M=128, N=160, K=16 MMA, which left the tensor core idle
+//               half the time when every k-block had its own wait.
 //   warp 9      scheduler: takes 4 tasks per group from the work queue (four claims in flight)
 //               and publishes the group descriptors into a ring of kDesc slots as far ahead as
 //               the ring allows, so that the queue atomics and task loads stay off the MMA warp.
-//   warps 10-11 CSR loaders, one per k-block parity: walk the group descriptors and, up to kCsr
-//               k-blocks of their parity ahead, copy each k-block's four 128-byte row segments
-//               with one 16-byte cp.async per lane into the ring, with a meta record (stage
-//               index, valid rows, stop / end) for the producers.
+//   warps 10-11 CSR loaders, one per block parity: walk the group descriptors and, up to kCsr
+//               blocks of their parity ahead, copy the four 128-byte row segments of each of the
+//               block's k-blocks with one 16-byte cp.async per lane into the ring, with a meta
+//               record (block index, valid row slots per k-block, end) for the producers.
 //   warps 12-15 epilogue (warp w reads TMEM quadrant w % 4 = row slot): TMEM -> registers,
 //               release the accumulator and the group's descriptor slot ("desc free"); a part
 //               of a split row goes to the part's scratch slot as an FP64 partial.  Records
@@ -93,15 +100,27 @@ static_assert((kTcThreads - 128) * kOtherRegs + 128 * kEpiRegs <= kTcThreads * k
 static_assert(kEpiWarp0 % 4 == 0 && kTcThreads - kEpiWarp0 * 32 == 128,
               "the epilogue must be the last warpgroup");
 constexpr int kStages = 24;               // gather stages in flight (even: stage s has parity s % 2)
+// Stages are handed from the producers to the MMA lane in blocks of kBlk consecutive k-blocks,
+// one "full" and one "empty" barrier per block: a barrier wait issued right after a tcgen05.mma
+// takes about as long as the MMA itself, so the MMA lane waits once per kBlk MMAs.
+constexpr int kBlk = 4;
+constexpr int kBlocks = kStages / kBlk;
 constexpr int kBlockBytes = 2 * 512;      // one column block: 2 K-atoms x 512 B
 constexpr int kStageBytes = 5 * kBlockBytes;
 constexpr int kSlots = 3;                 // TMEM accumulators
 constexpr int kSlotCols = 160;            // columns of one accumulator (N = 160)
-constexpr int kCsr = 8;                   // CSR ring slots per parity (k-blocks of that parity ahead)
+constexpr int kCsr = 4;                   // CSR ring slots per parity (blocks of that parity ahead)
 constexpr int kDesc = 64;                 // group descriptor ring
+// The scheduler claims a new group from the work queue only while fewer than kAheadKb k-blocks
+// of its published groups still wait for the MMAs: the queue then hands out groups as each CTA
+// consumes them, which balances the CTAs' work (a 64-group ring claimed at once fixed most of
+// the assignment at the start and left CTAs' end times 20-30% apart).  It must exceed the
+// k-blocks the producers and loaders run ahead of the MMAs.
+constexpr int kAheadKb = 96;
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
 constexpr int kGramRec = 32 * 32 + 32;    // Gram record: 32 x 32 row-major Gram, then the rhs
 static_assert(kStages % kParity == 0, "a stage's k-blocks all have the same parity");
+static_assert(kStages % kBlk == 0, "stages come in whole blocks");
 
 struct GroupDesc {
   int row[4];
@@ -111,7 +130,8 @@ struct GroupDesc {
   int nparts[4];
   int slot[4];
   int rkb[4];  // k-blocks of each row (its padded length / 16)
-  int nkb;     // k-blocks of the group (>= 1)
+  int nkb;     // k-blocks of the group (>= 1; the stop group has kBlk, which completes the last
+               // block the MMA lane waits for)
   int stop;    // 1: no more work
 };
 
@@ -119,14 +139,14 @@ struct GroupDesc {
 // epilogue released group g ("desc free"), and the producers, the MMA lane and the epilogue all
 // read a group's descriptor before the epilogue releases it.  The ring must cover the groups
 // the producers run ahead of the MMAs (at most kStages + kCsr k-blocks) and the accumulators.
-static_assert(kDesc > kStages + kParity * kCsr + kSlots, "descriptor ring too small");
+static_assert(kDesc > kStages + kParity * kCsr * kBlk + kSlots + 1, "descriptor ring too small");
+static_assert(kAheadKb > kStages + kParity * kCsr * kBlk + kBlk, "claim window too small");
 
-constexpr int kMetaStop = 16;  // meta flag: the stop group's k-block (nothing valid)
-constexpr int kMetaEnd = 32;   // meta flag: no more k-blocks of this parity
+constexpr int kMetaEnd = 1 << 16;  // meta flag: no more blocks of this parity
 
 struct TcShared {
-  uint64_t full[kStages];      // 4 producer arrivals + the gathered bytes
-  uint64_t empty[kStages];     // tcgen05.commit
+  uint64_t full[kBlocks];      // one producer arrival per row slot and k-block of the block
+  uint64_t empty[kBlocks];     // tcgen05.commit after the block's MMAs
   uint64_t acc_full[kSlots];
   uint64_t acc_empty[kSlots];  // 4 epilogue warps
   uint64_t drain;
@@ -135,10 +155,11 @@ struct TcShared {
   uint64_t desc_free[kDesc];   // epilogue (4 warps) -> scheduler
   uint64_t csr_full[kParity][kCsr];   // 32 cp.async completions + the loader's meta arrive
   uint64_t csr_empty[kParity][kCsr];  // the 4 producers of the parity are done with the slot
-  int2 meta[kParity][kCsr];           // {global k-block index t, valid-row bits | kStop | kEnd}
-  alignas(16) uint2 csr[kParity][kCsr][4][16];  // CSR entries of one k-block: [row slot][16]
+  int2 meta[kParity][kCsr];           // {block index, valid bits (bit 4u + r) | kMetaEnd}
+  alignas(16) uint2 csr[kParity][kCsr][kBlk][4][16];  // CSR entries of one block: [kb][slot][16]
   uint32_t tmem_base;
   int abort;
+  int mma_kb;             // k-blocks the MMA lane has taken (written after each block)
   long long wait_cycles;  // budget of one barrier wait (SampleParams::wait_cycles, or kWaitCycles)
   GroupDesc desc[kDesc];
 };
@@ -203,6 +224,24 @@ __device__ __forceinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, TcS
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, TcShared* sh, Ctl* ctl) {
   if (mbar_test(b, parity)) return true;
   return mbar_wait_slow(b, parity, sh, ctl);
+}
+
+// Bounded wait until the MMA lane has taken `target` k-blocks (polled with sleeps; false on
+// timeout or abort, like mbar_wait).
+__device__ __forceinline__ bool wait_mma_kb(TcShared* sh, int target, Ctl* ctl) {
+  if (*(volatile int*)&sh->mma_kb >= target) return true;
+  const long long t0 = clock64();
+  const long long budget = sh->wait_cycles;
+  for (;;) {
+    __nanosleep(256);
+    if (*(volatile int*)&sh->mma_kb >= target) return true;
+    if (*(volatile int*)&sh->abort) return false;
+    if (clock64() - t0 > budget) {
+      atomicOr(&ctl->status, kStatTimeout);
+      *(volatile int*)&sh->abort = 1;
+      return false;
+    }
+  }
 }
 
 // Waits for every cp.async of this thread.
@@ -298,9 +337,11 @@ __device__ __forceinline__ uint32_t stage_off(int mn, int j) {
 }
 
 // Writes the descriptor of group g (tasks t0 .. t0 + 3; lanes 0-3 hold their task in `tk`,
-// valid when `has`) and publishes it.  Returns true for the stop group (t0 past the end).
+// valid when `has`) and publishes it; `nkb_out` = its k-blocks.  Returns true for the stop group
+// (t0 past the end).
 __device__ __forceinline__ bool publish_group(TcShared* sh, int g, int t0, int ntasks,
-                                              const RowTask& tk, bool has, int lane) {
+                                              const RowTask& tk, bool has, int lane,
+                                              int& nkb_out) {
   GroupDesc& d = sh->desc[g % kDesc];
   const bool stop = t0 >= ntasks;
   int rkb = 0;
@@ -318,8 +359,9 @@ __device__ __forceinline__ bool publish_group(TcShared* sh, int g, int t0, int n
 #pragma unroll
   for (int o = 1; o < 4; o <<= 1) nkb = max(nkb, __shfl_xor_sync(0xffffffffu, nkb, o));
   nkb = __shfl_sync(0xffffffffu, nkb, 0);
+  nkb_out = stop ? kBlk : max(nkb, 1);
   if (lane == 0) {
-    d.nkb = stop ? 1 : max(nkb, 1);
+    d.nkb = nkb_out;
     d.stop = stop ? 1 : 0;
   }
   __syncwarp();
@@ -674,9 +716,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   for (int e = threadIdx.x; e < kStages * kStageBytes / 16; e += blockDim.x)
     reinterpret_cast<uint4*>(stages)[e] = make_uint4(0u, 0u, 0u, 0u);
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; s++) {
-      mbar_init(&sh->full[s], kRowSlots);  // one arrive per producer (after its copies landed)
-      mbar_init(&sh->empty[s], 1);
+    for (int b = 0; b < kBlocks; b++) {
+      mbar_init(&sh->full[b], kRowSlots);  // one arrive per producer (the block's copies landed)
+      mbar_init(&sh->empty[b], 1);
     }
     for (int s = 0; s < kSlots; s++) {
       mbar_init(&sh->acc_full[s], 1);
@@ -694,6 +736,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         mbar_init(&sh->csr_empty[h][c], kRowSlots);
       }
     sh->abort = 0;
+    sh->mma_kb = 0;
     sh->wait_cycles = p.wait_cycles > 0 ? p.wait_cycles : kWaitCycles;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -715,11 +758,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (warp < kProducers) {
     if constexpr (kFused) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kOtherRegs));
     // ================= producer of row slot r, parity h =================
-    // lane l copies 16-byte chunk l % 4 of the rows of entries l / 4 and l / 4 + 8.  A k-block's
-    // copies form one cp.async group; kLag k-blocks later the producer waits for that group,
+    // Blocks b = h (mod 2): per block the producer takes row r's 4 x 16 CSR entries from the
+    // CSR ring of its parity and, for each k-block u of the block, issues two 16-byte cp.async
+    // per lane (lane l: chunk l % 4 of entries l / 4 and l / 4 + 8) and stores the 16 weights;
+    // the block's copies form one cp.async group.  One block later it waits for that group,
     // fences the async proxy (its copies and weights before the tensor cores read them) and
-    // arrives on the stage's "full" barrier.
-    constexpr int kLag = 1;
+    // arrives on the block's "full" barrier.
     const int r = warp % kRowSlots, h = warp / kRowSlots;
     const int ch = lane & 3, e0 = lane >> 2;
     // this lane's weight element in a stage: lanes 0-15 hold the BF16 weight of entry lane % 16
@@ -730,102 +774,101 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const __nv_bfloat16* V = reinterpret_cast<const __nv_bfloat16*>(p.other);
     const unsigned sentinel = (unsigned)p.nother;  // the zero row of the BF16 factor
     const float wscale = (float)packed_scale(p);     // 1 unless the noise is adaptive
-    int pend[kLag + 1];  // stages of the k-blocks whose arrive is pending (ring by i % (kLag + 1))
-    int npend = 0, i = 0;
-    for (;; i++) {
+    int pend = -1;  // block whose "full" arrive is pending
+    for (int i = 0;; i++) {
       const int slot = i % kCsr;
       if (!mbar_wait(&sh->csr_full[h][slot], (uint32_t)((i / kCsr) & 1), sh, p.ctl)) break;
       const int2 m = sh->meta[h][slot];
       if (m.y & kMetaEnd) break;
-      const bool v = (m.y >> r) & 1;
-      const unsigned col0 = v ? sh->csr[h][slot][r][e0].x : sentinel;
-      const unsigned col1 = v ? sh->csr[h][slot][r][e0 + 8].x : sentinel;
-      const float w = v ? __uint_as_float(sh->csr[h][slot][r][lane & 15].y) * wscale : 0.f;
-      const __nv_bfloat16 w_hi = __float2bfloat16_rn(w);
-      const __nv_bfloat16 w_st =
-          lane < 16 ? w_hi : __float2bfloat16_rn(w - __bfloat162float(w_hi));
-      const int stage = m.x % kStages;
-      const uint32_t phase = (uint32_t)((m.x / kStages) & 1);
+      unsigned col0[kBlk], col1[kBlk];
+      __nv_bfloat16 w_st[kBlk];
+#pragma unroll
+      for (int u = 0; u < kBlk; u++) {
+        const bool v = (m.y >> (4 * u + r)) & 1;
+        const uint2* e = sh->csr[h][slot][u][r];
+        col0[u] = v ? e[e0].x : sentinel;
+        col1[u] = v ? e[e0 + 8].x : sentinel;
+        const float w = v ? __uint_as_float(e[lane & 15].y) * wscale : 0.f;
+        const __nv_bfloat16 w_hi = __float2bfloat16_rn(w);
+        w_st[u] = lane < 16 ? w_hi : __float2bfloat16_rn(w - __bfloat162float(w_hi));
+      }
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh->csr_empty[h][slot]);  // the entries are in registers
-      if (!mbar_wait(&sh->empty[stage], phase ^ 1, sh, p.ctl)) break;
-      unsigned char* sbase = stages + (size_t)stage * kStageBytes;
-      cp16(sbase + o0, V + (size_t)col0 * 32 + 8 * ch);
-      cp16(sbase + o1, V + (size_t)col1 * 32 + 8 * ch);
-      cp_commit();
-      *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = w_st;
+      const int blk = m.x % kBlocks;
+      if (!mbar_wait(&sh->empty[blk], (uint32_t)(((m.x / kBlocks) & 1) ^ 1), sh, p.ctl)) break;
 #pragma unroll
-      for (int q = 0; q <= kLag; q++)
-        if (q == i % (kLag + 1)) pend[q] = stage;
-      if (++npend > kLag) {
-        // the k-block of kLag iterations ago: its copies have landed (kLag groups may remain)
-        cp_wait_group<kLag>();
+      for (int u = 0; u < kBlk; u++) {
+        unsigned char* sbase = stages + (size_t)(blk * kBlk + u) * kStageBytes;
+        cp16(sbase + o0, V + (size_t)col0[u] * 32 + 8 * ch);
+        cp16(sbase + o1, V + (size_t)col1[u] * 32 + 8 * ch);
+        *reinterpret_cast<__nv_bfloat16*>(sbase + woff) = w_st[u];
+      }
+      cp_commit();
+      if (pend >= 0) {
+        // the previous block's copies have landed (this block's group may remain)
+        cp_wait_group<1>();
         fence_proxy_async();
         __syncwarp();
-        const int qo = (i + 1) % (kLag + 1);
-        int so = 0;
-#pragma unroll
-        for (int q = 0; q <= kLag; q++)
-          if (q == qo) so = pend[q];
-        if (lane == 0) mbar_arrive(&sh->full[so]);
-        npend--;
+        if (lane == 0) mbar_arrive(&sh->full[pend]);
       }
+      pend = blk;
     }
-    // the pending k-blocks, oldest first
+    // the pending block
     cp_wait_all();
     fence_proxy_async();
     __syncwarp();
-    for (int k = npend; k > 0; k--) {
-      const int qo = (i - k + 3 * (kLag + 1)) % (kLag + 1);
-      int so = 0;
-#pragma unroll
-      for (int q = 0; q <= kLag; q++)
-        if (q == qo) so = pend[q];
-      if (lane == 0) mbar_arrive(&sh->full[so]);
-    }
+    if (pend >= 0 && lane == 0) mbar_arrive(&sh->full[pend]);
   } else if (warp < kEpiWarp0) {
     if constexpr (kFused) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kOtherRegs));
     if (warp == kMmaWarp) {
-    // ================= MMA issuer =================
-    int stage = 0;
-    uint32_t phase = 0;
-    // test hook: a wait that runs out (the abort path then ends every role)
-    const bool go = !p.wait_test || mbar_wait(&sh->never, 0, sh, p.ctl);
-    for (int g = 0; go; g++) {
-      const int slot = g % kSlots;
-      if (g >= kSlots &&
-          !mbar_wait(&sh->acc_empty[slot], (uint32_t)(((g / kSlots) & 1) ^ 1), sh, p.ctl))
-        break;
-      if (!mbar_wait(&sh->desc_full[g % kDesc], (uint32_t)((g / kDesc) & 1), sh, p.ctl)) break;
-      tc_fence_after();
-      const uint32_t d_tmem = tmem + (uint32_t)(slot * kSlotCols);
-      const GroupDesc& d = sh->desc[g % kDesc];
-      const int nkb = d.nkb, stop = d.stop;
-      bool ok = true;
-      for (int kb = 0; kb < nkb; kb++) {
-        if (!mbar_wait(&sh->full[stage], phase, sh, p.ctl)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        if (lane == 0) {
-          const uint32_t sa = su32(stages + (size_t)stage * kStageBytes);
-          mma_bf16(d_tmem, smem_desc(sa), smem_desc(sa), kb > 0 ? 1u : 0u);
-          mma_commit(&sh->empty[stage]);
-        }
-        __syncwarp();
-        if (++stage == kStages) {
-          stage = 0;
-          phase ^= 1;
-        }
-      }
-      if (!ok) break;
-      if (lane == 0) mma_commit(&sh->acc_full[slot]);
-      __syncwarp();
-      if (stop) break;
-    }
-    // drain: wait for every issued MMA before TMEM is released
+    // ================= MMA issuer (lane 0) =================
     if (lane == 0) {
+      // test hook: a wait that runs out (the abort path then ends every role)
+      bool ok = !p.wait_test || mbar_wait(&sh->never, 0, sh, p.ctl);
+      // the open group: g, its accumulator slot, k-blocks done / of the group, stop flag
+      int g = 0, kb = 0, nkb = 0, slot = 0, stop = 0;
+      uint32_t d_tmem = tmem;
+      // opens group g: waits for its accumulator to be free and its descriptor published
+      auto open_group = [&]() -> bool {
+        slot = g % kSlots;
+        if (g >= kSlots &&
+            !mbar_wait(&sh->acc_empty[slot], (uint32_t)(((g / kSlots) & 1) ^ 1), sh, p.ctl))
+          return false;
+        if (!mbar_wait(&sh->desc_full[g % kDesc], (uint32_t)((g / kDesc) & 1), sh, p.ctl))
+          return false;
+        tc_fence_after();
+        const GroupDesc& d = sh->desc[g % kDesc];
+        nkb = d.nkb;
+        stop = d.stop;
+        kb = 0;
+        d_tmem = tmem + (uint32_t)(slot * kSlotCols);
+        // the stop group has no MMAs: its accumulator is published at once (the epilogue
+        // reads only the descriptor's stop flag)
+        if (stop) mma_commit(&sh->acc_full[slot]);
+        return true;
+      };
+      ok = ok && open_group();
+      for (int b = 0; ok && !stop; b++) {
+        const int blk = b % kBlocks;
+        if (!mbar_wait(&sh->full[blk], (uint32_t)((b / kBlocks) & 1), sh, p.ctl)) break;
+        tc_fence_after();
+        for (int u = 0; u < kBlk && !stop; u++) {
+          const uint32_t sa =
+              su32(stages + (size_t)((b * kBlk + u) % kStages) * kStageBytes);
+          mma_bf16(d_tmem, smem_desc(sa), smem_desc(sa), kb > 0 ? 1u : 0u);
+          if (++kb == nkb) {
+            mma_commit(&sh->acc_full[slot]);
+            g++;
+            if (!open_group()) {
+              ok = false;
+              break;
+            }
+          }
+        }
+        mma_commit(&sh->empty[blk]);
+        *(volatile int*)&sh->mma_kb = (b + 1) * kBlk;
+      }
+      // drain: wait for every issued MMA before TMEM is released
       mma_commit(&sh->drain);
       const long long t0 = clock64();
       while (!mbar_test(&sh->drain, 0) && clock64() - t0 < kWaitCycles) __nanosleep(128);
@@ -842,10 +885,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     int t_cur = __shfl_sync(0xffffffffu, q[0], 0);
     RowTask tk_cur = p.tasks[min(t_cur + lane, p.ntasks - 1)];
+    int pub_kb = 0;  // k-blocks of the published groups
     for (int g = 0;; g++) {
       if (g >= kDesc && !mbar_wait(&sh->desc_free[g % kDesc],
                                    (uint32_t)(((g / kDesc) - 1) & 1), sh, p.ctl))
         break;
+      if (!wait_mma_kb(sh, pub_kb - kAheadKb, p.ctl)) break;
       if (lane == 0) {
         q[0] = q[1];
         q[1] = q[2];
@@ -855,37 +900,43 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const int t_nxt = __shfl_sync(0xffffffffu, q[0], 0);
       const RowTask tk_nxt = p.tasks[min(t_nxt + lane, p.ntasks - 1)];
       const bool has = lane < 4 && t_cur + lane < p.ntasks;
-      if (publish_group(sh, g, t_cur, p.ntasks, tk_cur, has, lane)) break;
+      int nkb = 0;
+      if (publish_group(sh, g, t_cur, p.ntasks, tk_cur, has, lane, nkb)) break;
+      pub_kb += nkb;
       t_cur = t_nxt;
       tk_cur = tk_nxt;
     }
     } else {
     // ================= CSR loader of parity h =================
-    // lane l copies entries 2 (l % 8) .. + 1 of row slot l / 8's k-block
+    // Blocks b = h (mod 2), up to kCsr of them ahead: for each k-block u of the block, lane l
+    // copies entries 2 (l % 8) .. + 1 of row slot l / 8 (one 16-byte cp.async) into the ring;
+    // the meta record carries the block index and the valid (row slot, k-block) bits.  The
+    // cursor then skips the other parity's block.
     const int h = warp - kCsrWarp0, rs = lane >> 3, c2 = 2 * (lane & 7);
     Cursor c{0, 0, 0, 0, 0, 0, false, false};
-    bool ok = cursor_load(c, sh, p.ctl, rs) && cursor_advance(c, h, sh, p.ctl, rs);
+    bool ok = cursor_load(c, sh, p.ctl, rs) && cursor_advance(c, h * kBlk, sh, p.ctl, rs);
     for (int i = 0; ok; i++) {
       const int slot = i % kCsr;
       if (i >= kCsr &&
           !mbar_wait(&sh->csr_empty[h][slot], (uint32_t)(((i / kCsr) - 1) & 1), sh, p.ctl))
         break;
-      const bool v = !c.end && !c.stop && c.kb < c.rkb;
-      if (v) cp16(&sh->csr[h][slot][rs][c2], p.packed + c.beg + 16LL * c.kb + c2);
-      cp_arrive_noinc(&sh->csr_full[h][slot]);
-      const unsigned vm = __ballot_sync(0xffffffffu, v);
-      if (lane == 0) {
-        int flags = 0;
+      const bool end = c.end;  // the block starts past the stop group: nothing more to do
+      int flags = 0;
 #pragma unroll
-        for (int q = 0; q < 4; q++) flags |= ((vm >> (8 * q)) & 1u) << q;
-        if (c.end) flags = kMetaEnd;
-        else if (c.stop) flags |= kMetaStop;
-        sh->meta[h][slot] = make_int2(c.t, flags);
+      for (int u = 0; u < kBlk; u++) {
+        const bool v = !c.end && !c.stop && c.kb < c.rkb;
+        if (v) cp16(&sh->csr[h][slot][u][rs][c2], p.packed + c.beg + 16LL * c.kb + c2);
+        const unsigned vm = __ballot_sync(0xffffffffu, v);
+#pragma unroll
+        for (int q = 0; q < 4; q++) flags |= (int)((vm >> (8 * q)) & 1u) << (4 * u + q);
+        if (ok) ok = cursor_advance(c, 1, sh, p.ctl, rs);
       }
+      cp_arrive_noinc(&sh->csr_full[h][slot]);
+      if (lane == 0) sh->meta[h][slot] = make_int2(h + kParity * i, end ? kMetaEnd : flags);
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh->csr_full[h][slot]);
-      if (c.end) break;
-      ok = cursor_advance(c, kParity, sh, p.ctl, rs);
+      if (end) break;
+      if (ok) ok = cursor_advance(c, (kParity - 1) * kBlk, sh, p.ctl, rs);
     }
     cp_wait_all();
     }

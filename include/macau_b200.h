@@ -276,7 +276,11 @@ int mg_batch_get_info(mg_batch* b, int64_t* out);
  *   "split_threshold"  the row samplers' work split for both modes, in [256, 16384] entries
  *                      (default nnz / (32 * SMs) clamped to that range); after the training data
  *   "cta_groups"       row groups per CTA of the CUDA-core sampler (0 = default; 4 or 2 at
- *                      K <= 32, 2 or 1 at K = 64, FP64 or BF16 Grams) */
+ *                      K <= 32, 2 or 1 at K = 64, FP64 or BF16 Grams)
+ *   "group_mix"        (default 16) order of the tensor-core sampler's row groups (four rows
+ *                      each) in its work queue: 0 = by descending length; n in [1, 64] = long
+ *                      and short groups interleaved, a finished row weighed as n k-blocks of
+ *                      gathers, so that each CTA meets both at once.  Changes no result. */
 int mg_set_option(mg_ctx* ctx, const char* name, int value);
 
 /* ---- Autotuner of the row samplers (no reference counterpart; the reference's OpenMP

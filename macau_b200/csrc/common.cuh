@@ -73,6 +73,8 @@ struct SampleParams {
   float* out_f32;              // mixed: FP32 master latents (row stride KP)
   __nv_bfloat16* out_bf16;     // mixed: BF16 copy used as the next half-sweep's gather source
   double* scratch;             // split-row partial Grams: (KP*KP + KP) doubles per slot
+  double* retry_work;          // fused tensor-core sampler: per (CTA, finisher warp) work area
+                               // of the FP64 redo of a row (tc_retry_work_doubles)
   unsigned* split_cnt;         // arrival counters of split rows (zero between launches)
   Ctl* ctl;
   int qslot;                   // which ctl->queue head this launch uses

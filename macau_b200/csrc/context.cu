@@ -513,6 +513,7 @@ class Context {
     sp.out_f32 = lat32_[mode].p;
     sp.out_bf16 = lat16_[mode].p;
     sp.scratch = scratch_.p;
+    sp.retry_work = retry_work_.p;
     sp.split_cnt = md.split_cnt.p;
     sp.ctl = ctl_.p;
     sp.qslot = mode;
@@ -1211,6 +1212,16 @@ class Context {
     }
     MG_CUDA(cudaStreamSynchronize(s_));
   }
+  // Order of the tensor-core sampler's row groups: 0 = by descending length, n > 0 = long and
+  // short groups interleaved with a finished row counted as n k-blocks (interleave_groups).
+  void set_group_mix(int v) {
+    if (v < 0 || v > 64) throw MgError(MG_ERR_ARG, "group_mix must be in [0, 64]");
+    group_mix_ = v;
+    if (!have_data_) return;
+    drop_graphs();
+    for (int m = 0; m < 2; m++) build_tasks(m, md_[m].thr);
+    MG_CUDA(cudaStreamSynchronize(s_));
+  }
   void set_cta_groups(int g) {
     const std::vector<int> opts = sample_group_options(KP_, mixed_, gram_);
     if (g != 0 && std::find(opts.begin(), opts.end(), g) == opts.end())
@@ -1309,6 +1320,7 @@ class Context {
       const long long thr16 = (thr + 15) / 16 * 16;
       int ns = 0, nsl = 0;
       std::vector<RowTask> tt = make_tasks(pptr, thr16, 16, ns, nsl, range_lo_[m], range_hi_[m]);
+      if (group_mix_ > 0) interleave_groups(tt, (double)group_mix_);
       md.ntasks_tc = (int)tt.size();
       md.nsplit_tc = ns;
       md.nslots_tc = nsl;
@@ -1326,6 +1338,7 @@ class Context {
                          std::max(md_[0].nslots_tc, md_[1].nslots_tc)) *
         (KP_ * KP_ + KP_);
     if (need > scratch_.n) scratch_.alloc(need);
+    if (mixed_ && KP_ == 32 && retry_work_.n == 0) retry_work_.alloc(tc_retry_work_doubles(num_sms_));
   }
 
   // Gram records of the tensor-core sampler of mode m: one per split row when the fused kernel
@@ -1377,6 +1390,8 @@ class Context {
   // The tensor-core sampler finishes rows in its Gram kernel's epilogue (option "fused_finish",
   // default on); off: Gram records in HBM and a separate finish kernel.
   bool fused_ = true;
+  // Row-group order of the tensor-core sampler (option "group_mix", set_group_mix).
+  int group_mix_ = 16;
   // Clock budget of each barrier wait of the tensor-core sampler (option "tc_wait_us", in
   // microseconds at 2 GHz; 0 = the kernel's default of about 2 s).  Tests shorten it to make a
   // wait run out.
@@ -1406,6 +1421,7 @@ class Context {
   DBuf<float> lat32_[2];
   DBuf<__nv_bfloat16> lat16_[2];
   DBuf<double> scratch_, stat_partials_, stat_final_, nwbuf_;
+  DBuf<double> retry_work_;  // the fused tensor-core sampler's FP64-redo work areas
   NwWork nw_{};
   DBuf<Ctl> ctl_;
   DBuf<int> trow_, tcol_;
@@ -1686,6 +1702,7 @@ int mg_set_option(mg_ctx* ctx, const char* name, int value) {
     else if (n == "autotune") c.set_autotune(value);
     else if (n == "split_threshold") c.set_split_threshold(value);
     else if (n == "cta_groups") c.set_cta_groups(value);
+    else if (n == "group_mix") c.set_group_mix(value);
     else throw mg::MgError(MG_ERR_ARG, "unknown option " + n);
   });
 }

@@ -87,18 +87,23 @@ constexpr int kMmaWarp = kProducers;                // warp 8   (warpgroup 2)
 constexpr int kSchedWarp = kProducers + 1;          // warp 9
 constexpr int kCsrWarp0 = kProducers + 2;           // warps 10-11
 constexpr int kEpiWarp0 = kProducers + 4;           // warps 12-15 (warpgroup 3)
-constexpr int kTcThreads = (kProducers + 8) * 32;
-// Fused kernel: registers per thread after the warpgroups rebalance (setmaxnreg) from the 128 of
-// the launch: warpgroups 0-2 give theirs up to the epilogue, whose four-row finish keeps 80
-// matrix entries per lane plus the dependency chains of four matrices in flight.  The split
-// must fit the launch allocation: 12 warps x 32 x 80 + 4 x 32 x 256 = 63,488 <= 512 x 128.
-constexpr int kLaunchRegs = 128;
-constexpr int kOtherRegs = 80;
-constexpr int kEpiRegs = 256;
-static_assert((kTcThreads - 128) * kOtherRegs + 128 * kEpiRegs <= kTcThreads * kLaunchRegs,
+constexpr int kFinWarp0 = kProducers + 8;           // warps 16-19 (warpgroup 4, fused kernel)
+constexpr int kTcThreads = (kProducers + 8) * 32;   // records kernel: 16 warps
+constexpr int kTcThreadsFused = kTcThreads + 128;   // fused kernel: 20 warps
+// Fused kernel: registers per thread after the warpgroups rebalance (setmaxnreg) from the 96 of
+// the launch (65,536 / 640 rounded down to a multiple of 8): warpgroups 0-3 give theirs up to the
+// finishers, whose four-row finish keeps 80 matrix entries per lane plus the dependency chains
+// of four matrices in flight.  The split must fit the launch allocation:
+// 16 warps x 32 x 56 + 4 x 32 x 256 = 61,440 <= 640 x 96.
+constexpr int kLaunchRegs = 96;
+constexpr int kOtherRegs = 56;
+constexpr int kFinRegs = 256;
+static_assert((kTcThreadsFused - 128) * kOtherRegs + 128 * kFinRegs <=
+                  kTcThreadsFused * kLaunchRegs,
               "register split exceeds the launch allocation");
-static_assert(kEpiWarp0 % 4 == 0 && kTcThreads - kEpiWarp0 * 32 == 128,
-              "the epilogue must be the last warpgroup");
+static_assert(kEpiWarp0 % 4 == 0 && kTcThreads - kEpiWarp0 * 32 == 128 &&
+                  kFinWarp0 * 32 == kTcThreads,
+              "the epilogue, then the finishers, must be the last warpgroups");
 constexpr int kStages = 24;               // gather stages in flight (even: stage s has parity s % 2)
 // Stages are handed from the producers to the MMA lane in blocks of kBlk consecutive k-blocks,
 // one "full" and one "empty" barrier per block: a barrier wait issued right after a tcgen05.mma
@@ -505,17 +510,18 @@ __device__ __forceinline__ void quad_rhs(const SampleParams& p, const FinConst* 
 
 // Finishes four rows, one per quarter (the quarter's row `row`, < 0: takes no part, computing on
 // row rw's draws): MM from its Gram at gp, FP32 factor, solves and the draw, the latents stored
-// when the factor held.  Returns the ballot of lanes whose quarter has a row and a failed factor
+// when the factor held.  `loaded()` runs once the Grams are in registers.  Returns the ballot of lanes whose quarter has a row and a failed factor
 // (bit 8q for quarter q).
-template <bool kStaged>
+template <bool kStaged, typename Loaded>
 __device__ __forceinline__ unsigned quad_finish(const SampleParams& p, const FinConst* fc,
                                                 const float* gp, int row, int rw, float alpha_f,
-                                                uint32_t sweep, int lane) {
+                                                uint32_t sweep, int lane, Loaded loaded) {
   const int i = lane & 7;
   const int K = p.K;
   float a[80], d0[4], rinv[4] = {1.f, 1.f, 1.f, 1.f}, b[4], z[4];
   quad_load_mm<kStaged>(fc, gp, i, K, alpha_f, a, d0);
   quad_rhs<kStaged>(p, fc, gp + 32 * 32, rw, i, b);
+  loaded();  // the Grams at gp are no longer read
   quad_noise(p, rw, K, i, sweep, z);
   const bool ok = quad_factor(a, rinv, i, d0);
   quad_solve(a, rinv, b, z, i);
@@ -685,18 +691,20 @@ __device__ __forceinline__ void stage_rows(float* st, const float (&gr)[32], flo
   st[32 * 32 + lane] = rhs;
 }
 
-// Shared memory of the fused kernel beyond TcShared: the finish constants and, per epilogue warp,
-// the staged Grams of its four groups (also the FP64 retry's L^T) and their quarters' tasks.
+// Shared memory of the fused kernel beyond TcShared: the finish constants and, per TMEM
+// quadrant qd, a ring of four staged Grams (slot q: group 4i + q) with their tasks, handed from
+// drainer qd to finisher qd by a pair of barriers per slot.
 struct FusedShared {
   FinConst fc;
   alignas(16) float stage[4][4 * kStageRec];
   long long begin[4][4];
-  int row[4][4], len[4][4];
+  int row[4][4], len[4][4], stop[4][4];
+  uint64_t staged[4][4];  // drainer qd staged slot q (1 arrival)
+  uint64_t sfree[4][4];   // finisher qd has read slot q (1 arrival)
 };
-static_assert(sizeof(float) * 4 * kStageRec >= (size_t)kFinWork, "retry work area");
 
 template <bool kFused>
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kFused ? kTcThreadsFused : kTcThreads, 1)
     k_gram_tc(const SampleParams p, float* gram) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // layout: stages (1024-aligned) | TcShared | FusedShared (fused kernel)
@@ -737,6 +745,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
     sh->abort = 0;
     sh->mma_kb = 0;
+    if constexpr (kFused) {
+      for (int qd = 0; qd < 4; qd++)
+        for (int q = 0; q < 4; q++) {
+          mbar_init(&fs->staged[qd][q], 1);
+          mbar_init(&fs->sfree[qd][q], 1);
+        }
+    }
     sh->wait_cycles = p.wait_cycles > 0 ? p.wait_cycles : kWaitCycles;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -940,61 +955,35 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     cp_wait_all();
     }
-  } else {
+  } else if (warp < kFinWarp0) {
     const int qd = warp & 3;  // TMEM quadrant = row slot of the group
     if constexpr (kFused) {
-      asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kEpiRegs));
-      // ================= epilogue: accumulators -> finished rows =================
-      // four groups at a time: each group's quadrant is staged in shared memory as it arrives
-      // (its accumulator released at once), then the warp finishes the four rows, quarter q the
-      // row of group g + q
-      const int et = threadIdx.x - kEpiWarp0 * 32;
-      const int ew = warp - kEpiWarp0;
-      fin_const_fill(&fs->fc, p, et, 128,
-                     [] { asm volatile("bar.sync 1, 128;" ::: "memory"); });
-      const float alpha_f = (float)noise_alpha(p);
-      const uint32_t sweep = p.ctl->sweep;
-      float* stage = fs->stage[ew];
-      for (int e = lane; e < 4 * kStageRec; e += 32) stage[e] = 0.f;
-      bool done = false;
-      for (int g = 0; !done; g += 4) {
-        int nq = 0;
-        for (int q = 0; q < 4; q++) {
-          EpiTask t;
-          float gr[32], rhs;
-          if (!epi_take(sh, p.ctl, tmem, g + q, qd, lane, t, gr, rhs)) {
-            done = true;
-            nq = 0;  // aborted: nothing is finished
-            break;
-          }
-          if (t.stop) {
-            done = true;
-            break;
-          }
-          stage_rows(stage + q * kStageRec, gr, rhs, lane);
+      asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kOtherRegs));
+      // ================= drainer of quadrant qd: accumulators -> staging ring =================
+      // group g goes to ring slot q = g % 4 of the quadrant once finisher qd has read the
+      // slot's previous group; the accumulator and the descriptor are released as soon as they
+      // are read, so the MMAs of the next groups overlap the finish of the staged ones.
+      for (int g = 0;; g++) {
+        const int q = g & 3;
+        if (g >= 4 &&
+            !mbar_wait(&fs->sfree[qd][q], (uint32_t)(((g >> 2) - 1) & 1), sh, p.ctl))
+          break;
+        EpiTask t;
+        float gr[32], rhs;
+        if (!epi_take(sh, p.ctl, tmem, g, qd, lane, t, gr, rhs)) break;
+        if (!t.stop) {
+          stage_rows(fs->stage[qd] + q * kStageRec, gr, rhs, lane);
           if (t.row >= 0 && t.nparts > 1) store_part(p, t, gr, rhs, lane);
-          if (lane == 0) {
-            fs->row[ew][q] = (t.row >= 0 && t.nparts == 1) ? t.row : -1;
-            fs->begin[ew][q] = t.begin;
-            fs->len[ew][q] = t.len;
-          }
-          nq = q + 1;
+        }
+        if (lane == 0) {
+          fs->row[qd][q] = (!t.stop && t.row >= 0 && t.nparts == 1) ? t.row : -1;
+          fs->begin[qd][q] = t.begin;
+          fs->len[qd][q] = t.len;
+          fs->stop[qd][q] = t.stop;
         }
         __syncwarp();
-        int first = -1;
-        for (int q = 0; q < nq; q++)
-          if (first < 0 && fs->row[ew][q] >= 0) first = fs->row[ew][q];
-        if (first < 0) continue;  // nothing to finish (done ends the loop)
-        const int qq = lane >> 3;
-        const int row = qq < nq ? fs->row[ew][qq] : -1;
-        const unsigned fails = quad_finish<true>(p, &fs->fc, stage + qq * kStageRec, row,
-                                                 row >= 0 ? row : first, alpha_f, sweep, lane);
-        __syncwarp();
-        for (int q = 0; q < nq; q++)
-          if ((fails >> (8 * q)) & 1u)
-            retry_row_from_csr(p, &fs->fc, fs->row[ew][q], fs->begin[ew][q], fs->len[ew][q],
-                               sweep, reinterpret_cast<unsigned char*>(stage));
-        __syncwarp();
+        if (lane == 0) mbar_arrive(&fs->staged[qd][q]);
+        if (t.stop) break;
       }
     } else {
       // ================= epilogue: accumulators -> Gram records =================
@@ -1041,6 +1030,70 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             gp[32 * 32 + lane] = rhs;
           }
         }
+      }
+    }
+  } else {
+    if constexpr (kFused) {
+      asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kFinRegs));
+      // ================= finisher of quadrant qd: staged Grams -> finished rows =================
+      // four groups at a time (ring slots 0-3 of the quadrant), quarter q the row of group
+      // 4i + q; the slots go back to the drainer once the rows are in registers.  A row whose
+      // FP32 factor fails is redone in FP64 from its CSR entries, with this warp's work area in
+      // global memory (the ring may already hold the next groups).
+      const int qd = warp - kFinWarp0;
+      fin_const_fill(&fs->fc, p, threadIdx.x - kFinWarp0 * 32, 128,
+                     [] { asm volatile("bar.sync 1, 128;" ::: "memory"); });
+      const float alpha_f = (float)noise_alpha(p);
+      const uint32_t sweep = p.ctl->sweep;
+      float* stage = fs->stage[qd];
+      unsigned char* work = reinterpret_cast<unsigned char*>(
+          p.retry_work + (size_t)(blockIdx.x * 4 + qd) * (kFinWork / sizeof(double)));
+      bool done = false;
+      for (int b = 0; !done; b++) {
+        int nq = 0;
+        for (int q = 0; q < 4; q++) {
+          if (!mbar_wait(&fs->staged[qd][q], (uint32_t)(b & 1), sh, p.ctl)) {
+            done = true;
+            nq = 0;  // aborted: nothing is finished
+            break;
+          }
+          if (fs->stop[qd][q]) {
+            done = true;
+            break;
+          }
+          nq = q + 1;
+        }
+        int rrow[4];
+        long long rbeg[4];
+        int rlen[4];
+        int first = -1;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          rrow[q] = q < nq ? fs->row[qd][q] : -1;
+          rbeg[q] = fs->begin[qd][q];
+          rlen[q] = fs->len[qd][q];
+          if (first < 0 && rrow[q] >= 0) first = rrow[q];
+        }
+        const auto release = [&] {
+          __syncwarp();
+          if (lane == 0)
+            for (int q = 0; q < nq; q++) mbar_arrive(&fs->sfree[qd][q]);
+        };
+        if (first < 0) {  // nothing to finish (done ends the loop)
+          release();
+          continue;
+        }
+        const int qq = lane >> 3;
+        const int row = rrow[qq & 3];
+        const unsigned fails = quad_finish<true>(p, &fs->fc, stage + qq * kStageRec, row,
+                                                 row >= 0 ? row : first, alpha_f, sweep, lane,
+                                                 release);
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if ((fails >> (8 * q)) & 1u)
+            retry_row_from_csr(p, &fs->fc, rrow[q], rbeg[q], rlen[q], sweep, work);
+        __syncwarp();
       }
     }
   }
@@ -1100,7 +1153,7 @@ __global__ void __launch_bounds__(kFinWarps * 32, 2)
     const int iw = have ? idx : 4 * w;
     const int rw = list ? list[iw].x : iw;
     const unsigned fails = quad_finish<false>(p, fc, gram + (size_t)iw * kGramRec, have ? rw : -1,
-                                              rw, alpha_f, sweep, lane);
+                                              rw, alpha_f, sweep, lane, [] {});
     __syncwarp();
     for (int q = 0; q < 4; q++)
       if ((fails >> (8 * q)) & 1u) {
@@ -1142,6 +1195,10 @@ __global__ void __launch_bounds__(256)
 }
 
 }  // namespace
+
+size_t tc_retry_work_doubles(int num_sms) {
+  return (size_t)num_sms * 4 * (kFinWork / sizeof(double));
+}
 
 size_t tc_smem_bytes(bool fused) {
   return (size_t)kStages * kStageBytes + (sizeof(TcShared) + 15) / 16 * 16 +
@@ -1205,7 +1262,9 @@ bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows
     }
     if (launch_regs < kLaunchRegs)
       throw MgError(MG_ERR_CUDA, "fused tensor-core sampler built with too few registers");
-    k_gram_tc<true><<<num_sms, kTcThreads, smem, s>>>(p, nullptr);
+    if (p.retry_work == nullptr)
+      throw MgError(MG_ERR_STATE, "fused tensor-core sampler without its retry work area");
+    k_gram_tc<true><<<num_sms, kTcThreadsFused, smem, s>>>(p, nullptr);
     MG_CUDA(cudaGetLastError());
     if (mid) MG_CUDA(cudaEventRecord(mid, s));
     if (nsplit > 0) {

@@ -121,4 +121,38 @@ inline std::vector<RowTask> make_tasks(const std::vector<long long>& ptr, long l
   return out;
 }
 
+// Reorders a task list sorted by descending length in groups of four consecutive tasks (the
+// tensor-core sampler's work unit) so that long and short groups alternate: a group costs its
+// k-blocks (longest task / 16) in the gather pipeline and `row_cost` k-blocks' worth of time per
+// unsplit row in the in-kernel finish, and the next group is the longest remaining one while
+// the finish work so far exceeds the gather work, else the shortest remaining one.  Each CTA
+// then meets a mix of both instead of a run of long groups (gather-bound, finishers idle)
+// followed by a run of short ones (finish-bound, gather pipeline idle).
+inline void interleave_groups(std::vector<RowTask>& tasks, double row_cost) {
+  const size_t n = tasks.size(), ng = (n + 3) / 4;
+  if (ng < 3) return;
+  auto gather = [&](size_t g) { return (double)(tasks[4 * g].len / 16); };
+  auto finish = [&](size_t g) {
+    double f = 0.0;
+    for (size_t t = 4 * g; t < std::min(n, 4 * g + 4); t++) f += tasks[t].nparts == 1 ? row_cost : 0.0;
+    return f;
+  };
+  std::vector<RowTask> out;
+  out.reserve(n);
+  size_t lo = 0, hi = ng - 1;
+  double balance = 0.0;  // gather minus finish work of the groups placed so far
+  // the last group may be partial: it stays last
+  const bool partial = n % 4 != 0;
+  if (partial) hi--;
+  while (lo <= hi && hi < ng) {
+    const size_t g = balance <= 0.0 ? lo++ : hi--;
+    balance += gather(g) - finish(g);
+    for (size_t t = 4 * g; t < 4 * g + 4; t++) out.push_back(tasks[t]);
+    if (hi == (size_t)-1) break;
+  }
+  if (partial)
+    for (size_t t = 4 * (ng - 1); t < n; t++) out.push_back(tasks[t]);
+  tasks.swap(out);
+}
+
 }  // namespace mg

@@ -61,6 +61,9 @@ void launch_copy16(const float* src, void* dst, long long n, bool half, cudaStre
 bool launch_sample_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,
                       int KP, cudaStream_t s, int num_sms, cudaEvent_t mid = nullptr,
                       bool fused = true);
+// Doubles of the fused kernel's FP64-redo work area (SampleParams::retry_work) for a grid of
+// num_sms CTAs.
+size_t tc_retry_work_doubles(int num_sms);
 // The Gram half of launch_sample_tc: k_gram_tc (+ k_sum_parts), no finish.  Returns false when
 // the configuration is not covered.
 bool launch_gram_tc(const SampleParams& p, float* gram, const int4* split_rows, int nsplit,

@@ -134,7 +134,6 @@ struct GroupDesc {
   int part[4];
   int nparts[4];
   int slot[4];
-  int rkb[4];  // k-blocks of each row (its padded length / 16)
   int nkb;     // k-blocks of the group (>= 1; the stop group has kBlk, which completes the last
                // block the MMA lane waits for)
   int stop;    // 1: no more work
@@ -357,8 +356,7 @@ __device__ __forceinline__ bool publish_group(TcShared* sh, int g, int t0, int n
     d.part[lane] = has ? tk.part : 0;
     d.nparts[lane] = has ? tk.nparts : 1;
     d.slot[lane] = has ? tk.slot : 0;
-    rkb = has ? tk.len >> 4 : 0;
-    d.rkb[lane] = rkb;
+    rkb = has ? tk.len >> 4 : 0;  // the k-blocks of each row (its padded length / 16)
   }
   int nkb = rkb;
 #pragma unroll
@@ -390,7 +388,7 @@ __device__ __forceinline__ bool cursor_load(Cursor& c, TcShared* sh, Ctl* ctl, i
   c.nkb = d.nkb;
   c.stop = d.stop != 0;
   c.beg = d.begin[r];
-  c.rkb = d.rkb[r];
+  c.rkb = d.len[r] >> 4;
   return true;
 }
 

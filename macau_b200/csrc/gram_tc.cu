@@ -16,7 +16,7 @@
 // whose diagonal blocks p == q are the four rows' Grams and whose columns 128 + p and 132 + p
 // sum to row p's right-hand side sum v (y - mean) alpha (the off-diagonal blocks are not used);
 // the weights thus enter with 16 significant bits, not BF16's 8.  D row r lives
-// in TMEM lane r, so the epilogue warp of quadrant p reads row p's Gram with one 32x32b load.
+// in TMEM lane r, so the warp of quadrant p reads row p's Gram with one 32x32b load.
 // (A TMA tile::gather4 variant of the producers was measured slower: a gather4 of 64-byte rows
 // into a 64B-swizzled stage must start on the 512-byte swizzle period, which leaves half of each
 // K-atom empty and doubles the MMAs, and each warp issues one TMA instruction per ~70-90 cycles.)
@@ -26,7 +26,7 @@
 // a sentinel gathers the zero row N_other of the BF16 factor, and so does a row slot with no
 // entries left in a k-block.
 //
-// Warp roles (one CTA of 16 warps per SM, persistent):
+// Warp roles (one persistent CTA per SM: 20 warps in the fused kernel, 16 in the records kernel):
 //   warps 0-7   producers: the k-blocks go through the pipeline in blocks of kBlk = 4 (global
 //               k-blocks 4b .. 4b + 3 in the stages of block b % 6), with one barrier handshake
 //               per block, not per k-block: a barrier wait or arrive costs tens to ~150 cycles,
@@ -44,23 +44,27 @@
 //               about as long as the M=128, N=160, K=16 MMA, which left the tensor core idle
 //               half the time when every k-block had its own wait.
 //   warp 9      scheduler: takes 4 tasks per group from the work queue (four claims in flight)
-//               and publishes the group descriptors into a ring of kDesc slots as far ahead as
-//               the ring allows, so that the queue atomics and task loads stay off the MMA warp.
+//               and publishes the group descriptors into a ring of kDesc slots, so that the
+//               queue atomics and task loads stay off the MMA warp; it claims a new group only
+//               while fewer than kAheadKb k-blocks of its published groups wait for the MMAs.
 //   warps 10-11 CSR loaders, one per block parity: walk the group descriptors and, up to kCsr
 //               blocks of their parity ahead, copy the four 128-byte row segments of each of the
 //               block's k-blocks with one 16-byte cp.async per lane into the ring, with a meta
 //               record (block index, valid row slots per k-block, end) for the producers.
-//   warps 12-15 epilogue (warp w reads TMEM quadrant w % 4 = row slot): TMEM -> registers,
-//               release the accumulator and the group's descriptor slot ("desc free"); a part
-//               of a split row goes to the part's scratch slot as an FP64 partial.  Records
-//               kernel: the row's FP32 Gram and rhs go to its Gram record.  Fused kernel: the
-//               warp takes groups four at a time, staging each quadrant in shared memory as it
-//               arrives, and finishes the four rows together (quarter q of the warp: the row of
-//               group 4i + q; the quad routines of warp_finish.cuh), so the factors of one batch
-//               overlap the MMAs of the next groups.  In the fused kernel the epilogue
-//               warpgroup takes registers from the other three (setmaxnreg).  A row whose FP32
-//               factor fails is redone by the whole warp in FP64 from the row's CSR entries and
-//               BF16 latents (retry_row_from_csr).
+//   warps 12-15 epilogue / drainers (warp w reads TMEM quadrant w % 4 = row slot): TMEM ->
+//               registers, release the accumulator and the group's descriptor slot ("desc
+//               free"); a part of a split row goes to the part's scratch slot as an FP64
+//               partial.  Records kernel: the row's FP32 Gram and rhs go to its Gram record.
+//               Fused kernel: the quadrant is staged in shared memory, in a ring of four groups
+//               per quadrant, for the finisher of the same quadrant.
+//   warps 16-19 finishers (fused kernel only, warpgroup 4, which takes registers from the other
+//               four by setmaxnreg): finisher qd takes four staged groups at a time, hands the
+//               ring slots back once the rows are in registers, and finishes the four rows
+//               together (quarter q of the warp: the row of group 4i + q; the quad routines of
+//               warp_finish.cuh), so the factors of one batch overlap the MMAs and the staging
+//               of the next groups.  A row whose FP32 factor fails is redone by the whole warp
+//               in FP64 from the row's CSR entries and BF16 latents (retry_row_from_csr), with
+//               the warp's work area in global memory (SampleParams::retry_work).
 // Every barrier wait is bounded by a clock budget (SampleParams::wait_cycles, about 2 s by
 // default); on expiry the CTA raises an abort flag, all roles leave their loops, the MMA lane
 // drains its MMAs (a wait of the full default budget), TMEM is freed and the status word reports

@@ -88,6 +88,15 @@ int mg_set_relation_data(mg_ctx* ctx, const int32_t* idx, int nmodes, const doub
 int mg_set_relation_data_test(mg_ctx* ctx, const int32_t* idx, int nmodes,
                               const double* values, int64_t nnz, const int32_t* dims);
 
+/* Macau::setRelationData(int* rows, int* cols, double* values, int N, int nrows, int ncols)
+ * (macau.h:37; MatrixData::setTrain, sparsetensor.cpp:78-85) and its test-set twin
+ * (macau.h:38; sparsetensor.cpp:87-90): the same data as the idx forms above, with the row and
+ * the column indices in two arrays, so a caller holding them apart needs no nnz x 2 copy. */
+int mg_set_relation_data_rc(mg_ctx* ctx, const int32_t* rows, const int32_t* cols,
+                            const double* values, int64_t nnz, int nrows, int ncols);
+int mg_set_relation_data_test_rc(mg_ctx* ctx, const int32_t* rows, const int32_t* cols,
+                                 const double* values, int64_t nnz, int nrows, int ncols);
+
 /* Side information for `mode` (MacauPrior<SparseDoubleFeat>, latentprior.h:82-125, built by
  * make_prior, macau.pyx:154-192): F is nrows x nfeat given as COO; vals == NULL means a binary
  * matrix (all ones).  lambda_beta / tol are MacauPrior::setLambdaBeta / setTol.  Without this

@@ -58,17 +58,13 @@ class MacauGpu {
     check(mg_set_samples(ctx_, burnin_, nsamples_));
   }
   void setRelationData(int* rows, int* cols, double* values, int nnz, int nrows, int ncols) {
-    std::vector<int32_t> idx = stack(rows, cols, nnz);
-    const int32_t dims[2] = {nrows, ncols};
-    check(mg_set_relation_data(ctx_, idx.data(), 2, values, nnz, dims));
+    check(mg_set_relation_data_rc(ctx_, rows, cols, values, nnz, nrows, ncols));
   }
   void setRelationData(int* idx, int nmodes, double* values, int nnz, int* dims) {
     check(mg_set_relation_data(ctx_, idx, nmodes, values, nnz, dims));
   }
   void setRelationDataTest(int* rows, int* cols, double* values, int nnz, int nrows, int ncols) {
-    std::vector<int32_t> idx = stack(rows, cols, nnz);
-    const int32_t dims[2] = {nrows, ncols};
-    check(mg_set_relation_data_test(ctx_, idx.data(), 2, values, nnz, dims));
+    check(mg_set_relation_data_test_rc(ctx_, rows, cols, values, nnz, nrows, ncols));
   }
   void setRelationDataTest(int* idx, int nmodes, double* values, int nnz, int* dims) {
     check(mg_set_relation_data_test(ctx_, idx, nmodes, values, nnz, dims));
@@ -102,14 +98,6 @@ class MacauGpu {
   int burnin = 50, nsamples = 100;  // Macau's defaults (macau.h:17-18)
 
  private:
-  static std::vector<int32_t> stack(const int* rows, const int* cols, int nnz) {
-    std::vector<int32_t> idx(2 * (size_t)(nnz > 0 ? nnz : 0));
-    for (int e = 0; e < nnz; e++) {
-      idx[e] = rows[e];
-      idx[(size_t)nnz + e] = cols[e];
-    }
-    return idx;
-  }
   std::vector<double> per_test(int (*get)(mg_ctx*, double*), int width) {
     int64_t ntest = 0;
     check(mg_get_dims(ctx_, nullptr, nullptr, nullptr, &ntest, nullptr));

@@ -63,6 +63,8 @@ _SIGS = {
     "mg_last_error": (C.c_char_p, [_p]),
     "mg_set_relation_data": (_i, [_p, _p, _i, _p, _i64, _p]),
     "mg_set_relation_data_test": (_i, [_p, _p, _i, _p, _i64, _p]),
+    "mg_set_relation_data_rc": (_i, [_p, _p, _p, _p, _i64, _i, _i]),
+    "mg_set_relation_data_test_rc": (_i, [_p, _p, _p, _p, _i64, _i, _i]),
     "mg_set_side": (_i, [_p, _i, _p, _p, _p, _i64, _i, _i, _d, _d]),
     "mg_set_samples": (_i, [_p, _i, _i]),
     "mg_init": (_i, [_p]),
@@ -176,18 +178,23 @@ class Sampler:
         check(code, self.h)
 
     def set_relation_data(self, rows, cols, vals, shape):
-        idx = np.concatenate([np.asarray(rows, np.int32), np.asarray(cols, np.int32)])
+        if not len(rows) == len(cols) == len(vals):
+            raise ValueError("rows, cols and vals must have the same length")
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
         vals = np.ascontiguousarray(vals, np.float64)
-        dims = np.asarray(shape, np.int32)
-        self._chk(lib().mg_set_relation_data(self.h, ptr(idx), 2, ptr(vals), len(vals), ptr(dims)))
+        self._chk(lib().mg_set_relation_data_rc(self.h, ptr(rows), ptr(cols), ptr(vals),
+                                                len(vals), int(shape[0]), int(shape[1])))
         self.dims = (int(shape[0]), int(shape[1]))
 
     def set_relation_data_test(self, rows, cols, vals, shape):
-        idx = np.concatenate([np.asarray(rows, np.int32), np.asarray(cols, np.int32)])
+        if not len(rows) == len(cols) == len(vals):
+            raise ValueError("rows, cols and vals must have the same length")
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
         vals = np.ascontiguousarray(vals, np.float64)
-        dims = np.asarray(shape, np.int32)
-        self._chk(lib().mg_set_relation_data_test(self.h, ptr(idx), 2, ptr(vals), len(vals),
-                                                  ptr(dims)))
+        self._chk(lib().mg_set_relation_data_test_rc(self.h, ptr(rows), ptr(cols), ptr(vals),
+                                                     len(vals), int(shape[0]), int(shape[1])))
         n = np.zeros(1, np.int64)
         self._chk(lib().mg_get_dims(self.h, None, None, None, ptr(n), None))
         self.ntest = int(n[0])

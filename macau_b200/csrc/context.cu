@@ -224,11 +224,14 @@ class Context {
   void set_train(const int32_t* idx, int nmodes, const double* vals, long long nnz,
                  const int32_t* dims) {
     if (nmodes != 2) throw MgError(MG_ERR_ARG, "MatrixData: tensor training input not supported.");
+    set_train(idx, idx + nnz, vals, nnz, dims[0], dims[1]);
+  }
+  // The same from separate row and column index arrays (MatrixData::setTrain(rows, cols, ...)).
+  void set_train(const int32_t* r, const int32_t* c, const double* vals, long long nnz,
+                 int nrows, int ncols) {
     if (nnz < 1) throw MgError(MG_ERR_ARG, "training data is empty");
-    dims_[0] = dims[0];
-    dims_[1] = dims[1];
-    const int* r = idx;
-    const int* c = idx + nnz;
+    dims_[0] = nrows;
+    dims_[1] = ncols;
     // CSR of the rows and of the columns, built on the device (build_kernels.cu), which also
     // checks the indices; a rejected set leaves the context without training data.
     have_data_ = false;
@@ -271,6 +274,11 @@ class Context {
   void set_test(const int32_t* idx, int nmodes, const double* vals, long long nnz,
                 const int32_t* dims) {
     if (nmodes != 2) throw MgError(MG_ERR_ARG, "MatrixData: tensor test input not supported.");
+    set_test(idx, idx + nnz, vals, nnz, dims);
+  }
+  // The same from separate row and column index arrays (MatrixData::setTest(rows, cols, ...)).
+  void set_test(const int32_t* r, const int32_t* c, const double* vals, long long nnz,
+                const int32_t* dims) {
     // Ytest in CSC order (sparseFromIJV -> column-major storage): entries sorted by (column,
     // row), duplicates summed in input order, built and index-checked on the device.
     ntest_ = 0;
@@ -278,8 +286,8 @@ class Context {
     if (nnz > 0) {
       DBuf<int> dr, dc;
       DBuf<double> dv;
-      dr.upload(idx, (size_t)nnz, s_);
-      dc.upload(idx + nnz, (size_t)nnz, s_);
+      dr.upload(r, (size_t)nnz, s_);
+      dc.upload(c, (size_t)nnz, s_);
       dv.upload(vals, (size_t)nnz, s_);
       trow_.alloc((size_t)nnz);
       tcol_.alloc((size_t)nnz);
@@ -1501,6 +1509,19 @@ int mg_set_relation_data_test(mg_ctx* ctx, const int32_t* idx, int nmodes,
                               const double* values, int64_t nnz, const int32_t* dims) {
   if ((nnz > 0 && (!idx || !values)) || !dims) return MG_ERR_ARG;
   return guarded(ctx, [&](mg::Context& c) { c.set_test(idx, nmodes, values, nnz, dims); });
+}
+
+int mg_set_relation_data_rc(mg_ctx* ctx, const int32_t* rows, const int32_t* cols,
+                            const double* values, int64_t nnz, int nrows, int ncols) {
+  if (!rows || !cols || !values || nrows < 1 || ncols < 1) return MG_ERR_ARG;
+  return guarded(ctx, [&](mg::Context& c) { c.set_train(rows, cols, values, nnz, nrows, ncols); });
+}
+
+int mg_set_relation_data_test_rc(mg_ctx* ctx, const int32_t* rows, const int32_t* cols,
+                                 const double* values, int64_t nnz, int nrows, int ncols) {
+  if ((nnz > 0 && (!rows || !cols || !values)) || nrows < 1 || ncols < 1) return MG_ERR_ARG;
+  const int32_t dims[2] = {nrows, ncols};
+  return guarded(ctx, [&](mg::Context& c) { c.set_test(rows, cols, values, nnz, dims); });
 }
 
 int mg_set_side(mg_ctx* ctx, int mode, const int32_t* rows, const int32_t* cols,

@@ -713,6 +713,48 @@ def test_eval_rmse_golden_on_gpu():  # tests.cpp:552-591 through mg_eval
     assert s.stds()[0] == pytest.approx(np.sqrt(14.0 / 2))
 
 
+def test_row_and_column_arrays_give_the_same_context_as_the_idx_form():
+    """mg_set_relation_data_rc / _test_rc (macau.h:37-38: separate row and column arrays) build
+    the same training and test data as the nnz x 2 idx forms (macau.h:39-40): two sweeps from the
+    same seed agree bit for bit, and so do the test sets."""
+    w = small_uniform(seed=8)
+    nr, nc = w["shape"]
+    rows, cols = np.asarray(w["rows"], np.int32), np.asarray(w["cols"], np.int32)
+    rows = np.concatenate([rows, rows[:50]])  # duplicates, summed in input order
+    cols = np.concatenate([cols, cols[:50]])
+    vals = np.concatenate([np.asarray(w["vals"], np.float64), np.linspace(-1, 1, 50)])
+    lib = _lib.lib()
+    dims = np.array([nr, nc], np.int32)
+    out = []
+    for form in ("idx", "rc"):
+        s = _lib.Sampler(8, 2.0, seed=4, compute=_lib.MG_COMPUTE_MIXED)
+        if form == "idx":
+            idx = np.concatenate([rows, cols])
+            s._chk(lib.mg_set_relation_data(s.h, _lib.ptr(idx), 2, _lib.ptr(vals), len(vals),
+                                            _lib.ptr(dims)))
+            tidx = np.concatenate([np.asarray(w["trows"], np.int32),
+                                   np.asarray(w["tcols"], np.int32)])
+            tv = np.ascontiguousarray(w["tvals"], np.float64)
+            s._chk(lib.mg_set_relation_data_test(s.h, _lib.ptr(tidx), 2, _lib.ptr(tv), len(tv),
+                                                 _lib.ptr(dims)))
+            s.dims = (nr, nc)
+            n = np.zeros(1, np.int64)
+            s._chk(lib.mg_get_dims(s.h, None, None, None, _lib.ptr(n), None))
+            s.ntest = int(n[0])
+        else:
+            s.set_relation_data(rows, cols, vals, w["shape"])
+            s.set_relation_data_test(w["trows"], w["tcols"], w["tvals"], w["shape"])
+        s.set_samples(0, 2)
+        s.init()
+        for it in range(2):
+            s.sweep(it, eval=True)
+        out.append((s.latents(0), s.latents(1), s.test_data(), s.rmse()))
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(np.asarray(a), np.asarray(b))
+    with pytest.raises(ValueError):
+        _lib.Sampler(8, 2.0).set_relation_data(rows, cols[:-1], vals, w["shape"])
+
+
 def test_device_index_checks_and_test_set_order():
     """Training and test indices are checked on the device during the CSR builds; the test set
     comes back in column-major order with duplicates summed (sparseFromIJV, bpmfutils.h:57-82),

@@ -1,8 +1,9 @@
 """The tensor-core sampler's fused epilogue (k_gram_tc<true>: each row factored, solved and drawn
 in the Gram kernel) against the two-kernel path it replaces (Gram records in HBM, then
 k_finish_tc): the same FP32 arithmetic, so the latents agree to the last bit; its FP64 retry of
-rows whose FP32 factor fails, against the oracle; and the bounded waits of the kernel, made to
-run out through a test hook, reported as MG_ERR_TIMEOUT with the context still usable."""
+rows whose FP32 factor fails, against the oracle; the order of the row groups in the work queue
+(option group_mix), which changes no result; and the bounded waits of the kernel, made to run
+out through a test hook, reported as MG_ERR_TIMEOUT with the context still usable."""
 import numpy as np
 import pytest
 
@@ -39,6 +40,23 @@ def test_fused_finish_matches_the_record_path(name, mode):
     a = _half_sweep(w, 1, mode)
     b = _half_sweep(w, 0, mode)
     assert np.array_equal(a, b), float(np.abs(a - b).max())
+
+
+@pytest.mark.parametrize("mix", [0, 4])
+def test_group_order_changes_no_result(mix):
+    # the row groups' order in the work queue (option group_mix, default 16) decides which CTA
+    # finishes which row and when, not the row's arithmetic: the same sweeps bit for bit
+    w = workloads.bpmf_powerlaw(scale=0.05, seed=2)
+    out = []
+    for m in (16, mix):
+        s = gpu_sampler(w, K, 2.0, 23, compute=_lib.MG_COMPUTE_MIXED)
+        s.set_option("group_mix", m)
+        for it in range(2):
+            s.sweep(it)
+        out.append((s.latents(0), s.latents(1)))
+        s.close()
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
 
 
 @pytest.mark.parametrize("adaptive", [False, True])

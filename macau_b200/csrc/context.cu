@@ -455,6 +455,10 @@ class Context {
     const long long maxN = std::max(dims_[0], dims_[1]);
     stat_partials_.alloc((size_t)stats_blocks(maxN) * (K_ + K_ * K_));
     stat_final_.alloc((size_t)(K_ + K_ * K_));
+    if (pair_priors()) {  // mode 1's own work of the two-mode prior update
+      stat_partials1_.alloc((size_t)stats_blocks(dims_[1]) * (K_ + K_ * K_));
+      stat_final1_.alloc((size_t)(K_ + K_ * K_));
+    }
     nwbuf_.alloc(3 * (size_t)K_ + 4 * (size_t)K_ * K_);
     nw_.vec = nwbuf_.p;
     nw_.m0 = nwbuf_.p + 3 * K_;
@@ -677,6 +681,33 @@ class Context {
     return mixed_ ? (const void*)lat32_[mode].p : (const void*)lat64_[mode].p;
   }
 
+  // Both modes have the plain BPMF prior at K <= 32: the sweep updates them together
+  // (launch_prior_pair: three launches instead of six, the same result bit for bit).  The
+  // phase-timed sweeps keep one mode after the other, so each mode's prior is timed alone.
+  bool pair_priors() const {
+    return K_ <= 32 && !prior_[0].macau && !prior_[0].one && !prior_[1].macau && !prior_[1].one;
+  }
+  void update_priors_pair() {
+    PriorPair pp{};
+    for (int m = 0; m < 2; m++) {
+      const Prior& p = prior_[m];
+      pp.U[m] = latents(m);
+      pp.N[m] = dims_[m];
+      pp.nblocks[m] = stats_blocks(dims_[m]);
+      pp.rows_per_block[m] = (dims_[m] + pp.nblocks[m] - 1) / pp.nblocks[m];
+      pp.partials[m] = m ? stat_partials1_.p : stat_partials_.p;
+      pp.final_[m] = m ? stat_final1_.p : stat_final_.p;
+      pp.mu0[m] = p.mu0.p;
+      pp.kappa[m] = p.b0;
+      pp.T0[m] = p.WI.p;
+      pp.nu[m] = p.df;
+      pp.mu[m] = p.mu.p;
+      pp.Lambda[m] = p.Lambda.p;
+    }
+    launch_prior_pair(pp, mixed_, K_, KP_, ctl_.p, cfg_.seed, s_);
+    launches_ += 3;
+  }
+
   void update_prior(int mode) {
     Prior& p = prior_[mode];
     const long long N = dims_[mode];
@@ -802,9 +833,13 @@ class Context {
     if (ev) MG_CUDA(cudaEventRecord(ev[1], s_));
     sample(1, nullptr, false, ev ? ev[7] : nullptr);
     if (ev) MG_CUDA(cudaEventRecord(ev[2], s_));
-    update_prior(0);
-    if (ev) MG_CUDA(cudaEventRecord(ev[3], s_));
-    update_prior(1);
+    if (!ev && pair_priors()) {
+      update_priors_pair();
+    } else {
+      update_prior(0);
+      if (ev) MG_CUDA(cudaEventRecord(ev[3], s_));
+      update_prior(1);
+    }
     if (ev) MG_CUDA(cudaEventRecord(ev[4], s_));
     update_noise();  // noise.update between the priors and the evaluation (macau.cpp:130-132)
     if (do_eval) eval(-1);
@@ -1429,6 +1464,7 @@ class Context {
   DBuf<float> lat32_[2];
   DBuf<__nv_bfloat16> lat16_[2];
   DBuf<double> scratch_, stat_partials_, stat_final_, nwbuf_;
+  DBuf<double> stat_partials1_, stat_final1_;  // mode 1's work of update_priors_pair
   DBuf<double> retry_work_;  // the fused tensor-core sampler's FP64-redo work areas
   NwWork nw_{};
   DBuf<Ctl> ctl_;

@@ -758,7 +758,66 @@ __global__ void __launch_bounds__(256)
            seed, mode, mu_out, Lambda_out);
 }
 
+// ---- both modes' BPMF prior updates in one launch per step (K <= 32): blocks of mode 0, then
+// of mode 1, each doing what the single-mode kernel's block does, so the results are the same
+// bit for bit; the two modes' steps only overlap ----
+template <typename T>
+__global__ void __launch_bounds__(kStatThreads)
+    k_stats32_pair(PriorPair pp, int K, int stride) {
+  const int m = blockIdx.x < pp.nblocks[0] ? 0 : 1;
+  const int b = blockIdx.x - (m ? pp.nblocks[0] : 0);
+  const long long r0 = (long long)b * pp.rows_per_block[m];
+  stats32_rows(static_cast<const T*>(pp.U[m]), nullptr, r0, min(pp.N[m], r0 + pp.rows_per_block[m]),
+               K, stride, 0, pp.partials[m] + (size_t)b * (K + K * K));
+}
+
+__global__ void __launch_bounds__(256) k_reduce_parts_pair(PriorPair pp, int len) {
+  __shared__ double ws[8][33];
+  const int nblk = (len + 31) / 32;
+  const int m = blockIdx.x < nblk ? 0 : 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = (blockIdx.x - (m ? nblk : 0)) * 32 + lane;
+  const double* parts = pp.partials[m];
+  const int nparts = pp.nblocks[m];
+  double s = 0.0;
+  if (e < len) {
+#pragma unroll 8
+    for (int b = warp; b < nparts; b += 8) s += parts[(size_t)b * len + e];
+  }
+  ws[warp][lane] = s;
+  __syncthreads();
+  if (warp == 0 && e < len) {
+    double t = ws[0][lane];
+#pragma unroll
+    for (int w = 1; w < 8; w++) t += ws[w][lane];
+    pp.final_[m][e] = t;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_nw32_pair(PriorPair pp, int K, Ctl* ctl,
+                                                   unsigned long long seed) {
+  const int m = blockIdx.x;
+  nw32_run(pp.final_[m], 1, pp.N[m], K, pp.mu0[m], pp.kappa[m], pp.T0[m], pp.nu[m], nullptr, 0,
+           nullptr, ctl, seed, m, pp.mu[m], pp.Lambda[m]);
+}
+
 }  // namespace
+
+void launch_prior_pair(const PriorPair& pp, bool f32, int K, int stride, Ctl* ctl,
+                       unsigned long long seed, cudaStream_t s) {
+  if (K > 32) throw MgError(MG_ERR_ARG, "the two-mode prior update needs K <= 32");
+  const int nb = pp.nblocks[0] + pp.nblocks[1];
+  if (f32)
+    k_stats32_pair<float><<<nb, kStatThreads, 0, s>>>(pp, K, stride);
+  else
+    k_stats32_pair<double><<<nb, kStatThreads, 0, s>>>(pp, K, stride);
+  MG_CUDA(cudaGetLastError());
+  const int len = K + K * K;
+  k_reduce_parts_pair<<<2 * ((len + 31) / 32), 256, 0, s>>>(pp, len);
+  MG_CUDA(cudaGetLastError());
+  k_nw32_pair<<<2, 256, 0, s>>>(pp, K, ctl, seed);
+  MG_CUDA(cudaGetLastError());
+}
 
 int stats_blocks(long long N) {  // at most two blocks per SM: fewer partials to reduce
   long long b = (N + 127) / 128;

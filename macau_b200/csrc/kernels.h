@@ -87,6 +87,28 @@ void launch_normal_wishart(const double* partials, int nparts, long long N, int 
                            const double* bb_partials, int bb_nparts, const double* lambda_beta,
                            const NwWork& w, Ctl* ctl, unsigned long long seed, int mode,
                            double* mu_out, double* Lambda_out, cudaStream_t s);
+// Both modes' BPMF prior updates (BPMFPrior::update_prior, latentprior.cpp:79-81) at once, for
+// K <= 32: statistics, reduction and Normal-Wishart draw of mode m from the latents U[m]
+// (N[m] rows, stride `stride`), partials[m] (nblocks[m] records, rows_per_block[m] rows each)
+// and final_[m] as work, into mu[m] / Lambda[m].  Three launches instead of six; each mode's
+// blocks compute what launch_stats / launch_reduce_parts / launch_normal_wishart compute, with
+// the same keyed draws, so the result is the same bit for bit.
+struct PriorPair {
+  const void* U[2];
+  long long N[2];
+  long long rows_per_block[2];
+  int nblocks[2];
+  double* partials[2];
+  double* final_[2];
+  const double* mu0[2];
+  double kappa[2];
+  const double* T0[2];
+  int nu[2];
+  double* mu[2];
+  double* Lambda[2];
+};
+void launch_prior_pair(const PriorPair& pp, bool f32, int K, int stride, Ctl* ctl,
+                       unsigned long long seed, cudaStream_t s);
 void launch_lambda_beta(const double* bb_partials, int nparts, int K, long long nfeat,
                         const double* Lambda, double nu, double mu, const Ctl* ctl,
                         unsigned long long seed, int mode, double* lambda_beta, cudaStream_t s);

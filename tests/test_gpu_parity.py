@@ -713,6 +713,23 @@ def test_eval_rmse_golden_on_gpu():  # tests.cpp:552-591 through mg_eval
     assert s.stds()[0] == pytest.approx(np.sqrt(14.0 / 2))
 
 
+@pytest.mark.parametrize("compute", [_lib.MG_COMPUTE_FP64, _lib.MG_COMPUTE_MIXED])
+def test_two_mode_prior_update_matches_one_mode_at_a_time(compute):
+    """A sweep updates both modes' BPMF priors together (three launches for the two modes'
+    statistics, reductions and Normal-Wishart draws); the phase-timed sweeps update them one mode
+    after the other.  The chains must agree bit for bit."""
+    w = small_uniform(seed=12)
+    out = []
+    for phased in (False, True):
+        s = gpu_sampler(w, 16, 2.0, 31, compute=compute)
+        s.time_sweeps(0, 3, eval=False, phase_events=phased)
+        out.append([s.latents(0), s.latents(1)] + [np.asarray(x) for m in (0, 1)
+                                                   for x in s.hyper(m)[:2]])
+        s.close()
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_row_and_column_arrays_give_the_same_context_as_the_idx_form():
     """mg_set_relation_data_rc / _test_rc (macau.h:37-38: separate row and column arrays) build
     the same training and test data as the nnz x 2 idx forms (macau.h:39-40): two sweeps from the
